@@ -1,0 +1,218 @@
+"""Seeded synthetic scenes and ray batches for the closest-hit workloads.
+
+No public dataset is involved: every workload is generated here from a recorded seed, so the
+GPU path, the CPU oracle and the CPU baseline all consume byte-identical float64 arrays.
+
+Workloads (names used by bench.py and the tests):
+
+* ``icosphere_pinhole``  -- unit icosphere subdivided 4 times (5,120 triangles, 5,112 vertices,
+  built like the reference's benchmark helper benchmarks/benchmark_helper/OriginSphere.h:12-119),
+  512 x 512 pinhole rays from (0, 0, 3), 60 degree vertical field of view.
+* ``mixed_primitives``   -- 10,000 spheres, 1,000 cylinders, 100 finite planes in
+  [-100, 100]^3; 1,048,576 incoherent rays from [-120, 120]^3 with isotropic directions.
+* ``heightfield``        -- 1024 x 1024 vertex grid over [0, 1000]^2 (2,093,058 triangles),
+  6-octave value-noise fBm heights; secondary rays leaving the surface (cosine-weighted).
+* ``batched_icospheres`` -- 256 radially perturbed icospheres (levels 3-7) with ray batches of
+  log-uniform size.
+* ``adjoint_scene``      -- perturbed level-6 icosphere with 10,000 extra split triangles plus
+  500 spheres, rays from a radius-4 sphere toward the unit ball.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+KINDS = ("mesh", "spheres", "planes", "cylinders")
+
+
+@dataclass
+class SceneSpec:
+    """Geometry of one scene, in the order the kinds are added (the order fixes geom ids)."""
+
+    order: List[str] = field(default_factory=list)
+    mesh: Optional[Dict[str, np.ndarray]] = None
+    spheres: Optional[Dict[str, np.ndarray]] = None
+    planes: Optional[Dict[str, np.ndarray]] = None
+    cylinders: Optional[Dict[str, np.ndarray]] = None
+
+    def add_mesh(self, vertices, faces):
+        self.mesh = dict(vertices=np.ascontiguousarray(vertices, np.float64).reshape(-1, 3),
+                         faces=np.ascontiguousarray(faces, np.uint32).reshape(-1, 3))
+        self.order.append("mesh")
+        return self
+
+    def add_spheres(self, centers, radii):
+        self.spheres = dict(centers=np.ascontiguousarray(centers, np.float64).reshape(-1, 3),
+                            radii=np.ascontiguousarray(radii, np.float64).reshape(-1))
+        self.order.append("spheres")
+        return self
+
+    def add_planes(self, centers, dxs, dys, rotations):
+        self.planes = dict(centers=np.ascontiguousarray(centers, np.float64).reshape(-1, 3),
+                           dxs=np.ascontiguousarray(dxs, np.float64).reshape(-1),
+                           dys=np.ascontiguousarray(dys, np.float64).reshape(-1),
+                           rotations=np.ascontiguousarray(rotations, np.float64).reshape(-1, 3, 3))
+        self.order.append("planes")
+        return self
+
+    def add_cylinders(self, centers, semi_axes_a, semi_axes_b, heights, rotations):
+        self.cylinders = dict(
+            centers=np.ascontiguousarray(centers, np.float64).reshape(-1, 3),
+            semi_axes_a=np.ascontiguousarray(semi_axes_a, np.float64).reshape(-1),
+            semi_axes_b=np.ascontiguousarray(semi_axes_b, np.float64).reshape(-1),
+            heights=np.ascontiguousarray(heights, np.float64).reshape(-1),
+            rotations=np.ascontiguousarray(rotations, np.float64).reshape(-1, 3, 3))
+        self.order.append("cylinders")
+        return self
+
+    def nbytes(self):
+        tot = 0
+        for k in KINDS:
+            d = getattr(self, k)
+            if d:
+                tot += sum(v.nbytes for v in d.values())
+        return tot
+
+
+@dataclass
+class RayBatch:
+    origins: np.ndarray      # n x 3 float64
+    directions: np.ndarray   # n x 3 float64 (need not be unit length)
+    tmin: Optional[np.ndarray] = None
+    tmax: Optional[np.ndarray] = None
+
+    @property
+    def n(self):
+        return int(self.origins.shape[0])
+
+    def slice(self, a, b):
+        return RayBatch(self.origins[a:b], self.directions[a:b],
+                        None if self.tmin is None else self.tmin[a:b],
+                        None if self.tmax is None else self.tmax[a:b])
+
+
+@dataclass
+class Workload:
+    name: str
+    scene: SceneSpec
+    rays: RayBatch
+    meta: dict = field(default_factory=dict)
+
+
+# ------------------------------------------------------------------------------------ helpers
+def _normalize_rows(v):
+    """Row-wise v * (1 / |v|) with |v| = sqrt((x*x + y*y) + z*z): the vector-normalisation
+    order used throughout this package."""
+    x, y, z = v[:, 0], v[:, 1], v[:, 2]
+    n = np.sqrt((x * x + y * y) + z * z)
+    il = np.where(n != 0.0, 1.0 / np.where(n != 0.0, n, 1.0), 0.0)
+    return v * il[:, None]
+
+
+def icosphere(level: int):
+    """Unit icosphere with the vertex and face order of the reference's OriginSphere helper
+    (benchmarks/benchmark_helper/OriginSphere.h:12-119): the golden ratio computed in float32,
+    midpoint vertices appended per triangle and edge without de-duplication (so level k has
+    12 + 3 * sum_{i<k} 20 * 4^i vertices), and four children per triangle in the order
+    (f0, f3, f5), (f3, f1, f4), (f4, f2, f5), (f3, f4, f5)."""
+    t = float((np.float32(1.0) + np.sqrt(np.float32(5.0))) / np.float32(2.0))
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t],
+                  [0, -1, -t], [0, 1, -t], [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]],
+                 dtype=np.float64)
+    v = _normalize_rows(v)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9],
+                  [5, 11, 4], [11, 10, 2], [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2],
+                  [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11], [6, 2, 10],
+                  [8, 6, 7], [9, 8, 1]], dtype=np.int64)
+    for _ in range(level):
+        nv, nf = v.shape[0], f.shape[0]
+        v0, v1, v2 = v[f[:, 0]], v[f[:, 1]], v[f[:, 2]]
+        m01 = _normalize_rows((v0 + v1) * 0.5)
+        m12 = _normalize_rows((v1 + v2) * 0.5)
+        m20 = _normalize_rows((v2 + v0) * 0.5)
+        newv = np.stack([m01, m12, m20], axis=1).reshape(-1, 3)
+        base = nv + 3 * np.arange(nf)
+        f3, f4, f5 = base, base + 1, base + 2
+        f0, f1, f2 = f[:, 0], f[:, 1], f[:, 2]
+        f = np.stack([np.stack([f0, f3, f5], 1), np.stack([f3, f1, f4], 1),
+                      np.stack([f4, f2, f5], 1), np.stack([f3, f4, f5], 1)], axis=1).reshape(-1, 3)
+        v = np.concatenate([v, newv], axis=0)
+    return np.ascontiguousarray(v), np.ascontiguousarray(f.astype(np.uint32))
+
+
+def rotation_to(axis):
+    """Rotation matrices R (n x 3 x 3, row-major) with R @ e_z = axis, by the Rodrigues formula
+    about e_z x axis (the construction of test/test_helpers.h:438-451 with the angle between
+    e_z and the axis)."""
+    axis = np.asarray(axis, np.float64).reshape(-1, 3)
+    n = axis.shape[0]
+    ez = np.array([0.0, 0.0, 1.0])
+    k = np.cross(np.broadcast_to(ez, axis.shape), axis)
+    s = np.linalg.norm(k, axis=1)
+    c = axis[:, 2]
+    R = np.zeros((n, 3, 3))
+    for i in range(n):
+        if s[i] < 1e-12:
+            R[i] = np.eye(3) if c[i] > 0 else np.diag([1.0, -1.0, -1.0])
+            continue
+        kk = k[i] / s[i]
+        ang = math.atan2(s[i], c[i])
+        K = np.array([[0, -kk[2], kk[1]], [kk[2], 0, -kk[0]], [-kk[1], kk[0], 0]])
+        R[i] = np.eye(3) + math.sin(ang) * K + (1 - math.cos(ang)) * (K @ K)
+    return R
+
+
+def _unit_sphere(rng, n):
+    g = rng.standard_normal((n, 3))
+    return g / np.linalg.norm(g, axis=1, keepdims=True)
+
+
+# ------------------------------------------------------------------------------------ workloads
+def icosphere_pinhole(level=4, width=512, height=512, fov_deg=60.0):
+    verts, faces = icosphere(level)
+    scene = SceneSpec().add_mesh(verts, faces)
+    tan = math.tan(math.radians(fov_deg) / 2.0)
+    i = np.arange(width, dtype=np.float64)
+    j = np.arange(height, dtype=np.float64)
+    u = (2.0 * (i + 0.5) / width - 1.0) * tan
+    v = (1.0 - 2.0 * (j + 0.5) / height) * tan
+    U, V = np.meshgrid(u, v)  # row-major over pixels (j, i)
+    d = np.stack([U.ravel(), V.ravel(), -np.ones(width * height)], axis=1)
+    d = d / np.linalg.norm(d, axis=1, keepdims=True)
+    o = np.broadcast_to(np.array([0.0, 0.0, 3.0]), d.shape).copy()
+    rays = RayBatch(o, np.ascontiguousarray(d), np.zeros(d.shape[0]),
+                    np.full(d.shape[0], np.inf))
+    return Workload("icosphere_pinhole", scene, rays,
+                    dict(level=level, triangles=int(faces.shape[0]), width=width, height=height))
+
+
+def mixed_primitives(n_rays=1 << 20, n_spheres=10_000, n_cylinders=1_000, n_planes=100, seed=2):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sc = rng.uniform(-100.0, 100.0, (n_spheres, 3))
+    sr = np.exp(rng.uniform(math.log(0.1), math.log(2.0), n_spheres))
+    cc = rng.uniform(-100.0, 100.0, (n_cylinders, 3))
+    cax = _unit_sphere(rng, n_cylinders)
+    crad = rng.uniform(0.1, 1.0, n_cylinders)
+    chalf = rng.uniform(0.5, 5.0, n_cylinders)
+    pc = rng.uniform(-100.0, 100.0, (n_planes, 3))
+    pn = _unit_sphere(rng, n_planes)
+    pdx = rng.uniform(1.0, 20.0, n_planes)
+    pdy = rng.uniform(1.0, 20.0, n_planes)
+    scene = SceneSpec()
+    scene.add_spheres(sc, sr)
+    scene.add_cylinders(cc, crad, crad, 2.0 * chalf, rotation_to(cax))
+    scene.add_planes(pc, pdx, pdy, rotation_to(pn))
+    o = rng.uniform(-120.0, 120.0, (n_rays, 3))
+    d = _unit_sphere(rng, n_rays)
+    rays = RayBatch(o, d, np.zeros(n_rays), np.full(n_rays, np.inf))
+    return Workload("mixed_primitives", scene, rays,
+                    dict(spheres=n_spheres, cylinders=n_cylinders, planes=n_planes, seed=seed))
+
+
+WORKLOADS = {
+    "icosphere_pinhole": icosphere_pinhole,
+    "mixed_primitives": mixed_primitives,
+}

@@ -1,0 +1,257 @@
+// C-ABI driver around the UNMODIFIED blazeRT headers (test infrastructure, not product code).
+//
+// oracle/Makefile compiles this file against the reference's own headers (blazert/scene.h and
+// everything it includes) and the blaze-API shim in oracle/shim/, writing the result to
+// oracle/_ref/.  It is used
+//   * by the tests, to pin the C restatement (oracle/bzr_oracle.c) and the CUDA path against the
+//     reference's own traversal and BVH build, and
+//   * by bench.py's CPU-baseline leg, as the reference's intersect1 loop parallelised with OpenMP
+//     over rows of 512 rays (the pattern of examples/scene_primitives/main.cc:86-110).
+//
+// Everything that computes lives in the reference headers; this file only converts plain arrays
+// into the reference's containers (blazert/scene.h:227-346 keeps const& to them, so they are
+// owned here) and copies RayHit fields out (blazert/ray.h:72-85).
+#include <blazert/blazert.h>
+
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+using namespace blazert;
+
+namespace {
+
+struct RefScene {
+  Vec3rList<double> verts;
+  Vec3iList faces;
+  Vec3rList<double> sph_c;
+  std::vector<double> sph_r;
+  Vec3rList<double> pl_c;
+  std::vector<double> pl_dx, pl_dy;
+  Mat3rList<double> pl_rot;
+  Vec3rList<double> cy_c;
+  std::vector<double> cy_a, cy_b, cy_h;
+  Mat3rList<double> cy_rot;
+  std::unique_ptr<BlazertScene<double>> scene;
+  double commit_seconds = 0.0;
+};
+
+Vec3r<double> v3(const double *p) { return Vec3r<double>{p[0], p[1], p[2]}; }
+Mat3r<double> m3(const double *p) {
+  Mat3r<double> m;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) m(i, j) = p[3 * i + j];
+  return m;
+}
+
+template <template <typename> class C>
+const BVH<double, C> *bvh_of(const RefScene *s);
+template <>
+const BVH<double, TriangleMesh> *bvh_of<TriangleMesh>(const RefScene *s) {
+  return s->scene->has_triangles ? s->scene->triangles_bvh.get() : nullptr;
+}
+template <>
+const BVH<double, SphereCollection> *bvh_of<SphereCollection>(const RefScene *s) {
+  return s->scene->has_spheres ? s->scene->spheres_bvh.get() : nullptr;
+}
+template <>
+const BVH<double, PlaneCollection> *bvh_of<PlaneCollection>(const RefScene *s) {
+  return s->scene->has_planes ? s->scene->planes_bvh.get() : nullptr;
+}
+template <>
+const BVH<double, CylinderCollection> *bvh_of<CylinderCollection>(const RefScene *s) {
+  return s->scene->has_cylinders ? s->scene->cylinders_bvh.get() : nullptr;
+}
+
+// Node dump: per node min[3], max[3], leaf, axis, children[2]; leaf primitives are appended to
+// prim_ids in node order, with prim_off[node] / prim_cnt[node] locating them.
+template <template <typename> class C>
+long dump_tree(const RefScene *s, double *bmin, double *bmax, uint32_t *leaf, uint32_t *axis,
+               uint32_t *children, uint32_t *prim_off, uint32_t *prim_cnt, uint32_t *prim_ids,
+               long prim_cap) {
+  const BVH<double, C> *bvh = bvh_of<C>(s);
+  if (!bvh) return -1;
+  long p = 0;
+  const long n = static_cast<long>(bvh->nodes.size());
+  if (!bmin) return n;
+  for (long i = 0; i < n; ++i) {
+    const auto &node = bvh->nodes[i];
+    for (int k = 0; k < 3; ++k) {
+      bmin[3 * i + k] = node.min[k];
+      bmax[3 * i + k] = node.max[k];
+    }
+    leaf[i] = node.leaf;
+    axis[i] = node.axis;
+    children[2 * i] = node.children[0];
+    children[2 * i + 1] = node.children[1];
+    prim_off[i] = static_cast<uint32_t>(p);
+    prim_cnt[i] = static_cast<uint32_t>(node.primitives.size());
+    for (const auto &prim : node.primitives) {
+      if (p < prim_cap) prim_ids[p] = prim.prim_id;
+      ++p;
+    }
+  }
+  return n;
+}
+
+}  // namespace
+
+extern "C" {
+
+// kinds: 0 mesh, 1 spheres, 2 planes, 3 cylinders.  order[] lists the kinds in add order
+// (the order decides geom ids, blazert/scene.h:235); n_order entries.
+void *ref_scene_create(const int *order, int n_order, const double *verts, long n_verts,
+                       const uint32_t *faces, long n_faces, const double *sph_c, const double *sph_r,
+                       long n_sph, const double *pl_c, const double *pl_dx, const double *pl_dy,
+                       const double *pl_rot, long n_pl, const double *cy_c, const double *cy_a,
+                       const double *cy_b, const double *cy_h, const double *cy_rot, long n_cy,
+                       unsigned min_leaf, unsigned max_depth, unsigned bins, uint32_t *geom_ids) {
+  auto *s = new RefScene();
+  for (long i = 0; i < n_verts; ++i) s->verts.push_back(v3(verts + 3 * i));
+  for (long i = 0; i < n_faces; ++i)
+    s->faces.push_back(Vec3ui{faces[3 * i], faces[3 * i + 1], faces[3 * i + 2]});
+  for (long i = 0; i < n_sph; ++i) {
+    s->sph_c.push_back(v3(sph_c + 3 * i));
+    s->sph_r.push_back(sph_r[i]);
+  }
+  for (long i = 0; i < n_pl; ++i) {
+    s->pl_c.push_back(v3(pl_c + 3 * i));
+    s->pl_dx.push_back(pl_dx[i]);
+    s->pl_dy.push_back(pl_dy[i]);
+    s->pl_rot.push_back(m3(pl_rot + 9 * i));
+  }
+  for (long i = 0; i < n_cy; ++i) {
+    s->cy_c.push_back(v3(cy_c + 3 * i));
+    s->cy_a.push_back(cy_a[i]);
+    s->cy_b.push_back(cy_b[i]);
+    s->cy_h.push_back(cy_h[i]);
+    s->cy_rot.push_back(m3(cy_rot + 9 * i));
+  }
+  s->scene = std::make_unique<BlazertScene<double>>();
+  // BVHBuildOptions has const members (blazert/bvh/options.h:16-18): rebuild it in place.
+  s->scene->build_options.~BVHBuildOptions<double>();
+  new (&s->scene->build_options) BVHBuildOptions<double>(min_leaf, max_depth, bins);
+  for (int k = 0; k < n_order; ++k) {
+    uint32_t id = UINT32_MAX;
+    switch (order[k]) {
+      case 0: id = s->scene->add_mesh(s->verts, s->faces); break;
+      case 1: id = s->scene->add_spheres(s->sph_c, s->sph_r); break;
+      case 2: id = s->scene->add_planes(s->pl_c, s->pl_dx, s->pl_dy, s->pl_rot); break;
+      case 3: id = s->scene->add_cylinders(s->cy_c, s->cy_a, s->cy_b, s->cy_h, s->cy_rot); break;
+    }
+    if (geom_ids) geom_ids[k] = id;
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  s->scene->commit();
+  s->commit_seconds =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return s;
+}
+
+double ref_scene_commit_seconds(void *h) { return static_cast<RefScene *>(h)->commit_seconds; }
+
+void ref_scene_destroy(void *h) { delete static_cast<RefScene *>(h); }
+
+// intersect1 over n rays.  Misses leave the default RayHit (blazert/ray.h:80-84).
+// nthreads <= 0 uses the OpenMP default.  Returns wall seconds of the ray loop.
+double ref_scene_intersect(void *h, long n, const double *org, const double *dir,
+                           const double *tmin, const double *tmax, double *t, double *uv,
+                           double *normal, uint32_t *prim, uint32_t *geom, uint8_t *hit,
+                           int nthreads) {
+  const RefScene *s = static_cast<RefScene *>(h);
+  const BlazertScene<double> &scene = *s->scene;
+  const long row = 512;
+  const long rows = (n + row - 1) / row;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+  const auto t0 = std::chrono::steady_clock::now();
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+  for (long r = 0; r < rows; ++r) {
+    const long end = (r + 1) * row < n ? (r + 1) * row : n;
+    for (long i = r * row; i < end; ++i) {
+      const Ray<double> ray{v3(org + 3 * i), v3(dir + 3 * i),
+                            tmin ? tmin[i] : 0.0,
+                            tmax ? tmax[i] : std::numeric_limits<double>::max()};
+      RayHit<double> rh;
+      const bool hh = intersect1(scene, ray, rh);
+      if (t) t[i] = rh.hit_distance;
+      if (uv) {
+        uv[2 * i] = rh.uv[0];
+        uv[2 * i + 1] = rh.uv[1];
+      }
+      if (normal)
+        for (int k = 0; k < 3; ++k) normal[3 * i + k] = rh.normal[k];
+      if (prim) prim[i] = rh.prim_id;
+      if (geom) geom[i] = rh.geom_id;
+      if (hit) hit[i] = hh ? 1 : 0;
+    }
+  }
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Tree dump for node-by-node comparison with the product's builder.  Call once with bmin == NULL
+// to get the node count, then with arrays sized for it (prim_ids sized by the primitive count).
+long ref_scene_tree(void *h, int kind, double *bmin, double *bmax, uint32_t *leaf, uint32_t *axis,
+                    uint32_t *children, uint32_t *prim_off, uint32_t *prim_cnt, uint32_t *prim_ids,
+                    long prim_cap) {
+  const RefScene *s = static_cast<RefScene *>(h);
+  switch (kind) {
+    case 0:
+      return dump_tree<TriangleMesh>(s, bmin, bmax, leaf, axis, children, prim_off, prim_cnt,
+                                     prim_ids, prim_cap);
+    case 1:
+      return dump_tree<SphereCollection>(s, bmin, bmax, leaf, axis, children, prim_off, prim_cnt,
+                                         prim_ids, prim_cap);
+    case 2:
+      return dump_tree<PlaneCollection>(s, bmin, bmax, leaf, axis, children, prim_off, prim_cnt,
+                                        prim_ids, prim_cap);
+    case 3:
+      return dump_tree<CylinderCollection>(s, bmin, bmax, leaf, axis, children, prim_off,
+                                           prim_cnt, prim_ids, prim_cap);
+  }
+  return -1;
+}
+
+// Traversal of ONE per-type BVH (blazert/bvh/accel.h:60-120) for n rays, as the reference's
+// benchmarks time it (benchmarks/benchmark_BVH/realistic/benchmark_BVH_traverse.cpp:33-60).
+double ref_scene_traverse_kind(void *h, int kind, long n, const double *org, const double *dir,
+                               double *t, uint32_t *prim, uint8_t *hit, int nthreads) {
+  const RefScene *s = static_cast<RefScene *>(h);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+  const auto t0 = std::chrono::steady_clock::now();
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 512)
+#endif
+  for (long i = 0; i < n; ++i) {
+    const Ray<double> ray{v3(org + 3 * i), v3(dir + 3 * i)};
+    RayHit<double> rh;
+    bool hh = false;
+    switch (kind) {
+      case 0: hh = traverse(*bvh_of<TriangleMesh>(s), ray, rh); break;
+      case 1: hh = traverse(*bvh_of<SphereCollection>(s), ray, rh); break;
+      case 2: hh = traverse(*bvh_of<PlaneCollection>(s), ray, rh); break;
+      case 3: hh = traverse(*bvh_of<CylinderCollection>(s), ray, rh); break;
+    }
+    t[i] = rh.hit_distance;
+    prim[i] = rh.prim_id;
+    hit[i] = hh;
+  }
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // extern "C"
