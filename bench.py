@@ -1,0 +1,345 @@
+#!/usr/bin/env python3
+"""Mrays/s of blazeRT closest-hit queries (intersect1 semantics) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload mixed_primitives] [--mode fp64|mixed]
+
+Workload (default): the mixed-primitive scene -- 10,000 spheres, 1,000 cylinders and 100
+finite planes in [-100, 100]^3 -- with 1,048,576 incoherent rays (origins in [-120, 120]^3,
+isotropic directions), float64, seeded.  A step is one intersectN over the whole batch.
+
+  value      Mrays/s over all ranks, rays resident in HBM, device time (CUDA events on the
+             launching stream), the L2 flushed (256 MiB written) between timed steps.
+  e2e        the same metric through the public host API (Scene.intersectN with pinned host
+             arrays): host->device copy of the rays, the kernel, device->host copy of all
+             results, every step.
+  roofline   algorithmic bytes of the traversal kernel / its event time, against the measured
+             HBM copy bandwidth (MEASURED_PEAKS.json).  Bytes per ray: ray I/O (121 B) +
+             64 B per box test (half of a 128-byte two-child FP64 node) + the leaf-ordered
+             primitive record per primitive test; counts come from the counting kernel.
+  cpu_baseline  the reference's own intersect1 loop (its headers, release flags, OpenMP over
+             all host cores) on the same rays, rank 0 at N = 1.
+
+Multi-GPU: one process per GPU (torchrun); every rank holds the scene and traces its own batch
+(weak scaling, no data-path collective); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+RAY_IO_BYTES = 24 + 24 + 8 + 8 + 8 + 16 + 24 + 4 + 4 + 1  # o, d, tmin, tmax | t, uv, n, ids, hit
+PRIM_RECORD_BYTES = {0: 96 + 4, 1: 32 + 4, 2: 112 + 4, 3: 128 + 4}
+BOX_TEST_BYTES = 64
+METRIC = "Mrays/s closest-hit on 1 B200: FP64 vs mixed FP32/FP64, same hits; vs CPU"
+
+
+def parse(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mixed_primitives")
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args(argv)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(workload, seconds, max_rays=0):
+    cmd = [sys.executable, "-m", "oracle.cpu_baseline", "--workload", workload,
+           "--seconds", str(seconds)]
+    if max_rays:
+        cmd += ["--max-rays", str(max_rays)]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        return {"error": r.stderr.strip()[-400:]}
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def config_of(args, wl, world):
+    m = wl.meta
+    return {"workload": args.workload, "rays_per_gpu": wl.rays.n,
+            "scene": {k: v for k, v in m.items() if k != "seed"},
+            "seed": m.get("seed"), "mode": args.mode, "parallelism": f"replicated-scene x{world}",
+            "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from blazert_b200 import workloads as W
+    from oracle.oracle import Oracle, RefScene
+    wl = W.WORKLOADS[args.workload]()
+    threads = os.cpu_count() or 1
+    kind = "reference" if RefScene.available("bench") else "port"
+    sc = RefScene(wl.scene, flavour="bench") if kind == "reference" else Oracle(wl.scene)
+    R = wl.rays
+
+    def step():
+        t0 = time.perf_counter()
+        sc.intersect(R.origins, R.directions, R.tmin, R.tmax, nthreads=threads)
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        step()
+    times = [step() for _ in range(args.steps)]
+    total = sum(times)
+    value = R.n * args.steps / total / 1e6
+    line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": config_of(args, wl, 1), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": kind,
+                             "sample": f"{args.workload}: full batch of {R.n} rays per step"},
+            "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        pg = dist
+    import blazert_b200 as B
+    from blazert_b200 import workloads as W
+
+    wl = W.WORKLOADS[args.workload]()
+    R = wl.rays
+    if rank > 0:  # each rank traces its own batch: rotate the rays so ranks differ
+        sh = (rank * 7919) % R.n
+        R = W.RayBatch(np.roll(R.origins, sh, 0), np.roll(R.directions, sh, 0), R.tmin, R.tmax)
+    scene = B.Scene()
+    for kind in wl.scene.order:
+        d = getattr(wl.scene, kind)
+        getattr(scene, "add_" + kind)(*d.values())
+    t0 = time.perf_counter()
+    scene.commit()
+    commit_s = time.perf_counter() - t0
+    n = R.n
+    o = torch.from_numpy(R.origins).to(dev)
+    d = torch.from_numpy(R.directions).to(dev)
+    tmn = torch.from_numpy(R.tmin).to(dev)
+    tmx = torch.from_numpy(R.tmax).to(dev)
+    f64 = torch.float64
+    out = dict(t=torch.empty(n, dtype=f64, device=dev), uv=torch.empty((n, 2), dtype=f64, device=dev),
+               normal=torch.empty((n, 3), dtype=f64, device=dev),
+               prim=torch.empty(n, dtype=torch.int32, device=dev),
+               geom=torch.empty(n, dtype=torch.int32, device=dev),
+               hit=torch.empty(n, dtype=torch.uint8, device=dev))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        scene.intersectN(o, d, tmn, tmx, mode=args.mode, out=out, stream=stream)
+
+    for i in range(args.warmup):
+        flush.fill_(i & 0xFF)
+        step()
+    torch.cuda.synchronize(dev)
+    scene.check()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    wall0 = time.perf_counter()
+    for i in range(args.steps):
+        flush.fill_((i + 1) & 0xFF)  # untimed: evicts the previous step's rays from L2
+        evs[i][0].record(stream)
+        step()
+        evs[i][1].record(stream)
+    torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - wall0
+    clocks = sampler.stop() if sampler else None
+    scene.check()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    if pg:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * n * args.steps / (total_ms / 1e3) / 1e6
+    hits = float(out["hit"].float().mean().item())
+
+    # roofline: algorithmic bytes from the kernel's own work counts (untimed counting run)
+    counts = scene.work_counts(o, d, tmn, tmx, stream=stream)
+    alg_bytes = n * RAY_IO_BYTES + BOX_TEST_BYTES * sum(counts["box"]) + \
+        sum(PRIM_RECORD_BYTES[k] * counts["prim"][k] for k in range(4))
+    mean_ms = statistics.mean(step_ms)
+    achieved = alg_bytes / (mean_ms / 1e3) / 1e9
+    peak, peak_src = load_peaks()
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", f"trace_fp64_{args.workload}.json")
+    if os.path.exists(tf):
+        with open(tf) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        ho, hd, htmn, htmx = pin(R.origins), pin(R.directions), pin(R.tmin), pin(R.tmax)
+        hout = dict(t=torch.empty(n, dtype=f64).pin_memory().numpy(),
+                    uv=torch.empty((n, 2), dtype=f64).pin_memory().numpy(),
+                    normal=torch.empty((n, 3), dtype=f64).pin_memory().numpy(),
+                    prim=torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+                    geom=torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+                    hit=torch.empty(n, dtype=torch.uint8).pin_memory().numpy())
+        for _ in range(max(1, args.warmup)):
+            scene.intersectN(ho, hd, htmn, htmx, mode=args.mode, out=hout)
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            scene.intersectN(ho, hd, htmn, htmx, mode=args.mode, out=hout)
+        el = time.perf_counter() - t0
+        if pg:
+            t = torch.tensor([el], dtype=torch.float64, device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            el = float(t.item())
+        e2e = {"value": world * n * args.steps / el / 1e6, "unit": "Mrays/s",
+               "h2d_bytes_per_step": n * (24 + 24 + 8 + 8),
+               "d2h_bytes_per_step": n * (8 + 16 + 24 + 4 + 4 + 1)}
+        ok = np.array_equal(hout["prim"], out["prim"].cpu().numpy().view(np.uint32))
+        if not ok:
+            e2e["warning"] = "host-path results differ from the device path"
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.workload, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": config_of(args, wl, world),
+            "e2e": e2e, "gpu_launches": args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_src,
+                         "alg_bytes_per_ray": alg_bytes / n,
+                         "box_tests_per_ray": [c / n for c in counts["box"]],
+                         "prim_tests_per_ray": [c / n for c in counts["prim"]]},
+            "cpu_baseline": cpu, "clocks": clocks, "hit_fraction": hits,
+            "commit_seconds": commit_s, "wall_seconds_timed": wall,
+            "step_ms_min_max": [min(step_ms), max(step_ms)],
+        }
+        print(json.dumps(line), flush=True)
+    scene.close()
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    args = parse(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

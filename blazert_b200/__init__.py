@@ -1,0 +1,334 @@
+"""blazert_b200 -- blazeRT's closest-hit ray query on B200, behind blazeRT's Scene API.
+
+Python mirror of the reference interface (blazert/scene.h, blazert/ray.h) over the C-ABI of
+``libblazert_b200.so`` (include/blazert_b200.h):
+
+    scene = Scene()
+    gid = scene.add_mesh(vertices, faces)          # BlazertScene::add_mesh, scene.h:227-240
+    scene.add_spheres(centers, radii)              # scene.h:258-271
+    scene.add_planes(centers, dxs, dys, rotations) # scene.h:293-307
+    scene.add_cylinders(centers, a, b, heights, rotations)   # scene.h:331-346
+    scene.commit()                                 # scene.h:91-115
+    hit = intersect1(scene, Ray(origin, direction), rayhit)  # scene.h:161-210
+    out = scene.intersectN(origins, directions)    # batched, one GPU launch
+
+As in the reference, ``add_*`` returns the geom id, or ``INVALID_ID`` (the reference's
+``static_cast<unsigned>(-1)``) when the kind was already added or the scene is committed.
+Errors other than that raise ``BlazertError``.  There is no CPU fallback: without the built
+library or a CUDA device the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libblazert_b200.so")
+
+INVALID_ID = 0xFFFFFFFF
+DBL_MAX = float(np.finfo(np.float64).max)
+MODES = {"fp64": 0, "mixed": 1}
+
+OK, EINVAL, ESTATE, ENOMEM, ECUDA, ETIMEOUT, EDEVICE_FLAG, ENODEV = 0, -1, -2, -3, -4, -5, -6, -7
+
+
+class BlazertError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{msg} (status {code})")
+        self.code = code
+
+
+_dp = C.POINTER(C.c_double)
+_u32p = C.POINTER(C.c_uint32)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class _RayHitC(C.Structure):
+    _fields_ = [("normal", C.c_double * 3), ("uv", C.c_double * 2), ("hit_distance", C.c_double),
+                ("prim_id", C.c_uint32), ("geom_id", C.c_uint32)]
+
+
+class _OptsC(C.Structure):
+    _fields_ = [("min_leaf_primitives", C.c_uint32), ("max_tree_depth", C.c_uint32),
+                ("bin_size", C.c_uint32)]
+
+
+_lib = None
+
+
+def library():
+    """Loads libblazert_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise BlazertError(ENODEV, f"{LIB_PATH} is missing: run `python -m blazert_b200.build`")
+        lib = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        lib.bzr_scene_create.argtypes = [C.POINTER(P)]
+        lib.bzr_scene_destroy.argtypes = [P]
+        lib.bzr_add_mesh.argtypes = [P, _dp, C.c_size_t, _u32p, C.c_size_t, _u32p]
+        lib.bzr_add_spheres.argtypes = [P, _dp, _dp, C.c_size_t, _u32p]
+        lib.bzr_add_planes.argtypes = [P, _dp, _dp, _dp, _dp, C.c_size_t, _u32p]
+        lib.bzr_add_cylinders.argtypes = [P, _dp, _dp, _dp, _dp, _dp, C.c_size_t, _u32p]
+        lib.bzr_commit.argtypes = [P, C.POINTER(_OptsC)]
+        lib.bzr_intersect1.argtypes = [P, _dp, _dp, C.c_double, C.c_double,
+                                       C.POINTER(_RayHitC), C.POINTER(C.c_int)]
+        lib.bzr_intersectN.argtypes = [P, C.c_size_t, P, P, P, P, P, P, P, P, P, P, C.c_int, P]
+        lib.bzr_scene_check.argtypes = [P, P, C.c_int, _u32p]
+        lib.bzr_work_counts.argtypes = [P, C.c_size_t, P, P, P, P, C.POINTER(C.c_uint64), P]
+        lib.bzr_scene_stats.argtypes = [P, C.c_int, C.POINTER(C.c_uint64), _u32p,
+                                        C.POINTER(C.c_double)]
+        lib.bzr_last_error_string.restype = C.c_char_p
+        _lib = lib
+    return _lib
+
+
+def _check(rc):
+    if rc != OK:
+        raise BlazertError(rc, library().bzr_last_error_string().decode())
+
+
+def _f64(a, cols=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a.reshape(-1, cols) if cols else a.reshape(-1)
+
+
+@dataclass
+class Ray:
+    """blazert/ray.h:56-65.  The direction need not be unit length."""
+
+    origin: np.ndarray
+    direction: np.ndarray
+    min_hit_distance: float = 0.0
+    max_hit_distance: float = DBL_MAX
+
+
+@dataclass
+class RayHit:
+    """blazert/ray.h:72-85, with the reference's defaults for a miss."""
+
+    normal: np.ndarray = field(default_factory=lambda: np.zeros(3))
+    uv: np.ndarray = field(default_factory=lambda: np.zeros(2))
+    hit_distance: float = DBL_MAX
+    prim_id: int = INVALID_ID
+    geom_id: int = INVALID_ID
+
+
+@dataclass
+class BuildOptions:
+    """blazert/bvh/options.h:15-29."""
+
+    min_leaf_primitives: int = 4
+    max_tree_depth: int = 28
+    bin_size: int = 64
+
+
+class Scene:
+    """BlazertScene<double> on the GPU (blazert/scene.h:38-115)."""
+
+    def __init__(self):
+        self._lib = library()
+        self._h = C.c_void_p()
+        _check(self._lib.bzr_scene_create(C.byref(self._h)))
+        self.committed = False
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.bzr_scene_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- geometry ---------------------------------------------------------------------------
+    def _add(self, rc, gid):
+        if rc == ESTATE:
+            return INVALID_ID
+        _check(rc)
+        return int(gid.value)
+
+    def add_mesh(self, vertices, triangles):
+        v = _f64(vertices, 3)
+        f = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+        gid = C.c_uint32()
+        return self._add(self._lib.bzr_add_mesh(self._h, v.ctypes.data_as(_dp), v.shape[0],
+                                                f.ctypes.data_as(_u32p), f.shape[0],
+                                                C.byref(gid)), gid)
+
+    def add_spheres(self, centers, radii):
+        c, r = _f64(centers, 3), _f64(radii)
+        if c.shape[0] != r.shape[0]:
+            raise BlazertError(EINVAL, "centers and radii differ in length")
+        gid = C.c_uint32()
+        return self._add(self._lib.bzr_add_spheres(self._h, c.ctypes.data_as(_dp),
+                                                   r.ctypes.data_as(_dp), r.shape[0],
+                                                   C.byref(gid)), gid)
+
+    def add_planes(self, centers, dxs, dys, rotations):
+        c, dx, dy = _f64(centers, 3), _f64(dxs), _f64(dys)
+        rot = _f64(rotations, 9)
+        n = c.shape[0]
+        if not (dx.shape[0] == dy.shape[0] == rot.shape[0] == n):
+            raise BlazertError(EINVAL, "plane arrays differ in length")
+        gid = C.c_uint32()
+        return self._add(self._lib.bzr_add_planes(self._h, c.ctypes.data_as(_dp),
+                                                  dx.ctypes.data_as(_dp), dy.ctypes.data_as(_dp),
+                                                  rot.ctypes.data_as(_dp), n, C.byref(gid)), gid)
+
+    def add_cylinders(self, centers, semi_axes_a, semi_axes_b, heights, rotations):
+        c, a, b, h = _f64(centers, 3), _f64(semi_axes_a), _f64(semi_axes_b), _f64(heights)
+        rot = _f64(rotations, 9)
+        n = c.shape[0]
+        if not (a.shape[0] == b.shape[0] == h.shape[0] == rot.shape[0] == n):
+            raise BlazertError(EINVAL, "cylinder arrays differ in length")
+        gid = C.c_uint32()
+        return self._add(self._lib.bzr_add_cylinders(self._h, c.ctypes.data_as(_dp),
+                                                     a.ctypes.data_as(_dp), b.ctypes.data_as(_dp),
+                                                     h.ctypes.data_as(_dp), rot.ctypes.data_as(_dp),
+                                                     n, C.byref(gid)), gid)
+
+    def commit(self, build_options: Optional[BuildOptions] = None):
+        o = build_options or BuildOptions()
+        opts = _OptsC(o.min_leaf_primitives, o.max_tree_depth, o.bin_size)
+        _check(self._lib.bzr_commit(self._h, C.byref(opts)))
+        self.committed = True
+        return True
+
+    def stats(self, kind):
+        kinds = ("mesh", "spheres", "planes", "cylinders")
+        n = C.c_uint64(); d = C.c_uint32(); s = C.c_double()
+        _check(self._lib.bzr_scene_stats(self._h, kinds.index(kind), C.byref(n), C.byref(d),
+                                         C.byref(s)))
+        return dict(nodes=int(n.value), max_depth=int(d.value), build_seconds=float(s.value))
+
+    # -- queries ----------------------------------------------------------------------------
+    def intersect1(self, ray: Ray, rayhit: Optional[RayHit] = None):
+        o, d = _f64(ray.origin), _f64(ray.direction)
+        rh = _RayHitC()
+        hit = C.c_int()
+        _check(self._lib.bzr_intersect1(self._h, o.ctypes.data_as(_dp), d.ctypes.data_as(_dp),
+                                        float(ray.min_hit_distance), float(ray.max_hit_distance),
+                                        C.byref(rh), C.byref(hit)))
+        if rayhit is None:
+            rayhit = RayHit()
+        if hit.value:  # on a miss the rayhit is left untouched, as in the reference
+            rayhit.normal = np.array(rh.normal[:])
+            rayhit.uv = np.array(rh.uv[:])
+            rayhit.hit_distance = rh.hit_distance
+            rayhit.prim_id = rh.prim_id
+            rayhit.geom_id = rh.geom_id
+        return bool(hit.value), rayhit
+
+    def intersectN(self, origins, directions, tmin=None, tmax=None, mode="fp64", out=None,
+                   stream=None):
+        """intersect1 over a batch.  numpy inputs: host path, returns numpy arrays when the
+        results are in place.  torch CUDA tensors: device path, queued on ``stream`` (default:
+        torch's current stream), returns torch tensors without waiting."""
+        try:
+            import torch
+            is_torch = isinstance(origins, torch.Tensor)
+        except ImportError:
+            is_torch = False
+        if is_torch and origins.is_cuda:
+            return self._intersect_device(origins, directions, tmin, tmax, mode, out, stream)
+        o, d = _f64(origins, 3), _f64(directions, 3)
+        n = o.shape[0]
+        tmn = None if tmin is None else np.ascontiguousarray(np.broadcast_to(tmin, (n,)), np.float64)
+        tmx = None if tmax is None else np.ascontiguousarray(np.broadcast_to(tmax, (n,)), np.float64)
+        if out is None:
+            out = dict(t=np.empty(n), uv=np.empty((n, 2)), normal=np.empty((n, 3)),
+                       prim=np.empty(n, np.uint32), geom=np.empty(n, np.uint32),
+                       hit=np.empty(n, np.uint8))
+        ptr = lambda a: None if a is None else a.ctypes.data
+        _check(self._lib.bzr_intersectN(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
+                                        ptr(out.get("t")), ptr(out.get("uv")),
+                                        ptr(out.get("normal")), ptr(out.get("prim")),
+                                        ptr(out.get("geom")), ptr(out.get("hit")),
+                                        MODES[mode], None))
+        return out
+
+    def _intersect_device(self, o, d, tmin, tmax, mode, out, stream):
+        import torch
+        n = o.shape[0]
+        dev = o.device
+        f64 = torch.float64
+        o = o.to(f64).contiguous()
+        d = d.to(device=dev, dtype=f64).contiguous()
+        tmn = None if tmin is None else torch.as_tensor(tmin, dtype=f64, device=dev).expand(n).contiguous()
+        tmx = None if tmax is None else torch.as_tensor(tmax, dtype=f64, device=dev).expand(n).contiguous()
+        if out is None:
+            out = dict(t=torch.empty(n, dtype=f64, device=dev),
+                       uv=torch.empty((n, 2), dtype=f64, device=dev),
+                       normal=torch.empty((n, 3), dtype=f64, device=dev),
+                       prim=torch.empty(n, dtype=torch.int32, device=dev),
+                       geom=torch.empty(n, dtype=torch.int32, device=dev),
+                       hit=torch.empty(n, dtype=torch.uint8, device=dev))
+        st = (stream or torch.cuda.current_stream(dev)).cuda_stream
+        ptr = lambda a: None if a is None else a.data_ptr()
+        _check(self._lib.bzr_intersectN(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
+                                        ptr(out.get("t")), ptr(out.get("uv")),
+                                        ptr(out.get("normal")), ptr(out.get("prim")),
+                                        ptr(out.get("geom")), ptr(out.get("hit")),
+                                        MODES[mode], C.c_void_p(st)))
+        out["_keep"] = (o, d, tmn, tmx)
+        return out
+
+    def work_counts(self, origins, directions, tmin=None, tmax=None, stream=None):
+        """Box tests and primitive tests per kind for a batch (counting kernel; see
+        bzr_work_counts).  Returns dict(box=[4], prim=[4])."""
+        tot = (C.c_uint64 * 8)()
+        try:
+            import torch
+            dev = isinstance(origins, torch.Tensor) and origins.is_cuda
+        except ImportError:
+            dev = False
+        if dev:
+            import torch
+            n = origins.shape[0]
+            o = origins.to(torch.float64).contiguous()
+            d = directions.to(torch.float64).contiguous()
+            tmn = None if tmin is None else torch.as_tensor(tmin, dtype=torch.float64, device=o.device).expand(n).contiguous()
+            tmx = None if tmax is None else torch.as_tensor(tmax, dtype=torch.float64, device=o.device).expand(n).contiguous()
+            st = (stream or torch.cuda.current_stream(o.device)).cuda_stream
+            ptr = lambda a: None if a is None else a.data_ptr()
+            _check(self._lib.bzr_work_counts(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
+                                             tot, C.c_void_p(st)))
+        else:
+            o, d = _f64(origins, 3), _f64(directions, 3)
+            n = o.shape[0]
+            tmn = None if tmin is None else np.ascontiguousarray(np.broadcast_to(tmin, (n,)), np.float64)
+            tmx = None if tmax is None else np.ascontiguousarray(np.broadcast_to(tmax, (n,)), np.float64)
+            ptr = lambda a: None if a is None else a.ctypes.data
+            _check(self._lib.bzr_work_counts(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
+                                             tot, None))
+        return dict(box=[int(x) for x in tot[:4]], prim=[int(x) for x in tot[4:]])
+
+    def check(self, stream=None, timeout_ms=60000):
+        """Waits (bounded) for queued device work and raises if a kernel's bounds check fired."""
+        flags = C.c_uint32()
+        st = None if stream is None else C.c_void_p(stream)
+        _check(self._lib.bzr_scene_check(self._h, st, int(timeout_ms), C.byref(flags)))
+        return int(flags.value)
+
+
+def intersect1(scene: Scene, ray: Ray, rayhit: RayHit) -> bool:
+    """blazert/scene.h:161-162: fills rayhit on a hit and returns whether anything was hit."""
+    hit, _ = scene.intersect1(ray, rayhit)
+    return hit
+
+
+__all__ = ["Scene", "Ray", "RayHit", "BuildOptions", "intersect1", "BlazertError", "INVALID_ID",
+           "DBL_MAX", "library"]

@@ -1,0 +1,480 @@
+// C-ABI of libblazert_b200.so (declared in include/blazert_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/blazert_b200.h"
+#include "layout.h"
+#include "scene.h"
+#include "trace.h"
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string &msg) {
+  g_error = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char *what) {
+  return fail(BZR_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+constexpr int kSlots = 256;  // work-counter slots, one per call in flight
+
+int default_timeout_ms() {
+  const char *s = std::getenv("BZR_TIMEOUT_MS");
+  const int v = s ? std::atoi(s) : 0;
+  return v > 0 ? v : 600000;
+}
+
+// Bounded wait on a stream: polls cudaStreamQuery until done or the deadline passes.
+int wait_stream(cudaStream_t st, int timeout_ms) {
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms);
+  int spins = 0;
+  for (;;) {
+    const cudaError_t e = cudaStreamQuery(st);
+    if (e == cudaSuccess) return BZR_OK;
+    if (e != cudaErrorNotReady) return cuda_fail(e, "stream");
+    if (timeout_ms > 0 && std::chrono::steady_clock::now() > deadline)
+      return fail(BZR_ETIMEOUT, "device work did not finish within the timeout");
+    if (++spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+}
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+struct bzr_scene {
+  bzr::HostScene host;
+  int device = -1;
+  void *arena = nullptr;  // every device array of the committed scene
+  bzr::SceneView view;
+  int blocks = 0;
+  uint32_t *slots = nullptr;  // kSlots x {work counter, error word}, then one sticky word
+  std::atomic<uint32_t> next_slot{0};
+  // host-pointer calls: staging buffers (grown on demand) and a private stream
+  std::mutex stage_mu;
+  void *stage_dev = nullptr;
+  size_t stage_bytes = 0;
+  uint32_t *pinned_err = nullptr;
+  cudaStream_t stream = nullptr;
+
+  ~bzr_scene() {
+    if (device >= 0) {
+      int cur = 0;
+      cudaGetDevice(&cur);
+      cudaSetDevice(device);
+      if (stream) cudaStreamSynchronize(stream);
+      cudaFree(arena);
+      cudaFree(slots);
+      cudaFree(stage_dev);
+      cudaFreeHost(pinned_err);
+      if (stream) cudaStreamDestroy(stream);
+      cudaSetDevice(cur);
+    }
+  }
+};
+
+extern "C" {
+
+const char *bzr_last_error_string(void) { return g_error.c_str(); }
+
+int bzr_scene_create(bzr_scene **out) {
+  if (!out) return fail(BZR_EINVAL, "out is null");
+  *out = new (std::nothrow) bzr_scene();
+  return *out ? BZR_OK : fail(BZR_ENOMEM, "scene allocation failed");
+}
+
+int bzr_scene_destroy(bzr_scene *scene) {
+  delete scene;
+  return BZR_OK;
+}
+
+static int add_guard(bzr_scene *s, int kind, uint32_t *geom_id) {
+  if (geom_id) *geom_id = BZR_INVALID_ID;
+  if (!s) return fail(BZR_EINVAL, "scene is null");
+  if (s->host.committed || s->host.kind[kind].present)
+    return fail(BZR_ESTATE, "kind already added or scene already committed");
+  return BZR_OK;
+}
+
+static int add_done(bzr_scene *s, int kind, uint32_t *geom_id) {
+  s->host.kind[kind].present = true;
+  s->host.kind[kind].geom_id = s->host.geometries++;
+  if (geom_id) *geom_id = s->host.kind[kind].geom_id;
+  return BZR_OK;
+}
+
+int bzr_add_mesh(bzr_scene *s, const double *v, size_t nv, const uint32_t *f, size_t nf,
+                 uint32_t *geom_id) {
+  int rc = add_guard(s, bzr::kMesh, geom_id);
+  if (rc) return rc;
+  if ((nv && !v) || (nf && !f)) return fail(BZR_EINVAL, "null mesh array");
+  if (nf >= bzr::kIdMask) return fail(BZR_EINVAL, "too many faces");
+  for (size_t i = 0; i < 3 * nf; ++i)
+    if (f[i] >= nv) return fail(BZR_EINVAL, "face index out of range");
+  try {
+    bzr::add_mesh(s->host, v, nv, f, nf);
+  } catch (const std::bad_alloc &) {
+    return fail(BZR_ENOMEM, "host allocation failed");
+  }
+  return add_done(s, bzr::kMesh, geom_id);
+}
+
+int bzr_add_spheres(bzr_scene *s, const double *c, const double *r, size_t n, uint32_t *geom_id) {
+  int rc = add_guard(s, bzr::kSpheres, geom_id);
+  if (rc) return rc;
+  if (n && (!c || !r)) return fail(BZR_EINVAL, "null sphere array");
+  if (n >= bzr::kIdMask) return fail(BZR_EINVAL, "too many spheres");
+  try {
+    bzr::add_spheres(s->host, c, r, n);
+  } catch (const std::bad_alloc &) {
+    return fail(BZR_ENOMEM, "host allocation failed");
+  }
+  return add_done(s, bzr::kSpheres, geom_id);
+}
+
+int bzr_add_planes(bzr_scene *s, const double *c, const double *dx, const double *dy,
+                   const double *rot, size_t n, uint32_t *geom_id) {
+  int rc = add_guard(s, bzr::kPlanes, geom_id);
+  if (rc) return rc;
+  if (n && (!c || !dx || !dy || !rot)) return fail(BZR_EINVAL, "null plane array");
+  if (n >= bzr::kIdMask) return fail(BZR_EINVAL, "too many planes");
+  try {
+    bzr::add_planes(s->host, c, dx, dy, rot, n);
+  } catch (const std::bad_alloc &) {
+    return fail(BZR_ENOMEM, "host allocation failed");
+  }
+  return add_done(s, bzr::kPlanes, geom_id);
+}
+
+int bzr_add_cylinders(bzr_scene *s, const double *c, const double *a, const double *b,
+                      const double *h, const double *rot, size_t n, uint32_t *geom_id) {
+  int rc = add_guard(s, bzr::kCylinders, geom_id);
+  if (rc) return rc;
+  if (n && (!c || !a || !b || !h || !rot)) return fail(BZR_EINVAL, "null cylinder array");
+  if (n >= bzr::kIdMask) return fail(BZR_EINVAL, "too many cylinders");
+  try {
+    bzr::add_cylinders(s->host, c, a, b, h, rot, n);
+  } catch (const std::bad_alloc &) {
+    return fail(BZR_ENOMEM, "host allocation failed");
+  }
+  return add_done(s, bzr::kCylinders, geom_id);
+}
+
+int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
+  if (!s) return fail(BZR_EINVAL, "scene is null");
+  if (s->host.committed) return fail(BZR_ESTATE, "scene already committed");
+  if (options) {
+    if (options->bin_size < 2 || options->max_tree_depth > 1000)
+      return fail(BZR_EINVAL, "bin_size must be >= 2 and max_tree_depth <= 1000");
+    s->host.opt.min_leaf = options->min_leaf_primitives;
+    s->host.opt.max_depth = options->max_tree_depth;
+    s->host.opt.bins = options->bin_size;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(BZR_ENODEV, "no CUDA device");
+  std::vector<bzr::KindImage> img(bzr::kNumKinds);
+  uint32_t depth = 0;
+  try {
+    for (int k = 0; k < bzr::kNumKinds; ++k) {
+      bzr::Collection &c = s->host.kind[k];
+      if (!c.present) continue;
+      c.tree = bzr::build_tree(c.boxes, s->host.opt);
+      depth = std::max(depth, c.tree.max_depth);
+      img[k] = bzr::flatten(s->host, k);
+    }
+  } catch (const std::bad_alloc &) {
+    return fail(BZR_ENOMEM, "host allocation failed during the build");
+  }
+  // One device arena holds every array, each 256-byte aligned.
+  struct Piece {
+    const void *src;
+    size_t bytes;
+    size_t off;
+  };
+  std::vector<Piece> pieces;
+  size_t total = 0;
+  auto place = [&](const void *src, size_t bytes) {
+    const size_t off = total;
+    pieces.push_back({src, bytes, off});
+    total = align_up(total + std::max<size_t>(bytes, 1), 256);
+    return off;
+  };
+  size_t off_nodes64[4], off_nodes32[4], off_payload[4], off_ids[4];
+  for (int k = 0; k < bzr::kNumKinds; ++k) {
+    off_nodes64[k] = place(img[k].nodes64.data(), img[k].nodes64.size() * sizeof(double));
+    off_nodes32[k] = place(img[k].nodes32.data(), img[k].nodes32.size() * sizeof(float));
+    off_payload[k] = place(img[k].payload.data(), img[k].payload.size() * sizeof(double));
+    off_ids[k] = place(img[k].prim_ids.data(), img[k].prim_ids.size() * sizeof(uint32_t));
+  }
+  const size_t off_faces = place(s->host.faces.data(), s->host.faces.size() * sizeof(uint32_t));
+  const size_t off_vn = place(s->host.vert_n.data(), s->host.vert_n.size() * sizeof(double));
+  cudaError_t e = cudaGetDevice(&s->device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  e = cudaMalloc(&s->arena, total);
+  if (e != cudaSuccess) return fail(BZR_ENOMEM, "device arena allocation failed");
+  for (const Piece &p : pieces) {
+    if (!p.bytes) continue;
+    e = cudaMemcpy(static_cast<char *>(s->arena) + p.off, p.src, p.bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "scene upload");
+  }
+  char *base = static_cast<char *>(s->arena);
+  for (int k = 0; k < bzr::kNumKinds; ++k) {
+    bzr::KindView &v = s->view.k[k];
+    const bzr::Collection &c = s->host.kind[k];
+    v.present = c.present ? 1 : 0;
+    v.geom_id = c.geom_id;
+    if (!c.present) continue;
+    v.nodes64 = reinterpret_cast<const double *>(base + off_nodes64[k]);
+    v.nodes32 = reinterpret_cast<const float *>(base + off_nodes32[k]);
+    v.payload = reinterpret_cast<const double *>(base + off_payload[k]);
+    v.prim_ids = reinterpret_cast<const uint32_t *>(base + off_ids[k]);
+    v.n_internal = img[k].n_internal;
+    v.n_prims = static_cast<uint32_t>(img[k].prim_ids.size());
+    v.root_ref = img[k].root_ref;
+    v.mixed_ok = img[k].mixed_ok ? 1 : 0;
+    std::memcpy(v.root_box, img[k].root_box, sizeof v.root_box);
+    std::memcpy(v.root_box32, img[k].root_box32, sizeof v.root_box32);
+  }
+  s->view.faces = reinterpret_cast<const uint32_t *>(base + off_faces);
+  s->view.vert_n = reinterpret_cast<const double *>(base + off_vn);
+  s->view.stack_cap = std::max<uint32_t>(8, depth + 2);
+  e = cudaMalloc(&s->slots, (2 * kSlots + 1) * sizeof(uint32_t));
+  if (e != cudaSuccess) return fail(BZR_ENOMEM, "slot allocation failed");
+  e = cudaMemset(s->slots, 0, (2 * kSlots + 1) * sizeof(uint32_t));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemset");
+  e = cudaMallocHost(&s->pinned_err, sizeof(uint32_t));
+  if (e != cudaSuccess) return fail(BZR_ENOMEM, "pinned allocation failed");
+  e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+  e = bzr::trace_grid(s->view.stack_cap, &s->blocks);
+  if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+  s->host.committed = true;
+  return BZR_OK;
+}
+
+static bool is_device_ptr(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Shared body of bzr_intersectN and bzr_work_counts; totals (device) selects the counting
+// kernel.
+static int run_batch(const bzr_scene *cs, size_t n, const double *org, const double *dir,
+                     const double *tmin, const double *tmax, double *t, double *uv,
+                     double *normal, uint32_t *prim, uint32_t *geom, uint8_t *hit, int mode,
+                     void *stream, unsigned long long *totals) {
+  bzr_scene *s = const_cast<bzr_scene *>(cs);
+  if (!s) return fail(BZR_EINVAL, "scene is null");
+  if (!s->host.committed) return fail(BZR_ESTATE, "scene is not committed");
+  if (mode != BZR_MODE_FP64 && mode != BZR_MODE_MIXED) return fail(BZR_EINVAL, "bad mode");
+  if (n == 0) return BZR_OK;
+  if (!org || !dir) return fail(BZR_EINVAL, "origins and directions are required");
+  if (n > 0x7FFFFFC0u) return fail(BZR_EINVAL, "batch too large (at most 2^31 - 64 rays)");
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != s->device) cudaSetDevice(s->device);
+  struct DevGuard {
+    int d;
+    ~DevGuard() { cudaSetDevice(d); }
+  } guard{cur};
+
+  const void *ptrs[10] = {org, dir, tmin, tmax, t, uv, normal, prim, geom, hit};
+  int n_dev = 0, n_given = 0;
+  for (const void *p : ptrs)
+    if (p) {
+      ++n_given;
+      n_dev += is_device_ptr(p) ? 1 : 0;
+    }
+  const uint32_t slot = s->next_slot.fetch_add(1) % kSlots;
+  uint32_t *counter = s->slots + 2 * slot;
+  bzr::RayIO io;
+  io.n = static_cast<uint32_t>(n);
+  io.work_counter = counter;
+
+  if (n_dev == n_given) {  // device arrays: queue on the caller's stream and return
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    io.org = org; io.dir = dir; io.tmin = tmin; io.tmax = tmax;
+    io.t = t; io.uv = uv; io.normal = normal; io.prim = prim; io.geom = geom; io.hit = hit;
+    io.error_word = s->slots + 2 * kSlots;  // sticky, read by bzr_scene_check
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    e = bzr::launch_trace(s->view, io, mode, s->blocks, st, totals);
+    return e == cudaSuccess ? BZR_OK : cuda_fail(e, "kernel launch");
+  }
+  if (n_dev != 0) return fail(BZR_EINVAL, "arrays must be all host or all device memory");
+
+  // Host arrays: stage through device buffers on the scene's stream.
+  std::lock_guard<std::mutex> lock(s->stage_mu);
+  // every staged array starts on a 256-byte boundary (see take() below)
+  const size_t piece_bytes[10] = {24 * n, 24 * n, tmin ? 8 * n : 0, tmax ? 8 * n : 0,
+                                  t ? 8 * n : 0, uv ? 16 * n : 0, normal ? 24 * n : 0,
+                                  prim ? 4 * n : 0, geom ? 4 * n : 0, hit ? n : 0};
+  size_t need = 0;
+  for (size_t b : piece_bytes)
+    if (b) need += align_up(b, 256);
+  if (s->stage_bytes < need) {
+    cudaFree(s->stage_dev);
+    s->stage_dev = nullptr;
+    s->stage_bytes = 0;
+    if (cudaMalloc(&s->stage_dev, need) != cudaSuccess)
+      return fail(BZR_ENOMEM, "staging allocation failed");
+    s->stage_bytes = need;
+  }
+  char *p = static_cast<char *>(s->stage_dev);
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char *q = p + off;
+    off = align_up(off + bytes, 256);
+    return q;
+  };
+  cudaStream_t st = s->stream;
+  cudaError_t e = cudaSuccess;
+  auto h2d = [&](const void *src, size_t bytes) -> void * {
+    if (!src) return nullptr;
+    void *d = take(bytes);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, st);
+    return d;
+  };
+  io.org = static_cast<const double *>(h2d(org, 24 * n));
+  io.dir = static_cast<const double *>(h2d(dir, 24 * n));
+  io.tmin = static_cast<const double *>(h2d(tmin, 8 * n));
+  io.tmax = static_cast<const double *>(h2d(tmax, 8 * n));
+  io.t = t ? reinterpret_cast<double *>(take(8 * n)) : nullptr;
+  io.uv = uv ? reinterpret_cast<double *>(take(16 * n)) : nullptr;
+  io.normal = normal ? reinterpret_cast<double *>(take(24 * n)) : nullptr;
+  io.prim = prim ? reinterpret_cast<uint32_t *>(take(4 * n)) : nullptr;
+  io.geom = geom ? reinterpret_cast<uint32_t *>(take(4 * n)) : nullptr;
+  io.hit = hit ? reinterpret_cast<uint8_t *>(take(n)) : nullptr;
+  io.error_word = counter + 1;
+  if (e == cudaSuccess) e = cudaMemsetAsync(counter, 0, 2 * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return cuda_fail(e, "staging copies");
+  e = bzr::launch_trace(s->view, io, mode, s->blocks, st, totals);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+  auto d2h = [&](void *dst, const void *src, size_t bytes) {
+    if (dst && e == cudaSuccess) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+  };
+  d2h(t, io.t, 8 * n);
+  d2h(uv, io.uv, 16 * n);
+  d2h(normal, io.normal, 24 * n);
+  d2h(prim, io.prim, 4 * n);
+  d2h(geom, io.geom, 4 * n);
+  d2h(hit, io.hit, n);
+  d2h(s->pinned_err, io.error_word, sizeof(uint32_t));
+  if (e != cudaSuccess) return cuda_fail(e, "result copies");
+  const int rc = wait_stream(st, default_timeout_ms());
+  if (rc) return rc;
+  if (*s->pinned_err)
+    return fail(BZR_EDEVICE_FLAG, "kernel bounds check fired (error bits " +
+                                      std::to_string(*s->pinned_err) + ")");
+  return BZR_OK;
+}
+
+int bzr_intersectN(const bzr_scene *s, size_t n, const double *org, const double *dir,
+                   const double *tmin, const double *tmax, double *t, double *uv, double *normal,
+                   uint32_t *prim, uint32_t *geom, uint8_t *hit, int mode, void *stream) {
+  return run_batch(s, n, org, dir, tmin, tmax, t, uv, normal, prim, geom, hit, mode, stream,
+                   nullptr);
+}
+
+int bzr_work_counts(const bzr_scene *cs, size_t n, const double *org, const double *dir,
+                    const double *tmin, const double *tmax, uint64_t totals[8], void *stream) {
+  bzr_scene *s = const_cast<bzr_scene *>(cs);
+  if (!s || !totals) return fail(BZR_EINVAL, "null argument");
+  if (!s->host.committed) return fail(BZR_ESTATE, "scene is not committed");
+  for (int k = 0; k < 8; ++k) totals[k] = 0;
+  if (n == 0) return BZR_OK;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(s->device);
+  unsigned long long *dev = nullptr;
+  cudaError_t e = cudaMalloc(&dev, 8 * sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    cudaSetDevice(cur);
+    return fail(BZR_ENOMEM, "counter allocation failed");
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  e = cudaMemsetAsync(dev, 0, 8 * sizeof(unsigned long long), st);
+  int rc = e == cudaSuccess ? BZR_OK : cuda_fail(e, "cudaMemsetAsync");
+  cudaSetDevice(cur);
+  if (rc == BZR_OK)
+    rc = run_batch(s, n, org, dir, tmin, tmax, nullptr, nullptr, nullptr, nullptr, nullptr,
+                   nullptr, BZR_MODE_FP64, stream, dev);
+  cudaSetDevice(s->device);
+  // the host path ran on the scene's stream; make the counter copy wait for both
+  if (rc == BZR_OK) rc = wait_stream(s->stream, default_timeout_ms());
+  if (rc == BZR_OK) rc = wait_stream(st, default_timeout_ms());
+  if (rc == BZR_OK) {
+    unsigned long long h[8];
+    e = cudaMemcpy(h, dev, sizeof h, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+      rc = cuda_fail(e, "counter read");
+    else
+      for (int k = 0; k < 8; ++k) totals[k] = h[k];
+  }
+  cudaFree(dev);
+  cudaSetDevice(cur);
+  return rc;
+}
+
+int bzr_intersect1(const bzr_scene *s, const double origin[3], const double direction[3],
+                   double tmin, double tmax, bzr_rayhit *rayhit, int *hit) {
+  if (!origin || !direction || !rayhit) return fail(BZR_EINVAL, "null argument");
+  uint8_t h = 0;
+  const int rc = bzr_intersectN(s, 1, origin, direction, &tmin, &tmax, &rayhit->hit_distance,
+                                rayhit->uv, rayhit->normal, &rayhit->prim_id, &rayhit->geom_id,
+                                &h, BZR_MODE_FP64, nullptr);
+  if (hit) *hit = h;
+  return rc;
+}
+
+int bzr_scene_check(const bzr_scene *s, void *stream, int timeout_ms, uint32_t *flags) {
+  if (!s) return fail(BZR_EINVAL, "scene is null");
+  if (flags) *flags = 0;
+  if (!s->host.committed) return BZR_OK;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(s->device);
+  int rc = wait_stream(static_cast<cudaStream_t>(stream), timeout_ms);
+  uint32_t word = 0;
+  if (rc == BZR_OK) {
+    const cudaError_t e =
+        cudaMemcpy(&word, s->slots + 2 * kSlots, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = cuda_fail(e, "error word read");
+  }
+  cudaSetDevice(cur);
+  if (rc) return rc;
+  if (flags) *flags = word;
+  return word ? fail(BZR_EDEVICE_FLAG, "kernel bounds check fired") : BZR_OK;
+}
+
+int bzr_scene_stats(const bzr_scene *s, int kind, uint64_t *n_nodes, uint32_t *max_depth,
+                    double *build_seconds) {
+  if (!s || kind < 0 || kind >= bzr::kNumKinds) return fail(BZR_EINVAL, "bad argument");
+  const bzr::Collection &c = s->host.kind[kind];
+  if (n_nodes) *n_nodes = c.tree.nodes.size();
+  if (max_depth) *max_depth = c.tree.max_depth;
+  if (build_seconds) *build_seconds = c.tree.build_seconds;
+  return BZR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,73 @@
+// Device data layout shared by the host flattener (scene.cpp) and the kernels (trace.cu).
+//
+// One BVH per primitive kind, as in the reference (blazert/scene.h:52-70).  The reference's
+// binary tree (blazert/bvh/node.h:15-41: each node holds its own box; leaves hold a vector of
+// primitives) is re-laid out for the GPU:
+//
+//  * Only INTERNAL nodes become device nodes, numbered breadth-first (so the top levels are a
+//    contiguous prefix).  A device node holds the boxes of its two CHILDREN, so one 128-byte
+//    line gives both slab tests, and a child is never fetched just to be rejected.
+//  * A child reference is either a device-node index, or kLeafBit | q where q is the position
+//    of the leaf's first primitive in the leaf-ordered primitive arrays.  The leaf's primitives
+//    follow contiguously in the reference's stored order (blazert/bvh/builder.h:133-148); the
+//    last one carries kLastBit in its id word.
+//  * The root's own box and reference live in KindView (the reference tests the root box
+//    first, blazert/bvh/accel.h:83-97).
+#pragma once
+#include <cstdint>
+
+namespace bzr {
+
+constexpr uint32_t kLeafBit = 0x80000000u;
+constexpr uint32_t kLastBit = 0x80000000u;
+constexpr uint32_t kIdMask = 0x7FFFFFFFu;
+
+enum Kind : int { kMesh = 0, kSpheres = 1, kPlanes = 2, kCylinders = 3, kNumKinds = 4 };
+
+// FP64 node, 16 doubles = 128 bytes (8 x 16-byte loads):
+//   d[0..5]   child 0: (lo.x, hi.x), (lo.y, hi.y), (lo.z, hi.z)
+//   d[6..11]  child 1: same
+//   d[12..13] uint32 {ref0, ref1, axis, 0}
+//   d[14..15] unused
+constexpr int kNode64Doubles = 16;
+// FP32 node for the mixed path, 16 floats = 64 bytes (4 x 16-byte loads); lo rounded toward
+// -inf, hi toward +inf, same slot order as the FP64 node:
+//   f[0..5]   child 0 pairs, f[6..11] child 1 pairs, f[12..15] uint32 {ref0, ref1, axis, 0}
+constexpr int kNode32Floats = 16;
+
+// Leaf-ordered primitive payload, doubles per primitive:
+//   mesh       12: v0(3), e1 = v0 - v1 (3), e2 = v2 - v0 (3), n = cross(e1, e2) (3)
+//                  (the Triangle of blazert/primitives/trimesh.h:19-31 plus its face normal)
+//   spheres     4: center(3), radius
+//   planes     14: center(3), dx, dy, rotation(9, row-major)
+//   cylinders  16: center(3), semi_axis_a, semi_axis_b, height, rotation(9), pad
+constexpr int kPayloadDoubles[kNumKinds] = {12, 4, 14, 16};
+
+struct KindView {
+  const double *nodes64 = nullptr;  // n_internal * kNode64Doubles
+  const float *nodes32 = nullptr;   // n_internal * kNode32Floats
+  const double *payload = nullptr;  // n_prims * kPayloadDoubles[kind]
+  const uint32_t *prim_ids = nullptr;  // n_prims: id | kLastBit on a leaf's last primitive
+  uint32_t n_internal = 0;
+  uint32_t n_prims = 0;
+  uint32_t root_ref = 0;
+  uint32_t geom_id = 0xFFFFFFFFu;
+  int present = 0;
+  int mixed_ok = 0;                 // all boxes finite: the FP32 path may be used
+  double root_box[6] = {0, 0, 0, 0, 0, 0};  // (lo.x, hi.x, lo.y, hi.y, lo.z, hi.z)
+  float root_box32[6] = {0, 0, 0, 0, 0, 0};
+};
+
+struct SceneView {
+  KindView k[kNumKinds];
+  const uint32_t *faces = nullptr;   // n_faces * 3, original order (triangle normals)
+  const double *vert_n = nullptr;    // n_vertices * 3 accumulated vertex normals
+  uint32_t stack_cap = 32;           // traversal stack entries per thread
+};
+
+// Kernel error word bits.
+constexpr uint32_t kErrStack = 1u;      // traversal stack would overflow
+constexpr uint32_t kErrNodeIndex = 2u;  // a child reference points outside the node array
+constexpr uint32_t kErrPrimIndex = 4u;  // a leaf runs past the primitive arrays
+
+}  // namespace bzr

@@ -1,0 +1,450 @@
+// Host side of a scene: precompute, binned-SAH build, flattening (see scene.h).
+//
+// Compiled with -ffp-contract=off.  The precomputed boxes, centres and normals, and every
+// decision of the builder, must be bit-identical to the reference's, because the GPU path is
+// required to return the reference's prim_id for every ray.  Vector arithmetic follows one
+// fixed order throughout: dot = (x0*y0 + x1*y1) + x2*y2, |v| = sqrt(dot(v, v)),
+// normalize(v) = v * (1/|v|), (R v)_i = (R_i0 v0 + R_i1 v1) + R_i2 v2.
+#include "scene.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <queue>
+
+namespace bzr {
+namespace {
+
+constexpr double kMax = std::numeric_limits<double>::max();
+
+struct V3 {
+  double x, y, z;
+  double operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+inline V3 load3(const double *p) { return {p[0], p[1], p[2]}; }
+inline void store3(double *p, V3 v) {
+  p[0] = v.x;
+  p[1] = v.y;
+  p[2] = v.z;
+}
+inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 operator/(V3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+inline V3 scale(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline double dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline V3 normalize(V3 a) {
+  const double len = std::sqrt(dot(a, a));
+  return scale(a, len != 0.0 ? 1.0 / len : 0.0);
+}
+inline V3 rotate(const double *R, V3 v) {
+  return {(R[0] * v.x + R[1] * v.y) + R[2] * v.z, (R[3] * v.x + R[4] * v.y) + R[5] * v.z,
+          (R[6] * v.x + R[7] * v.y) + R[8] * v.z};
+}
+
+// Grow the box (mn, mx) by (bmn, bmx) with std::min / std::max argument order of the
+// reference's box union (blazert/datatypes.h:87-93).
+inline void grow(double *mn, double *mx, const double *bmn, const double *bmx) {
+  for (int k = 0; k < 3; ++k) {
+    mn[k] = std::min(bmn[k], mn[k]);
+    mx[k] = std::max(bmx[k], mx[k]);
+  }
+}
+
+void alloc_boxes(PrimBoxes &b, size_t n) {
+  b.n = n;
+  b.bmin.assign(3 * n, 0.0);
+  b.bmax.assign(3 * n, 0.0);
+  b.center.assign(3 * n, 0.0);
+}
+
+// Box of six points, reduced with std::min / std::max over an initializer list as the
+// plane and cylinder collections do (first extreme value wins).
+void six_point_box(const V3 (&p)[6], double *mn, double *mx) {
+  for (int k = 0; k < 3; ++k) {
+    mn[k] = std::min({p[0][k], p[1][k], p[2][k], p[3][k], p[4][k], p[5][k]});
+    mx[k] = std::max({p[0][k], p[1][k], p[2][k], p[3][k], p[4][k], p[5][k]});
+  }
+}
+
+// ------------------------------------------------------------------------------ builder
+struct Bin {
+  double mn[3], mx[3];
+  uint32_t count;
+  double cost;
+  void clear() {
+    mn[0] = mn[1] = mn[2] = kMax;
+    mx[0] = mx[1] = mx[2] = -kMax;
+    count = 0;
+    cost = 0.0;
+  }
+};
+
+// Surface area of a box as the reference computes it (blazert/bvh/binbuffer.h:16-19).
+inline double surface(const double *mn, const double *mx) {
+  const double e0 = std::abs(mx[0] - mn[0]), e1 = std::abs(mx[1] - mn[1]),
+               e2 = std::abs(mx[2] - mn[2]);
+  return 2.0 * ((e0 * e1 + e1 * e2) + e2 * e0);
+}
+
+class SahBuilder {
+ public:
+  SahBuilder(const PrimBoxes &p, const BuildOptions &o, Tree &t)
+      : p_(p), o_(o), t_(t), bins_(3 * size_t(o.bins)) {}
+
+  // Returns the index of the node created for [begin, end) (blazert/bvh/builder.h:84-115).
+  uint32_t node(uint32_t *begin, uint32_t *end, uint32_t depth) {
+    const auto self = static_cast<uint32_t>(t_.nodes.size());
+    t_.max_depth = std::max(t_.max_depth, depth);
+    t_.nodes.emplace_back();
+    TreeNode nd{};
+    nd.leaf = nd.axis = nd.child[0] = nd.child[1] = 0xFFFFFFFFu;
+    for (int k = 0; k < 3; ++k) {
+      nd.mn[k] = kMax;
+      nd.mx[k] = -kMax;
+    }
+    for (const uint32_t *it = begin; it != end; ++it)
+      grow(nd.mn, nd.mx, &p_.bmin[3 * *it], &p_.bmax[3 * *it]);
+    const auto n = static_cast<uint32_t>(end - begin);
+    if (n <= o_.min_leaf || depth >= o_.max_depth) {
+      nd.leaf = 1;
+      nd.prim_off = static_cast<uint32_t>(t_.leaf_prims.size());
+      nd.prim_cnt = n;
+      t_.leaf_prims.insert(t_.leaf_prims.end(), begin, end);
+      t_.nodes[self] = nd;
+      return self;
+    }
+    uint32_t *mid = nullptr;
+    nd.leaf = 0;
+    nd.axis = split(begin, end, nd.mn, nd.mx, mid);
+    nd.prim_off = nd.prim_cnt = 0;
+    t_.nodes[self] = nd;
+    const uint32_t c0 = node(begin, mid, depth + 1);
+    t_.nodes[self].child[0] = c0;
+    const uint32_t c1 = node(mid, end, depth + 1);
+    t_.nodes[self].child[1] = c1;
+    return self;
+  }
+
+ private:
+  // Binned SAH split (blazert/bvh/binbuffer.h:66-167) followed by the partition with its
+  // middle-split fallback that tries the next axis (blazert/bvh/builder.h:201-226).
+  uint32_t split(uint32_t *begin, uint32_t *end, const double *mn, const double *mx,
+                 uint32_t *&mid) {
+    const uint32_t nb = o_.bins;
+    for (auto &b : bins_) b.clear();
+    double inv[3];
+    for (int k = 0; k < 3; ++k) {
+      const double ext = mx[k] - mn[k];
+      inv[k] = ext > 0.0 ? 1.0 / ext : 0.0;
+    }
+    for (const uint32_t *it = begin; it != end; ++it) {
+      const double *c = &p_.center[3 * *it];
+      for (int k = 0; k < 3; ++k) {
+        const double pos = ((c[k] - mn[k]) * inv[k]) * static_cast<double>(nb - 1);
+        const uint32_t slot =
+            std::min(nb - 1, unsigned(std::max(0u, unsigned(std::round(pos)))));
+        Bin &b = bins_[k * nb + slot];
+        ++b.count;
+        grow(b.mn, b.mx, &p_.bmin[3 * *it], &p_.bmax[3 * *it]);
+      }
+    }
+    double cut[3];
+    double best[3] = {kMax, kMax, kMax};
+    for (int k = 0; k < 3; ++k) {
+      Bin *row = &bins_[k * nb];
+      double amn[3] = {kMax, kMax, kMax}, amx[3] = {-kMax, -kMax, -kMax};
+      size_t count = 0;
+      for (uint32_t i = nb - 1; i > 0; --i) {  // right-hand costs
+        grow(amn, amx, row[i].mn, row[i].mx);
+        count += row[i].count;
+        row[i].cost = static_cast<double>(count) * surface(amn, amx);
+      }
+      for (int q = 0; q < 3; ++q) {
+        amn[q] = kMax;
+        amx[q] = -kMax;
+      }
+      count = 0;
+      uint32_t first_right = 1;
+      for (uint32_t i = 0; i + 1 < nb; ++i) {  // left sweep, full cost
+        grow(amn, amx, row[i].mn, row[i].mx);
+        count += row[i].count;
+        const double cost = static_cast<double>(count) * surface(amn, amx) + row[i + 1].cost;
+        if (cost < best[k]) {
+          best[k] = cost;
+          first_right = i + 1;
+        }
+      }
+      cut[k] = static_cast<double>(first_right) * ((mx[k] - mn[k]) / static_cast<double>(nb)) +
+               mn[k];
+    }
+    uint32_t axis = 0;
+    if (best[0] > best[1]) axis = 1;
+    if (best[axis] > best[2]) axis = 2;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+      const double pos = cut[axis];
+      const double *ctr = p_.center.data();
+      const uint32_t ax = axis;
+      mid = std::partition(begin, end,
+                           [ctr, ax, pos](uint32_t id) { return ctr[3 * id + ax] < pos; });
+      if (mid == begin || mid == end) {
+        ++t_.bad_splits;
+        mid = begin + ((end - begin) >> 1);
+        axis = (axis + 1) % 3;
+      } else {
+        break;
+      }
+    }
+    return axis;
+  }
+
+  const PrimBoxes &p_;
+  const BuildOptions &o_;
+  Tree &t_;
+  std::vector<Bin> bins_;
+};
+
+// Outward rounding of a double bound to float.
+inline float round_down(double d) {
+  float f = static_cast<float>(d);
+  if (static_cast<double>(f) > d) f = std::nextafter(f, -std::numeric_limits<float>::infinity());
+  return f;
+}
+inline float round_up(double d) {
+  float f = static_cast<float>(d);
+  if (static_cast<double>(f) < d) f = std::nextafter(f, std::numeric_limits<float>::infinity());
+  return f;
+}
+
+}  // namespace
+
+// blazert/bvh/builder.h:46-65
+Tree build_tree(const PrimBoxes &boxes, const BuildOptions &opt) {
+  Tree t;
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<uint32_t> ids(boxes.n);
+  std::iota(ids.begin(), ids.end(), 0u);
+  t.nodes.reserve(2 * boxes.n + 1);
+  t.leaf_prims.reserve(boxes.n);
+  SahBuilder b(boxes, opt, t);
+  b.node(ids.data(), ids.data() + ids.size(), 0);
+  t.build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return t;
+}
+
+// blazert/primitives/trimesh.h:78-130: centre (v0+v1+v2)/3, box of the corners, unit face
+// normal of cross(v1-v0, v2-v0) accumulated /3 into each corner's vertex normal.
+void add_mesh(HostScene &s, const double *v, size_t nv, const uint32_t *f, size_t nf) {
+  Collection &c = s.kind[kMesh];
+  s.vertices.assign(v, v + 3 * nv);
+  s.faces.assign(f, f + 3 * nf);
+  s.vert_n.assign(3 * nv, 0.0);
+  c.n = nf;
+  alloc_boxes(c.boxes, nf);
+  for (size_t i = 0; i < nf; ++i) {
+    const uint32_t *F = &s.faces[3 * i];
+    const V3 a = load3(&s.vertices[3 * F[0]]), b = load3(&s.vertices[3 * F[1]]),
+             cc = load3(&s.vertices[3 * F[2]]);
+    store3(&c.boxes.center[3 * i], ((a + b) + cc) / 3.0);
+    double mn[3] = {a.x, a.y, a.z}, mx[3] = {a.x, a.y, a.z};
+    const double pb[3] = {b.x, b.y, b.z}, pc[3] = {cc.x, cc.y, cc.z};
+    grow(mn, mx, pb, pb);
+    grow(mn, mx, pc, pc);
+    std::memcpy(&c.boxes.bmin[3 * i], mn, sizeof mn);
+    std::memcpy(&c.boxes.bmax[3 * i], mx, sizeof mx);
+    const V3 share = normalize(cross(b - a, cc - a)) / 3.0;
+    for (int j = 0; j < 3; ++j) {
+      double *vn = &s.vert_n[3 * F[j]];
+      store3(vn, load3(vn) + share);
+    }
+  }
+}
+
+// blazert/primitives/sphere.h:93-100: box = centre -+ radius.
+void add_spheres(HostScene &s, const double *ctr, const double *r, size_t n) {
+  Collection &c = s.kind[kSpheres];
+  c.n = n;
+  c.a.assign(ctr, ctr + 3 * n);
+  c.b.assign(r, r + n);
+  alloc_boxes(c.boxes, n);
+  for (size_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) {
+      c.boxes.bmin[3 * i + k] = c.a[3 * i + k] - c.b[i];
+      c.boxes.bmax[3 * i + k] = c.a[3 * i + k] + c.b[i];
+      c.boxes.center[3 * i + k] = c.a[3 * i + k];
+    }
+}
+
+// blazert/primitives/plane.h:113-150: box of the four rotated corners and the two points
+// +-DBL_MIN along the rotated normal.
+void add_planes(HostScene &s, const double *ctr, const double *dx, const double *dy,
+                const double *rot, size_t n) {
+  Collection &c = s.kind[kPlanes];
+  c.n = n;
+  c.a.assign(ctr, ctr + 3 * n);
+  c.b.assign(dx, dx + n);
+  c.c.assign(dy, dy + n);
+  c.d.assign(rot, rot + 9 * n);
+  alloc_boxes(c.boxes, n);
+  const double th = std::numeric_limits<double>::min();
+  for (size_t i = 0; i < n; ++i) {
+    const V3 o = load3(&c.a[3 * i]);
+    const double *R = &c.d[9 * i];
+    const double hx = c.b[i], hy = c.c[i];
+    const V3 p[6] = {o + rotate(R, {-hx / 2.0, -hy / 2.0, 0.0}),
+                     o + rotate(R, {hx / 2.0, -hy / 2.0, 0.0}),
+                     o + rotate(R, {-hx / 2.0, hy / 2.0, 0.0}),
+                     o + rotate(R, {hx / 2.0, hy / 2.0, 0.0}),
+                     o + rotate(R, {0.0, 0.0, -th}),
+                     o + rotate(R, {0.0, 0.0, th})};
+    six_point_box(p, &c.boxes.bmin[3 * i], &c.boxes.bmax[3 * i]);
+    store3(&c.boxes.center[3 * i], o);
+  }
+}
+
+// blazert/primitives/cylinder.h:115-147: box of the six points centre +- R a e_x,
+// +- R b e_y, +- R (h/2) e_z (not the true box of a rotated cylinder).
+void add_cylinders(HostScene &s, const double *ctr, const double *a, const double *b,
+                   const double *h, const double *rot, size_t n) {
+  Collection &c = s.kind[kCylinders];
+  c.n = n;
+  c.a.assign(ctr, ctr + 3 * n);
+  c.b.assign(a, a + n);
+  c.c.assign(b, b + n);
+  c.d.assign(h, h + n);
+  c.e.assign(rot, rot + 9 * n);
+  alloc_boxes(c.boxes, n);
+  for (size_t i = 0; i < n; ++i) {
+    const V3 o = load3(&c.a[3 * i]);
+    const double *R = &c.e[9 * i];
+    const V3 ra = rotate(R, {c.b[i], 0.0, 0.0}), rb = rotate(R, {0.0, c.c[i], 0.0}),
+             rh = rotate(R, {0.0, 0.0, c.d[i] / 2.0});
+    const V3 p[6] = {o + ra, o + rb, o - ra, o - rb, o + rh, o - rh};
+    six_point_box(p, &c.boxes.bmin[3 * i], &c.boxes.bmax[3 * i]);
+    store3(&c.boxes.center[3 * i], o);
+  }
+}
+
+KindImage flatten(const HostScene &s, int kind) {
+  const Collection &c = s.kind[kind];
+  const Tree &t = c.tree;
+  KindImage img;
+  const size_t nn = t.nodes.size();
+  // Leaf positions in the leaf-ordered primitive arrays follow the tree's node order.
+  std::vector<uint32_t> leaf_pos(nn, 0), dev_index(nn, 0xFFFFFFFFu);
+  uint32_t pos = 0;
+  for (size_t i = 0; i < nn; ++i)
+    if (t.nodes[i].leaf == 1) {
+      leaf_pos[i] = pos;
+      pos += t.nodes[i].prim_cnt;
+    }
+  // Breadth-first numbering of the internal nodes.
+  std::vector<uint32_t> order;
+  if (nn && t.nodes[0].leaf != 1) {
+    std::queue<uint32_t> q;
+    q.push(0);
+    while (!q.empty()) {
+      const uint32_t i = q.front();
+      q.pop();
+      dev_index[i] = static_cast<uint32_t>(order.size());
+      order.push_back(i);
+      for (int j = 0; j < 2; ++j) {
+        const uint32_t ch = t.nodes[i].child[j];
+        if (t.nodes[ch].leaf != 1) q.push(ch);
+      }
+    }
+  }
+  auto ref_of = [&](uint32_t i) {
+    return t.nodes[i].leaf == 1 ? (kLeafBit | leaf_pos[i]) : dev_index[i];
+  };
+  auto finite_box = [](const TreeNode &nd) {
+    for (int k = 0; k < 3; ++k)
+      if (!std::isfinite(nd.mn[k]) || !std::isfinite(nd.mx[k])) return false;
+    return true;
+  };
+  img.n_internal = static_cast<uint32_t>(order.size());
+  img.nodes64.assign(size_t(img.n_internal) * kNode64Doubles, 0.0);
+  img.nodes32.assign(size_t(img.n_internal) * kNode32Floats, 0.0f);
+  for (uint32_t g = 0; g < img.n_internal; ++g) {
+    const TreeNode &nd = t.nodes[order[g]];
+    double *d = &img.nodes64[size_t(g) * kNode64Doubles];
+    float *f = &img.nodes32[size_t(g) * kNode32Floats];
+    for (int j = 0; j < 2; ++j) {
+      const TreeNode &ch = t.nodes[nd.child[j]];
+      if (!finite_box(ch)) img.mixed_ok = false;
+      for (int k = 0; k < 3; ++k) {
+        d[6 * j + 2 * k] = ch.mn[k];
+        d[6 * j + 2 * k + 1] = ch.mx[k];
+        f[6 * j + 2 * k] = round_down(ch.mn[k]);
+        f[6 * j + 2 * k + 1] = round_up(ch.mx[k]);
+      }
+    }
+    const uint32_t meta[4] = {ref_of(nd.child[0]), ref_of(nd.child[1]), nd.axis, 0u};
+    std::memcpy(d + 12, meta, sizeof meta);
+    std::memcpy(f + 12, meta, sizeof meta);
+  }
+  if (nn) {
+    const TreeNode &root = t.nodes[0];
+    img.root_ref = ref_of(0);
+    if (!finite_box(root)) img.mixed_ok = false;
+    for (int k = 0; k < 3; ++k) {
+      img.root_box[2 * k] = root.mn[k];
+      img.root_box[2 * k + 1] = root.mx[k];
+      img.root_box32[2 * k] = round_down(root.mn[k]);
+      img.root_box32[2 * k + 1] = round_up(root.mx[k]);
+    }
+  }
+  // Leaf-ordered primitives.
+  const size_t np = t.leaf_prims.size();
+  const int stride = kPayloadDoubles[kind];
+  img.prim_ids.resize(np);
+  img.payload.assign(np * stride, 0.0);
+  for (size_t i = 0; i < nn; ++i) {
+    const TreeNode &nd = t.nodes[i];
+    if (nd.leaf != 1) continue;
+    for (uint32_t q = 0; q < nd.prim_cnt; ++q) {
+      const uint32_t at = leaf_pos[i] + q;
+      const uint32_t id = t.leaf_prims[nd.prim_off + q];
+      img.prim_ids[at] = id | (q + 1 == nd.prim_cnt ? kLastBit : 0u);
+      double *p = &img.payload[size_t(at) * stride];
+      switch (kind) {
+        case kMesh: {
+          const uint32_t *F = &s.faces[3 * id];
+          const V3 v0 = load3(&s.vertices[3 * F[0]]), v1 = load3(&s.vertices[3 * F[1]]),
+                   v2 = load3(&s.vertices[3 * F[2]]);
+          const V3 e1 = v0 - v1, e2 = v2 - v0;  // the reference Triangle's c and b
+          store3(p, v0);
+          store3(p + 3, e1);
+          store3(p + 6, e2);
+          store3(p + 9, cross(e1, e2));
+          break;
+        }
+        case kSpheres:
+          for (int k = 0; k < 3; ++k) p[k] = c.a[3 * id + k];
+          p[3] = c.b[id];
+          break;
+        case kPlanes:
+          for (int k = 0; k < 3; ++k) p[k] = c.a[3 * id + k];
+          p[3] = c.b[id];
+          p[4] = c.c[id];
+          for (int k = 0; k < 9; ++k) p[5 + k] = c.d[9 * id + k];
+          break;
+        case kCylinders:
+          for (int k = 0; k < 3; ++k) p[k] = c.a[3 * id + k];
+          p[3] = c.b[id];
+          p[4] = c.c[id];
+          p[5] = c.d[id];
+          for (int k = 0; k < 9; ++k) p[6 + k] = c.e[9 * id + k];
+          break;
+      }
+    }
+  }
+  return img;
+}
+
+}  // namespace bzr

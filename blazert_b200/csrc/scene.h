@@ -1,0 +1,85 @@
+// Host side of a scene: the primitive collections with their precomputed boxes and centres,
+// the binned-SAH builder that reproduces the reference's tree node for node, and the
+// flattening into the device layout of layout.h.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "layout.h"
+
+namespace bzr {
+
+struct BuildOptions {
+  uint32_t min_leaf = 4;  // blazert/bvh/options.h:20-21 defaults
+  uint32_t max_depth = 28;
+  uint32_t bins = 64;
+};
+
+// Per-primitive boxes and centres of one collection, n x 3 each.
+struct PrimBoxes {
+  size_t n = 0;
+  std::vector<double> bmin, bmax, center;
+};
+
+// The reference tree (blazert/bvh/node.h:15-41) in its DFS pre-order.
+struct TreeNode {
+  double mn[3], mx[3];
+  uint32_t leaf, axis, child[2];
+  uint32_t prim_off, prim_cnt;  // into Tree::leaf_prims for leaves
+};
+
+struct Tree {
+  std::vector<TreeNode> nodes;
+  std::vector<uint32_t> leaf_prims;  // primitive ids, leaves in node order
+  uint32_t max_depth = 0;
+  uint32_t bad_splits = 0;
+  double build_seconds = 0.0;
+};
+
+Tree build_tree(const PrimBoxes &boxes, const BuildOptions &opt);
+
+// Host copy of one collection (the caller's arrays are copied at add time).
+struct Collection {
+  bool present = false;
+  uint32_t geom_id = 0xFFFFFFFFu;
+  size_t n = 0;
+  std::vector<double> a, b, c, d, e;  // kind-specific raw arrays (see scene.cpp)
+  PrimBoxes boxes;
+  Tree tree;
+};
+
+struct HostScene {
+  Collection kind[kNumKinds];
+  std::vector<double> vertices;   // mesh: n_vertices x 3
+  std::vector<uint32_t> faces;    // mesh: n_faces x 3
+  std::vector<double> vert_n;     // mesh: accumulated vertex normals
+  uint32_t geometries = 0;
+  bool committed = false;
+  BuildOptions opt;
+};
+
+// Collection constructors: copy and precompute (blazert/primitives/*.h collection ctors).
+void add_mesh(HostScene &s, const double *v, size_t nv, const uint32_t *f, size_t nf);
+void add_spheres(HostScene &s, const double *c, const double *r, size_t n);
+void add_planes(HostScene &s, const double *c, const double *dx, const double *dy,
+                const double *rot, size_t n);
+void add_cylinders(HostScene &s, const double *c, const double *a, const double *b,
+                   const double *h, const double *rot, size_t n);
+
+// Device image of one kind, ready to upload.
+struct KindImage {
+  std::vector<double> nodes64;
+  std::vector<float> nodes32;
+  std::vector<double> payload;
+  std::vector<uint32_t> prim_ids;
+  uint32_t n_internal = 0;
+  uint32_t root_ref = 0;
+  double root_box[6] = {0, 0, 0, 0, 0, 0};
+  float root_box32[6] = {0, 0, 0, 0, 0, 0};
+  bool mixed_ok = true;
+};
+
+KindImage flatten(const HostScene &s, int kind);
+
+}  // namespace bzr

@@ -1,0 +1,519 @@
+// Per-ray closest-hit traversal, shared by the sm_100a kernels (trace.cu) and, compiled as
+// host code, by the test-only CPU emulator (tests/emu/).  Exactness rules are stated in
+// trace.cu.  Everything here is a pure function of the scene view and one ray.
+#pragma once
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+
+#include "layout.h"
+
+#if defined(__CUDACC__)
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#define BZR_HD __host__ __device__ __forceinline__
+#define BZR_NOINLINE __host__ __device__ __noinline__
+#define BZR_INF (__builtin_inf())
+#else
+#include <vector_types.h>
+#include <vector_functions.h>
+#define BZR_HD inline
+#define BZR_NOINLINE inline
+#define BZR_INF (__builtin_inf())
+#endif
+
+namespace bzr {
+
+// Portability shims: the same source runs as device code and as host code.
+template <class T>
+BZR_HD T ldg(const T *p) {
+#if defined(__CUDA_ARCH__)
+  return __ldg(p);
+#else
+  return *p;
+#endif
+}
+BZR_HD void flag_error(uint32_t *err, uint32_t bit) {
+#if defined(__CUDA_ARCH__)
+  atomicOr(err, bit);
+#else
+  *err |= bit;
+#endif
+}
+BZR_HD long long dbits(double x) {
+#if defined(__CUDA_ARCH__)
+  return __double_as_longlong(x);
+#else
+  long long r;
+  std::memcpy(&r, &x, 8);
+  return r;
+#endif
+}
+BZR_HD double bitsd(long long x) {
+#if defined(__CUDA_ARCH__)
+  return __longlong_as_double(x);
+#else
+  double r;
+  std::memcpy(&r, &x, 8);
+  return r;
+#endif
+}
+
+constexpr double kL1 = 1.0 + 4.0 * 2.220446049250313080847e-16;  // 1 + 4 * DBL_EPSILON
+constexpr double kTol = 4.0 * 2.220446049250313080847e-16;      // trimesh.h:156
+constexpr double kDblMax = 1.7976931348623157e308;
+
+struct D3 {
+  double x, y, z;
+};
+BZR_HD D3 d3(double a, double b, double c) { return {a, b, c}; }
+BZR_HD D3 add(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+BZR_HD D3 sub(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+BZR_HD D3 mul(D3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+BZR_HD D3 divs(D3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+BZR_HD double dot(D3 a, D3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+BZR_HD D3 cross(D3 a, D3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+BZR_HD double norm(D3 a) { return sqrt(dot(a, a)); }
+BZR_HD D3 normalize(D3 a) {
+  const double len = norm(a);
+  return mul(a, len != 0.0 ? 1.0 / len : 0.0);
+}
+// R * v and trans(R) * v for a row-major 3x3 R
+BZR_HD D3 rot(const double *R, D3 v) {
+  return {(R[0] * v.x + R[1] * v.y) + R[2] * v.z, (R[3] * v.x + R[4] * v.y) + R[5] * v.z,
+          (R[6] * v.x + R[7] * v.y) + R[8] * v.z};
+}
+BZR_HD D3 rot_t(const double *R, D3 v) {
+  return {(R[0] * v.x + R[3] * v.y) + R[6] * v.z, (R[1] * v.x + R[4] * v.y) + R[7] * v.z,
+          (R[2] * v.x + R[5] * v.y) + R[8] * v.z};
+}
+// x with its sign flipped when y is negative (blazert/datatypes.h:83-85)
+BZR_HD double product_sign(double x, double y) {
+  return bitsd(dbits(x) ^ (dbits(y) & (long long)0x8000000000000000ULL));
+}
+
+struct Ray {
+  D3 o, d, inv;  // origin, normalized direction, 1 / raw direction
+  unsigned sx, sy, sz;
+  double tmin, tmax;
+};
+
+// blazert/ray.h:56-65
+BZR_HD Ray make_ray(const double *o, const double *raw, double tmin,
+                                        double tmax) {
+  Ray r;
+  r.o = d3(o[0], o[1], o[2]);
+  const D3 w = d3(raw[0], raw[1], raw[2]);
+  r.d = normalize(w);
+  r.inv = d3(1.0 / w.x, 1.0 / w.y, 1.0 / w.z);
+  r.sx = w.x < 0.0;
+  r.sy = w.y < 0.0;
+  r.sz = w.z < 0.0;
+  r.tmin = tmin;
+  r.tmax = tmax;
+  return r;
+}
+
+// One axis of the slab test; lo/hi are the box's bounds on that axis.
+BZR_HD void slab_axis(double lo, double hi, unsigned s, double o, double inv,
+                                          double &mn, double &mx, bool &nan) {
+  const double entry = s ? hi : lo;
+  const double exit = s ? lo : hi;
+  const double a = (entry - o) * inv;
+  const double b = ((exit - o) * inv) * kL1;
+  mn = (a < mn) ? mn : a;  // std::max(a, mn)
+  nan |= (b != b);
+  mx = (mx < b) ? mx : b;  // std::min(b, mx)
+}
+
+// Hit-independent part of intersect_node for a box given as (lo, hi) pairs per axis.
+// Returns whether the box can be accepted for some hit distance; *key is the entry distance
+// to compare with the hit distance at pop time (-inf when the reference ignores it).
+BZR_HD bool box_test(double2 px, double2 py, double2 pz, const Ray &r,
+                                         double &key) {
+  double mn = r.tmin, mx = BZR_INF;
+  bool nan = false;
+  slab_axis(px.x, px.y, r.sx, r.o.x, r.inv.x, mn, mx, nan);
+  slab_axis(py.x, py.y, r.sy, r.o.y, r.inv.y, mn, mx, nan);
+  slab_axis(pz.x, pz.y, r.sz, r.o.z, r.inv.z, mn, mx, nan);
+  key = nan ? -BZR_INF : mn;
+  return mn <= mx;
+}
+
+// Per-kind intersector state (the reference's *Intersector after prepare_traversal).
+struct KState {
+  double hit;     // intersector.hit_distance
+  double u, v;    // uv (triangles only; 0 otherwise)
+  uint32_t pos;   // leaf-order position of the primitive hit
+  D3 n;           // plane / cylinder normal as computed at hit time (not yet normalized)
+};
+
+BZR_HD double2 ld2(const double *p) {
+  return ldg(reinterpret_cast<const double2 *>(p));
+}
+
+// blazert/primitives/trimesh.h:153-181 with the precomputed n = cross(e1, e2)
+BZR_HD bool isect_triangle(const double *P, uint32_t pos, const Ray &r,
+                                               KState &st) {
+  const double2 q0 = ld2(P), q1 = ld2(P + 2), q2 = ld2(P + 4), q3 = ld2(P + 6), q4 = ld2(P + 8),
+                q5 = ld2(P + 10);
+  const D3 v0 = d3(q0.x, q0.y, q1.x), e1 = d3(q1.y, q2.x, q2.y), e2 = d3(q3.x, q3.y, q4.x),
+           n = d3(q4.y, q5.x, q5.y);
+  const D3 c = sub(v0, r.o);
+  const D3 rr = cross(r.d, c);
+  const double det = dot(n, r.d);
+  const double abs_det = fabs(det);
+  const double u = product_sign(dot(rr, e2), det);
+  const double v = product_sign(dot(rr, e1), det);
+  const double w = (abs_det - u) - v;
+  if (u >= -kTol && v >= -kTol && w >= -kTol) {
+    const double t = product_sign(dot(n, c), det);
+    if (t >= abs_det * r.tmin && abs_det * st.hit > t) {
+      const double inv_det = 1.0 / abs_det;
+      st.hit = t * inv_det;
+      st.u = u * inv_det;
+      st.v = v * inv_det;
+      st.pos = pos;
+      return true;
+    }
+  }
+  return false;
+}
+
+// blazert/primitives/sphere.h:135-177
+BZR_HD bool isect_sphere(const double *P, uint32_t pos, const Ray &r,
+                                             KState &st) {
+  const double2 q0 = ld2(P), q1 = ld2(P + 2);
+  const D3 center = d3(q0.x, q0.y, q1.x);
+  const double radius = q1.y;
+  const D3 v = sub(r.o, center);
+  const double A = dot(r.d, r.d);
+  const double B = 2.0 * dot(v, r.d);
+  const double C = dot(v, v) - radius * radius;
+  const double D = B * B - (4.0 * A) * C;
+  if (D < 0.0) return false;
+  const double Q = sqrt(D);
+  const double rcpA = 1.0 / A;
+  const double t0 = (0.5 * rcpA) * (-B - Q);
+  const double t1 = (0.5 * rcpA) * (-B + Q);
+  if ((t0 > r.tmin) && (t0 < st.hit)) {
+    st.hit = norm(mul(r.d, t0));
+    st.pos = pos;
+    return true;
+  }
+  if ((t1 > r.tmin) && (t1 < st.hit)) {
+    st.hit = norm(mul(r.d, t1));
+    st.pos = pos;
+    return true;
+  }
+  return false;
+}
+
+// blazert/primitives/plane.h:180-270
+BZR_HD bool isect_plane(const double *P, uint32_t pos, const Ray &r,
+                                            KState &st) {
+  double R[9];
+  const double2 q0 = ld2(P), q1 = ld2(P + 2), q2 = ld2(P + 4), q3 = ld2(P + 6), q4 = ld2(P + 8),
+                q5 = ld2(P + 10), q6 = ld2(P + 12);
+  const D3 center = d3(q0.x, q0.y, q1.x);
+  const double dx = q1.y, dy = q2.x;
+  R[0] = q2.y; R[1] = q3.x; R[2] = q3.y; R[3] = q4.x; R[4] = q4.y;
+  R[5] = q5.x; R[6] = q5.y; R[7] = q6.x; R[8] = q6.y;
+  const D3 org = rot_t(R, sub(r.o, center));
+  const D3 dir = rot_t(R, r.d);
+  const double t1 = -org.z / dir.z;
+  if (!((t1 > r.tmin) && (t1 < st.hit))) return false;
+  const D3 ic = add(org, mul(dir, t1));
+  const double x_min = -dx / 2, x_max = dx / 2, y_min = -dy / 2, y_max = dy / 2;
+  const double x = ic.x, y = ic.y;
+  const double sz = org.z / fabs(org.z);
+  D3 n;
+  if ((x > x_min) && (x < x_max) && (y > y_min) && (y < y_max)) {
+    const D3 ez = rot(R, d3(0.0, 0.0, 1.0));
+    n = d3(sz * ez.x, sz * ez.y, sz * ez.z);
+  } else if ((x == x_min) && (x < x_max) && (y > y_min) && (y < y_max)) {  // edges
+    n = rot(R, d3(-1.0, 0.0, sz));
+  } else if ((x > x_min) && (x == x_max) && (y > y_min) && (y < y_max)) {
+    n = rot(R, d3(1.0, 0.0, sz));
+  } else if ((x > x_min) && (x < x_max) && (y == y_min) && (y < y_max)) {
+    n = rot(R, d3(0.0, -1.0, sz));
+  } else if ((x > x_min) && (x < x_max) && (y > y_min) && (y == y_max)) {
+    n = rot(R, d3(0.0, 1.0, sz));
+  } else if ((x == x_min) && (x < x_max) && (y == y_min) && (y < y_max)) {  // corners
+    n = rot(R, d3(-1.0, -1.0, sz));
+  } else if ((x == x_min) && (x < x_max) && (y > y_min) && (y == y_max)) {
+    n = rot(R, d3(-1.0, 1.0, sz));
+  } else if ((x > x_min) && (x == x_max) && (y == y_min) && (y < y_max)) {
+    n = rot(R, d3(1.0, -1.0, sz));
+  } else if ((x > x_min) && (x == x_max) && (y > y_min) && (y == y_max)) {
+    n = rot(R, d3(1.0, 1.0, sz));
+  } else {
+    return false;
+  }
+  st.n = n;
+  st.hit = norm(mul(dir, t1));
+  st.pos = pos;
+  return true;
+}
+
+BZR_HD bool cyl_hit(KState &st, uint32_t pos, D3 n, double t, D3 dir) {
+  st.n = n;
+  st.hit = norm(mul(dir, t));
+  st.pos = pos;
+  return true;
+}
+
+// blazert/primitives/cylinder.h:181-495 (no hit-distance test; unrotated normal in one branch)
+BZR_NOINLINE bool isect_cylinder(const double *P, uint32_t pos, const Ray &r,
+                                            KState &st) {
+  double R[9];
+  const double2 q0 = ld2(P), q1 = ld2(P + 2), q2 = ld2(P + 4), q3 = ld2(P + 6), q4 = ld2(P + 8),
+                q5 = ld2(P + 10), q6 = ld2(P + 12), q7 = ld2(P + 14);
+  const D3 center = d3(q0.x, q0.y, q1.x);
+  const double a = q1.y, b = q2.x, h = q2.y;
+  R[0] = q3.x; R[1] = q3.y; R[2] = q4.x; R[3] = q4.y; R[4] = q5.x;
+  R[5] = q5.y; R[6] = q6.x; R[7] = q6.y; R[8] = q7.x;
+  const D3 org = rot_t(R, sub(r.o, center));
+  const D3 dir = rot_t(R, r.d);
+  const double x0 = org.x, y0 = org.y, z0 = org.z;
+  const double j = dir.x, k = dir.y, l = dir.z;
+  const double h2 = h / 2.0, mh2 = -h / 2.0;
+  auto ng = [&](D3 n) { return divs(rot(R, n), norm(n)); };
+  auto shell_n = [&](D3 ic) { return d3(2 * ic.x / (a * a), 2 * ic.y / (b * b), 0.0); };
+  // the elliptic-shell quadratic, in the reference's operation order
+  auto quad = [&](double &t0, double &t1, D3 &i0, D3 &i1) {
+    const double A = a * a * k * k + b * b * j * j;
+    const double B = a * a * k * y0 + b * b * j * x0;
+    const double C = a * a * k * k + b * b * j * j - j * j * y0 * y0 + 2 * j * k * x0 * y0 -
+                     k * k * x0 * x0;
+    if (C < 0) return false;
+    t0 = 1.0 / A * (-B + a * b * sqrt(C));
+    t1 = -1.0 / A * (B + a * b * sqrt(C));
+    i0 = add(org, mul(dir, t0));
+    i1 = add(org, mul(dir, t1));
+    return true;
+  };
+  double t0, t1;
+  D3 i0, i1;
+  if (z0 > h2 || z0 < mh2) {  // areas 1 and 2: origin above or below the caps
+    if (l == 0) return false;
+    const double zc = z0 > h2 ? h2 : mh2;
+    const double tc = (zc - z0) / l;
+    if (tc < 0) return false;
+    const D3 ic = add(org, mul(dir, tc));
+    if (b * b * ic.x * ic.x + a * a * ic.y * ic.y <= a * a * b * b)
+      return cyl_hit(st, pos, ng(d3(0.0, 0.0, z0 > h2 ? 1.0 : -1.0)), tc, dir);
+    if (!quad(t0, t1, i0, i1)) return false;
+    if ((t1 > 0) && (t1 < t0) && (i1.z <= h2) && (i1.z >= mh2))
+      return cyl_hit(st, pos, ng(shell_n(i1)), t1, dir);
+    if ((t0 > 0) && (t0 < t1) && (i0.z <= h2) && (i0.z >= mh2))
+      return cyl_hit(st, pos, ng(shell_n(i0)), t0, dir);
+    return false;  // area 4 cannot hold when z0 is outside [-h/2, h/2]
+  }
+  const double ell = x0 * x0 * b * b + y0 * y0 * a * a;
+  if ((z0 > mh2) && (z0 < h2) && (ell > a * a * b * b)) {  // area 3: beside the shell
+    if (!quad(t0, t1, i0, i1)) return false;
+    if ((t1 > 0) && (t1 < t0) && (i1.z <= h2) && (i1.z >= mh2))
+      return cyl_hit(st, pos, ng(shell_n(i1)), t1, dir);
+    if ((t0 > 0) && (t0 < t1) && (i0.z <= h2) && (i0.z >= mh2))
+      return cyl_hit(st, pos, ng(shell_n(i0)), t0, dir);
+    return false;
+  }
+  if ((z0 >= mh2) && (z0 <= h2) && (ell <= a * a * b * b)) {  // area 4: inside
+    if (l == 0) {
+      if ((z0 == mh2) || (z0 == h2)) return false;
+      if (!quad(t0, t1, i0, i1)) return false;
+      if ((t1 > 0) && (i1.z <= h2) && (i1.z >= mh2))
+        return cyl_hit(st, pos, ng(shell_n(i1)), t1, dir);
+      if ((t0 > 0) && (i0.z <= h2) && (i0.z >= mh2))
+        return cyl_hit(st, pos, ng(shell_n(i0)), t0, dir);
+    } else if ((j == 0.0) && (k == 0)) {
+      if (b * b * x0 * x0 + a * a * y0 * y0 == a * a * b * b) return false;
+      if (l < 0) return cyl_hit(st, pos, ng(d3(0.0, 0.0, -1.0)), (mh2 - z0) / l, dir);
+      if (l > 0) return cyl_hit(st, pos, ng(d3(0.0, 0.0, 1.0)), (h2 - z0) / l, dir);
+    } else {
+      if (!quad(t0, t1, i0, i1)) return false;
+      if ((t1 > 0) && (i1.z <= h2) && (i1.z >= mh2))
+        return cyl_hit(st, pos, ng(shell_n(i1)), t1, dir);
+      if ((t0 > 0) && (i0.z <= h2) && (i0.z >= mh2))
+        return cyl_hit(st, pos, shell_n(i0), t0, dir);  // unrotated (cylinder.h:462-463)
+      if (l < 0) return cyl_hit(st, pos, ng(d3(0.0, 0.0, -1.0)), (mh2 - z0) / l, dir);
+      if (l > 0) return cyl_hit(st, pos, ng(d3(0.0, 0.0, 1.0)), (h2 - z0) / l, dir);
+    }
+  }
+  return false;
+}
+
+template <int KIND>
+BZR_HD bool isect(const double *payload, uint32_t pos, const Ray &r,
+                                      KState &st) {
+  const double *P = payload + size_t(pos) * kPayloadDoubles[KIND];
+  if (KIND == kMesh) return isect_triangle(P, pos, r, st);
+  if (KIND == kSpheres) return isect_sphere(P, pos, r, st);
+  if (KIND == kPlanes) return isect_plane(P, pos, r, st);
+  return isect_cylinder(P, pos, r, st);
+}
+
+// Traversal stack in shared memory, entry j of thread t at [j * blockDim.x + t].
+struct Stack {
+  double *key;
+  uint32_t *ref;
+  uint32_t cap, stride;
+};
+
+// Work counters of one ray (counting kernels only): per kind the box tests (the reference's
+// node pops: the root plus both children of every accepted internal node) and primitive tests.
+struct Counts {
+  uint32_t box[kNumKinds];
+  uint32_t prim[kNumKinds];
+};
+
+// blazert/bvh/accel.h:80-120 for one kind.  Returns the reference's hit flag.
+template <int KIND, bool COUNT>
+BZR_HD bool traverse(const KindView &K, const Ray &r, KState &st, const Stack &sk,
+                     uint32_t tid, uint32_t *err, Counts *cnt) {
+  st.hit = r.tmax;
+  st.u = st.v = 0.0;
+  st.pos = 0xFFFFFFFFu;
+  st.n = d3(0.0, 0.0, 0.0);
+  double key;
+  {
+    const double2 bx = make_double2(K.root_box[0], K.root_box[1]);
+    const double2 by = make_double2(K.root_box[2], K.root_box[3]);
+    const double2 bz = make_double2(K.root_box[4], K.root_box[5]);
+    if (COUNT) cnt->box[KIND] += 1;
+    if (!box_test(bx, by, bz, r, key) || key > st.hit) return false;
+  }
+  uint32_t cur = K.root_ref;
+  uint32_t sp = 0;
+  for (;;) {
+    if (cur & kLeafBit) {
+      uint32_t pos = cur & kIdMask;
+      for (;;) {  // intersect_leaf (blazert/bvh/intersect.h:67-78)
+        if (pos >= K.n_prims) {
+          flag_error(err, kErrPrimIndex);
+          return false;
+        }
+        const uint32_t id = ldg(K.prim_ids + pos);
+        if (COUNT) cnt->prim[KIND] += 1;
+        isect<KIND>(K.payload, pos, r, st);
+        if (id & kLastBit) break;
+        ++pos;
+      }
+    } else {
+      if (cur >= K.n_internal) {
+        flag_error(err, kErrNodeIndex);
+        return false;
+      }
+      const double *nd = K.nodes64 + size_t(cur) * kNode64Doubles;
+      const double2 a0 = ld2(nd), a1 = ld2(nd + 2), a2 = ld2(nd + 4);
+      const double2 b0 = ld2(nd + 6), b1 = ld2(nd + 8), b2 = ld2(nd + 10);
+      const uint4 meta = ldg(reinterpret_cast<const uint4 *>(nd + 12));
+      double k0, k1;
+      if (COUNT) cnt->box[KIND] += 2;
+      const bool p0 = box_test(a0, a1, a2, r, k0);
+      const bool p1 = box_test(b0, b1, b2, r, k1);
+      const unsigned near = meta.z == 0 ? r.sx : (meta.z == 1 ? r.sy : r.sz);
+      const bool pn = near ? p1 : p0, pf = near ? p0 : p1;
+      const double kn = near ? k1 : k0, kf = near ? k0 : k1;
+      const uint32_t rn = near ? meta.y : meta.x, rf = near ? meta.x : meta.y;
+      if (pf) {  // far child pushed first, as the reference does
+        if (sp >= sk.cap) {
+          flag_error(err, kErrStack);
+          return false;
+        }
+        sk.key[sp * sk.stride + tid] = kf;
+        sk.ref[sp * sk.stride + tid] = rf;
+        ++sp;
+      }
+      if (pn && !(kn > st.hit)) {  // the near child is popped next, with the same hit distance
+        cur = rn;
+        continue;
+      }
+    }
+    // pop until an entry passes its deferred hit-distance test
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      if (!(sk.key[sp * sk.stride + tid] > st.hit)) {
+        cur = sk.ref[sp * sk.stride + tid];
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  return st.hit < r.tmax;
+}
+
+struct Best {
+  double t, u, v;
+  D3 n;
+  uint32_t prim, geom;
+  bool hit;
+};
+
+// post_traversal (trimesh.h:133-143, sphere.h:107-114, plane.h:153-159, cylinder.h:154-160)
+template <int KIND>
+BZR_HD void take(const SceneView &S, const Ray &r, const KState &st,
+                                     Best &best) {
+  const KindView &K = S.k[KIND];
+  best.t = st.hit;
+  best.u = st.u;
+  best.v = st.v;
+  best.prim = ldg(K.prim_ids + st.pos) & kIdMask;
+  best.geom = K.geom_id;
+  best.hit = true;
+  if (KIND == kMesh) {
+    const uint32_t *F = S.faces + 3 * size_t(best.prim);
+    const uint32_t f0 = ldg(F), f1 = ldg(F + 1), f2 = ldg(F + 2);
+    const D3 n0 = d3(ldg(S.vert_n + 3 * f0), ldg(S.vert_n + 3 * f0 + 1),
+                     ldg(S.vert_n + 3 * f0 + 2));
+    const D3 n1 = d3(ldg(S.vert_n + 3 * f1), ldg(S.vert_n + 3 * f1 + 1),
+                     ldg(S.vert_n + 3 * f1 + 2));
+    const D3 n2 = d3(ldg(S.vert_n + 3 * f2), ldg(S.vert_n + 3 * f2 + 1),
+                     ldg(S.vert_n + 3 * f2 + 2));
+    const double w = (1.0 - st.u) - st.v;
+    best.n = normalize(add(add(mul(n0, w), mul(n1, st.u)), mul(n2, st.v)));
+  } else if (KIND == kSpheres) {
+    const double *P = K.payload + size_t(st.pos) * kPayloadDoubles[kSpheres];
+    const D3 c = d3(ldg(P), ldg(P + 1), ldg(P + 2));
+    best.n = normalize(sub(add(r.o, mul(r.d, st.hit)), c));
+  } else {
+    best.n = normalize(st.n);
+  }
+}
+
+template <int KIND, bool COUNT>
+BZR_HD void run_kind(const SceneView &S, const Ray &r, const Stack &sk, uint32_t tid,
+                     uint32_t *err, Best &best, Counts *cnt) {
+  const KindView &K = S.k[KIND];
+  if (!K.present || K.n_prims == 0) return;
+  KState st;
+  const bool h = traverse<KIND, COUNT>(K, r, st, sk, tid, err, cnt);
+  if (h && (KIND == kMesh || st.hit < best.t)) take<KIND>(S, r, st, best);
+}
+
+BZR_HD void init_best(Best &best) {
+  best.t = 1.7976931348623157e308;  // RayHit defaults (blazert/ray.h:80-84)
+  best.u = best.v = 0.0;
+  best.n = d3(0.0, 0.0, 0.0);
+  best.prim = best.geom = 0xFFFFFFFFu;
+  best.hit = false;
+}
+
+// intersect1 for one ray (blazert/scene.h:161-210).  cnt is used only when COUNT is true.
+template <bool COUNT = false>
+BZR_HD void trace_ray(const SceneView &S, const Ray &r, const Stack &sk, uint32_t tid,
+                      uint32_t *err, Best &best, Counts *cnt = nullptr) {
+  init_best(best);
+  run_kind<kMesh, COUNT>(S, r, sk, tid, err, best, cnt);
+  run_kind<kSpheres, COUNT>(S, r, sk, tid, err, best, cnt);
+  run_kind<kPlanes, COUNT>(S, r, sk, tid, err, best, cnt);
+  run_kind<kCylinders, COUNT>(S, r, sk, tid, err, best, cnt);
+}
+
+}  // namespace bzr

@@ -1,0 +1,138 @@
+/* blazert_b200 -- B200-native closest-hit ray queries behind blazeRT's Scene API.
+ *
+ * C-ABI of libblazert_b200.so.  Plain pointers and sizes only.  Every function returns an
+ * int status (BZR_OK == 0, negative on error); bzr_last_error_string() describes the last
+ * failure of the calling thread.
+ *
+ * The entry points replace the reference's compile-time Scene interface (paths inside the
+ * reference project):
+ *   bzr_scene_create / _destroy   BlazertScene<T> ctor / dtor       blazert/scene.h:38-73
+ *   bzr_add_mesh                  BlazertScene<T>::add_mesh         blazert/scene.h:227-240
+ *   bzr_add_spheres               BlazertScene<T>::add_spheres      blazert/scene.h:258-271
+ *   bzr_add_planes                BlazertScene<T>::add_planes       blazert/scene.h:293-307
+ *   bzr_add_cylinders             BlazertScene<T>::add_cylinders    blazert/scene.h:331-346
+ *   bzr_commit                    BlazertScene<T>::commit           blazert/scene.h:91-115
+ *                                 with BVHBuildOptions              blazert/bvh/options.h:15-29
+ *   bzr_intersect1                intersect1(scene, ray, rayhit)    blazert/scene.h:161-210
+ *                                 with Ray / RayHit                 blazert/ray.h:56-85
+ *   bzr_intersectN                new: intersect1 over a batch of rays, one GPU launch
+ *   bzr_work_counts, bzr_scene_check, bzr_scene_stats   new: measurement and error reporting
+ *
+ * Semantics kept from the reference:
+ *   - add_* may be called once per primitive kind and only before commit; otherwise the
+ *     returned geom id is UINT32_MAX (the reference's static_cast<unsigned>(-1)) and the status
+ *     is BZR_ESTATE.  Geom ids count up from 0 in add order.
+ *   - intersect1 semantics per ray: per-kind BVHs traversed in the fixed order triangles,
+ *     spheres, planes, cylinders; the first (triangles) is copied when hit, later kinds only
+ *     when strictly closer.  A ray that hits nothing keeps the default RayHit: hit_distance =
+ *     DBL_MAX, uv = normal = 0, prim_id = geom_id = UINT32_MAX, hit = 0.
+ *   - Directions need not be unit length: as in the reference the ray direction is normalized
+ *     and the slab test uses the inverse of the raw direction.
+ * Deliberate difference: add_* COPY the caller's arrays (the reference keeps const& to them), so
+ * the caller may free them after the call.  Results are identical.
+ *
+ * Array layout: vec3 arrays are n x 3 row-major float64; rotation matrices n x 9 row-major
+ * float64 (R[3*i + j] = R(i, j)); faces n x 3 uint32.
+ */
+#ifndef BLAZERT_B200_H_
+#define BLAZERT_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BZR_OK 0
+#define BZR_EINVAL (-1)       /* bad argument (null pointer, size, mode) */
+#define BZR_ESTATE (-2)       /* wrong scene state (add after commit, second add, not committed) */
+#define BZR_ENOMEM (-3)       /* host or device allocation failed */
+#define BZR_ECUDA (-4)        /* a CUDA runtime call failed */
+#define BZR_ETIMEOUT (-5)     /* a bounded wait for the device ran out */
+#define BZR_EDEVICE_FLAG (-6) /* a kernel's own bounds check fired (error word set) */
+#define BZR_ENODEV (-7)       /* no CUDA device */
+
+#define BZR_INVALID_ID 0xFFFFFFFFu
+
+/* Precision of the traversal (the primitive tests and the closest-hit compare are always FP64). */
+#define BZR_MODE_FP64 0  /* slab tests in FP64: bit-exact with the reference */
+#define BZR_MODE_MIXED 1 /* conservative FP32 slab tests, exact FP64 re-test at leaves */
+
+typedef struct bzr_scene bzr_scene;
+
+/* BVHBuildOptions (blazert/bvh/options.h:15-29); defaults 4 / 28 / 64. */
+typedef struct {
+  uint32_t min_leaf_primitives; /* a node with this many primitives or fewer becomes a leaf */
+  uint32_t max_tree_depth;
+  uint32_t bin_size;
+} bzr_build_options;
+
+/* RayHit (blazert/ray.h:72-85). */
+typedef struct {
+  double normal[3];
+  double uv[2];
+  double hit_distance;
+  uint32_t prim_id;
+  uint32_t geom_id;
+} bzr_rayhit;
+
+int bzr_scene_create(bzr_scene **out);
+int bzr_scene_destroy(bzr_scene *scene);
+
+int bzr_add_mesh(bzr_scene *scene, const double *vertices, size_t n_vertices,
+                 const uint32_t *faces, size_t n_faces, uint32_t *geom_id);
+int bzr_add_spheres(bzr_scene *scene, const double *centers, const double *radii, size_t n,
+                    uint32_t *geom_id);
+int bzr_add_planes(bzr_scene *scene, const double *centers, const double *dxs, const double *dys,
+                   const double *rotations, size_t n, uint32_t *geom_id);
+int bzr_add_cylinders(bzr_scene *scene, const double *centers, const double *semi_axes_a,
+                      const double *semi_axes_b, const double *heights, const double *rotations,
+                      size_t n, uint32_t *geom_id);
+
+/* Builds the per-kind binned-SAH BVHs on the host (the reference's tree, node for node),
+ * flattens them into the device layout and uploads them to the current CUDA device.
+ * options may be NULL for the defaults. */
+int bzr_commit(bzr_scene *scene, const bzr_build_options *options);
+
+/* One ray (Ray{origin, direction, tmin, tmax}); *hit receives intersect1's return value. */
+int bzr_intersect1(const bzr_scene *scene, const double origin[3], const double direction[3],
+                   double tmin, double tmax, bzr_rayhit *rayhit, int *hit);
+
+/* A batch of n rays, structure-of-arrays.  Inputs: origins, directions (n x 3); tmin, tmax (n,
+ * or NULL for 0 and DBL_MAX).  Outputs (each may be NULL to skip it): hit_distance (n), uv
+ * (n x 2), normal (n x 3), prim_id, geom_id (n), hit (n, 0/1).
+ * Either ALL given arrays are host memory -- copied to and from the device inside the call,
+ * which returns when the results are in place -- or ALL are device memory of the scene's
+ * device, in which case the work is queued on `stream` (a cudaStream_t, NULL for the default
+ * stream) and the call returns without waiting.  Mixed placement is BZR_EINVAL. */
+int bzr_intersectN(const bzr_scene *scene, size_t n, const double *origins,
+                   const double *directions, const double *tmin, const double *tmax,
+                   double *hit_distance, double *uv, double *normal, uint32_t *prim_id,
+                   uint32_t *geom_id, uint8_t *hit, int mode, void *stream);
+
+/* Work of a batch (no counterpart in the reference; a measurement aid): runs the counting
+ * variant of the FP64 kernel over n rays and returns per kind (0 mesh, 1 spheres, 2 planes,
+ * 3 cylinders) the number of box tests -- the reference's node pops, blazert/bvh/accel.h:94-97
+ * -- in totals[0..3] and of primitive tests (blazert/bvh/intersect.h:71-76) in totals[4..7].
+ * Arrays as for bzr_intersectN; returns when the totals are in place. */
+int bzr_work_counts(const bzr_scene *scene, size_t n, const double *origins,
+                    const double *directions, const double *tmin, const double *tmax,
+                    uint64_t totals[8], void *stream);
+
+/* Waits for the scene's queued work (bounded by timeout_ms; <= 0 waits without bound) and
+ * reports the kernels' error word: BZR_OK, BZR_EDEVICE_FLAG (with *flags receiving the bits)
+ * or BZR_ETIMEOUT. */
+int bzr_scene_check(const bzr_scene *scene, void *stream, int timeout_ms, uint32_t *flags);
+
+/* Statistics of the last commit: per kind (0 mesh, 1 spheres, 2 planes, 3 cylinders) the
+ * number of reference BVH nodes, the maximum depth and the host build time in seconds. */
+int bzr_scene_stats(const bzr_scene *scene, int kind, uint64_t *n_nodes, uint32_t *max_depth,
+                    double *build_seconds);
+
+const char *bzr_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BLAZERT_B200_H_ */

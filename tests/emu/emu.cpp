@@ -1,0 +1,147 @@
+// CPU emulator of the GPU traversal (TEST INFRASTRUCTURE ONLY, never linked into the product).
+//
+// Compiles the kernels' own per-ray code (blazert_b200/csrc/trace_core.cuh) and the product's
+// host builder and flattener (scene.cpp) as host code, so that the tests can check the device
+// layout and the deferred-key traversal against the oracle on machines without a GPU.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../blazert_b200/csrc/layout.h"
+#include "../../blazert_b200/csrc/scene.h"
+#include "../../blazert_b200/csrc/trace_core.cuh"
+
+namespace {
+struct Emu {
+  bzr::HostScene host;
+  std::vector<bzr::KindImage> img;
+  bzr::SceneView view;
+};
+}  // namespace
+
+extern "C" {
+
+void *emu_scene_create(const int *order, int n_order, const double *verts, long n_verts,
+                 const uint32_t *faces, long n_faces, const double *sph_c, const double *sph_r,
+                 long n_sph, const double *pl_c, const double *pl_dx, const double *pl_dy,
+                 const double *pl_rot, long n_pl, const double *cy_c, const double *cy_a,
+                 const double *cy_b, const double *cy_h, const double *cy_rot, long n_cy,
+                 unsigned min_leaf, unsigned max_depth, unsigned bins, uint32_t *geom_ids) {
+  auto *e = new Emu();
+  bzr::HostScene &s = e->host;
+  for (int j = 0; j < n_order; ++j) {
+    const int k = order[j];
+    uint32_t id = 0xFFFFFFFFu;
+    if (k >= 0 && k < 4 && !s.kind[k].present) {
+      switch (k) {
+        case 0: bzr::add_mesh(s, verts, n_verts, faces, n_faces); break;
+        case 1: bzr::add_spheres(s, sph_c, sph_r, n_sph); break;
+        case 2: bzr::add_planes(s, pl_c, pl_dx, pl_dy, pl_rot, n_pl); break;
+        case 3: bzr::add_cylinders(s, cy_c, cy_a, cy_b, cy_h, cy_rot, n_cy); break;
+      }
+      s.kind[k].present = true;
+      id = s.kind[k].geom_id = s.geometries++;
+    }
+    if (geom_ids) geom_ids[j] = id;
+  }
+  s.opt.min_leaf = min_leaf;
+  s.opt.max_depth = max_depth;
+  s.opt.bins = bins;
+  e->img.resize(4);
+  uint32_t depth = 0;
+  for (int k = 0; k < 4; ++k) {
+    bzr::Collection &c = s.kind[k];
+    bzr::KindView &v = e->view.k[k];
+    v.present = c.present;
+    v.geom_id = c.geom_id;
+    if (!c.present) continue;
+    c.tree = bzr::build_tree(c.boxes, s.opt);
+    depth = depth > c.tree.max_depth ? depth : c.tree.max_depth;
+    e->img[k] = bzr::flatten(s, k);
+    const bzr::KindImage &im = e->img[k];
+    v.nodes64 = im.nodes64.data();
+    v.nodes32 = im.nodes32.data();
+    v.payload = im.payload.data();
+    v.prim_ids = im.prim_ids.data();
+    v.n_internal = im.n_internal;
+    v.n_prims = static_cast<uint32_t>(im.prim_ids.size());
+    v.root_ref = im.root_ref;
+    v.mixed_ok = im.mixed_ok;
+    std::memcpy(v.root_box, im.root_box, sizeof v.root_box);
+    std::memcpy(v.root_box32, im.root_box32, sizeof v.root_box32);
+  }
+  e->view.faces = s.faces.data();
+  e->view.vert_n = s.vert_n.data();
+  e->view.stack_cap = (depth + 2) < 8 ? 8 : depth + 2;
+  return e;
+}
+
+void emu_scene_destroy(void *h) { delete static_cast<Emu *>(h); }
+
+// Same dump layout as the oracle's ora_scene_tree.
+long emu_scene_tree(void *h, int kind, double *bmin, double *bmax, uint32_t *leaf, uint32_t *axis,
+              uint32_t *children, uint32_t *prim_off, uint32_t *prim_cnt, uint32_t *prim_ids,
+              long prim_cap) {
+  const Emu *e = static_cast<Emu *>(h);
+  if (kind < 0 || kind > 3 || !e->host.kind[kind].present) return -1;
+  const bzr::Tree &t = e->host.kind[kind].tree;
+  const long n = static_cast<long>(t.nodes.size());
+  if (!bmin) return n;
+  uint32_t running = 0;
+  for (long i = 0; i < n; ++i) {
+    const bzr::TreeNode &nd = t.nodes[i];
+    std::memcpy(bmin + 3 * i, nd.mn, 24);
+    std::memcpy(bmax + 3 * i, nd.mx, 24);
+    leaf[i] = nd.leaf;
+    axis[i] = nd.axis;
+    children[2 * i] = nd.child[0];
+    children[2 * i + 1] = nd.child[1];
+    prim_off[i] = running;
+    prim_cnt[i] = nd.leaf == 1 ? nd.prim_cnt : 0;
+    running += prim_cnt[i];
+  }
+  for (long i = 0; i < static_cast<long>(t.leaf_prims.size()) && i < prim_cap; ++i)
+    prim_ids[i] = t.leaf_prims[i];
+  return n;
+}
+
+// Runs the kernel's per-ray code; returns the accumulated error word.
+uint32_t emu_scene_intersect(void *h, long n, const double *org, const double *dir, const double *tmin,
+                       const double *tmax, double *t, double *uv, double *normal, uint32_t *prim,
+                       uint32_t *geom, uint8_t *hit, uint32_t stack_cap_override) {
+  const Emu *e = static_cast<Emu *>(h);
+  bzr::SceneView view = e->view;
+  if (stack_cap_override) view.stack_cap = stack_cap_override;
+  uint32_t err = 0;
+#pragma omp parallel reduction(| : err)
+  {
+    std::vector<double> key(view.stack_cap);
+    std::vector<uint32_t> ref(view.stack_cap);
+    bzr::Stack sk;
+    sk.key = key.data();
+    sk.ref = ref.data();
+    sk.cap = view.stack_cap;
+    sk.stride = 1;
+#pragma omp for schedule(dynamic, 256)
+    for (long i = 0; i < n; ++i) {
+      const bzr::Ray r = bzr::make_ray(org + 3 * i, dir + 3 * i, tmin ? tmin[i] : 0.0,
+                                       tmax ? tmax[i] : 1.7976931348623157e308);
+      bzr::Best best;
+      uint32_t my_err = 0;
+      bzr::trace_ray(view, r, sk, 0, &my_err, best);
+      err |= my_err;
+      t[i] = best.t;
+      uv[2 * i] = best.u;
+      uv[2 * i + 1] = best.v;
+      normal[3 * i] = best.n.x;
+      normal[3 * i + 1] = best.n.y;
+      normal[3 * i + 2] = best.n.z;
+      prim[i] = best.prim;
+      geom[i] = best.geom;
+      hit[i] = best.hit ? 1 : 0;
+    }
+  }
+  return err;
+}
+
+}  // extern "C"

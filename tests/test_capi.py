@@ -1,0 +1,68 @@
+"""The C-ABI library: it loads, exports every function include/blazert_b200.h declares, and keeps
+the reference's add/commit state rules (blazert/scene.h:227-346) without touching a GPU."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import blazert_b200 as B
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", fn)).read()
+            text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+            names += re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(bzr_[A-Za-z0-9_]+)\s*\(", text, re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = B.library()
+    names = declared_functions()
+    assert "bzr_intersectN" in names and "bzr_commit" in names
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_add_rules_without_gpu():
+    s = B.Scene()
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float64)
+    f = np.array([[0, 1, 2]], np.uint32)
+    assert s.add_mesh(v, f) == 0
+    assert s.add_mesh(v, f) == B.INVALID_ID  # second add of a kind
+    assert s.add_spheres(np.zeros((1, 3)), np.ones(1)) == 1
+    assert s.add_cylinders(np.zeros((1, 3)), np.ones(1), np.ones(1), np.ones(1), np.eye(3)[None]) == 2
+    assert s.add_planes(np.zeros((1, 3)), np.ones(1), np.ones(1), np.eye(3)[None]) == 3
+    s.close()
+
+
+def test_errors_are_reported():
+    s = B.Scene()
+    with pytest.raises(B.BlazertError) as e:
+        s.add_mesh(np.zeros((3, 3)), np.array([[0, 1, 5]], np.uint32))  # index out of range
+    assert e.value.code == B.EINVAL
+    with pytest.raises(B.BlazertError) as e:  # query before commit
+        s.intersectN(np.zeros((1, 3)), np.ones((1, 3)))
+    assert e.value.code == B.ESTATE
+    lib = B.library()
+    assert lib.bzr_add_spheres(None, None, None, 0, None) == B.EINVAL
+    s.close()
+
+
+def test_commit_without_device_fails_loudly():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    s = B.Scene()
+    s.add_spheres(np.zeros((1, 3)), np.ones(1))
+    with pytest.raises(B.BlazertError) as e:
+        s.commit()
+    assert e.value.code == B.ENODEV
+    s.close()

@@ -1,0 +1,50 @@
+"""The GPU kernels' per-ray code (blazert_b200/csrc/trace_core.cuh), compiled as host code by
+the test-only emulator, against the CPU oracle: checks the device layout, the deferred-key
+traversal and the primitive tests without a GPU."""
+import numpy as np
+import pytest
+
+from blazert_b200 import workloads as W
+from oracle.oracle import Oracle
+from tests.emu.emu import EmuScene
+from tests.helpers import mismatches
+from tests.scenes import edge_case_scenes
+
+
+@pytest.mark.parametrize("name", ["icosphere_pinhole", "mixed_primitives"])
+def test_workloads(name):
+    wl = W.WORKLOADS[name]() if name != "mixed_primitives" else W.mixed_primitives(n_rays=100_000)
+    R = wl.rays
+    ref = Oracle(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax)
+    got = EmuScene(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax)
+    assert got["error_word"] == 0
+    assert mismatches(got, ref) == []
+
+
+@pytest.mark.parametrize("case", edge_case_scenes(), ids=lambda c: c[0])
+def test_edge_cases(case):
+    _, spec, R = case
+    ref = Oracle(spec).intersect(R.origins, R.directions, R.tmin, R.tmax)
+    got = EmuScene(spec).intersect(R.origins, R.directions, R.tmin, R.tmax)
+    assert got["error_word"] == 0
+    assert mismatches(got, ref) == []
+
+
+def test_build_options():
+    wl = W.mixed_primitives(n_rays=20_000, n_spheres=3000, n_cylinders=300, n_planes=50, seed=9)
+    R = wl.rays
+    for opts in (dict(min_leaf=1, max_depth=28, bins=64), dict(min_leaf=8, max_depth=6, bins=16),
+                 dict(min_leaf=2, max_depth=40, bins=3)):
+        ref = Oracle(wl.scene, **opts).intersect(R.origins, R.directions)
+        got = EmuScene(wl.scene, **opts).intersect(R.origins, R.directions)
+        assert got["error_word"] == 0
+        assert mismatches(got, ref) == [], opts
+
+
+def test_stack_overflow_is_flagged_not_silent():
+    """A stack too small for the tree sets the error word and the ray stops; it never writes
+    outside the stack (the GPU kernels run the same code)."""
+    wl = W.icosphere_pinhole(level=4, width=64, height=64)
+    R = wl.rays
+    got = EmuScene(wl.scene).intersect(R.origins, R.directions, stack_cap=1)
+    assert got["error_word"] & 1
