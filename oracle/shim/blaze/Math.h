@@ -22,7 +22,8 @@
 //   trans(M)                           transpose (exact)
 //   abs/min/max(a[, b])                element-wise std:: functions
 //
-// Like blaze's own Math.h, it makes <cstdint>, <memory> and <limits> available to its includers.
+// Like blaze's own Math.h, it makes <cstdint>, <complex>, <memory> and <limits> available to its
+// includers.
 //
 // Builds that must be bit-comparable with the CUDA path compile with -ffp-contract=off.
 #pragma once
@@ -31,6 +32,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstddef>
 #include <cstdint>
 #include <cstdlib>

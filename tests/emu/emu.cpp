@@ -144,4 +144,26 @@ uint32_t emu_scene_intersect(void *h, long n, const double *org, const double *d
   return err;
 }
 
+// Precomputed box and centre of one primitive (the product's collection precompute).
+int emu_prim_box(void *h, int kind, uint32_t id, double *mn, double *mx, double *center) {
+  const Emu *e = static_cast<Emu *>(h);
+  if (kind < 0 || kind > 3 || !e->host.kind[kind].present || id >= e->host.kind[kind].n) return -1;
+  const bzr::PrimBoxes &b = e->host.kind[kind].boxes;
+  std::memcpy(mn, &b.bmin[3 * size_t(id)], 24);
+  std::memcpy(mx, &b.bmax[3 * size_t(id)], 24);
+  std::memcpy(center, &b.center[3 * size_t(id)], 24);
+  return 0;
+}
+
+// The kernels' slab test of one box, decided for the hit distance `tmax` as at pop time:
+// returns 1 when the reference's intersect_node(tmin, tmax, box, ray) would accept the box.
+int emu_box_accept(const double *bmin, const double *bmax, const double *org, const double *dir,
+                   double tmin, double tmax) {
+  const bzr::Ray r = bzr::make_ray(org, dir, tmin, tmax);
+  double key;
+  const bool p = bzr::box_test(make_double2(bmin[0], bmax[0]), make_double2(bmin[1], bmax[1]),
+                               make_double2(bmin[2], bmax[2]), r, key);
+  return (p && !(key > tmax)) ? 1 : 0;
+}
+
 }  // extern "C"

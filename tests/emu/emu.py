@@ -3,6 +3,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import subprocess
 
 import numpy as np
 
@@ -10,11 +11,12 @@ from oracle.oracle import _Base, _CREATE_ARGS, _TREE_ARGS, _dp, _outputs, _ptr, 
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libbzr_emu.so")
+KINDS = ("mesh", "spheres", "planes", "cylinders")
+_lib = None
 
 
 def build(force=False):
     """Compiles the emulator with the host compiler (no GPU or nvcc needed)."""
-    import subprocess
     root = os.path.dirname(os.path.dirname(HERE))
     srcs = [os.path.join(HERE, "emu.cpp"), os.path.join(root, "blazert_b200", "csrc", "scene.cpp")]
     deps = srcs + [os.path.join(root, "blazert_b200", "csrc", f)
@@ -27,23 +29,44 @@ def build(force=False):
     return LIB
 
 
+def load():
+    global _lib
+    if _lib is None:
+        lib = C.CDLL(build())
+        lib.emu_scene_create.restype = C.c_void_p
+        lib.emu_scene_create.argtypes = _CREATE_ARGS
+        lib.emu_scene_destroy.argtypes = [C.c_void_p]
+        lib.emu_scene_tree.restype = C.c_long
+        lib.emu_scene_tree.argtypes = _TREE_ARGS
+        lib.emu_scene_intersect.restype = C.c_uint32
+        lib.emu_scene_intersect.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _dp, _dp, _dp, _dp,
+                                            _dp, _u32p, _u32p, _u8p, C.c_uint32]
+        lib.emu_prim_box.argtypes = [C.c_void_p, C.c_int, C.c_uint32, _dp, _dp, _dp]
+        lib.emu_box_accept.argtypes = [_dp, _dp, _dp, _dp, C.c_double, C.c_double]
+        _lib = lib
+    return _lib
+
+
+def box_accept(bmin, bmax, org, direction, tmin, tmax):
+    """Decision of the kernels' deferred slab test for one box at hit distance tmax."""
+    f = lambda a: np.ascontiguousarray(a, np.float64)
+    return bool(load().emu_box_accept(_ptr(f(bmin), _dp), _ptr(f(bmax), _dp), _ptr(f(org), _dp),
+                                      _ptr(f(direction), _dp), float(tmin), float(tmax)))
+
+
 class EmuScene(_Base):
     _prefix = "emu_"
-    _lib = None
 
     def __init__(self, spec, **kw):
-        if EmuScene._lib is None:
-            lib = C.CDLL(build())
-            lib.emu_scene_create.restype = C.c_void_p
-            lib.emu_scene_create.argtypes = _CREATE_ARGS
-            lib.emu_scene_destroy.argtypes = [C.c_void_p]
-            lib.emu_scene_tree.restype = C.c_long
-            lib.emu_scene_tree.argtypes = _TREE_ARGS
-            lib.emu_scene_intersect.restype = C.c_uint32
-            lib.emu_scene_intersect.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
-                                          _u32p, _u32p, _u8p, C.c_uint32]
-            EmuScene._lib = lib
+        self._lib = load()
         super().__init__(spec, **kw)
+
+    def prim_box(self, kind, prim_id):
+        mn, mx, c = np.zeros(3), np.zeros(3), np.zeros(3)
+        rc = self._lib.emu_prim_box(self._h, KINDS.index(kind), prim_id, _ptr(mn, _dp),
+                                    _ptr(mx, _dp), _ptr(c, _dp))
+        assert rc == 0
+        return mn, mx, c
 
     def intersect(self, org, dirs, tmin=None, tmax=None, stack_cap=0):
         org, dirs, tmin, tmax, n = _rays(org, dirs, tmin, tmax)

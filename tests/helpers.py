@@ -38,3 +38,96 @@ def mismatches(got, ref):
         if not np.array_equal(a, b):
             bad.append(f"{k}: {int(np.count_nonzero((a != b).reshape(len(a), -1).any(1)))} rays")
     return bad
+
+
+# ----------------------------------------------------------------------------- golden fixtures
+import json as _json
+import os as _os
+
+GOLDEN = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "golden")
+
+
+def load_kats():
+    with open(_os.path.join(GOLDEN, "kats.json")) as f:
+        return _json.load(f)
+
+
+def kat_spec(rec):
+    """SceneSpec of a captured KAT record (one collection, or the stored scene)."""
+    from blazert_b200 import workloads as W
+
+    if rec["check"] == "scene":
+        s = W.SceneSpec()
+        for kind in rec["scene"]["order"]:
+            getattr(s, "add_" + kind)(*[np.asarray(v) for v in rec["scene"][kind].values()])
+        return s
+    k = rec["kind"]
+    s = W.SceneSpec()
+    if k == "mesh":
+        s.add_mesh(np.array(rec["vertices"], float).reshape(-1, 3),
+                   np.array(rec["faces"], np.uint32).reshape(-1, 3))
+    elif k == "spheres":
+        s.add_spheres(np.array(rec["centers"], float), np.array(rec["radii"], float))
+    elif k == "planes":
+        s.add_planes(np.array(rec["centers"], float), np.array(rec["dxs"], float),
+                     np.array(rec["dys"], float), np.array(rec["rotations"], float).reshape(-1, 3, 3))
+    else:
+        s.add_cylinders(np.array(rec["centers"], float), np.array(rec["semi_axes_a"], float),
+                        np.array(rec["semi_axes_b"], float), np.array(rec["heights"], float),
+                        np.array(rec["rotations"], float).reshape(-1, 3, 3))
+    return s
+
+
+def bits_equal(a, b):
+    return np.array_equal(np.asarray(a, np.float64).view(np.uint64), np.asarray(b, np.float64).view(np.uint64))
+
+
+def same_result(got, want, i=0):
+    """got: batched outputs (numpy or torch); want: a fixture result dict."""
+    got = to_numpy(got)
+    return (bool(got["hit"][i]) == want["hit"]
+            and int(got["prim"].view(np.uint32)[i]) == want["prim_id"]
+            and int(got["geom"].view(np.uint32)[i]) == want.get("geom_id", int(got["geom"].view(np.uint32)[i]))
+            and bits_equal(got["t"][i], want["distance"])
+            and bits_equal(got["uv"][i], want["uv"])
+            and bits_equal(got["normal"][i], want["normal"]))
+
+
+def approx(x, v, eps=float(np.finfo(np.float32).eps) * 100, scale=1.0):
+    """doctest::Approx, the tolerance of the reference's own tests."""
+    return abs(x - v) < eps * (scale + max(abs(x), abs(v)))
+
+
+def scene_primitives_workload():
+    """examples/scene_primitives/main.cc:32-115: two cylinders (added first) and two spheres,
+    1080 x 720 rays from (0, 5, 20) with directions (x/1080 - 0.5, y/720 - 0.5, -1)."""
+    from blazert_b200 import workloads as W
+
+    rot = np.array([[[0, 0, 1], [0, 1, 0], [-1, 0, 0]]], float).repeat(2, 0)
+    s = W.SceneSpec()
+    s.add_cylinders(np.array([[-3, 3, 0], [1, 4, 0]], float), np.array([1, 0.5]), np.array([1, 0.5]),
+                    np.array([1, 2.0]), rot)
+    s.add_spheres(np.array([[1, 1, 0], [-2, 10, 0]], float), np.array([0.5, 1.5]))
+    w, h = 1080, 720
+    y, x = np.meshgrid(np.arange(h, dtype=float), np.arange(w, dtype=float), indexing="ij")
+    d = np.stack([x.ravel() / float(w) - 0.5, y.ravel() / float(h) - 0.5, -np.ones(w * h)], 1)
+    o = np.broadcast_to([0.0, 5.0, 20.0], d.shape).copy()
+    return s, W.RayBatch(o, d), (w, h)
+
+
+def image_classes(out, w, h):
+    """Pixel classes as the example writes them: row (h - y - 1); 1 red (prim 0), 2 green."""
+    out = to_numpy(out)
+    hit = out["hit"].reshape(h, w).astype(bool)
+    prim0 = out["prim"].view(np.uint32).reshape(h, w) == 0
+    cls = np.where(hit, np.where(prim0, 1, 2), 0)
+    return cls[::-1]
+
+
+def golden_image_classes():
+    g = np.load(_os.path.join(GOLDEN, "scene_primitives_classes.npz"))
+    hh, ww = g["shape"]
+    n = hh * ww
+    red = np.unpackbits(g["red"])[:n].reshape(hh, ww).astype(bool)
+    green = np.unpackbits(g["green"])[:n].reshape(hh, ww).astype(bool)
+    return np.where(red, 1, np.where(green, 2, 0))
