@@ -263,6 +263,8 @@ def run_ours(args):
         total_ms = float(t.item())
     value = world * n * args.steps / (total_ms / 1e3) / 1e6
     hits = float(out["hit"].float().mean().item())
+    # one traversal kernel per primitive kind present, per step
+    n_passes = sum(1 for k in wl.scene.order if len(next(iter(getattr(wl.scene, k).values()))))
 
     # roofline: algorithmic bytes from the kernel's own work counts (untimed counting run)
     counts = scene.work_counts(o, d, tmn, tmx, stream=stream)
@@ -316,7 +318,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)", "config": config_of(args, wl, world),
-            "e2e": e2e, "gpu_launches": args.steps,
+            "e2e": e2e, "gpu_launches": args.steps * n_passes,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_src,

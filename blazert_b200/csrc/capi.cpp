@@ -30,7 +30,15 @@ int cuda_fail(cudaError_t e, const char *what) {
   return fail(BZR_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-constexpr int kSlots = 256;  // work-counter slots, one per call in flight
+// Per-call device words: kSlots slots of kSlotWords = {work counter per kind pass (4), error
+// word, 3 spare}; one sticky error word for device-array calls follows the slots.
+constexpr int kSlots = 256;
+constexpr int kSlotWords = 8;
+constexpr int kStickyWord = kSlots * kSlotWords;
+// Host-array batches: split into at most kMaxChunks chunks of at least kMinChunk rays.
+constexpr int kStreams = 3;
+constexpr size_t kMaxChunks = 8;
+constexpr size_t kMinChunk = size_t(1) << 17;
 
 int default_timeout_ms() {
   const char *s = std::getenv("BZR_TIMEOUT_MS");
@@ -61,27 +69,29 @@ struct bzr_scene {
   int device = -1;
   void *arena = nullptr;  // every device array of the committed scene
   bzr::SceneView view;
-  int blocks = 0;
-  uint32_t *slots = nullptr;  // kSlots x {work counter, error word}, then one sticky word
+  bzr::LaunchPlan plan;
+  uint32_t *slots = nullptr;  // see kSlots
   std::atomic<uint32_t> next_slot{0};
   // host-pointer calls: staging buffers (grown on demand) and a private stream
   std::mutex stage_mu;
   void *stage_dev = nullptr;
   size_t stage_bytes = 0;
-  uint32_t *pinned_err = nullptr;
-  cudaStream_t stream = nullptr;
+  uint32_t *pinned_err = nullptr;  // one error word per chunk
+  cudaStream_t streams[kStreams] = {nullptr, nullptr, nullptr};
 
   ~bzr_scene() {
     if (device >= 0) {
       int cur = 0;
       cudaGetDevice(&cur);
       cudaSetDevice(device);
-      if (stream) cudaStreamSynchronize(stream);
+      for (cudaStream_t st : streams)
+        if (st) cudaStreamSynchronize(st);
       cudaFree(arena);
       cudaFree(slots);
       cudaFree(stage_dev);
       cudaFreeHost(pinned_err);
-      if (stream) cudaStreamDestroy(stream);
+      for (cudaStream_t st : streams)
+        if (st) cudaStreamDestroy(st);
       cudaSetDevice(cur);
     }
   }
@@ -253,15 +263,17 @@ int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
   s->view.faces = reinterpret_cast<const uint32_t *>(base + off_faces);
   s->view.vert_n = reinterpret_cast<const double *>(base + off_vn);
   s->view.stack_cap = std::max<uint32_t>(8, depth + 2);
-  e = cudaMalloc(&s->slots, (2 * kSlots + 1) * sizeof(uint32_t));
+  e = cudaMalloc(&s->slots, (kStickyWord + 1) * sizeof(uint32_t));
   if (e != cudaSuccess) return fail(BZR_ENOMEM, "slot allocation failed");
-  e = cudaMemset(s->slots, 0, (2 * kSlots + 1) * sizeof(uint32_t));
+  e = cudaMemset(s->slots, 0, (kStickyWord + 1) * sizeof(uint32_t));
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemset");
-  e = cudaMallocHost(&s->pinned_err, sizeof(uint32_t));
+  e = cudaMallocHost(&s->pinned_err, kMaxChunks * sizeof(uint32_t));
   if (e != cudaSuccess) return fail(BZR_ENOMEM, "pinned allocation failed");
-  e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
-  e = bzr::trace_grid(s->view.stack_cap, &s->blocks);
+  for (cudaStream_t &st : s->streams) {
+    e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+  }
+  e = bzr::trace_prepare(s->view, &s->plan);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   s->host.committed = true;
   return BZR_OK;
@@ -306,19 +318,22 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
       n_dev += is_device_ptr(p) ? 1 : 0;
     }
   const uint32_t slot = s->next_slot.fetch_add(1) % kSlots;
-  uint32_t *counter = s->slots + 2 * slot;
+  uint32_t *counters = s->slots + kSlotWords * slot;
   bzr::RayIO io;
   io.n = static_cast<uint32_t>(n);
-  io.work_counter = counter;
 
   if (n_dev == n_given) {  // device arrays: queue on the caller's stream and return
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     io.org = org; io.dir = dir; io.tmin = tmin; io.tmax = tmax;
     io.t = t; io.uv = uv; io.normal = normal; io.prim = prim; io.geom = geom; io.hit = hit;
-    io.error_word = s->slots + 2 * kSlots;  // sticky, read by bzr_scene_check
-    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), st);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-    e = bzr::launch_trace(s->view, io, mode, s->blocks, st, totals);
+    io.error_word = s->slots + kStickyWord;  // sticky, read by bzr_scene_check
+    cudaError_t e = cudaSuccess;
+    if (!t) {  // the passes carry the closest distance in t: stream-ordered scratch
+      e = cudaMallocAsync(reinterpret_cast<void **>(&io.t), 8 * n, st);
+      if (e != cudaSuccess) return fail(BZR_ENOMEM, "distance scratch allocation failed");
+    }
+    e = bzr::launch_trace(s->view, io, mode, s->plan, st, counters, totals);
+    if (!t) cudaFreeAsync(io.t, st);
     return e == cudaSuccess ? BZR_OK : cuda_fail(e, "kernel launch");
   }
   if (n_dev != 0) return fail(BZR_EINVAL, "arrays must be all host or all device memory");
@@ -327,7 +342,7 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
   std::lock_guard<std::mutex> lock(s->stage_mu);
   // every staged array starts on a 256-byte boundary (see take() below)
   const size_t piece_bytes[10] = {24 * n, 24 * n, tmin ? 8 * n : 0, tmax ? 8 * n : 0,
-                                  t ? 8 * n : 0, uv ? 16 * n : 0, normal ? 24 * n : 0,
+                                  8 * n, uv ? 16 * n : 0, normal ? 24 * n : 0,
                                   prim ? 4 * n : 0, geom ? 4 * n : 0, hit ? n : 0};
   size_t need = 0;
   for (size_t b : piece_bytes)
@@ -347,45 +362,69 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
     off = align_up(off + bytes, 256);
     return q;
   };
-  cudaStream_t st = s->stream;
+  double *d_org = reinterpret_cast<double *>(take(24 * n));
+  double *d_dir = reinterpret_cast<double *>(take(24 * n));
+  double *d_tmin = tmin ? reinterpret_cast<double *>(take(8 * n)) : nullptr;
+  double *d_tmax = tmax ? reinterpret_cast<double *>(take(8 * n)) : nullptr;
+  double *d_t = reinterpret_cast<double *>(take(8 * n));  // always: the passes carry the distance
+  double *d_uv = uv ? reinterpret_cast<double *>(take(16 * n)) : nullptr;
+  double *d_normal = normal ? reinterpret_cast<double *>(take(24 * n)) : nullptr;
+  uint32_t *d_prim = prim ? reinterpret_cast<uint32_t *>(take(4 * n)) : nullptr;
+  uint32_t *d_geom = geom ? reinterpret_cast<uint32_t *>(take(4 * n)) : nullptr;
+  uint8_t *d_hit = hit ? reinterpret_cast<uint8_t *>(take(n)) : nullptr;
+  // Chunks round-robin over the scene's streams, so that the copies in of one chunk, the
+  // kernels of another and the copies out of a third overlap.
+  const size_t chunk = n <= kMinChunk ? n : std::max(kMinChunk, (n + kMaxChunks - 1) / kMaxChunks);
+  const size_t nchunks = (n + chunk - 1) / chunk;
   cudaError_t e = cudaSuccess;
-  auto h2d = [&](const void *src, size_t bytes) -> void * {
-    if (!src) return nullptr;
-    void *d = take(bytes);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, st);
-    return d;
-  };
-  io.org = static_cast<const double *>(h2d(org, 24 * n));
-  io.dir = static_cast<const double *>(h2d(dir, 24 * n));
-  io.tmin = static_cast<const double *>(h2d(tmin, 8 * n));
-  io.tmax = static_cast<const double *>(h2d(tmax, 8 * n));
-  io.t = t ? reinterpret_cast<double *>(take(8 * n)) : nullptr;
-  io.uv = uv ? reinterpret_cast<double *>(take(16 * n)) : nullptr;
-  io.normal = normal ? reinterpret_cast<double *>(take(24 * n)) : nullptr;
-  io.prim = prim ? reinterpret_cast<uint32_t *>(take(4 * n)) : nullptr;
-  io.geom = geom ? reinterpret_cast<uint32_t *>(take(4 * n)) : nullptr;
-  io.hit = hit ? reinterpret_cast<uint8_t *>(take(n)) : nullptr;
-  io.error_word = counter + 1;
-  if (e == cudaSuccess) e = cudaMemsetAsync(counter, 0, 2 * sizeof(uint32_t), st);
-  if (e != cudaSuccess) return cuda_fail(e, "staging copies");
-  e = bzr::launch_trace(s->view, io, mode, s->blocks, st, totals);
-  if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-  auto d2h = [&](void *dst, const void *src, size_t bytes) {
-    if (dst && e == cudaSuccess) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
-  };
-  d2h(t, io.t, 8 * n);
-  d2h(uv, io.uv, 16 * n);
-  d2h(normal, io.normal, 24 * n);
-  d2h(prim, io.prim, 4 * n);
-  d2h(geom, io.geom, 4 * n);
-  d2h(hit, io.hit, n);
-  d2h(s->pinned_err, io.error_word, sizeof(uint32_t));
-  if (e != cudaSuccess) return cuda_fail(e, "result copies");
-  const int rc = wait_stream(st, default_timeout_ms());
-  if (rc) return rc;
-  if (*s->pinned_err)
+  for (size_t c = 0; c < nchunks && e == cudaSuccess; ++c) {
+    const size_t a = c * chunk, m = std::min(n, a + chunk) - a;
+    cudaStream_t st = s->streams[c % kStreams];
+    uint32_t *cnt = c == 0 ? counters : s->slots + kSlotWords * (s->next_slot.fetch_add(1) % kSlots);
+    auto h2d = [&](double *dst, const double *src, size_t per) {
+      if (src && e == cudaSuccess)
+        e = cudaMemcpyAsync(dst + per * a, src + per * a, 8 * per * m, cudaMemcpyHostToDevice, st);
+    };
+    h2d(d_org, org, 3);
+    h2d(d_dir, dir, 3);
+    h2d(d_tmin, tmin, 1);
+    h2d(d_tmax, tmax, 1);
+    bzr::RayIO ci;
+    ci.n = static_cast<uint32_t>(m);
+    ci.org = d_org + 3 * a;
+    ci.dir = d_dir + 3 * a;
+    ci.tmin = d_tmin ? d_tmin + a : nullptr;
+    ci.tmax = d_tmax ? d_tmax + a : nullptr;
+    ci.t = d_t + a;
+    ci.uv = d_uv ? d_uv + 2 * a : nullptr;
+    ci.normal = d_normal ? d_normal + 3 * a : nullptr;
+    ci.prim = d_prim ? d_prim + a : nullptr;
+    ci.geom = d_geom ? d_geom + a : nullptr;
+    ci.hit = d_hit ? d_hit + a : nullptr;
+    ci.error_word = cnt + bzr::kNumKinds;
+    if (e == cudaSuccess) e = cudaMemsetAsync(ci.error_word, 0, sizeof(uint32_t), st);
+    if (e == cudaSuccess) e = bzr::launch_trace(s->view, ci, mode, s->plan, st, cnt, totals);
+    auto d2h = [&](void *dst, const void *src, size_t bytes) {
+      if (dst && e == cudaSuccess) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+    };
+    d2h(t ? t + a : nullptr, ci.t, 8 * m);
+    d2h(uv ? uv + 2 * a : nullptr, ci.uv, 16 * m);
+    d2h(normal ? normal + 3 * a : nullptr, ci.normal, 24 * m);
+    d2h(prim ? prim + a : nullptr, ci.prim, 4 * m);
+    d2h(geom ? geom + a : nullptr, ci.geom, 4 * m);
+    d2h(hit ? hit + a : nullptr, ci.hit, m);
+    d2h(s->pinned_err + c, ci.error_word, sizeof(uint32_t));
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "batch submission");
+  for (int k = 0; k < kStreams; ++k) {
+    const int rc = wait_stream(s->streams[k], default_timeout_ms());
+    if (rc) return rc;
+  }
+  uint32_t bits = 0;
+  for (size_t c = 0; c < nchunks; ++c) bits |= s->pinned_err[c];
+  if (bits)
     return fail(BZR_EDEVICE_FLAG, "kernel bounds check fired (error bits " +
-                                      std::to_string(*s->pinned_err) + ")");
+                                      std::to_string(bits) + ")");
   return BZR_OK;
 }
 
@@ -420,8 +459,9 @@ int bzr_work_counts(const bzr_scene *cs, size_t n, const double *org, const doub
     rc = run_batch(s, n, org, dir, tmin, tmax, nullptr, nullptr, nullptr, nullptr, nullptr,
                    nullptr, BZR_MODE_FP64, stream, dev);
   cudaSetDevice(s->device);
-  // the host path ran on the scene's stream; make the counter copy wait for both
-  if (rc == BZR_OK) rc = wait_stream(s->stream, default_timeout_ms());
+  // the host path ran on the scene's streams; make the counter copy wait for all of them
+  for (cudaStream_t q : s->streams)
+    if (rc == BZR_OK) rc = wait_stream(q, default_timeout_ms());
   if (rc == BZR_OK) rc = wait_stream(st, default_timeout_ms());
   if (rc == BZR_OK) {
     unsigned long long h[8];
@@ -458,7 +498,7 @@ int bzr_scene_check(const bzr_scene *s, void *stream, int timeout_ms, uint32_t *
   uint32_t word = 0;
   if (rc == BZR_OK) {
     const cudaError_t e =
-        cudaMemcpy(&word, s->slots + 2 * kSlots, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        cudaMemcpy(&word, s->slots + kStickyWord, sizeof(uint32_t), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) rc = cuda_fail(e, "error word read");
   }
   cudaSetDevice(cur);

@@ -1,8 +1,16 @@
 // Closest-hit traversal kernels for sm_100a.
 //
-// One thread per ray, persistent warps that fetch 32 rays at a time from a global counter.
-// Per ray the per-kind BVHs are traversed in the reference's fixed order (triangles, spheres,
-// planes, cylinders; blazert/scene.h:161-210) and merged with its strict "<".
+// A batch runs as one persistent kernel per primitive kind present, in the reference's fixed
+// order (triangles, spheres, planes, cylinders; blazert/scene.h:161-210).  Each pass merges its
+// hits into the output record with the reference's rule (finalize_kind), so the result equals
+// intersect1's.  Splitting by kind keeps each kernel small (registers, instruction cache) and
+// keeps one kind's nodes and primitives hot in L1/L2 at a time.
+//
+// Work distribution: each warp owns a pool of ray indices taken from a global counter in
+// chunks of kChunk (one atomic per chunk).  A lane whose ray finishes takes the next index of
+// its warp's pool at once, so lanes do not idle until the slowest ray of a fixed group of 32
+// is done.  Within a ray the traversal alternates "walk internal nodes to the next leaf" and
+// "test the leaf's primitives", so the lanes of a warp run their leaf tests together.
 //
 // Exactness.  The kernels reproduce the reference's visit order and arithmetic bit for bit:
 //  * compiled with --fmad=false; every expression keeps the reference's evaluation order;
@@ -29,57 +37,125 @@
 namespace bzr {
 namespace {
 
-// COUNT = true: also sums the work counters of all rays into totals[8] (box tests per kind,
-// then primitive tests per kind); used to derive the algorithmic bytes of a workload.
-template <bool COUNT>
+constexpr uint32_t kChunk = 64;  // rays taken from the global counter per warp fetch
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// One kind over the whole batch.  first: this pass writes the whole output record.
+// COUNT: also sums the work counters into totals[8] (box tests per kind, then primitive
+// tests per kind).
+template <int KIND, bool COUNT>
 __global__ void __launch_bounds__(kTraceThreads)
-    trace_fp64_kernel(SceneView S, RayIO io, unsigned long long *totals) {
+    trace_kind_kernel(SceneView S, RayIO io, int first, uint32_t *work_counter,
+                      unsigned long long *totals) {
   extern __shared__ __align__(16) unsigned char smem[];
   Stack sk;
   sk.stride = blockDim.x;
   sk.cap = S.stack_cap;
   sk.key = reinterpret_cast<double *>(smem);
   sk.ref = reinterpret_cast<uint32_t *>(sk.key + size_t(sk.cap) * sk.stride);
+  const KindView &K = S.k[KIND];
   const unsigned lane = threadIdx.x & 31u;
+  const unsigned below = (1u << lane) - 1u;
+  const uint32_t tid = threadIdx.x;
+  uint32_t pool_next = 0, pool_end = 0;  // warp-uniform
+  bool exhausted = false;                // warp-uniform
+  bool active = false;
+  uint32_t i = 0;
+  Ray r;
+  KState st;
+  Trav tv;
   Counts cnt = {};
   for (;;) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(io.work_counter, 32u);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base >= io.n) break;
-    const uint64_t i = uint64_t(base) + lane;
-    if (i >= io.n) continue;
-    const Ray r = make_ray(io.org + 3 * i, io.dir + 3 * i, io.tmin ? io.tmin[i] : 0.0,
-                           io.tmax ? io.tmax[i] : kDblMax);
-    Best best;
-    trace_ray<COUNT>(S, r, sk, threadIdx.x, io.error_word, best, &cnt);
-    if (io.t) io.t[i] = best.t;
-    if (io.uv) {
-      io.uv[2 * i] = best.u;
-      io.uv[2 * i + 1] = best.v;
+    const unsigned idle = __ballot_sync(kFull, !active);
+    if (idle && !exhausted) {
+      const uint32_t want = __popc(idle), avail = pool_end - pool_next;
+      uint32_t base = 0;
+      if (want > avail) {
+        if (lane == 0) base = atomicAdd(work_counter, kChunk);
+        base = __shfl_sync(kFull, base, 0);
+      }
+      if (!active) {
+        const uint32_t rank = __popc(idle & below);
+        const uint32_t idx = rank < avail ? pool_next + rank : base + (rank - avail);
+        if (idx < io.n) {
+          i = idx;
+          active = true;
+          r = make_ray(io.org + 3 * size_t(i), io.dir + 3 * size_t(i), io.tmin ? io.tmin[i] : 0.0,
+                       io.tmax ? io.tmax[i] : kDblMax);
+          trav_begin<KIND, COUNT>(K, r, st, tv, &cnt);
+        }
+      }
+      if (want > avail) {
+        pool_next = base + (want - avail);
+        pool_end = base + kChunk;
+        if (base >= io.n) exhausted = true;
+      } else {
+        pool_next += want;
+      }
     }
-    if (io.normal) {
-      io.normal[3 * i] = best.n.x;
-      io.normal[3 * i + 1] = best.n.y;
-      io.normal[3 * i + 2] = best.n.z;
+    if (!__any_sync(kFull, active)) break;
+    if (active) {
+      if (tv.live) trav_to_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, io.error_word, &cnt);
+      if (tv.live) trav_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, io.error_word, &cnt);
+      if (!tv.live) {
+        finalize_kind<KIND>(S, r, st, i, first != 0, io.t, io.uv, io.normal, io.prim, io.geom,
+                            io.hit);
+        active = false;
+      }
     }
-    if (io.prim) io.prim[i] = best.prim;
-    if (io.geom) io.geom[i] = best.geom;
-    if (io.hit) io.hit[i] = best.hit ? 1 : 0;
   }
   if (COUNT) {
     for (int k = 0; k < kNumKinds; ++k) {
       unsigned long long b = cnt.box[k], p = cnt.prim[k];
       for (int off = 16; off > 0; off >>= 1) {
-        b += __shfl_down_sync(0xFFFFFFFFu, b, off);
-        p += __shfl_down_sync(0xFFFFFFFFu, p, off);
+        b += __shfl_down_sync(kFull, b, off);
+        p += __shfl_down_sync(kFull, p, off);
       }
       if (lane == 0) {
-        atomicAdd(totals + k, b);
-        atomicAdd(totals + kNumKinds + k, p);
+        if (b) atomicAdd(totals + k, b);
+        if (p) atomicAdd(totals + kNumKinds + k, p);
       }
     }
   }
+}
+
+// Output defaults for every ray of a scene without primitives (blazert/ray.h:80-84).
+__global__ void fill_defaults_kernel(RayIO io) {
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < io.n;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    if (io.t) io.t[i] = kDblMax;
+    if (io.uv) io.uv[2 * i] = io.uv[2 * i + 1] = 0.0;
+    if (io.normal) io.normal[3 * i] = io.normal[3 * i + 1] = io.normal[3 * i + 2] = 0.0;
+    if (io.prim) io.prim[i] = 0xFFFFFFFFu;
+    if (io.geom) io.geom[i] = 0xFFFFFFFFu;
+    if (io.hit) io.hit[i] = 0;
+  }
+}
+
+template <int KIND, bool COUNT>
+cudaError_t launch_kind(const SceneView &S, const RayIO &io, int first, int blocks,
+                        cudaStream_t stream, uint32_t *counter, unsigned long long *totals) {
+  const size_t smem = trace_smem_bytes(S.stack_cap, kTraceThreads);
+  trace_kind_kernel<KIND, COUNT><<<blocks, kTraceThreads, smem, stream>>>(S, io, first, counter,
+                                                                         totals);
+  return cudaGetLastError();
+}
+
+template <int KIND>
+cudaError_t prepare_kind(uint32_t stack_cap, int sms, int *blocks) {
+  const size_t smem = trace_smem_bytes(stack_cap, kTraceThreads);
+  cudaError_t e = cudaFuncSetAttribute(trace_kind_kernel<KIND, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(trace_kind_kernel<KIND, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kind_kernel<KIND, false>,
+                                                    kTraceThreads, smem);
+  if (e != cudaSuccess) return e;
+  *blocks = sms * (per_sm > 0 ? per_sm : 1);
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -88,35 +164,66 @@ size_t trace_smem_bytes(uint32_t stack_cap, int threads) {
   return size_t(stack_cap) * threads * (sizeof(double) + sizeof(uint32_t));
 }
 
-cudaError_t trace_grid(uint32_t stack_cap, int *blocks) {
-  int dev = 0, sms = 0, per_sm = 0;
+cudaError_t trace_prepare(const SceneView &S, LaunchPlan *plan) {
+  int dev = 0, sms = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
-  const size_t smem = trace_smem_bytes(stack_cap, kTraceThreads);
-  e = cudaFuncSetAttribute(trace_fp64_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           int(smem));
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(trace_fp64_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           int(smem));
-  if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_fp64_kernel<false>,
-                                                    kTraceThreads, smem);
-  if (e != cudaSuccess) return e;
-  *blocks = sms * (per_sm > 0 ? per_sm : 1);
-  return cudaSuccess;
+  plan->sms = sms;
+  if ((e = prepare_kind<kMesh>(S.stack_cap, sms, &plan->blocks[kMesh])) != cudaSuccess) return e;
+  if ((e = prepare_kind<kSpheres>(S.stack_cap, sms, &plan->blocks[kSpheres])) != cudaSuccess)
+    return e;
+  if ((e = prepare_kind<kPlanes>(S.stack_cap, sms, &plan->blocks[kPlanes])) != cudaSuccess)
+    return e;
+  return prepare_kind<kCylinders>(S.stack_cap, sms, &plan->blocks[kCylinders]);
 }
 
-cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, int blocks,
-                         cudaStream_t stream, unsigned long long *totals) {
+int trace_passes(const SceneView &S) {
+  int n = 0;
+  for (int k = 0; k < kNumKinds; ++k) n += (S.k[k].present && S.k[k].n_prims) ? 1 : 0;
+  return n;
+}
+
+cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const LaunchPlan &plan,
+                         cudaStream_t stream, uint32_t *counters, unsigned long long *totals) {
   (void)mode;
-  const size_t smem = trace_smem_bytes(S.stack_cap, kTraceThreads);
-  if (totals)
-    trace_fp64_kernel<true><<<blocks, kTraceThreads, smem, stream>>>(S, io, totals);
-  else
-    trace_fp64_kernel<false><<<blocks, kTraceThreads, smem, stream>>>(S, io, nullptr);
-  return cudaGetLastError();
+  cudaError_t e = cudaMemsetAsync(counters, 0, kNumKinds * sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  int first = 1;
+  for (int k = 0; k < kNumKinds; ++k) {
+    if (!S.k[k].present || S.k[k].n_prims == 0) continue;
+    const int b = plan.blocks[k];
+    uint32_t *c = counters + k;
+    switch (k) {
+      case kMesh:
+        e = totals ? launch_kind<kMesh, true>(S, io, first, b, stream, c, totals)
+                   : launch_kind<kMesh, false>(S, io, first, b, stream, c, nullptr);
+        break;
+      case kSpheres:
+        e = totals ? launch_kind<kSpheres, true>(S, io, first, b, stream, c, totals)
+                   : launch_kind<kSpheres, false>(S, io, first, b, stream, c, nullptr);
+        break;
+      case kPlanes:
+        e = totals ? launch_kind<kPlanes, true>(S, io, first, b, stream, c, totals)
+                   : launch_kind<kPlanes, false>(S, io, first, b, stream, c, nullptr);
+        break;
+      default:
+        e = totals ? launch_kind<kCylinders, true>(S, io, first, b, stream, c, totals)
+                   : launch_kind<kCylinders, false>(S, io, first, b, stream, c, nullptr);
+        break;
+    }
+    if (e != cudaSuccess) return e;
+    first = 0;
+  }
+  if (first) {  // nothing to trace
+    const int threads = 256;
+    const uint64_t want = (uint64_t(io.n) + threads - 1) / threads;
+    const int blocks = int(want < uint64_t(plan.sms) * 8 ? want : uint64_t(plan.sms) * 8);
+    fill_defaults_kernel<<<blocks > 0 ? blocks : 1, threads, 0, stream>>>(io);
+    e = cudaGetLastError();
+  }
+  return e;
 }
 
 }  // namespace bzr

@@ -11,8 +11,8 @@ namespace bzr {
 
 constexpr int kTraceThreads = 128;
 
-// Device pointers of one batch.  tmin / tmax may be null (0 and DBL_MAX); each output may be
-// null.  work_counter must be zero when the kernel starts; error_word collects kErr* bits.
+// Device pointers of one batch.  tmin / tmax may be null (0 and DBL_MAX); each output except t
+// may be null.  error_word collects kErr* bits.
 struct RayIO {
   const double *org = nullptr;
   const double *dir = nullptr;
@@ -25,16 +25,26 @@ struct RayIO {
   uint32_t *geom = nullptr;
   uint8_t *hit = nullptr;
   uint32_t n = 0;
-  uint32_t *work_counter = nullptr;
   uint32_t *error_word = nullptr;
 };
 
+// Grid of each per-kind persistent kernel: SMs x resident blocks per SM.
+struct LaunchPlan {
+  int sms = 0;
+  int blocks[kNumKinds] = {0, 0, 0, 0};
+};
+
 size_t trace_smem_bytes(uint32_t stack_cap, int threads);
-// Persistent grid size for the current device: SMs x resident blocks per SM.
-cudaError_t trace_grid(uint32_t stack_cap, int *blocks);
-// totals (device, 8 x uint64, or null): when given, the counting kernel also adds per kind the
-// box tests (totals[0..3]) and primitive tests (totals[4..7]) of every ray.
-cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, int blocks,
-                         cudaStream_t stream, unsigned long long *totals = nullptr);
+cudaError_t trace_prepare(const SceneView &S, LaunchPlan *plan);
+// Number of per-kind passes a batch runs (kinds present with at least one primitive).
+int trace_passes(const SceneView &S);
+// Queues a batch on `stream`: one kernel per kind present, merged into io's outputs.  io.t must
+// be non-null when trace_passes(S) > 1 (it carries the closest distance between passes).
+// counters: kNumKinds device words, zeroed here.  totals (device, 8 x uint64, or null): when
+// given, the counting kernels add per kind the box tests (totals[0..3]) and primitive tests
+// (totals[4..7]) of every ray.
+cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const LaunchPlan &plan,
+                         cudaStream_t stream, uint32_t *counters,
+                         unsigned long long *totals = nullptr);
 
 }  // namespace bzr

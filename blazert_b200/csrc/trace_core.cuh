@@ -371,80 +371,112 @@ struct Counts {
   uint32_t prim[kNumKinds];
 };
 
-// blazert/bvh/accel.h:80-120 for one kind.  Returns the reference's hit flag.
+// Resumable traversal of one kind (blazert/bvh/accel.h:80-120).  trav_begin tests the root;
+// trav_to_leaf walks internal nodes until the current reference is a leaf; trav_leaf runs the
+// leaf's primitives (blazert/bvh/intersect.h:67-78) and pops the next accepted entry.  The
+// persistent kernels interleave these steps across the lanes of a warp; traverse() runs them
+// to completion.
+struct Trav {
+  uint32_t cur;  // node index, or kLeafBit | first primitive position of a leaf
+  uint32_t sp;   // stack depth
+  bool live;     // false once the stack is exhausted
+};
+
 template <int KIND, bool COUNT>
-BZR_HD bool traverse(const KindView &K, const Ray &r, KState &st, const Stack &sk,
-                     uint32_t tid, uint32_t *err, Counts *cnt) {
-  st.hit = r.tmax;
+BZR_HD void trav_begin(const KindView &K, const Ray &r, KState &st, Trav &tv, Counts *cnt) {
+  st.hit = r.tmax;  // prepare_traversal
   st.u = st.v = 0.0;
   st.pos = 0xFFFFFFFFu;
   st.n = d3(0.0, 0.0, 0.0);
+  tv.sp = 0;
+  tv.cur = K.root_ref;
   double key;
-  {
-    const double2 bx = make_double2(K.root_box[0], K.root_box[1]);
-    const double2 by = make_double2(K.root_box[2], K.root_box[3]);
-    const double2 bz = make_double2(K.root_box[4], K.root_box[5]);
-    if (COUNT) cnt->box[KIND] += 1;
-    if (!box_test(bx, by, bz, r, key) || key > st.hit) return false;
+  const double2 bx = make_double2(K.root_box[0], K.root_box[1]);
+  const double2 by = make_double2(K.root_box[2], K.root_box[3]);
+  const double2 bz = make_double2(K.root_box[4], K.root_box[5]);
+  if (COUNT) cnt->box[KIND] += 1;
+  tv.live = box_test(bx, by, bz, r, key) && !(key > st.hit);
+}
+
+// Pops until an entry passes its deferred hit-distance test; ends the traversal otherwise.
+BZR_HD void trav_pop(Trav &tv, const KState &st, const Stack &sk, uint32_t tid) {
+  while (tv.sp > 0) {
+    --tv.sp;
+    if (!(sk.key[tv.sp * sk.stride + tid] > st.hit)) {
+      tv.cur = sk.ref[tv.sp * sk.stride + tid];
+      return;
+    }
   }
-  uint32_t cur = K.root_ref;
-  uint32_t sp = 0;
-  for (;;) {
-    if (cur & kLeafBit) {
-      uint32_t pos = cur & kIdMask;
-      for (;;) {  // intersect_leaf (blazert/bvh/intersect.h:67-78)
-        if (pos >= K.n_prims) {
-          flag_error(err, kErrPrimIndex);
-          return false;
-        }
-        const uint32_t id = ldg(K.prim_ids + pos);
-        if (COUNT) cnt->prim[KIND] += 1;
-        isect<KIND>(K.payload, pos, r, st);
-        if (id & kLastBit) break;
-        ++pos;
+  tv.live = false;
+}
+
+template <int KIND, bool COUNT>
+BZR_HD void trav_to_leaf(const KindView &K, const Ray &r, const KState &st, Trav &tv,
+                         const Stack &sk, uint32_t tid, uint32_t *err, Counts *cnt) {
+  while (tv.live && !(tv.cur & kLeafBit)) {
+    if (tv.cur >= K.n_internal) {
+      flag_error(err, kErrNodeIndex);
+      tv.live = false;
+      return;
+    }
+    const double *nd = K.nodes64 + size_t(tv.cur) * kNode64Doubles;
+    const double2 a0 = ld2(nd), a1 = ld2(nd + 2), a2 = ld2(nd + 4);
+    const double2 b0 = ld2(nd + 6), b1 = ld2(nd + 8), b2 = ld2(nd + 10);
+    const uint4 meta = ldg(reinterpret_cast<const uint4 *>(nd + 12));
+    double k0, k1;
+    if (COUNT) cnt->box[KIND] += 2;
+    const bool p0 = box_test(a0, a1, a2, r, k0);
+    const bool p1 = box_test(b0, b1, b2, r, k1);
+    const unsigned near = meta.z == 0 ? r.sx : (meta.z == 1 ? r.sy : r.sz);
+    const bool pn = near ? p1 : p0, pf = near ? p0 : p1;
+    const double kn = near ? k1 : k0, kf = near ? k0 : k1;
+    const uint32_t rn = near ? meta.y : meta.x, rf = near ? meta.x : meta.y;
+    if (pf) {  // far child pushed first, as the reference does
+      if (tv.sp >= sk.cap) {
+        flag_error(err, kErrStack);
+        tv.live = false;
+        return;
       }
+      sk.key[tv.sp * sk.stride + tid] = kf;
+      sk.ref[tv.sp * sk.stride + tid] = rf;
+      ++tv.sp;
+    }
+    if (pn && !(kn > st.hit)) {  // the near child is popped next, with the same hit distance
+      tv.cur = rn;
     } else {
-      if (cur >= K.n_internal) {
-        flag_error(err, kErrNodeIndex);
-        return false;
-      }
-      const double *nd = K.nodes64 + size_t(cur) * kNode64Doubles;
-      const double2 a0 = ld2(nd), a1 = ld2(nd + 2), a2 = ld2(nd + 4);
-      const double2 b0 = ld2(nd + 6), b1 = ld2(nd + 8), b2 = ld2(nd + 10);
-      const uint4 meta = ldg(reinterpret_cast<const uint4 *>(nd + 12));
-      double k0, k1;
-      if (COUNT) cnt->box[KIND] += 2;
-      const bool p0 = box_test(a0, a1, a2, r, k0);
-      const bool p1 = box_test(b0, b1, b2, r, k1);
-      const unsigned near = meta.z == 0 ? r.sx : (meta.z == 1 ? r.sy : r.sz);
-      const bool pn = near ? p1 : p0, pf = near ? p0 : p1;
-      const double kn = near ? k1 : k0, kf = near ? k0 : k1;
-      const uint32_t rn = near ? meta.y : meta.x, rf = near ? meta.x : meta.y;
-      if (pf) {  // far child pushed first, as the reference does
-        if (sp >= sk.cap) {
-          flag_error(err, kErrStack);
-          return false;
-        }
-        sk.key[sp * sk.stride + tid] = kf;
-        sk.ref[sp * sk.stride + tid] = rf;
-        ++sp;
-      }
-      if (pn && !(kn > st.hit)) {  // the near child is popped next, with the same hit distance
-        cur = rn;
-        continue;
-      }
+      trav_pop(tv, st, sk, tid);
     }
-    // pop until an entry passes its deferred hit-distance test
-    bool found = false;
-    while (sp > 0) {
-      --sp;
-      if (!(sk.key[sp * sk.stride + tid] > st.hit)) {
-        cur = sk.ref[sp * sk.stride + tid];
-        found = true;
-        break;
-      }
+  }
+}
+
+template <int KIND, bool COUNT>
+BZR_HD void trav_leaf(const KindView &K, const Ray &r, KState &st, Trav &tv, const Stack &sk,
+                      uint32_t tid, uint32_t *err, Counts *cnt) {
+  uint32_t pos = tv.cur & kIdMask;
+  for (;;) {
+    if (pos >= K.n_prims) {
+      flag_error(err, kErrPrimIndex);
+      tv.live = false;
+      return;
     }
-    if (!found) break;
+    const uint32_t id = ldg(K.prim_ids + pos);
+    if (COUNT) cnt->prim[KIND] += 1;
+    isect<KIND>(K.payload, pos, r, st);
+    if (id & kLastBit) break;
+    ++pos;
+  }
+  trav_pop(tv, st, sk, tid);
+}
+
+// The whole traversal of one kind.  Returns the reference's hit flag.
+template <int KIND, bool COUNT>
+BZR_HD bool traverse(const KindView &K, const Ray &r, KState &st, const Stack &sk,
+                     uint32_t tid, uint32_t *err, Counts *cnt) {
+  Trav tv;
+  trav_begin<KIND, COUNT>(K, r, st, tv, cnt);
+  while (tv.live) {
+    trav_to_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, err, cnt);
+    if (tv.live) trav_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, err, cnt);
   }
   return st.hit < r.tmax;
 }
@@ -487,33 +519,40 @@ BZR_HD void take(const SceneView &S, const Ray &r, const KState &st,
   }
 }
 
-template <int KIND, bool COUNT>
-BZR_HD void run_kind(const SceneView &S, const Ray &r, const Stack &sk, uint32_t tid,
-                     uint32_t *err, Best &best, Counts *cnt) {
-  const KindView &K = S.k[KIND];
-  if (!K.present || K.n_prims == 0) return;
-  KState st;
-  const bool h = traverse<KIND, COUNT>(K, r, st, sk, tid, err, cnt);
-  if (h && (KIND == kMesh || st.hit < best.t)) take<KIND>(S, r, st, best);
-}
-
-BZR_HD void init_best(Best &best) {
-  best.t = 1.7976931348623157e308;  // RayHit defaults (blazert/ray.h:80-84)
-  best.u = best.v = 0.0;
-  best.n = d3(0.0, 0.0, 0.0);
-  best.prim = best.geom = 0xFFFFFFFFu;
-  best.hit = false;
-}
-
-// intersect1 for one ray (blazert/scene.h:161-210).  cnt is used only when COUNT is true.
-template <bool COUNT = false>
-BZR_HD void trace_ray(const SceneView &S, const Ray &r, const Stack &sk, uint32_t tid,
-                      uint32_t *err, Best &best, Counts *cnt = nullptr) {
-  init_best(best);
-  run_kind<kMesh, COUNT>(S, r, sk, tid, err, best, cnt);
-  run_kind<kSpheres, COUNT>(S, r, sk, tid, err, best, cnt);
-  run_kind<kPlanes, COUNT>(S, r, sk, tid, err, best, cnt);
-  run_kind<kCylinders, COUNT>(S, r, sk, tid, err, best, cnt);
+// Merge of one kind's result into the output record of ray i (blazert/scene.h:161-210): the
+// first kind traced writes the whole record (a miss writes the RayHit defaults); later kinds
+// overwrite it only when they hit strictly closer -- except triangles, which are always traced
+// first and copy unconditionally.  post_traversal supplies the normal.
+template <int KIND>
+BZR_HD void finalize_kind(const SceneView &S, const Ray &r, const KState &st, uint64_t i,
+                          bool first, double *t, double *uv, double *normal, uint32_t *prim,
+                          uint32_t *geom, uint8_t *hit) {
+  const bool hit_k = st.hit < r.tmax;
+  const double prev = first ? 1.7976931348623157e308 : t[i];
+  if (hit_k && (KIND == kMesh || st.hit < prev)) {
+    Best b;
+    take<KIND>(S, r, st, b);
+    t[i] = b.t;
+    if (uv) {
+      uv[2 * i] = b.u;
+      uv[2 * i + 1] = b.v;
+    }
+    if (normal) {
+      normal[3 * i] = b.n.x;
+      normal[3 * i + 1] = b.n.y;
+      normal[3 * i + 2] = b.n.z;
+    }
+    if (prim) prim[i] = b.prim;
+    if (geom) geom[i] = b.geom;
+    if (hit) hit[i] = 1;
+  } else if (first) {
+    t[i] = 1.7976931348623157e308;
+    if (uv) uv[2 * i] = uv[2 * i + 1] = 0.0;
+    if (normal) normal[3 * i] = normal[3 * i + 1] = normal[3 * i + 2] = 0.0;
+    if (prim) prim[i] = 0xFFFFFFFFu;
+    if (geom) geom[i] = 0xFFFFFFFFu;
+    if (hit) hit[i] = 0;
+  }
 }
 
 }  // namespace bzr

@@ -105,15 +105,17 @@ long emu_scene_tree(void *h, int kind, double *bmin, double *bmax, uint32_t *lea
   return n;
 }
 
-// Runs the kernel's per-ray code; returns the accumulated error word.
-uint32_t emu_scene_intersect(void *h, long n, const double *org, const double *dir, const double *tmin,
-                       const double *tmax, double *t, double *uv, double *normal, uint32_t *prim,
-                       uint32_t *geom, uint8_t *hit, uint32_t stack_cap_override) {
-  const Emu *e = static_cast<Emu *>(h);
-  bzr::SceneView view = e->view;
-  if (stack_cap_override) view.stack_cap = stack_cap_override;
-  uint32_t err = 0;
-#pragma omp parallel reduction(| : err)
+// Runs the kernels' per-ray code with the kernels' data flow: one pass per kind present, in the
+// reference's kind order, each merged into the output arrays by finalize_kind.  Returns the
+// accumulated error word.
+}  // extern "C"
+
+template <int KIND>
+static void emu_pass(const bzr::SceneView &view, long n, const double *org, const double *dir,
+                     const double *tmin, const double *tmax, bool first, double *t, double *uv,
+                     double *normal, uint32_t *prim, uint32_t *geom, uint8_t *hit, uint32_t &err) {
+  uint32_t e = 0;
+#pragma omp parallel reduction(| : e)
   {
     std::vector<double> key(view.stack_cap);
     std::vector<uint32_t> ref(view.stack_cap);
@@ -126,21 +128,43 @@ uint32_t emu_scene_intersect(void *h, long n, const double *org, const double *d
     for (long i = 0; i < n; ++i) {
       const bzr::Ray r = bzr::make_ray(org + 3 * i, dir + 3 * i, tmin ? tmin[i] : 0.0,
                                        tmax ? tmax[i] : 1.7976931348623157e308);
-      bzr::Best best;
-      uint32_t my_err = 0;
-      bzr::trace_ray(view, r, sk, 0, &my_err, best);
-      err |= my_err;
-      t[i] = best.t;
-      uv[2 * i] = best.u;
-      uv[2 * i + 1] = best.v;
-      normal[3 * i] = best.n.x;
-      normal[3 * i + 1] = best.n.y;
-      normal[3 * i + 2] = best.n.z;
-      prim[i] = best.prim;
-      geom[i] = best.geom;
-      hit[i] = best.hit ? 1 : 0;
+      bzr::KState st;
+      bzr::traverse<KIND, false>(view.k[KIND], r, st, sk, 0, &e, nullptr);
+      bzr::finalize_kind<KIND>(view, r, st, uint64_t(i), first, t, uv, normal, prim, geom, hit);
     }
   }
+  err |= e;
+}
+
+extern "C" {
+
+uint32_t emu_scene_intersect(void *h, long n, const double *org, const double *dir,
+                             const double *tmin, const double *tmax, double *t, double *uv,
+                             double *normal, uint32_t *prim, uint32_t *geom, uint8_t *hit,
+                             uint32_t stack_cap_override) {
+  const Emu *e = static_cast<Emu *>(h);
+  bzr::SceneView view = e->view;
+  if (stack_cap_override) view.stack_cap = stack_cap_override;
+  uint32_t err = 0;
+  bool first = true;
+  for (int k = 0; k < 4; ++k) {
+    if (!view.k[k].present || view.k[k].n_prims == 0) continue;
+    switch (k) {
+      case 0: emu_pass<0>(view, n, org, dir, tmin, tmax, first, t, uv, normal, prim, geom, hit, err); break;
+      case 1: emu_pass<1>(view, n, org, dir, tmin, tmax, first, t, uv, normal, prim, geom, hit, err); break;
+      case 2: emu_pass<2>(view, n, org, dir, tmin, tmax, first, t, uv, normal, prim, geom, hit, err); break;
+      case 3: emu_pass<3>(view, n, org, dir, tmin, tmax, first, t, uv, normal, prim, geom, hit, err); break;
+    }
+    first = false;
+  }
+  if (first)
+    for (long i = 0; i < n; ++i) {
+      t[i] = 1.7976931348623157e308;
+      uv[2 * i] = uv[2 * i + 1] = 0.0;
+      normal[3 * i] = normal[3 * i + 1] = normal[3 * i + 2] = 0.0;
+      prim[i] = geom[i] = 0xFFFFFFFFu;
+      hit[i] = 0;
+    }
   return err;
 }
 
