@@ -54,6 +54,8 @@ def parse(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--sort", default="auto", choices=["auto", "on", "off"],
+                    help="coherence sort of each batch; auto = chosen by blazert_b200.autotune")
     return ap.parse_args(argv)
 
 
@@ -225,6 +227,13 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
+    tuning = None
+    if args.sort == "auto":
+        from blazert_b200.autotune import autotune
+        tuning = autotune(scene, o, d, tmn, tmx, mode=args.mode, stream=stream)
+    else:
+        scene.tune(sort=args.sort == "on")
+
     def step():
         scene.intersectN(o, d, tmn, tmx, mode=args.mode, out=out, stream=stream)
 
@@ -326,7 +335,7 @@ def run_ours(args):
                          "box_tests_per_ray": [c / n for c in counts["box"]],
                          "prim_tests_per_ray": [c / n for c in counts["prim"]]},
             "cpu_baseline": cpu, "clocks": clocks, "hit_fraction": hits,
-            "commit_seconds": commit_s, "wall_seconds_timed": wall,
+            "commit_seconds": commit_s, "wall_seconds_timed": wall, "tuning": tuning,
             "step_ms_min_max": [min(step_ms), max(step_ms)],
         }
         print(json.dumps(line), flush=True)

@@ -80,6 +80,7 @@ def library():
         lib.bzr_intersectN.argtypes = [P, C.c_size_t, P, P, P, P, P, P, P, P, P, P, C.c_int, P]
         lib.bzr_scene_check.argtypes = [P, P, C.c_int, _u32p]
         lib.bzr_work_counts.argtypes = [P, C.c_size_t, P, P, P, P, C.POINTER(C.c_uint64), P]
+        lib.bzr_scene_tune.argtypes = [P, C.c_int, C.c_int64]
         lib.bzr_scene_stats.argtypes = [P, C.c_int, C.POINTER(C.c_uint64), _u32p,
                                         C.POINTER(C.c_double)]
         lib.bzr_last_error_string.restype = C.c_char_p
@@ -285,6 +286,13 @@ class Scene:
                                         MODES[mode], C.c_void_p(st)))
         out["_keep"] = (o, d, tmn, tmx)
         return out
+
+    def tune(self, sort=None, sort_min_rays=None):
+        """Speed knobs (bzr_scene_tune); results do not depend on them."""
+        if sort is not None:
+            _check(self._lib.bzr_scene_tune(self._h, 1, int(bool(sort))))
+        if sort_min_rays is not None:
+            _check(self._lib.bzr_scene_tune(self._h, 2, int(sort_min_rays)))
 
     def work_counts(self, origins, directions, tmin=None, tmax=None, stream=None):
         """Box tests and primitive tests per kind for a batch (counting kernel; see

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
@@ -70,6 +71,7 @@ struct bzr_scene {
   void *arena = nullptr;  // every device array of the committed scene
   bzr::SceneView view;
   bzr::LaunchPlan plan;
+  bool sort_possible = false;  // finite scene bounds: the coherence sort can be used
   uint32_t *slots = nullptr;  // see kSlots
   std::atomic<uint32_t> next_slot{0};
   // host-pointer calls: staging buffers (grown on demand) and a private stream
@@ -275,6 +277,28 @@ int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
   }
   e = bzr::trace_prepare(s->view, &s->plan);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+  {  // origin quantisation box of the coherence sort: union of the per-kind root boxes
+    double lo[3] = {std::numeric_limits<double>::max(), std::numeric_limits<double>::max(),
+                    std::numeric_limits<double>::max()};
+    double hi[3] = {-lo[0], -lo[1], -lo[2]};
+    for (int k = 0; k < bzr::kNumKinds; ++k) {
+      const bzr::KindView &v = s->view.k[k];
+      if (!v.present || !v.n_prims) continue;
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], v.root_box[2 * a]);
+        hi[a] = std::max(hi[a], v.root_box[2 * a + 1]);
+      }
+    }
+    bool ok = true;
+    for (int a = 0; a < 3; ++a) {
+      const double ext = hi[a] - lo[a];
+      ok = ok && std::isfinite(ext) && std::abs(lo[a]) < 1e30 && std::abs(hi[a]) < 1e30;
+      s->plan.sort.lo[a] = static_cast<float>(lo[a]);
+      s->plan.sort.scale[a] = ext > 0 ? static_cast<float>(512.0 / ext) : 0.0f;
+    }
+    s->plan.sort.enabled = ok;
+    s->sort_possible = ok;
+  }
   s->host.committed = true;
   return BZR_OK;
 }
@@ -505,6 +529,22 @@ int bzr_scene_check(const bzr_scene *s, void *stream, int timeout_ms, uint32_t *
   if (rc) return rc;
   if (flags) *flags = word;
   return word ? fail(BZR_EDEVICE_FLAG, "kernel bounds check fired") : BZR_OK;
+}
+
+int bzr_scene_tune(bzr_scene *s, int option, int64_t value) {
+  if (!s) return fail(BZR_EINVAL, "scene is null");
+  if (!s->host.committed) return fail(BZR_ESTATE, "tune after commit");
+  switch (option) {
+    case BZR_TUNE_SORT:
+      if (value != 0 && value != 1) return fail(BZR_EINVAL, "sort must be 0 or 1");
+      s->plan.sort.enabled = value == 1 && s->sort_possible;
+      return BZR_OK;
+    case BZR_TUNE_SORT_MIN_RAYS:
+      if (value < 0 || value > 0x7FFFFFFF) return fail(BZR_EINVAL, "bad sort threshold");
+      s->plan.sort_min_rays = static_cast<uint32_t>(value);
+      return BZR_OK;
+  }
+  return fail(BZR_EINVAL, "unknown tuning option");
 }
 
 int bzr_scene_stats(const bzr_scene *s, int kind, uint64_t *n_nodes, uint32_t *max_depth,

@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(kTraceThreads)
         const uint32_t rank = __popc(idle & below);
         const uint32_t idx = rank < avail ? pool_next + rank : base + (rank - avail);
         if (idx < io.n) {
-          i = idx;
+          i = io.perm ? io.perm[idx] : idx;
           active = true;
           r = make_ray(io.org + 3 * size_t(i), io.dir + 3 * size_t(i), io.tmin ? io.tmin[i] : 0.0,
                        io.tmax ? io.tmax[i] : kDblMax);
@@ -129,6 +129,67 @@ __global__ void fill_defaults_kernel(RayIO io) {
     if (io.prim) io.prim[i] = 0xFFFFFFFFu;
     if (io.geom) io.geom[i] = 0xFFFFFFFFu;
     if (io.hit) io.hit[i] = 0;
+  }
+}
+
+// -------------------------------------------------------------------------- coherence sort
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 9 bits -> every third bit
+  v &= 0x1FFu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__device__ __forceinline__ uint32_t ray_key(const RayIO &io, const RaySort &rs, uint32_t i) {
+  const double *o = io.org + 3 * size_t(i), *d = io.dir + 3 * size_t(i);
+  uint32_t q[3];
+  for (int a = 0; a < 3; ++a) {
+    float x = (float(o[a]) - rs.lo[a]) * rs.scale[a];
+    x = fminf(fmaxf(x, 0.0f), 511.0f);  // NaN maps to 0
+    q[a] = uint32_t(x);
+  }
+  const uint32_t oct = (d[0] < 0.0 ? 4u : 0u) | (d[1] < 0.0 ? 2u : 0u) | (d[2] < 0.0 ? 1u : 0u);
+  return (oct << 27) | (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+}
+
+__global__ void sort_histogram_kernel(RayIO io, RaySort rs, uint32_t *keys, uint32_t *counts) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < io.n; i += gridDim.x * blockDim.x) {
+    const uint32_t k = ray_key(io, rs, i);
+    keys[i] = k;
+    atomicAdd(counts + (k >> (32 - kSortBits)), 1u);
+  }
+}
+
+// In-place exclusive scan of 2^kSortBits counts; one block of 1024 threads.
+__global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t *counts) {
+  constexpr int kPer = (1 << kSortBits) / 1024;
+  __shared__ uint32_t part[1024];
+  uint32_t *c = counts + threadIdx.x * kPer;
+  uint32_t sum = 0;
+  for (int j = 0; j < kPer; ++j) sum += c[j];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scan
+    const uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  uint32_t run = part[threadIdx.x] - sum;
+  for (int j = 0; j < kPer; ++j) {
+    const uint32_t v = c[j];
+    c[j] = run;
+    run += v;
+  }
+}
+
+__global__ void sort_scatter_kernel(uint32_t n, const uint32_t *keys, uint32_t *offsets,
+                                    uint32_t *perm) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t pos = atomicAdd(offsets + (keys[i] >> (32 - kSortBits)), 1u);
+    if (pos < n) perm[pos] = i;
   }
 }
 
@@ -190,6 +251,24 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
   (void)mode;
   cudaError_t e = cudaMemsetAsync(counters, 0, kNumKinds * sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
+  RayIO sorted = io;
+  uint32_t *scratch = nullptr;
+  if (plan.sort.enabled && io.n >= plan.sort_min_rays && trace_passes(S) > 0) {
+    const size_t nb = size_t(1) << kSortBits;
+    e = cudaMallocAsync(reinterpret_cast<void **>(&scratch),
+                        (2 * size_t(io.n) + nb) * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    uint32_t *keys = scratch, *perm = scratch + io.n, *counts = scratch + 2 * size_t(io.n);
+    e = cudaMemsetAsync(counts, 0, nb * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    const int blocks = plan.sms * 8;
+    sort_histogram_kernel<<<blocks, 256, 0, stream>>>(io, plan.sort, keys, counts);
+    sort_scan_kernel<<<1, 1024, 0, stream>>>(counts);
+    sort_scatter_kernel<<<blocks, 256, 0, stream>>>(io.n, keys, counts, perm);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    sorted.perm = perm;
+  }
+  const RayIO &run = sorted;
   int first = 1;
   for (int k = 0; k < kNumKinds; ++k) {
     if (!S.k[k].present || S.k[k].n_prims == 0) continue;
@@ -197,20 +276,20 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
     uint32_t *c = counters + k;
     switch (k) {
       case kMesh:
-        e = totals ? launch_kind<kMesh, true>(S, io, first, b, stream, c, totals)
-                   : launch_kind<kMesh, false>(S, io, first, b, stream, c, nullptr);
+        e = totals ? launch_kind<kMesh, true>(S, run, first, b, stream, c, totals)
+                   : launch_kind<kMesh, false>(S, run, first, b, stream, c, nullptr);
         break;
       case kSpheres:
-        e = totals ? launch_kind<kSpheres, true>(S, io, first, b, stream, c, totals)
-                   : launch_kind<kSpheres, false>(S, io, first, b, stream, c, nullptr);
+        e = totals ? launch_kind<kSpheres, true>(S, run, first, b, stream, c, totals)
+                   : launch_kind<kSpheres, false>(S, run, first, b, stream, c, nullptr);
         break;
       case kPlanes:
-        e = totals ? launch_kind<kPlanes, true>(S, io, first, b, stream, c, totals)
-                   : launch_kind<kPlanes, false>(S, io, first, b, stream, c, nullptr);
+        e = totals ? launch_kind<kPlanes, true>(S, run, first, b, stream, c, totals)
+                   : launch_kind<kPlanes, false>(S, run, first, b, stream, c, nullptr);
         break;
       default:
-        e = totals ? launch_kind<kCylinders, true>(S, io, first, b, stream, c, totals)
-                   : launch_kind<kCylinders, false>(S, io, first, b, stream, c, nullptr);
+        e = totals ? launch_kind<kCylinders, true>(S, run, first, b, stream, c, totals)
+                   : launch_kind<kCylinders, false>(S, run, first, b, stream, c, nullptr);
         break;
     }
     if (e != cudaSuccess) return e;
@@ -222,6 +301,10 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
     const int blocks = int(want < uint64_t(plan.sms) * 8 ? want : uint64_t(plan.sms) * 8);
     fill_defaults_kernel<<<blocks > 0 ? blocks : 1, threads, 0, stream>>>(io);
     e = cudaGetLastError();
+  }
+  if (scratch) {
+    const cudaError_t f = cudaFreeAsync(scratch, stream);
+    if (e == cudaSuccess) e = f;
   }
   return e;
 }

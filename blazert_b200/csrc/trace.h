@@ -26,12 +26,26 @@ struct RayIO {
   uint8_t *hit = nullptr;
   uint32_t n = 0;
   uint32_t *error_word = nullptr;
+  const uint32_t *perm = nullptr;  // optional processing order (ray indices), see RaySort
+};
+
+// Coherence sort of a batch: rays are processed in the order of a 32-bit key -- the direction
+// octant (3 bits) over a Morton code of the origin quantised inside the scene bounds (9 bits
+// per axis) -- bucketed on the key's top kSortBits bits by a device counting sort.  The order
+// affects only speed: every ray's result is written to its own index.
+constexpr int kSortBits = 16;
+struct RaySort {
+  bool enabled = false;
+  float lo[3] = {0, 0, 0};     // origin quantisation box
+  float scale[3] = {0, 0, 0};  // 512 / extent per axis
 };
 
 // Grid of each per-kind persistent kernel: SMs x resident blocks per SM.
 struct LaunchPlan {
   int sms = 0;
   int blocks[kNumKinds] = {0, 0, 0, 0};
+  RaySort sort;
+  uint32_t sort_min_rays = 1u << 16;  // smaller batches are traced in their own order
 };
 
 size_t trace_smem_bytes(uint32_t stack_cap, int threads);
@@ -40,6 +54,8 @@ cudaError_t trace_prepare(const SceneView &S, LaunchPlan *plan);
 int trace_passes(const SceneView &S);
 // Queues a batch on `stream`: one kernel per kind present, merged into io's outputs.  io.t must
 // be non-null when trace_passes(S) > 1 (it carries the closest distance between passes).
+// When plan.sort.enabled and the batch has at least plan.sort_min_rays rays, a coherence sort
+// runs first (scratch from the stream-ordered allocator).
 // counters: kNumKinds device words, zeroed here.  totals (device, 8 x uint64, or null): when
 // given, the counting kernels add per kind the box tests (totals[0..3]) and primitive tests
 // (totals[4..7]) of every ray.

@@ -212,7 +212,150 @@ def mixed_primitives(n_rays=1 << 20, n_spheres=10_000, n_cylinders=1_000, n_plan
                     dict(spheres=n_spheres, cylinders=n_cylinders, planes=n_planes, seed=seed))
 
 
+def _value_noise(x, y, rng_seed, octave):
+    """Value noise in [-1, 1]: seeded random values on the integer lattice, smoothstep blend."""
+    rng = np.random.Generator(np.random.PCG64([rng_seed, octave]))
+    ix, iy = np.floor(x).astype(np.int64), np.floor(y).astype(np.int64)
+    fx, fy = x - ix, y - iy
+    size = int(max(ix.max(), iy.max())) + 2
+    lattice = rng.uniform(-1.0, 1.0, (size + 1, size + 1))
+    sx, sy = fx * fx * (3 - 2 * fx), fy * fy * (3 - 2 * fy)
+    a = lattice[ix, iy] + sx * (lattice[ix + 1, iy] - lattice[ix, iy])
+    b = lattice[ix, iy + 1] + sx * (lattice[ix + 1, iy + 1] - lattice[ix, iy + 1])
+    return a + sy * (b - a)
+
+
+def heightfield_mesh(n=1024, extent=1000.0, amplitude=100.0, octaves=6, lacunarity=2.0, gain=0.5,
+                     base_frequency=4.0 / 1000.0, seed=3):
+    """n x n vertex grid over [0, extent]^2, heights from fBm value noise; two triangles per
+    quad with a fixed diagonal: 2 (n-1)^2 triangles."""
+    xs = np.linspace(0.0, extent, n)
+    X, Y = np.meshgrid(xs, xs, indexing="xy")
+    Z = np.zeros_like(X)
+    amp, freq, norm = 1.0, base_frequency, 0.0
+    for o in range(octaves):
+        Z += amp * _value_noise(X * freq, Y * freq, seed, o)
+        norm += amp
+        amp *= gain
+        freq *= lacunarity
+    Z *= amplitude / norm
+    v = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    j, i = np.meshgrid(np.arange(n - 1), np.arange(n - 1), indexing="ij")
+    a = (j * n + i).ravel()
+    f = np.concatenate([np.stack([a, a + 1, a + n + 1], 1), np.stack([a, a + n + 1, a + n], 1)])
+    f = f.reshape(2, -1, 3).transpose(1, 0, 2).reshape(-1, 3)  # interleave the two per quad
+    return np.ascontiguousarray(v), np.ascontiguousarray(f.astype(np.uint32))
+
+
+def _cosine_dirs(rng, normals):
+    """Cosine-weighted directions about each unit normal."""
+    n = normals.shape[0]
+    r1, r2 = rng.random(n), rng.random(n)
+    phi = 2.0 * np.pi * r1
+    sr = np.sqrt(r2)
+    local = np.stack([sr * np.cos(phi), sr * np.sin(phi), np.sqrt(1.0 - r2)], 1)
+    # orthonormal frame (t, b, n) per normal
+    helper = np.where(np.abs(normals[:, 2:3]) < 0.9, [[0.0, 0.0, 1.0]], [[1.0, 0.0, 0.0]])
+    t = np.cross(helper, normals)
+    t /= np.linalg.norm(t, axis=1, keepdims=True)
+    b = np.cross(normals, t)
+    return local[:, :1] * t + local[:, 1:2] * b + local[:, 2:3] * normals
+
+
+def heightfield(n_rays=1 << 23, grid=1024, seed=3):
+    verts, faces = heightfield_mesh(grid, seed=seed)
+    scene = SceneSpec().add_mesh(verts, faces)
+    rng = np.random.Generator(np.random.PCG64(seed + 1000))
+    v0, v1, v2 = verts[faces[:, 0]], verts[faces[:, 1]], verts[faces[:, 2]]
+    cr = np.cross(v1 - v0, v2 - v0)
+    area = 0.5 * np.linalg.norm(cr, axis=1)
+    nf = cr / (2.0 * area[:, None])
+    nf *= np.sign(nf[:, 2:3])  # oriented +z
+    cdf = np.cumsum(area)
+    tri = np.minimum(np.searchsorted(cdf, rng.random(n_rays) * cdf[-1]), len(area) - 1)
+    r1, r2 = np.sqrt(rng.random(n_rays)), rng.random(n_rays)
+    p = ((1 - r1)[:, None] * v0[tri] + (r1 * (1 - r2))[:, None] * v1[tri]
+         + (r1 * r2)[:, None] * v2[tri])
+    nrm = nf[tri]
+    o = p + 1e-6 * nrm
+    d = _cosine_dirs(rng, nrm)
+    rays = RayBatch(np.ascontiguousarray(o), np.ascontiguousarray(d), np.zeros(n_rays),
+                    np.full(n_rays, np.inf))
+    return Workload("heightfield", scene, rays,
+                    dict(triangles=int(faces.shape[0]), grid=grid, seed=seed))
+
+
+def _dedup_noise(v, rng_seed, sigma, radial):
+    """Perturbation that moves bitwise-identical vertex positions together (the icosphere
+    helper duplicates midpoint vertices per triangle), so the mesh stays watertight."""
+    uniq, inv = np.unique(v, axis=0, return_inverse=True)
+    rng = np.random.Generator(np.random.PCG64(rng_seed))
+    if radial:
+        eps = rng.normal(0.0, sigma, uniq.shape[0])
+        return uniq[inv.ravel()] * (1.0 + eps[inv.ravel()])[:, None]
+    return uniq[inv.ravel()] + rng.normal(0.0, sigma, uniq.shape)[inv.ravel()]
+
+
+def _rays_to_ball(rng, n, radius):
+    """Origins uniform on a sphere of the given radius, directions toward points uniform in
+    the unit ball."""
+    o = _unit_sphere(rng, n) * radius
+    q = _unit_sphere(rng, n) * np.cbrt(rng.random(n))[:, None]
+    d = q - o
+    return o, d / np.linalg.norm(d, axis=1, keepdims=True)
+
+
+def batched_icospheres(n_scenes=256, seed=4, min_rays=1_000, max_rays=1_000_000, scale=1.0):
+    """Per scene: a target triangle count log-uniform in [1k, 500k] mapped to the nearest
+    icosphere level in 3..7, radial perturbation N(0, 0.02) per unique vertex; a ray batch of
+    log-uniform size in [min_rays, max_rays] (times scale) from a radius-3 sphere toward the
+    unit ball."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    cache = {}
+    out = []
+    for sidx in range(n_scenes):
+        target = math.exp(rng.uniform(math.log(1e3), math.log(5e5)))
+        level = int(np.clip(np.round(np.log(target / 20.0) / np.log(4.0)), 3, 7))
+        if level not in cache:
+            cache[level] = icosphere(level)
+        v, f = cache[level]
+        v = _dedup_noise(v, seed * 100003 + sidx, 0.02, radial=True)
+        n = max(1, int(math.exp(rng.uniform(math.log(min_rays), math.log(max_rays))) * scale))
+        o, d = _rays_to_ball(rng, n, 3.0)
+        out.append(Workload(f"icosphere_{sidx}", SceneSpec().add_mesh(v, f),
+                            RayBatch(o, d, np.zeros(n), np.full(n, np.inf)),
+                            dict(level=level, triangles=int(f.shape[0]))))
+    return out
+
+
+def adjoint_scene(n_rays=1 << 22, seed=5, level=6, n_split=10_000, n_spheres=500):
+    """Level-6 icosphere with n_split triangles split at an edge midpoint (one more triangle
+    each), isotropic vertex noise N(0, 0.01) per unique vertex, plus spheres with centres in
+    [-2, 2]^3 and radii in [0.05, 0.2]; rays from a radius-4 sphere toward the unit ball and
+    per-ray loss weights w ~ N(0, 1)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    v, f = icosphere(level)
+    v = _dedup_noise(v, seed * 7919, 0.01, radial=False)
+    pick = rng.choice(f.shape[0], n_split, replace=False)
+    a, b, c = f[pick, 0], f[pick, 1], f[pick, 2]
+    mid = 0.5 * (v[a] + v[b])
+    m = v.shape[0] + np.arange(n_split)
+    v = np.concatenate([v, mid])
+    f = f.astype(np.int64).copy()
+    f[pick] = np.stack([a, m, c], 1)
+    f = np.concatenate([f, np.stack([m, b, c], 1)])
+    sc = rng.uniform(-2.0, 2.0, (n_spheres, 3))
+    sr = rng.uniform(0.05, 0.2, n_spheres)
+    scene = SceneSpec().add_mesh(v, f.astype(np.uint32)).add_spheres(sc, sr)
+    o, d = _rays_to_ball(rng, n_rays, 4.0)
+    w = rng.standard_normal(n_rays)
+    return Workload("adjoint_scene", scene, RayBatch(o, d, np.zeros(n_rays), np.full(n_rays, np.inf)),
+                    dict(triangles=int(f.shape[0]), spheres=n_spheres, seed=seed, weights=w))
+
+
 WORKLOADS = {
     "icosphere_pinhole": icosphere_pinhole,
     "mixed_primitives": mixed_primitives,
+    "heightfield": heightfield,
+    "adjoint_scene": adjoint_scene,
 }

@@ -16,7 +16,8 @@
  *   bzr_intersect1                intersect1(scene, ray, rayhit)    blazert/scene.h:161-210
  *                                 with Ray / RayHit                 blazert/ray.h:56-85
  *   bzr_intersectN                new: intersect1 over a batch of rays, one GPU launch
- *   bzr_work_counts, bzr_scene_check, bzr_scene_stats   new: measurement and error reporting
+ *   bzr_work_counts, bzr_scene_check, bzr_scene_stats, bzr_scene_tune
+ *                                 new: measurement, error reporting and tuning
  *
  * Semantics kept from the reference:
  *   - add_* may be called once per primitive kind and only before commit; otherwise the
@@ -124,6 +125,15 @@ int bzr_work_counts(const bzr_scene *scene, size_t n, const double *origins,
  * reports the kernels' error word: BZR_OK, BZR_EDEVICE_FLAG (with *flags receiving the bits)
  * or BZR_ETIMEOUT. */
 int bzr_scene_check(const bzr_scene *scene, void *stream, int timeout_ms, uint32_t *flags);
+
+/* Tuning knobs of a committed scene (no counterpart in the reference; they change speed,
+ * never results).  BZR_TUNE_SORT: 1 (default when the scene has finite bounds) sorts each
+ * batch of at least BZR_TUNE_SORT_MIN_RAYS rays (default 65536) by direction octant and origin
+ * Morton code before tracing, so that the rays of a warp take similar paths; 0 traces in the
+ * caller's order. */
+#define BZR_TUNE_SORT 1
+#define BZR_TUNE_SORT_MIN_RAYS 2
+int bzr_scene_tune(bzr_scene *scene, int option, int64_t value);
 
 /* Statistics of the last commit: per kind (0 mesh, 1 spheres, 2 planes, 3 cylinders) the
  * number of reference BVH nodes, the maximum depth and the host build time in seconds. */

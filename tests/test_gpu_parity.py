@@ -51,3 +51,42 @@ def test_intersect1_matches_batch():
         assert hit == bool(ref["hit"][i])
         assert rh.prim_id == ref["prim"][i] and rh.geom_id == ref["geom"][i]
         assert np.float64(rh.hit_distance).view(np.uint64) == ref["t"][i].view(np.uint64)
+
+
+def test_sort_changes_speed_not_results():
+    import torch
+
+    wl = W.mixed_primitives(n_rays=300_000, seed=8)
+    R = wl.rays
+    s = product_scene(wl.scene)
+    dev = torch.device("cuda", 0)
+    o, d = torch.from_numpy(R.origins).to(dev), torch.from_numpy(R.directions).to(dev)
+    outs = []
+    for sort in (False, True):
+        s.tune(sort=sort, sort_min_rays=0)
+        outs.append({k: v.cpu().numpy() for k, v in s.intersectN(o, d).items() if not k.startswith("_")})
+    s.check()
+    ref = Oracle(wl.scene).intersect(R.origins, R.directions)
+    assert mismatches(outs[0], ref) == [] and mismatches(outs[1], ref) == []
+
+
+@pytest.mark.parametrize("mode", ["fp64"])
+def test_heightfield_full_size(mode):
+    """2,093,058-triangle heightfield, 8,388,608 secondary rays, against the oracle."""
+    wl = W.heightfield()
+    ref, out_dev, _ = _run_both_device_only(wl, mode)
+    assert mismatches(out_dev, ref) == []
+
+
+def _run_both_device_only(wl, mode):
+    import torch
+
+    R = wl.rays
+    ref = Oracle(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax)
+    s = product_scene(wl.scene)
+    dev = torch.device("cuda", 0)
+    out = s.intersectN(torch.from_numpy(R.origins).to(dev), torch.from_numpy(R.directions).to(dev),
+                       torch.from_numpy(R.tmin).to(dev), torch.from_numpy(R.tmax).to(dev), mode=mode)
+    torch.cuda.synchronize()
+    s.check()
+    return ref, out, None
