@@ -54,6 +54,8 @@ def parse(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--rays", type=int, default=0,
+                    help="override the workload's ray count (smaller cases for profiling)")
     ap.add_argument("--sort", default="auto", choices=["auto", "on", "off"],
                     help="coherence sort of each batch; auto = chosen by blazert_b200.autotune")
     return ap.parse_args(argv)
@@ -156,7 +158,7 @@ def run_reference(args):
         return 0
     from blazert_b200 import workloads as W
     from oracle.oracle import Oracle, RefScene
-    wl = W.WORKLOADS[args.workload]()
+    wl = W.WORKLOADS[args.workload](**({"n_rays": args.rays} if args.rays else {}))
     threads = os.cpu_count() or 1
     kind = "reference" if RefScene.available("bench") else "port"
     sc = RefScene(wl.scene, flavour="bench") if kind == "reference" else Oracle(wl.scene)
@@ -201,7 +203,7 @@ def run_ours(args):
     import blazert_b200 as B
     from blazert_b200 import workloads as W
 
-    wl = W.WORKLOADS[args.workload]()
+    wl = W.WORKLOADS[args.workload](**({"n_rays": args.rays} if args.rays else {}))
     R = wl.rays
     if rank > 0:  # each rank traces its own batch: rotate the rays so ranks differ
         sh = (rank * 7919) % R.n

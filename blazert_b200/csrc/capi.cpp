@@ -94,6 +94,7 @@ struct bzr_scene {
       cudaFreeHost(pinned_err);
       for (cudaStream_t st : streams)
         if (st) cudaStreamDestroy(st);
+      if (plan.pool) cudaMemPoolDestroy(plan.pool);  // released once pending frees complete
       cudaSetDevice(cur);
     }
   }
@@ -260,7 +261,7 @@ int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
     v.root_ref = img[k].root_ref;
     v.mixed_ok = img[k].mixed_ok ? 1 : 0;
     std::memcpy(v.root_box, img[k].root_box, sizeof v.root_box);
-    std::memcpy(v.root_box32, img[k].root_box32, sizeof v.root_box32);
+    v.coord_max = img[k].coord_max;
   }
   s->view.faces = reinterpret_cast<const uint32_t *>(base + off_faces);
   s->view.vert_n = reinterpret_cast<const double *>(base + off_vn);
@@ -277,6 +278,17 @@ int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
   }
   e = bzr::trace_prepare(s->view, &s->plan);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+  {  // per-scene memory pool for per-call scratch; it keeps freed memory for reuse
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = s->device;
+    e = cudaMemPoolCreate(&s->plan.pool, &props);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemPoolCreate");
+    uint64_t keep = UINT64_MAX;
+    e = cudaMemPoolSetAttribute(s->plan.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemPoolSetAttribute");
+  }
   {  // origin quantisation box of the coherence sort: union of the per-kind root boxes
     double lo[3] = {std::numeric_limits<double>::max(), std::numeric_limits<double>::max(),
                     std::numeric_limits<double>::max()};
@@ -353,7 +365,7 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
     io.error_word = s->slots + kStickyWord;  // sticky, read by bzr_scene_check
     cudaError_t e = cudaSuccess;
     if (!t) {  // the passes carry the closest distance in t: stream-ordered scratch
-      e = cudaMallocAsync(reinterpret_cast<void **>(&io.t), 8 * n, st);
+      e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&io.t), 8 * n, s->plan.pool, st);
       if (e != cudaSuccess) return fail(BZR_ENOMEM, "distance scratch allocation failed");
     }
     e = bzr::launch_trace(s->view, io, mode, s->plan, st, counters, totals);

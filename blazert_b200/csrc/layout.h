@@ -55,7 +55,7 @@ struct KindView {
   int present = 0;
   int mixed_ok = 0;                 // all boxes finite: the FP32 path may be used
   double root_box[6] = {0, 0, 0, 0, 0, 0};  // (lo.x, hi.x, lo.y, hi.y, lo.z, hi.z)
-  float root_box32[6] = {0, 0, 0, 0, 0, 0};
+  float coord_max = 0.0f;           // largest |coordinate| of any box (mixed-mode error bound)
 };
 
 struct SceneView {

@@ -392,12 +392,13 @@ KindImage flatten(const HostScene &s, int kind) {
     const TreeNode &root = t.nodes[0];
     img.root_ref = ref_of(0);
     if (!finite_box(root)) img.mixed_ok = false;
+    double cmax = 0.0;
     for (int k = 0; k < 3; ++k) {
       img.root_box[2 * k] = root.mn[k];
       img.root_box[2 * k + 1] = root.mx[k];
-      img.root_box32[2 * k] = round_down(root.mn[k]);
-      img.root_box32[2 * k + 1] = round_up(root.mx[k]);
+      cmax = std::max(cmax, std::max(std::abs(root.mn[k]), std::abs(root.mx[k])));
     }
+    img.coord_max = round_up(cmax);
   }
   // Leaf-ordered primitives.
   const size_t np = t.leaf_prims.size();

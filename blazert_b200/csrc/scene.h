@@ -76,7 +76,7 @@ struct KindImage {
   uint32_t n_internal = 0;
   uint32_t root_ref = 0;
   double root_box[6] = {0, 0, 0, 0, 0, 0};
-  float root_box32[6] = {0, 0, 0, 0, 0, 0};
+  float coord_max = 0.0f;  // largest |coordinate| of the root box, rounded up
   bool mixed_ok = true;
 };
 

@@ -43,7 +43,7 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 // One kind over the whole batch.  first: this pass writes the whole output record.
 // COUNT: also sums the work counters into totals[8] (box tests per kind, then primitive
 // tests per kind).
-template <int KIND, bool COUNT>
+template <int KIND, bool COUNT, bool MIXED>
 __global__ void __launch_bounds__(kTraceThreads)
     trace_kind_kernel(SceneView S, RayIO io, int first, uint32_t *work_counter,
                       unsigned long long *totals) {
@@ -62,6 +62,8 @@ __global__ void __launch_bounds__(kTraceThreads)
   bool active = false;
   uint32_t i = 0;
   Ray r;
+  RayF f;
+  bool use32 = false;
   KState st;
   Trav tv;
   Counts cnt = {};
@@ -82,6 +84,10 @@ __global__ void __launch_bounds__(kTraceThreads)
           active = true;
           r = make_ray(io.org + 3 * size_t(i), io.dir + 3 * size_t(i), io.tmin ? io.tmin[i] : 0.0,
                        io.tmax ? io.tmax[i] : kDblMax);
+          if (MIXED) {
+            f = make_ray_f(r, K.coord_max);
+            use32 = K.mixed_ok && f.ok;
+          }
           trav_begin<KIND, COUNT>(K, r, st, tv, &cnt);
         }
       }
@@ -95,8 +101,13 @@ __global__ void __launch_bounds__(kTraceThreads)
     }
     if (!__any_sync(kFull, active)) break;
     if (active) {
-      if (tv.live) trav_to_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, io.error_word, &cnt);
-      if (tv.live) trav_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, io.error_word, &cnt);
+      if (MIXED && use32) {
+        if (tv.live) trav_to_leaf32<KIND, COUNT>(K, r, f, st, tv, sk, tid, io.error_word, &cnt);
+        if (tv.live) trav_leaf32<KIND, COUNT>(K, r, f, st, tv, sk, tid, io.error_word, &cnt);
+      } else {
+        if (tv.live) trav_to_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, io.error_word, &cnt);
+        if (tv.live) trav_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, io.error_word, &cnt);
+      }
       if (!tv.live) {
         finalize_kind<KIND>(S, r, st, i, first != 0, io.t, io.uv, io.normal, io.prim, io.geom,
                             io.hit);
@@ -194,28 +205,37 @@ __global__ void sort_scatter_kernel(uint32_t n, const uint32_t *keys, uint32_t *
 }
 
 template <int KIND, bool COUNT>
-cudaError_t launch_kind(const SceneView &S, const RayIO &io, int first, int blocks,
+cudaError_t launch_kind(const SceneView &S, const RayIO &io, int mode, int first, int blocks,
                         cudaStream_t stream, uint32_t *counter, unsigned long long *totals) {
   const size_t smem = trace_smem_bytes(S.stack_cap, kTraceThreads);
-  trace_kind_kernel<KIND, COUNT><<<blocks, kTraceThreads, smem, stream>>>(S, io, first, counter,
-                                                                         totals);
+  if (mode == kModeMixed)
+    trace_kind_kernel<KIND, COUNT, true><<<blocks, kTraceThreads, smem, stream>>>(
+        S, io, first, counter, totals);
+  else
+    trace_kind_kernel<KIND, COUNT, false><<<blocks, kTraceThreads, smem, stream>>>(
+        S, io, first, counter, totals);
   return cudaGetLastError();
 }
 
 template <int KIND>
-cudaError_t prepare_kind(uint32_t stack_cap, int sms, int *blocks) {
+cudaError_t prepare_kind(uint32_t stack_cap, int sms, int *blocks, int *blocks32) {
   const size_t smem = trace_smem_bytes(stack_cap, kTraceThreads);
-  cudaError_t e = cudaFuncSetAttribute(trace_kind_kernel<KIND, false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  const void *fns[4] = {reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, false>),
+                        reinterpret_cast<const void *>(trace_kind_kernel<KIND, true, false>),
+                        reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, true>),
+                        reinterpret_cast<const void *>(trace_kind_kernel<KIND, true, true>)};
+  for (const void *fn : fns) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+  }
+  int per_sm = 0, per_sm32 = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fns[0], kTraceThreads, smem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(trace_kind_kernel<KIND, true>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (e != cudaSuccess) return e;
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kind_kernel<KIND, false>,
-                                                    kTraceThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, fns[2], kTraceThreads, smem);
   if (e != cudaSuccess) return e;
   *blocks = sms * (per_sm > 0 ? per_sm : 1);
+  *blocks32 = sms * (per_sm32 > 0 ? per_sm32 : 1);
   return cudaSuccess;
 }
 
@@ -232,12 +252,17 @@ cudaError_t trace_prepare(const SceneView &S, LaunchPlan *plan) {
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
   plan->sms = sms;
-  if ((e = prepare_kind<kMesh>(S.stack_cap, sms, &plan->blocks[kMesh])) != cudaSuccess) return e;
-  if ((e = prepare_kind<kSpheres>(S.stack_cap, sms, &plan->blocks[kSpheres])) != cudaSuccess)
+  if ((e = prepare_kind<kMesh>(S.stack_cap, sms, &plan->blocks[kMesh],
+                               &plan->blocks32[kMesh])) != cudaSuccess)
     return e;
-  if ((e = prepare_kind<kPlanes>(S.stack_cap, sms, &plan->blocks[kPlanes])) != cudaSuccess)
+  if ((e = prepare_kind<kSpheres>(S.stack_cap, sms, &plan->blocks[kSpheres],
+                                  &plan->blocks32[kSpheres])) != cudaSuccess)
     return e;
-  return prepare_kind<kCylinders>(S.stack_cap, sms, &plan->blocks[kCylinders]);
+  if ((e = prepare_kind<kPlanes>(S.stack_cap, sms, &plan->blocks[kPlanes],
+                                 &plan->blocks32[kPlanes])) != cudaSuccess)
+    return e;
+  return prepare_kind<kCylinders>(S.stack_cap, sms, &plan->blocks[kCylinders],
+                                  &plan->blocks32[kCylinders]);
 }
 
 int trace_passes(const SceneView &S) {
@@ -248,15 +273,14 @@ int trace_passes(const SceneView &S) {
 
 cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const LaunchPlan &plan,
                          cudaStream_t stream, uint32_t *counters, unsigned long long *totals) {
-  (void)mode;
   cudaError_t e = cudaMemsetAsync(counters, 0, kNumKinds * sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
   RayIO sorted = io;
   uint32_t *scratch = nullptr;
   if (plan.sort.enabled && io.n >= plan.sort_min_rays && trace_passes(S) > 0) {
     const size_t nb = size_t(1) << kSortBits;
-    e = cudaMallocAsync(reinterpret_cast<void **>(&scratch),
-                        (2 * size_t(io.n) + nb) * sizeof(uint32_t), stream);
+    e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&scratch),
+                                (2 * size_t(io.n) + nb) * sizeof(uint32_t), plan.pool, stream);
     if (e != cudaSuccess) return e;
     uint32_t *keys = scratch, *perm = scratch + io.n, *counts = scratch + 2 * size_t(io.n);
     e = cudaMemsetAsync(counts, 0, nb * sizeof(uint32_t), stream);
@@ -272,24 +296,24 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
   int first = 1;
   for (int k = 0; k < kNumKinds; ++k) {
     if (!S.k[k].present || S.k[k].n_prims == 0) continue;
-    const int b = plan.blocks[k];
+    const int b = mode == kModeMixed ? plan.blocks32[k] : plan.blocks[k];
     uint32_t *c = counters + k;
     switch (k) {
       case kMesh:
-        e = totals ? launch_kind<kMesh, true>(S, run, first, b, stream, c, totals)
-                   : launch_kind<kMesh, false>(S, run, first, b, stream, c, nullptr);
+        e = totals ? launch_kind<kMesh, true>(S, run, mode, first, b, stream, c, totals)
+                   : launch_kind<kMesh, false>(S, run, mode, first, b, stream, c, nullptr);
         break;
       case kSpheres:
-        e = totals ? launch_kind<kSpheres, true>(S, run, first, b, stream, c, totals)
-                   : launch_kind<kSpheres, false>(S, run, first, b, stream, c, nullptr);
+        e = totals ? launch_kind<kSpheres, true>(S, run, mode, first, b, stream, c, totals)
+                   : launch_kind<kSpheres, false>(S, run, mode, first, b, stream, c, nullptr);
         break;
       case kPlanes:
-        e = totals ? launch_kind<kPlanes, true>(S, run, first, b, stream, c, totals)
-                   : launch_kind<kPlanes, false>(S, run, first, b, stream, c, nullptr);
+        e = totals ? launch_kind<kPlanes, true>(S, run, mode, first, b, stream, c, totals)
+                   : launch_kind<kPlanes, false>(S, run, mode, first, b, stream, c, nullptr);
         break;
       default:
-        e = totals ? launch_kind<kCylinders, true>(S, run, first, b, stream, c, totals)
-                   : launch_kind<kCylinders, false>(S, run, first, b, stream, c, nullptr);
+        e = totals ? launch_kind<kCylinders, true>(S, run, mode, first, b, stream, c, totals)
+                   : launch_kind<kCylinders, false>(S, run, mode, first, b, stream, c, nullptr);
         break;
     }
     if (e != cudaSuccess) return e;

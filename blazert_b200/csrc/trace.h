@@ -10,6 +10,8 @@
 namespace bzr {
 
 constexpr int kTraceThreads = 128;
+constexpr int kModeFp64 = 0;   // BZR_MODE_FP64
+constexpr int kModeMixed = 1;  // BZR_MODE_MIXED
 
 // Device pointers of one batch.  tmin / tmax may be null (0 and DBL_MAX); each output except t
 // may be null.  error_word collects kErr* bits.
@@ -43,9 +45,11 @@ struct RaySort {
 // Grid of each per-kind persistent kernel: SMs x resident blocks per SM.
 struct LaunchPlan {
   int sms = 0;
-  int blocks[kNumKinds] = {0, 0, 0, 0};
+  int blocks[kNumKinds] = {0, 0, 0, 0};    // FP64 kernels
+  int blocks32[kNumKinds] = {0, 0, 0, 0};  // mixed-precision kernels
   RaySort sort;
   uint32_t sort_min_rays = 1u << 16;  // smaller batches are traced in their own order
+  cudaMemPool_t pool = nullptr;       // stream-ordered scratch (keeps its memory mapped)
 };
 
 size_t trace_smem_bytes(uint32_t stack_cap, int threads);
@@ -55,7 +59,7 @@ int trace_passes(const SceneView &S);
 // Queues a batch on `stream`: one kernel per kind present, merged into io's outputs.  io.t must
 // be non-null when trace_passes(S) > 1 (it carries the closest distance between passes).
 // When plan.sort.enabled and the batch has at least plan.sort_min_rays rays, a coherence sort
-// runs first (scratch from the stream-ordered allocator).
+// runs first (scratch from plan.pool, stream-ordered).
 // counters: kNumKinds device words, zeroed here.  totals (device, 8 x uint64, or null): when
 // given, the counting kernels add per kind the box tests (totals[0..3]) and primitive tests
 // (totals[4..7]) of every ray.

@@ -18,6 +18,8 @@
 #else
 #include <vector_types.h>
 #include <vector_functions.h>
+using std::isfinite;
+using std::isnan;
 #define BZR_HD inline
 #define BZR_NOINLINE inline
 #define BZR_INF (__builtin_inf())
@@ -477,6 +479,236 @@ BZR_HD bool traverse(const KindView &K, const Ray &r, KState &st, const Stack &s
   while (tv.live) {
     trav_to_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, err, cnt);
     if (tv.live) trav_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, err, cnt);
+  }
+  return st.hit < r.tmax;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Mixed precision (BZR_MODE_MIXED): slab tests in FP32 on the 64-byte nodes, with every
+// decision equal to the FP64 one.
+//
+// For an eligible ray, every FP32 entry/exit distance a32 = (fl32(plane) - fl32(o)) * fl32(inv)
+// is within delta of the FP64 value of the reference's slab test:
+//   |a32 - a64| <= 2^-21 * max|inv| * (coord_max + max|o|)  (+ tiny absolute terms),
+// from the relative errors of the five FP32 roundings (<= 3 * 2^-23 in all) and the FP64 ones
+// (l1 = 1 + 2^-50 included).  A child is accepted or rejected in FP32 only when the FP32
+// comparison holds with that margin (sums rounded outward); otherwise its exact FP64 test
+// runs on the FP64 node.  The pop-time comparison of the entry distance with the hit distance
+// is decided the same way, re-testing the child in FP64 when it falls inside the margin.  So
+// the accepted nodes, and hence the leaves, primitive tests and results, are exactly the FP64
+// path's.  Rays that are not eligible (a zero, tiny or non-finite direction component, huge
+// coordinates, non-finite tmin, NaN tmax) and kinds with a non-finite box use the FP64 path.
+struct RayF {
+  float o[3], inv[3];
+  float tmin, delta;
+  bool ok;
+};
+
+BZR_HD float fadd_up(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fadd_ru(a, b);
+#else
+  return nextafterf(float(double(a) + double(b)), __builtin_inff());  // conservative
+#endif
+}
+BZR_HD float fadd_down(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fadd_rd(a, b);
+#else
+  return nextafterf(float(double(a) + double(b)), -__builtin_inff());
+#endif
+}
+
+BZR_HD RayF make_ray_f(const Ray &r, float coord_max) {
+  RayF f;
+  const double inv[3] = {r.inv.x, r.inv.y, r.inv.z}, o[3] = {r.o.x, r.o.y, r.o.z};
+  double imax = 0.0, imin = 1e300, omax = 0.0;
+  bool ok = isfinite(r.tmin) && !isnan(r.tmax) && isfinite(coord_max) &&
+            coord_max <= 1e18f;
+  for (int a = 0; a < 3; ++a) {
+    const double ai = fabs(inv[a]);
+    ok = ok && isfinite(inv[a]) && ai > 0.0 && isfinite(o[a]) && fabs(o[a]) <= 1e18;
+    imax = ai > imax ? ai : imax;
+    imin = ai < imin ? ai : imin;
+    omax = fabs(o[a]) > omax ? fabs(o[a]) : omax;
+    f.o[a] = float(o[a]);
+    f.inv[a] = float(inv[a]);
+  }
+  ok = ok && imax <= 16384.0 * imin && imax <= 1e18;
+  const double d = 4.76837158203125e-07 /* 2^-21 */ * (imax * (double(coord_max) + omax) + fabs(r.tmin)) +
+                   1e-30 * (1.0 + imax);
+  f.tmin = float(r.tmin);
+  f.delta = ok ? nextafterf(float(d), __builtin_inff()) : 0.0f;
+  f.ok = ok && isfinite(f.delta);
+  return f;
+}
+
+// FP32 slab test of one box given as (lo, hi) pairs per axis: 1 accept for some hit distance,
+// 0 reject for every hit distance, 2 undecided in FP32.  mn receives the FP32 entry distance.
+BZR_HD int box_test32(float lx, float hx, float ly, float hy, float lz, float hz, const RayF &f,
+                      const Ray &r, float &mn) {
+  const float ax = ((r.sx ? hx : lx) - f.o[0]) * f.inv[0];
+  const float bx = ((r.sx ? lx : hx) - f.o[0]) * f.inv[0];
+  const float ay = ((r.sy ? hy : ly) - f.o[1]) * f.inv[1];
+  const float by = ((r.sy ? ly : hy) - f.o[1]) * f.inv[1];
+  const float az = ((r.sz ? hz : lz) - f.o[2]) * f.inv[2];
+  const float bz = ((r.sz ? lz : hz) - f.o[2]) * f.inv[2];
+  mn = fmaxf(fmaxf(f.tmin, ax), fmaxf(ay, az));
+  const float ex = fminf(fminf(bx, by), bz);
+  if (fadd_up(mn, f.delta) <= fadd_down(ex, -f.delta)) return 1;
+  if (fadd_down(mn, -f.delta) > fadd_up(ex, f.delta)) return 0;
+  return 2;
+}
+
+// Exact FP64 slab test of child `slot` of FP64 node `node`.
+BZR_HD bool child_test64(const KindView &K, uint32_t node, int slot, const Ray &r, double &key) {
+  const double *nd = K.nodes64 + size_t(node) * kNode64Doubles + 6 * slot;
+  return box_test(ld2(nd), ld2(nd + 2), ld2(nd + 4), r, key);
+}
+
+// Mixed stack entry: ref in sk.ref; the key slot holds {float key, uint32 aux} with
+// aux = parent << 2 | slot << 1 | exact.  exact: key is fl32 of the FP64 entry distance.
+BZR_HD void push32(const Stack &sk, uint32_t tid, uint32_t sp, uint32_t ref, float key,
+                   uint32_t aux) {
+  uint32_t *w = reinterpret_cast<uint32_t *>(sk.key + sp * sk.stride + tid);
+  float kk = key;
+  uint32_t kb;
+  std::memcpy(&kb, &kk, 4);
+  w[0] = kb;
+  w[1] = aux;
+  sk.ref[sp * sk.stride + tid] = ref;
+}
+
+// Pop-time decision !(key64 > h) from the FP32 key and its margin; -1 when undecided.
+BZR_HD int key_decide(float key, float margin, double h) {
+  if (double(fadd_up(key, margin)) <= h) return 1;
+  if (double(fadd_down(key, -margin)) > h) return 0;
+  return -1;
+}
+BZR_HD float exact_margin(float key) {
+  return nextafterf(fabsf(key) * 1.1920928955078125e-07f, __builtin_inff()) + 1.4e-45f;
+}
+
+template <int KIND>
+BZR_HD void trav_pop32(const KindView &K, const Ray &r, const RayF &f, Trav &tv, const KState &st,
+                       const Stack &sk, uint32_t tid) {
+  while (tv.sp > 0) {
+    --tv.sp;
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(sk.key + tv.sp * sk.stride + tid);
+    const uint32_t kb = w[0], aux = w[1];
+    float key;
+    std::memcpy(&key, &kb, 4);
+    int d = key_decide(key, (aux & 1u) ? exact_margin(key) : f.delta, st.hit);
+    if (d < 0) {
+      double k64;
+      child_test64(K, aux >> 2, int((aux >> 1) & 1u), r, k64);
+      d = !(k64 > st.hit);
+    }
+    if (d) {
+      tv.cur = sk.ref[tv.sp * sk.stride + tid];
+      return;
+    }
+  }
+  tv.live = false;
+}
+
+template <int KIND, bool COUNT>
+BZR_HD void trav_to_leaf32(const KindView &K, const Ray &r, const RayF &f, const KState &st,
+                           Trav &tv, const Stack &sk, uint32_t tid, uint32_t *err, Counts *cnt) {
+  while (tv.live && !(tv.cur & kLeafBit)) {
+    if (tv.cur >= K.n_internal) {
+      flag_error(err, kErrNodeIndex);
+      tv.live = false;
+      return;
+    }
+    const float *nf = K.nodes32 + size_t(tv.cur) * kNode32Floats;
+    const float4 q0 = ldg(reinterpret_cast<const float4 *>(nf));
+    const float4 q1 = ldg(reinterpret_cast<const float4 *>(nf + 4));
+    const float4 q2 = ldg(reinterpret_cast<const float4 *>(nf + 8));
+    const uint4 meta = ldg(reinterpret_cast<const uint4 *>(nf + 12));
+    if (COUNT) cnt->box[KIND] += 2;
+    float m0, m1;
+    int d0 = box_test32(q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, f, r, m0);
+    int d1 = box_test32(q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, f, r, m1);
+    bool e0 = false, e1 = false;
+    double k0 = 0.0, k1 = 0.0;
+    if (d0 == 2) {
+      d0 = child_test64(K, tv.cur, 0, r, k0) ? 1 : 0;
+      e0 = true;
+    }
+    if (d1 == 2) {
+      d1 = child_test64(K, tv.cur, 1, r, k1) ? 1 : 0;
+      e1 = true;
+    }
+    const unsigned near = meta.z == 0 ? r.sx : (meta.z == 1 ? r.sy : r.sz);
+    const int dn = near ? d1 : d0, df = near ? d0 : d1;
+    const bool en = near ? e1 : e0, ef = near ? e0 : e1;
+    const double kn = near ? k1 : k0, kf = near ? k0 : k1;
+    const float mnn = near ? m1 : m0, mnf = near ? m0 : m1;
+    const uint32_t rn = near ? meta.y : meta.x, rf = near ? meta.x : meta.y;
+    if (df) {
+      if (tv.sp >= sk.cap) {
+        flag_error(err, kErrStack);
+        tv.live = false;
+        return;
+      }
+      push32(sk, tid, tv.sp, rf, ef ? float(kf) : mnf,
+             (tv.cur << 2) | ((near ? 0u : 1u) << 1) | (ef ? 1u : 0u));
+      ++tv.sp;
+    }
+    bool take_near = false;
+    if (dn) {
+      if (en) {
+        take_near = !(kn > st.hit);
+      } else {
+        const int d = key_decide(mnn, f.delta, st.hit);
+        if (d >= 0) {
+          take_near = d;
+        } else {
+          double k;
+          child_test64(K, tv.cur, int(near), r, k);
+          take_near = !(k > st.hit);
+        }
+      }
+    }
+    if (take_near) {
+      tv.cur = rn;
+    } else {
+      trav_pop32<KIND>(K, r, f, tv, st, sk, tid);
+    }
+  }
+}
+
+template <int KIND, bool COUNT>
+BZR_HD void trav_leaf32(const KindView &K, const Ray &r, const RayF &f, KState &st, Trav &tv,
+                        const Stack &sk, uint32_t tid, uint32_t *err, Counts *cnt) {
+  uint32_t pos = tv.cur & kIdMask;
+  for (;;) {
+    if (pos >= K.n_prims) {
+      flag_error(err, kErrPrimIndex);
+      tv.live = false;
+      return;
+    }
+    const uint32_t id = ldg(K.prim_ids + pos);
+    if (COUNT) cnt->prim[KIND] += 1;
+    isect<KIND>(K.payload, pos, r, st);
+    if (id & kLastBit) break;
+    ++pos;
+  }
+  trav_pop32<KIND>(K, r, f, tv, st, sk, tid);
+}
+
+// Whole traversal of one kind in mixed precision (FP64 for rays or kinds not eligible).
+template <int KIND, bool COUNT>
+BZR_HD bool traverse_mixed(const KindView &K, const Ray &r, KState &st, const Stack &sk,
+                           uint32_t tid, uint32_t *err, Counts *cnt) {
+  const RayF f = make_ray_f(r, K.coord_max);
+  if (!(K.mixed_ok && f.ok)) return traverse<KIND, COUNT>(K, r, st, sk, tid, err, cnt);
+  Trav tv;
+  trav_begin<KIND, COUNT>(K, r, st, tv, cnt);
+  while (tv.live) {
+    trav_to_leaf32<KIND, COUNT>(K, r, f, st, tv, sk, tid, err, cnt);
+    if (tv.live) trav_leaf32<KIND, COUNT>(K, r, f, st, tv, sk, tid, err, cnt);
   }
   return st.hit < r.tmax;
 }

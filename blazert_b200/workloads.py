@@ -171,7 +171,9 @@ def _unit_sphere(rng, n):
 
 
 # ------------------------------------------------------------------------------------ workloads
-def icosphere_pinhole(level=4, width=512, height=512, fov_deg=60.0):
+def icosphere_pinhole(level=4, width=512, height=512, fov_deg=60.0, n_rays=None):
+    if n_rays:  # square image with about n_rays pixels
+        width = height = max(1, int(round(math.sqrt(n_rays))))
     verts, faces = icosphere(level)
     scene = SceneSpec().add_mesh(verts, faces)
     tan = math.tan(math.radians(fov_deg) / 2.0)

@@ -1,0 +1,190 @@
+// blazert_b200 C++ facade: blazeRT's Scene API (blazert/scene.h, blazert/ray.h) over the
+// C-ABI of libblazert_b200.so, so that reference-style call sites compile with a namespace
+// change.  Header-only; link with -lblazert_b200.
+//
+// Types mirror the reference's aliases (blazert/datatypes.h:31-59) with standard containers:
+// Vec3r<T> = std::array<T, 3>, Vec3rList<T> = std::vector<Vec3r<T>>, Mat3r<T> a row-major 3x3
+// with nested-brace construction.  Only T = double is supported (the GPU path is FP64).
+#pragma once
+
+#include <array>
+#include <cstddef>
+#include <cstdint>
+#include <initializer_list>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../blazert_b200.h"
+
+namespace blazert_b200 {
+
+template <typename T>
+using Vec3r = std::array<T, 3>;
+template <typename T>
+using Vec2r = std::array<T, 2>;
+using Vec3ui = std::array<unsigned int, 3>;
+template <typename T>
+using Vec3rList = std::vector<Vec3r<T>>;
+using Vec3iList = std::vector<Vec3ui>;
+
+template <typename T>
+struct Mat3r {
+  T m[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  Mat3r() = default;
+  Mat3r(std::initializer_list<std::initializer_list<T>> rows) {
+    int i = 0;
+    for (const auto &row : rows) {
+      int j = 0;
+      for (const T &x : row) m[i][j++] = x;
+      ++i;
+    }
+  }
+  static Mat3r identity() { return Mat3r{{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}; }
+  T &operator()(size_t i, size_t j) { return m[i][j]; }
+  const T &operator()(size_t i, size_t j) const { return m[i][j]; }
+};
+template <typename T>
+using Mat3rList = std::vector<Mat3r<T>>;
+
+// blazert/ray.h:56-65: the direction need not be unit length.
+template <typename T>
+struct Ray {
+  Vec3r<T> origin;
+  Vec3r<T> direction;
+  T min_hit_distance = T(0);
+  T max_hit_distance = std::numeric_limits<T>::max();
+  Ray(const Vec3r<T> &o, const Vec3r<T> &d, T tmin = T(0),
+      T tmax = std::numeric_limits<T>::max())
+      : origin(o), direction(d), min_hit_distance(tmin), max_hit_distance(tmax) {}
+};
+
+// blazert/ray.h:72-85, with the reference's defaults.
+template <typename T>
+struct RayHit {
+  Vec3r<T> normal{0, 0, 0};
+  Vec2r<T> uv{0, 0};
+  T hit_distance = std::numeric_limits<T>::max();
+  unsigned int prim_id = static_cast<unsigned int>(-1);
+  unsigned int geom_id = static_cast<unsigned int>(-1);
+};
+
+// blazert/bvh/options.h:15-29
+template <typename T>
+struct BVHBuildOptions {
+  unsigned int min_leaf_primitives = 4;
+  unsigned int max_tree_depth = 28;
+  unsigned int bin_size = 64;
+};
+
+class Error : public std::runtime_error {
+ public:
+  Error(int code, const std::string &what) : std::runtime_error(what), code(code) {}
+  int code;
+};
+
+inline void check(int rc) {
+  if (rc != BZR_OK) throw Error(rc, bzr_last_error_string());
+}
+
+// blazert/scene.h:38-115
+template <typename T>
+class Scene {
+  static_assert(std::is_same<T, double>::value, "blazert_b200 scenes are double precision");
+
+ public:
+  BVHBuildOptions<T> build_options;
+
+  Scene() { check(bzr_scene_create(&s_)); }
+  ~Scene() { bzr_scene_destroy(s_); }
+  Scene(const Scene &) = delete;
+  Scene &operator=(const Scene &) = delete;
+
+  // Each returns the geom id, or static_cast<unsigned>(-1) for a second add of a kind or an
+  // add after commit (as the reference does); other errors throw blazert_b200::Error.
+  unsigned int add_mesh(const Vec3rList<T> &vertices, const Vec3iList &triangles) {
+    uint32_t id;
+    return added(bzr_add_mesh(s_, flat(vertices), vertices.size(),
+                              reinterpret_cast<const uint32_t *>(triangles.data()),
+                              triangles.size(), &id), id);
+  }
+  unsigned int add_spheres(const Vec3rList<T> &centers, const std::vector<T> &radii) {
+    uint32_t id;
+    if (centers.size() != radii.size()) throw Error(BZR_EINVAL, "centers and radii differ");
+    return added(bzr_add_spheres(s_, flat(centers), radii.data(), radii.size(), &id), id);
+  }
+  unsigned int add_planes(const Vec3rList<T> &centers, const std::vector<T> &dxs,
+                          const std::vector<T> &dys, const Mat3rList<T> &rotations) {
+    uint32_t id;
+    const size_t n = centers.size();
+    if (dxs.size() != n || dys.size() != n || rotations.size() != n)
+      throw Error(BZR_EINVAL, "plane arrays differ in length");
+    return added(bzr_add_planes(s_, flat(centers), dxs.data(), dys.data(), flat(rotations), n,
+                                &id), id);
+  }
+  unsigned int add_cylinders(const Vec3rList<T> &centers, const std::vector<T> &semi_axes_a,
+                             const std::vector<T> &semi_axes_b, const std::vector<T> &heights,
+                             const Mat3rList<T> &rotations) {
+    uint32_t id;
+    const size_t n = centers.size();
+    if (semi_axes_a.size() != n || semi_axes_b.size() != n || heights.size() != n ||
+        rotations.size() != n)
+      throw Error(BZR_EINVAL, "cylinder arrays differ in length");
+    return added(bzr_add_cylinders(s_, flat(centers), semi_axes_a.data(), semi_axes_b.data(),
+                                   heights.data(), flat(rotations), n, &id), id);
+  }
+
+  bool commit() {
+    const bzr_build_options o{build_options.min_leaf_primitives, build_options.max_tree_depth,
+                              build_options.bin_size};
+    check(bzr_commit(s_, &o));
+    return true;
+  }
+
+  // Batched query, structure of arrays (see bzr_intersectN); returns nothing, fills outputs.
+  void intersectN(size_t n, const T *origins, const T *directions, const T *tmin,
+                  const T *tmax, T *hit_distance, T *uv, T *normal, uint32_t *prim_id,
+                  uint32_t *geom_id, uint8_t *hit, int mode = BZR_MODE_FP64,
+                  void *stream = nullptr) const {
+    check(bzr_intersectN(s_, n, origins, directions, tmin, tmax, hit_distance, uv, normal,
+                         prim_id, geom_id, hit, mode, stream));
+  }
+
+  const bzr_scene *handle() const { return s_; }
+
+ private:
+  template <typename V>
+  static const T *flat(const std::vector<V> &v) {
+    static_assert(sizeof(V) % sizeof(T) == 0, "contiguous scalar storage");
+    return reinterpret_cast<const T *>(v.data());
+  }
+  static unsigned int added(int rc, uint32_t id) {
+    if (rc == BZR_ESTATE) return static_cast<unsigned int>(-1);
+    check(rc);
+    return id;
+  }
+  bzr_scene *s_ = nullptr;
+};
+
+// blazert/scene.h:161-210.  Starts from a default RayHit: the reference compares later kinds
+// against the caller's incoming rayhit.hit_distance (scene.h:181), which equals the default
+// for the fresh RayHit every reference example and test passes.
+template <typename T>
+inline bool intersect1(const Scene<T> &scene, const Ray<T> &ray, RayHit<T> &rayhit) {
+  bzr_rayhit rh;
+  int hit = 0;
+  check(bzr_intersect1(scene.handle(), ray.origin.data(), ray.direction.data(),
+                       ray.min_hit_distance, ray.max_hit_distance, &rh, &hit));
+  if (hit) {
+    rayhit.normal = {rh.normal[0], rh.normal[1], rh.normal[2]};
+    rayhit.uv = {rh.uv[0], rh.uv[1]};
+    rayhit.hit_distance = rh.hit_distance;
+    rayhit.prim_id = rh.prim_id;
+    rayhit.geom_id = rh.geom_id;
+  }
+  return hit != 0;
+}
+
+}  // namespace blazert_b200

@@ -68,7 +68,7 @@ void *emu_scene_create(const int *order, int n_order, const double *verts, long 
     v.root_ref = im.root_ref;
     v.mixed_ok = im.mixed_ok;
     std::memcpy(v.root_box, im.root_box, sizeof v.root_box);
-    std::memcpy(v.root_box32, im.root_box32, sizeof v.root_box32);
+    v.coord_max = im.coord_max;
   }
   e->view.faces = s.faces.data();
   e->view.vert_n = s.vert_n.data();
@@ -113,7 +113,8 @@ long emu_scene_tree(void *h, int kind, double *bmin, double *bmax, uint32_t *lea
 template <int KIND>
 static void emu_pass(const bzr::SceneView &view, long n, const double *org, const double *dir,
                      const double *tmin, const double *tmax, bool first, double *t, double *uv,
-                     double *normal, uint32_t *prim, uint32_t *geom, uint8_t *hit, uint32_t &err) {
+                     double *normal, uint32_t *prim, uint32_t *geom, uint8_t *hit, uint32_t &err,
+                     int mode) {
   uint32_t e = 0;
 #pragma omp parallel reduction(| : e)
   {
@@ -129,7 +130,10 @@ static void emu_pass(const bzr::SceneView &view, long n, const double *org, cons
       const bzr::Ray r = bzr::make_ray(org + 3 * i, dir + 3 * i, tmin ? tmin[i] : 0.0,
                                        tmax ? tmax[i] : 1.7976931348623157e308);
       bzr::KState st;
-      bzr::traverse<KIND, false>(view.k[KIND], r, st, sk, 0, &e, nullptr);
+      if (mode == 1)
+        bzr::traverse_mixed<KIND, false>(view.k[KIND], r, st, sk, 0, &e, nullptr);
+      else
+        bzr::traverse<KIND, false>(view.k[KIND], r, st, sk, 0, &e, nullptr);
       bzr::finalize_kind<KIND>(view, r, st, uint64_t(i), first, t, uv, normal, prim, geom, hit);
     }
   }
@@ -141,7 +145,7 @@ extern "C" {
 uint32_t emu_scene_intersect(void *h, long n, const double *org, const double *dir,
                              const double *tmin, const double *tmax, double *t, double *uv,
                              double *normal, uint32_t *prim, uint32_t *geom, uint8_t *hit,
-                             uint32_t stack_cap_override) {
+                             uint32_t stack_cap_override, int mode) {
   const Emu *e = static_cast<Emu *>(h);
   bzr::SceneView view = e->view;
   if (stack_cap_override) view.stack_cap = stack_cap_override;
@@ -150,10 +154,10 @@ uint32_t emu_scene_intersect(void *h, long n, const double *org, const double *d
   for (int k = 0; k < 4; ++k) {
     if (!view.k[k].present || view.k[k].n_prims == 0) continue;
     switch (k) {
-      case 0: emu_pass<0>(view, n, org, dir, tmin, tmax, first, t, uv, normal, prim, geom, hit, err); break;
-      case 1: emu_pass<1>(view, n, org, dir, tmin, tmax, first, t, uv, normal, prim, geom, hit, err); break;
-      case 2: emu_pass<2>(view, n, org, dir, tmin, tmax, first, t, uv, normal, prim, geom, hit, err); break;
-      case 3: emu_pass<3>(view, n, org, dir, tmin, tmax, first, t, uv, normal, prim, geom, hit, err); break;
+      case 0: emu_pass<0>(view, n, org, dir, tmin, tmax, first, t, uv, normal, prim, geom, hit, err, mode); break;
+      case 1: emu_pass<1>(view, n, org, dir, tmin, tmax, first, t, uv, normal, prim, geom, hit, err, mode); break;
+      case 2: emu_pass<2>(view, n, org, dir, tmin, tmax, first, t, uv, normal, prim, geom, hit, err, mode); break;
+      case 3: emu_pass<3>(view, n, org, dir, tmin, tmax, first, t, uv, normal, prim, geom, hit, err, mode); break;
     }
     first = false;
   }

@@ -40,7 +40,7 @@ def load():
         lib.emu_scene_tree.argtypes = _TREE_ARGS
         lib.emu_scene_intersect.restype = C.c_uint32
         lib.emu_scene_intersect.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _dp, _dp, _dp, _dp,
-                                            _dp, _u32p, _u32p, _u8p, C.c_uint32]
+                                            _dp, _u32p, _u32p, _u8p, C.c_uint32, C.c_int]
         lib.emu_prim_box.argtypes = [C.c_void_p, C.c_int, C.c_uint32, _dp, _dp, _dp]
         lib.emu_box_accept.argtypes = [_dp, _dp, _dp, _dp, C.c_double, C.c_double]
         _lib = lib
@@ -68,11 +68,12 @@ class EmuScene(_Base):
         assert rc == 0
         return mn, mx, c
 
-    def intersect(self, org, dirs, tmin=None, tmax=None, stack_cap=0):
+    def intersect(self, org, dirs, tmin=None, tmax=None, stack_cap=0, mode="fp64"):
         org, dirs, tmin, tmax, n = _rays(org, dirs, tmin, tmax)
         out = _outputs(n)
         out["error_word"] = int(self._lib.emu_scene_intersect(
             self._h, n, _ptr(org, _dp), _ptr(dirs, _dp), _ptr(tmin, _dp), _ptr(tmax, _dp),
             _ptr(out["t"], _dp), _ptr(out["uv"], _dp), _ptr(out["normal"], _dp),
-            _ptr(out["prim"], _u32p), _ptr(out["geom"], _u32p), _ptr(out["hit"], _u8p), stack_cap))
+            _ptr(out["prim"], _u32p), _ptr(out["geom"], _u32p), _ptr(out["hit"], _u8p), stack_cap,
+            1 if mode == "mixed" else 0))
         return out

@@ -11,21 +11,31 @@ from tests.helpers import mismatches
 from tests.scenes import edge_case_scenes
 
 
-@pytest.mark.parametrize("name", ["icosphere_pinhole", "mixed_primitives"])
-def test_workloads(name):
-    wl = W.WORKLOADS[name]() if name != "mixed_primitives" else W.mixed_primitives(n_rays=100_000)
+MODES = ["fp64", "mixed"]
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("name", ["icosphere_pinhole", "mixed_primitives", "heightfield"])
+def test_workloads(name, mode):
+    if name == "mixed_primitives":
+        wl = W.mixed_primitives(n_rays=100_000)
+    elif name == "heightfield":
+        wl = W.heightfield(n_rays=50_000, grid=256)
+    else:
+        wl = W.WORKLOADS[name]()
     R = wl.rays
     ref = Oracle(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax)
-    got = EmuScene(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax)
+    got = EmuScene(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax, mode=mode)
     assert got["error_word"] == 0
     assert mismatches(got, ref) == []
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("case", edge_case_scenes(), ids=lambda c: c[0])
-def test_edge_cases(case):
+def test_edge_cases(case, mode):
     _, spec, R = case
     ref = Oracle(spec).intersect(R.origins, R.directions, R.tmin, R.tmax)
-    got = EmuScene(spec).intersect(R.origins, R.directions, R.tmin, R.tmax)
+    got = EmuScene(spec).intersect(R.origins, R.directions, R.tmin, R.tmax, mode=mode)
     assert got["error_word"] == 0
     assert mismatches(got, ref) == []
 
@@ -36,9 +46,10 @@ def test_build_options():
     for opts in (dict(min_leaf=1, max_depth=28, bins=64), dict(min_leaf=8, max_depth=6, bins=16),
                  dict(min_leaf=2, max_depth=40, bins=3)):
         ref = Oracle(wl.scene, **opts).intersect(R.origins, R.directions)
-        got = EmuScene(wl.scene, **opts).intersect(R.origins, R.directions)
-        assert got["error_word"] == 0
-        assert mismatches(got, ref) == [], opts
+        for mode in MODES:
+            got = EmuScene(wl.scene, **opts).intersect(R.origins, R.directions, mode=mode)
+            assert got["error_word"] == 0
+            assert mismatches(got, ref) == [], (opts, mode)
 
 
 def test_stack_overflow_is_flagged_not_silent():

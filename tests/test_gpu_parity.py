@@ -29,10 +29,11 @@ def _run_both(wl, mode="fp64"):
     return ref, out_dev, out_host
 
 
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
 @pytest.mark.parametrize("name", ["icosphere_pinhole", "mixed_primitives"])
-def test_workload_bit_exact(name):
+def test_workload_bit_exact(name, mode):
     wl = W.WORKLOADS[name]()
-    ref, out_dev, out_host = _run_both(wl)
+    ref, out_dev, out_host = _run_both(wl, mode)
     assert ref["hit"].sum() > 0
     assert mismatches(out_dev, ref) == []
     assert mismatches(out_host, ref) == []
@@ -70,23 +71,24 @@ def test_sort_changes_speed_not_results():
     assert mismatches(outs[0], ref) == [] and mismatches(outs[1], ref) == []
 
 
-@pytest.mark.parametrize("mode", ["fp64"])
-def test_heightfield_full_size(mode):
-    """2,093,058-triangle heightfield, 8,388,608 secondary rays, against the oracle."""
+@pytest.fixture(scope="module")
+def heightfield_ref():
     wl = W.heightfield()
-    ref, out_dev, _ = _run_both_device_only(wl, mode)
-    assert mismatches(out_dev, ref) == []
+    R = wl.rays
+    return wl, Oracle(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax)
 
 
-def _run_both_device_only(wl, mode):
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_heightfield_full_size(mode, heightfield_ref):
+    """2,093,058-triangle heightfield, 8,388,608 secondary rays, against the oracle."""
     import torch
 
+    wl, ref = heightfield_ref
     R = wl.rays
-    ref = Oracle(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax)
     s = product_scene(wl.scene)
     dev = torch.device("cuda", 0)
     out = s.intersectN(torch.from_numpy(R.origins).to(dev), torch.from_numpy(R.directions).to(dev),
                        torch.from_numpy(R.tmin).to(dev), torch.from_numpy(R.tmax).to(dev), mode=mode)
     torch.cuda.synchronize()
     s.check()
-    return ref, out, None
+    assert mismatches(out, ref) == []
