@@ -81,6 +81,7 @@ def library():
         lib.bzr_scene_check.argtypes = [P, P, C.c_int, _u32p]
         lib.bzr_work_counts.argtypes = [P, C.c_size_t, P, P, P, P, C.POINTER(C.c_uint64), P]
         lib.bzr_scene_tune.argtypes = [P, C.c_int, C.c_int64]
+        lib.bzr_adjoint_hit.argtypes = [P, C.c_size_t] + [P] * 14 + [P]
         lib.bzr_scene_stats.argtypes = [P, C.c_int, C.POINTER(C.c_uint64), _u32p,
                                         C.POINTER(C.c_double)]
         lib.bzr_last_error_string.restype = C.c_char_p
@@ -323,6 +324,34 @@ class Scene:
             _check(self._lib.bzr_work_counts(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
                                              tot, None))
         return dict(box=[int(x) for x in tot[:4]], prim=[int(x) for x in tot[4:]])
+
+    def adjoint(self, origins, directions, fwd, grad_t=None, grad_uv=None, grad_normal=None,
+                n_vertices=0, n_spheres=0, stream=None):
+        """Gradients of the closest-hit outputs (bzr_adjoint_hit).  All tensors on the scene's
+        CUDA device; fwd is the dict returned by intersectN.  Returns dict of gradients:
+        origins, directions (n x 3), vertices (n_vertices x 3), centers (n_spheres x 3),
+        radii (n_spheres)."""
+        import torch
+
+        dev = origins.device
+        f64 = torch.float64
+        n = origins.shape[0]
+        g = dict(origins=torch.empty((n, 3), dtype=f64, device=dev),
+                 directions=torch.empty((n, 3), dtype=f64, device=dev),
+                 vertices=torch.empty((n_vertices, 3), dtype=f64, device=dev) if n_vertices else None,
+                 centers=torch.empty((n_spheres, 3), dtype=f64, device=dev) if n_spheres else None,
+                 radii=torch.empty(n_spheres, dtype=f64, device=dev) if n_spheres else None)
+        ptr = lambda a: None if a is None else a.contiguous().data_ptr()
+        keep = [origins.contiguous(), directions.contiguous()] + \
+            [None if x is None else x.contiguous().to(f64) for x in (grad_t, grad_uv, grad_normal)]
+        st = (stream or torch.cuda.current_stream(dev)).cuda_stream
+        _check(self._lib.bzr_adjoint_hit(
+            self._h, n, ptr(keep[0]), ptr(keep[1]), ptr(fwd["t"]), ptr(fwd["prim"]),
+            ptr(fwd["geom"]), ptr(fwd["hit"]), ptr(keep[2]), ptr(keep[3]), ptr(keep[4]),
+            ptr(g["vertices"]), ptr(g["centers"]), ptr(g["radii"]), ptr(g["origins"]),
+            ptr(g["directions"]), C.c_void_p(st)))
+        g["_keep"] = keep
+        return g
 
     def check(self, stream=None, timeout_ms=60000):
         """Waits (bounded) for queued device work and raises if a kernel's bounds check fired."""

@@ -17,6 +17,7 @@
 #include "../../include/blazert_b200.h"
 #include "layout.h"
 #include "scene.h"
+#include "adjoint.h"
 #include "trace.h"
 
 namespace {
@@ -70,6 +71,7 @@ struct bzr_scene {
   int device = -1;
   void *arena = nullptr;  // every device array of the committed scene
   bzr::SceneView view;
+  bzr::AdjointView adj;
   bzr::LaunchPlan plan;
   bool sort_possible = false;  // finite scene bounds: the coherence sort can be used
   uint32_t *slots = nullptr;  // see kSlots
@@ -236,6 +238,12 @@ int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
   }
   const size_t off_faces = place(s->host.faces.data(), s->host.faces.size() * sizeof(uint32_t));
   const size_t off_vn = place(s->host.vert_n.data(), s->host.vert_n.size() * sizeof(double));
+  // input-order geometry for the adjoint
+  const size_t off_verts =
+      place(s->host.vertices.data(), s->host.vertices.size() * sizeof(double));
+  const bzr::Collection &sph = s->host.kind[bzr::kSpheres];
+  const size_t off_sc = place(sph.a.data(), sph.a.size() * sizeof(double));
+  const size_t off_sr = place(sph.b.data(), sph.b.size() * sizeof(double));
   cudaError_t e = cudaGetDevice(&s->device);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
   e = cudaMalloc(&s->arena, total);
@@ -265,6 +273,18 @@ int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
   }
   s->view.faces = reinterpret_cast<const uint32_t *>(base + off_faces);
   s->view.vert_n = reinterpret_cast<const double *>(base + off_vn);
+  if (s->host.kind[bzr::kMesh].present) {
+    s->adj.verts = reinterpret_cast<const double *>(base + off_verts);
+    s->adj.faces = s->view.faces;
+    s->adj.vert_n = s->view.vert_n;
+    s->adj.n_faces = s->host.faces.size() / 3;
+    s->adj.mesh_geom = s->host.kind[bzr::kMesh].geom_id;
+  }
+  if (sph.present) {
+    s->adj.centers = reinterpret_cast<const double *>(base + off_sc);
+    s->adj.radii = reinterpret_cast<const double *>(base + off_sr);
+    s->adj.sphere_geom = sph.geom_id;
+  }
   s->view.stack_cap = std::max<uint32_t>(8, depth + 2);
   e = cudaMalloc(&s->slots, (kStickyWord + 1) * sizeof(uint32_t));
   if (e != cudaSuccess) return fail(BZR_ENOMEM, "slot allocation failed");
@@ -510,6 +530,61 @@ int bzr_work_counts(const bzr_scene *cs, size_t n, const double *org, const doub
   cudaFree(dev);
   cudaSetDevice(cur);
   return rc;
+}
+
+int bzr_adjoint_hit(const bzr_scene *cs, size_t n, const double *origins,
+                    const double *directions, const double *hit_distance, const uint32_t *prim_id,
+                    const uint32_t *geom_id, const uint8_t *hit, const double *grad_t,
+                    const double *grad_uv, const double *grad_normal, double *grad_vertices,
+                    double *grad_centers, double *grad_radii, double *grad_origins,
+                    double *grad_directions, void *stream) {
+  bzr_scene *s = const_cast<bzr_scene *>(cs);
+  if (!s) return fail(BZR_EINVAL, "scene is null");
+  if (!s->host.committed) return fail(BZR_ESTATE, "scene is not committed");
+  if (n == 0) return BZR_OK;
+  if (!origins || !directions || !hit_distance || !prim_id || !geom_id || !hit)
+    return fail(BZR_EINVAL, "forward results are required");
+  const void *ptrs[] = {origins, directions, hit_distance, prim_id, geom_id, hit, grad_t,
+                        grad_uv, grad_normal, grad_vertices, grad_centers, grad_radii,
+                        grad_origins, grad_directions};
+  for (const void *p : ptrs)
+    if (p && !is_device_ptr(p)) return fail(BZR_EINVAL, "adjoint arrays must be device memory");
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(s->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  bzr::AdjointIO io;
+  io.n = n;
+  io.org = origins;
+  io.dir = directions;
+  io.t = hit_distance;
+  io.prim = prim_id;
+  io.geom = geom_id;
+  io.hit = hit;
+  io.grad_t = grad_t;
+  io.grad_uv = grad_uv;
+  io.grad_normal = grad_normal;
+  io.grad_verts = grad_vertices;
+  io.grad_centers = grad_centers;
+  io.grad_radii = grad_radii;
+  io.grad_org = grad_origins;
+  io.grad_dir = grad_directions;
+  io.error_word = s->slots + kStickyWord;
+  const size_t nv = s->host.vertices.size() / 3, ns = s->host.kind[bzr::kSpheres].n;
+  cudaError_t e = cudaSuccess;
+  if (grad_vertices) e = cudaMemsetAsync(grad_vertices, 0, 24 * nv, st);
+  if (e == cudaSuccess && grad_centers) e = cudaMemsetAsync(grad_centers, 0, 24 * ns, st);
+  if (e == cudaSuccess && grad_radii) e = cudaMemsetAsync(grad_radii, 0, 8 * ns, st);
+  double *gvn = nullptr;
+  if (e == cudaSuccess && grad_vertices && nv) {
+    e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&gvn), 24 * nv, s->plan.pool, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(gvn, 0, 24 * nv, st);
+  }
+  io.grad_vert_n = gvn;
+  if (e == cudaSuccess) e = bzr::launch_adjoint(s->adj, io, s->plan.sms, st);
+  if (gvn) cudaFreeAsync(gvn, st);
+  cudaSetDevice(cur);
+  return e == cudaSuccess ? BZR_OK : cuda_fail(e, "adjoint launch");
 }
 
 int bzr_intersect1(const bzr_scene *s, const double origin[3], const double direction[3],

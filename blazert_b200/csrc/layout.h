@@ -69,5 +69,6 @@ struct SceneView {
 constexpr uint32_t kErrStack = 1u;      // traversal stack would overflow
 constexpr uint32_t kErrNodeIndex = 2u;  // a child reference points outside the node array
 constexpr uint32_t kErrPrimIndex = 4u;  // a leaf runs past the primitive arrays
+constexpr uint32_t kErrAdjointKind = 8u;  // a ray's hit kind has no adjoint (plane, cylinder)
 
 }  // namespace bzr

@@ -16,6 +16,7 @@
  *   bzr_intersect1                intersect1(scene, ray, rayhit)    blazert/scene.h:161-210
  *                                 with Ray / RayHit                 blazert/ray.h:56-85
  *   bzr_intersectN                new: intersect1 over a batch of rays, one GPU launch
+ *   bzr_adjoint_hit               new: gradients of the outputs (differentiation form)
  *   bzr_work_counts, bzr_scene_check, bzr_scene_stats, bzr_scene_tune
  *                                 new: measurement, error reporting and tuning
  *
@@ -111,6 +112,21 @@ int bzr_intersectN(const bzr_scene *scene, size_t n, const double *origins,
                    const double *directions, const double *tmin, const double *tmax,
                    double *hit_distance, double *uv, double *normal, uint32_t *prim_id,
                    uint32_t *geom_id, uint8_t *hit, int mode, void *stream);
+
+/* Adjoint of the closest-hit outputs (no counterpart in the reference): given a batch's
+ * forward results (as returned by bzr_intersectN) and upstream gradients dL/dhit_distance (n),
+ * dL/duv (n x 2), dL/dnormal (n x 3) -- each may be NULL for zero -- computes dL/d(triangle
+ * vertices) (n_vertices x 3), dL/d(sphere centres) (n x 3), dL/d(sphere radii), dL/d(ray
+ * origins) and dL/d(raw ray directions) (n x 3 each); any output may be NULL.  The hit
+ * primitive is held fixed (recomputed from prim_id, no re-traversal).  Rays whose hit is a
+ * plane or cylinder get zero gradients and set kernel error bit 8 (read by bzr_scene_check).
+ * Device arrays only; queued on `stream`. */
+int bzr_adjoint_hit(const bzr_scene *scene, size_t n, const double *origins,
+                    const double *directions, const double *hit_distance, const uint32_t *prim_id,
+                    const uint32_t *geom_id, const uint8_t *hit, const double *grad_t,
+                    const double *grad_uv, const double *grad_normal, double *grad_vertices,
+                    double *grad_centers, double *grad_radii, double *grad_origins,
+                    double *grad_directions, void *stream);
 
 /* Work of a batch (no counterpart in the reference; a measurement aid): runs the counting
  * variant of the FP64 kernel over n rays and returns per kind (0 mesh, 1 spheres, 2 planes,
