@@ -82,6 +82,10 @@ def library():
         lib.bzr_work_counts.argtypes = [P, C.c_size_t, P, P, P, P, C.POINTER(C.c_uint64), P]
         lib.bzr_scene_tune.argtypes = [P, C.c_int, C.c_int64]
         lib.bzr_adjoint_hit.argtypes = [P, C.c_size_t] + [P] * 14 + [P]
+        lib.bzr_batch_create.argtypes = [C.POINTER(P), C.POINTER(P), C.c_size_t]
+        lib.bzr_batch_destroy.argtypes = [P]
+        lib.bzr_batch_intersect.argtypes = [P, C.POINTER(C.c_uint64)] + [P] * 11 + [C.c_int, P]
+        lib.bzr_batch_check.argtypes = [P, P, _u32p]
         lib.bzr_scene_stats.argtypes = [P, C.c_int, C.POINTER(C.c_uint64), _u32p,
                                         C.POINTER(C.c_double)]
         lib.bzr_last_error_string.restype = C.c_char_p
@@ -361,11 +365,64 @@ class Scene:
         return int(flags.value)
 
 
+class Batch:
+    """Many committed scenes traced together (bzr_batch_*), device arrays only."""
+
+    def __init__(self, scenes):
+        self._lib = library()
+        self.scenes = list(scenes)  # keep the scenes alive
+        arr = (C.c_void_p * len(self.scenes))(*[s._h.value for s in self.scenes])
+        self._h = C.c_void_p()
+        _check(self._lib.bzr_batch_create(C.byref(self._h), arr, len(self.scenes)))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.bzr_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def intersect(self, ray_offsets, origins, directions, tmin=None, tmax=None, out=None,
+                  timestamps=None, mode="fp64", stream=None):
+        """ray_offsets: host sequence of n_scenes + 1 ints; rays: torch CUDA tensors (all
+        scenes concatenated).  timestamps: optional int64 CUDA tensor of n_scenes + 1."""
+        import torch
+
+        n = origins.shape[0]
+        dev = origins.device
+        f64 = torch.float64
+        if out is None:
+            out = dict(t=torch.empty(n, dtype=f64, device=dev),
+                       uv=torch.empty((n, 2), dtype=f64, device=dev),
+                       normal=torch.empty((n, 3), dtype=f64, device=dev),
+                       prim=torch.empty(n, dtype=torch.int32, device=dev),
+                       geom=torch.empty(n, dtype=torch.int32, device=dev),
+                       hit=torch.empty(n, dtype=torch.uint8, device=dev))
+        offs = (C.c_uint64 * len(ray_offsets))(*[int(x) for x in ray_offsets])
+        ptr = lambda a: None if a is None else a.data_ptr()
+        st = (stream or torch.cuda.current_stream(dev)).cuda_stream
+        _check(self._lib.bzr_batch_intersect(
+            self._h, offs, ptr(origins), ptr(directions), ptr(tmin), ptr(tmax), ptr(out.get("t")),
+            ptr(out.get("uv")), ptr(out.get("normal")), ptr(out.get("prim")), ptr(out.get("geom")),
+            ptr(out.get("hit")), ptr(timestamps), MODES[mode], C.c_void_p(st)))
+        return out
+
+    def check(self, stream=None):
+        flags = C.c_uint32()
+        _check(self._lib.bzr_batch_check(self._h, None if stream is None else C.c_void_p(stream),
+                                         C.byref(flags)))
+        return int(flags.value)
+
+
 def intersect1(scene: Scene, ray: Ray, rayhit: RayHit) -> bool:
     """blazert/scene.h:161-162: fills rayhit on a hit and returns whether anything was hit."""
     hit, _ = scene.intersect1(ray, rayhit)
     return hit
 
 
-__all__ = ["Scene", "Ray", "RayHit", "BuildOptions", "intersect1", "BlazertError", "INVALID_ID",
+__all__ = ["Scene", "Batch", "Ray", "RayHit", "BuildOptions", "intersect1", "BlazertError", "INVALID_ID",
            "DBL_MAX", "library"]

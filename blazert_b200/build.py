@@ -27,8 +27,9 @@ HOST_FLAGS = ["-std=c++17", "-O3", "-fPIC", "-ffp-contract=off", "-Wall", "-Wext
 CU_FLAGS = ARCH + ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler",
                    "-fPIC,-ffp-contract=off", "-ccbin", CXX]
 
-SOURCES = [("scene.cpp", "cxx"), ("capi.cpp", "cxx"), ("trace.cu", "cu"), ("adjoint.cu", "cu")]
-HEADERS = ["layout.h", "scene.h", "trace.h", "trace_core.cuh", "adjoint.h"]
+SOURCES = [("scene.cpp", "cxx"), ("capi.cpp", "cxx"), ("trace.cu", "cu"), ("adjoint.cu", "cu"),
+           ("batch.cpp", "cxx")]
+HEADERS = ["layout.h", "scene.h", "trace.h", "trace_core.cuh", "adjoint.h", "capi_internal.h"]
 
 
 def _cuda_home():

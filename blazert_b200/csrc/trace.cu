@@ -130,6 +130,135 @@ __global__ void __launch_bounds__(kTraceThreads)
   }
 }
 
+// Batching form: one kind over many scenes.  Warps take chunks of one scene's rays; a lane
+// keeps its own ray's scene, so a warp may finish rays of one scene while starting another's.
+// The pass of a scene's first kind writes its whole record; the pass of its last kind
+// completes it and stamps the scene's completion time.
+template <int KIND, bool MIXED>
+__global__ void __launch_bounds__(kTraceThreads)
+    trace_batch_kernel(BatchView B, RayIO io, uint32_t *chunk_counter, uint32_t stack_cap) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  Stack sk;
+  sk.stride = blockDim.x;
+  sk.cap = stack_cap;
+  sk.key = reinterpret_cast<double *>(smem);
+  sk.ref = reinterpret_cast<uint32_t *>(sk.key + size_t(sk.cap) * sk.stride);
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned below = (1u << lane) - 1u;
+  const uint32_t tid = threadIdx.x;
+  uint32_t pool_next = 0, pool_end = 0, pool_scene = 0;  // warp-uniform
+  bool exhausted = false;
+  bool active = false;
+  uint32_t i = 0, sc = 0;
+  const KindView *K = nullptr;
+  Ray r;
+  RayF f;
+  bool use32 = false;
+  KState st;
+  Trav tv;
+  Counts cnt = {};
+  for (;;) {
+    const unsigned idle = __ballot_sync(kFull, !active);
+    if (idle && !exhausted) {
+      const uint32_t want = __popc(idle), avail = pool_end - pool_next;
+      const uint32_t rank = __popc(idle & below);
+      uint32_t base = 0, cbegin = 0, cend = 0, cscene = 0;
+      bool got_chunk = false;
+      if (want > avail) {  // next chunk that has this kind
+        uint32_t c = 0;
+        for (;;) {
+          if (lane == 0) c = atomicAdd(chunk_counter, 1u);
+          c = __shfl_sync(kFull, c, 0);
+          if (c >= B.n_chunks) {
+            exhausted = true;
+            break;
+          }
+          const BatchChunk ch = B.chunks[c];
+          if (B.views[ch.scene].k[KIND].present && B.views[ch.scene].k[KIND].n_prims) {
+            cbegin = ch.begin;
+            cend = ch.end;
+            cscene = ch.scene;
+            got_chunk = true;
+            break;
+          }
+        }
+        base = cbegin;
+      }
+      if (!active) {
+        uint32_t idx = 0, s2 = 0;
+        bool ok = false;
+        if (rank < avail) {
+          idx = pool_next + rank;
+          s2 = pool_scene;
+          ok = true;
+        } else if (got_chunk && base + (rank - avail) < cend) {
+          idx = base + (rank - avail);
+          s2 = cscene;
+          ok = true;
+        }
+        if (ok) {
+          i = idx;
+          sc = s2;
+          active = true;
+          K = &B.views[sc].k[KIND];
+          r = make_ray(io.org + 3 * size_t(i), io.dir + 3 * size_t(i), io.tmin ? io.tmin[i] : 0.0,
+                       io.tmax ? io.tmax[i] : kDblMax);
+          if (MIXED) {
+            f = make_ray_f(r, K->coord_max);
+            use32 = K->mixed_ok && f.ok;
+          }
+          trav_begin<KIND, false>(*K, r, st, tv, &cnt);
+        }
+      }
+      if (want > avail) {
+        if (got_chunk) {
+          const uint32_t used = want - avail;
+          pool_next = cbegin + (used < cend - cbegin ? used : cend - cbegin);
+          pool_end = cend;
+          pool_scene = cscene;
+        } else {
+          pool_next = pool_end;
+        }
+      } else {
+        pool_next += want;
+      }
+    }
+    if (!__any_sync(kFull, active)) break;
+    if (active) {
+      if (MIXED && use32) {
+        if (tv.live) trav_to_leaf32<KIND, false>(*K, r, f, st, tv, sk, tid, io.error_word, &cnt);
+        if (tv.live) trav_leaf32<KIND, false>(*K, r, f, st, tv, sk, tid, io.error_word, &cnt);
+      } else {
+        if (tv.live) trav_to_leaf<KIND, false>(*K, r, st, tv, sk, tid, io.error_word, &cnt);
+        if (tv.live) trav_leaf<KIND, false>(*K, r, st, tv, sk, tid, io.error_word, &cnt);
+      }
+      if (!tv.live) {
+        finalize_kind<KIND>(B.views[sc], r, st, i, B.first_kind[sc] == KIND, io.t, io.uv,
+                            io.normal, io.prim, io.geom, io.hit);
+        if (B.last_kind[sc] == KIND && B.scene_left) {
+          if (atomicSub(B.scene_left + sc, 1u) == 1u && B.scene_done_ns) {
+            __threadfence();
+            unsigned long long now;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+            B.scene_done_ns[sc] = now;
+          }
+        }
+        active = false;
+      }
+    }
+  }
+}
+
+__global__ void batch_start_kernel(BatchView B, uint32_t n_scenes) {
+  for (uint32_t s = threadIdx.x; s < n_scenes; s += blockDim.x)
+    if (B.scene_left) B.scene_left[s] = B.scene_rays[s];
+  if (threadIdx.x == 0 && B.start_ns) {
+    unsigned long long now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    *B.start_ns = now;
+  }
+}
+
 // Output defaults for every ray of a scene without primitives (blazert/ray.h:80-84).
 __global__ void fill_defaults_kernel(RayIO io) {
   for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < io.n;
@@ -241,6 +370,14 @@ cudaError_t prepare_kind(uint32_t stack_cap, int sms, int *blocks, int *blocks32
 
 }  // namespace
 
+cudaError_t launch_defaults(const RayIO &io, int sms, cudaStream_t stream) {
+  const int threads = 256;
+  const uint64_t want = (uint64_t(io.n) + threads - 1) / threads;
+  const int blocks = int(want < uint64_t(sms) * 8 ? (want ? want : 1) : uint64_t(sms) * 8);
+  fill_defaults_kernel<<<blocks, threads, 0, stream>>>(io);
+  return cudaGetLastError();
+}
+
 size_t trace_smem_bytes(uint32_t stack_cap, int threads) {
   return size_t(stack_cap) * threads * (sizeof(double) + sizeof(uint32_t));
 }
@@ -331,6 +468,76 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
     if (e == cudaSuccess) e = f;
   }
   return e;
+}
+
+namespace {
+template <int KIND>
+cudaError_t prepare_batch_kind(uint32_t stack_cap, int sms, int *blocks, int *blocks32) {
+  const size_t smem = trace_smem_bytes(stack_cap, kTraceThreads);
+  const void *fns[2] = {reinterpret_cast<const void *>(trace_batch_kernel<KIND, false>),
+                        reinterpret_cast<const void *>(trace_batch_kernel<KIND, true>)};
+  int per[2] = {0, 0};
+  for (int j = 0; j < 2; ++j) {
+    cudaError_t e =
+        cudaFuncSetAttribute(fns[j], cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[j], fns[j], kTraceThreads, smem);
+    if (e != cudaSuccess) return e;
+  }
+  *blocks = sms * (per[0] > 0 ? per[0] : 1);
+  *blocks32 = sms * (per[1] > 0 ? per[1] : 1);
+  return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t batch_prepare(uint32_t stack_cap, BatchPlan *plan) {
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  plan->sms = sms;
+  plan->stack_cap = stack_cap;
+  if ((e = prepare_batch_kind<kMesh>(stack_cap, sms, &plan->blocks[kMesh],
+                                     &plan->blocks32[kMesh])) != cudaSuccess)
+    return e;
+  if ((e = prepare_batch_kind<kSpheres>(stack_cap, sms, &plan->blocks[kSpheres],
+                                        &plan->blocks32[kSpheres])) != cudaSuccess)
+    return e;
+  if ((e = prepare_batch_kind<kPlanes>(stack_cap, sms, &plan->blocks[kPlanes],
+                                       &plan->blocks32[kPlanes])) != cudaSuccess)
+    return e;
+  return prepare_batch_kind<kCylinders>(stack_cap, sms, &plan->blocks[kCylinders],
+                                        &plan->blocks32[kCylinders]);
+}
+
+cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const BatchPlan &plan,
+                         cudaStream_t stream, uint32_t *counters) {
+  cudaError_t e = cudaMemsetAsync(counters, 0, kNumKinds * sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  batch_start_kernel<<<1, 256, 0, stream>>>(B, B.n_scenes);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const size_t smem = trace_smem_bytes(plan.stack_cap, kTraceThreads);
+  for (int k = 0; k < kNumKinds; ++k) {
+    if (!(plan.kinds_present & (1 << k))) continue;
+    const bool m = mode == kModeMixed;
+    const int b = m ? plan.blocks32[k] : plan.blocks[k];
+    uint32_t *c = counters + k;
+#define BZR_BATCH_LAUNCH(KK)                                                                  \
+  if (m)                                                                                      \
+    trace_batch_kernel<KK, true><<<b, kTraceThreads, smem, stream>>>(B, io, c, plan.stack_cap); \
+  else                                                                                        \
+    trace_batch_kernel<KK, false><<<b, kTraceThreads, smem, stream>>>(B, io, c, plan.stack_cap);
+    switch (k) {
+      case kMesh: BZR_BATCH_LAUNCH(kMesh); break;
+      case kSpheres: BZR_BATCH_LAUNCH(kSpheres); break;
+      case kPlanes: BZR_BATCH_LAUNCH(kPlanes); break;
+      default: BZR_BATCH_LAUNCH(kCylinders); break;
+    }
+#undef BZR_BATCH_LAUNCH
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace bzr

@@ -52,6 +52,41 @@ struct LaunchPlan {
   cudaMemPool_t pool = nullptr;       // stream-ordered scratch (keeps its memory mapped)
 };
 
+// Many scenes in one launch per kind (the batching form).  Rays of scene s occupy
+// [ray_offset[s], ray_offset[s+1]) of the concatenated arrays in io.  Chunks of at most
+// kBatchChunk rays never cross scenes.
+constexpr uint32_t kBatchChunk = 64;
+struct BatchChunk {
+  uint32_t scene;
+  uint32_t begin, end;  // ray range in the concatenated batch
+};
+struct BatchView {
+  const SceneView *views = nullptr;    // n_scenes device copies of the scenes' views
+  const BatchChunk *chunks = nullptr;  // n_chunks
+  uint32_t n_chunks = 0;
+  uint32_t n_scenes = 0;
+  const int8_t *first_kind = nullptr;  // per scene: kind whose pass writes the whole record
+  const int8_t *last_kind = nullptr;   // per scene: kind whose pass completes the scene
+  const uint32_t *scene_rays = nullptr;  // per scene: ray count
+  uint32_t *scene_left = nullptr;      // per scene: rays not yet completed (set to scene_rays)
+  unsigned long long *scene_done_ns = nullptr;  // per scene completion time (%globaltimer), or null
+  unsigned long long *start_ns = nullptr;       // batch start time, or null
+};
+struct BatchPlan {
+  int sms = 0;
+  int blocks[kNumKinds] = {0, 0, 0, 0};
+  int blocks32[kNumKinds] = {0, 0, 0, 0};
+  uint32_t stack_cap = 32;
+  int kinds_present = 0;  // bit k: some scene has kind k
+};
+cudaError_t batch_prepare(uint32_t stack_cap, BatchPlan *plan);
+// counters: kNumKinds device words (chunk counters), zeroed here.
+cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const BatchPlan &plan,
+                         cudaStream_t stream, uint32_t *counters);
+
+// RayHit defaults for every ray of io (a scene without primitives).
+cudaError_t launch_defaults(const RayIO &io, int sms, cudaStream_t stream);
+
 size_t trace_smem_bytes(uint32_t stack_cap, int threads);
 cudaError_t trace_prepare(const SceneView &S, LaunchPlan *plan);
 // Number of per-kind passes a batch runs (kinds present with at least one primitive).

@@ -17,6 +17,7 @@
  *                                 with Ray / RayHit                 blazert/ray.h:56-85
  *   bzr_intersectN                new: intersect1 over a batch of rays, one GPU launch
  *   bzr_adjoint_hit               new: gradients of the outputs (differentiation form)
+ *   bzr_batch_*                   new: many scenes per launch, CUDA graph (batching form)
  *   bzr_work_counts, bzr_scene_check, bzr_scene_stats, bzr_scene_tune
  *                                 new: measurement, error reporting and tuning
  *
@@ -113,6 +114,26 @@ int bzr_intersectN(const bzr_scene *scene, size_t n, const double *origins,
                    double *hit_distance, double *uv, double *normal, uint32_t *prim_id,
                    uint32_t *geom_id, uint8_t *hit, int mode, void *stream);
 
+/* Batching form (no counterpart in the reference): many committed scenes of one device, each
+ * with its own batch of rays, traced together -- one persistent kernel per primitive kind for
+ * all scenes -- with the launch sequence captured in a CUDA graph and replayed while the
+ * arguments stay the same.  Results per scene equal bzr_intersectN on that scene. */
+typedef struct bzr_batch bzr_batch;
+int bzr_batch_create(bzr_batch **out, const bzr_scene *const *scenes, size_t n_scenes);
+int bzr_batch_destroy(bzr_batch *batch);
+/* Rays of scene s are [ray_offsets[s], ray_offsets[s+1]) of the concatenated device arrays
+ * (ray_offsets: host array of n_scenes + 1, starting at 0).  hit_distance is required; other
+ * outputs may be NULL.  scene_done_ns (device, n_scenes + 1, or NULL) receives each scene's
+ * completion time and, in its last entry, the batch start time (GPU global timer, ns).
+ * Queued on `stream`. */
+int bzr_batch_intersect(bzr_batch *batch, const uint64_t *ray_offsets, const double *origins,
+                        const double *directions, const double *tmin, const double *tmax,
+                        double *hit_distance, double *uv, double *normal, uint32_t *prim_id,
+                        uint32_t *geom_id, uint8_t *hit, uint64_t *scene_done_ns, int mode,
+                        void *stream);
+/* Waits for `stream` and reports the batch kernels' error word (as bzr_scene_check). */
+int bzr_batch_check(bzr_batch *batch, void *stream, uint32_t *flags);
+
 /* Adjoint of the closest-hit outputs (no counterpart in the reference): given a batch's
  * forward results (as returned by bzr_intersectN) and upstream gradients dL/dhit_distance (n),
  * dL/duv (n x 2), dL/dnormal (n x 3) -- each may be NULL for zero -- computes dL/d(triangle
@@ -143,9 +164,9 @@ int bzr_work_counts(const bzr_scene *scene, size_t n, const double *origins,
 int bzr_scene_check(const bzr_scene *scene, void *stream, int timeout_ms, uint32_t *flags);
 
 /* Tuning knobs of a committed scene (no counterpart in the reference; they change speed,
- * never results).  BZR_TUNE_SORT: 1 (default when the scene has finite bounds) sorts each
- * batch of at least BZR_TUNE_SORT_MIN_RAYS rays (default 65536) by direction octant and origin
- * Morton code before tracing, so that the rays of a warp take similar paths; 0 traces in the
+ * never results).  BZR_TUNE_SORT: 1 sorts each batch of at least BZR_TUNE_SORT_MIN_RAYS rays
+ * (default 65536) by direction octant and origin Morton code before tracing, so that the rays
+ * of a warp take similar paths (needs finite scene bounds); 0 (the default) traces in the
  * caller's order. */
 #define BZR_TUNE_SORT 1
 #define BZR_TUNE_SORT_MIN_RAYS 2

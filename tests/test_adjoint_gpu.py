@@ -1,5 +1,5 @@
 """The CUDA adjoint (bzr_adjoint_hit) and its torch.autograd wrapper against the host analytic
-FP64 gradient and FP64 central finite differences (h = 1e-6) of the GPU forward pass."""
+FP64 gradient and FP64 central finite differences (h = 1e-7) of the GPU forward pass."""
 import numpy as np
 import pytest
 
@@ -9,7 +9,7 @@ from tests.helpers import product_scene, to_numpy
 from tests.test_adjoint_ref import small_scene
 
 pytestmark = pytest.mark.gpu
-H = 1e-6
+H = 1e-7
 
 
 def _dev(a):
@@ -35,10 +35,17 @@ def _adjoint_vs_analytic(spec, o, d, rng, with_uv_normal):
     assert s.check() == 0
     ref = adjoint_ref.gradients(spec, o, d, f, gt, guv, gn)
     for k in ("origins", "directions", "vertices", "centers", "radii"):
-        got = g[k].cpu().numpy()
-        scale = np.abs(ref[k]).max() + 1e-300
-        assert np.abs(got - ref[k]).max() <= 1e-9 * scale, k
+        assert_close(g[k].cpu().numpy(), ref[k], k)
     return s, f, wt
+
+
+def assert_close(got, ref, what):
+    """Two independent FP64 evaluations of the same gradient: per element within 1e-7
+    relative (rays that graze a triangle have 1/(n.d) condition numbers near 1e8), plus an
+    absolute floor of 1e-10 of the largest magnitude."""
+    tol = 1e-7 * np.abs(ref) + 1e-10 * (np.abs(ref).max() + 1e-300)
+    bad = np.abs(got - ref) > tol
+    assert not bad.any(), (what, int(bad.sum()), float(np.abs(got - ref).max()))
 
 
 def test_adjoint_matches_analytic_small():
@@ -50,7 +57,7 @@ def test_adjoint_scene_analytic_and_finite_differences():
     """The differentiation workload (91,920-triangle perturbed icosphere + 500 spheres), loss
     L = sum w_i t_i^2: CUDA adjoint vs the host analytic gradient on all rays, and vs central
     differences on a seeded subsample of parameters (rays whose hit primitive changes under the
-    perturbation are left out of the difference quotient)."""
+    perturbation, and grazing hits, are left out of the difference quotient)."""
     wl = W.adjoint_scene(n_rays=1 << 20)
     spec, R = wl.scene, wl.rays
     rng = np.random.Generator(np.random.PCG64(55))
@@ -62,12 +69,11 @@ def test_adjoint_scene_analytic_and_finite_differences():
     g = s.adjoint(to, td, fwd, grad_t=_dev(2 * wt * f["t"] * hit), n_vertices=nv, n_spheres=ns)
     gv, gc, gr = (g[k].cpu().numpy() for k in ("vertices", "centers", "radii"))
 
-    def loss(spec_, stable):
-        sc = product_scene(spec_)
-        out = to_numpy(sc.intersectN(to, td))
-        assert np.array_equal(out["prim"][stable], f["prim"][stable])
-        t = np.where(out["hit"][stable].astype(bool), out["t"][stable], 0.0)
-        return float(np.sum(wt[stable] * t * t)), out
+    # Grazing hits (|cos| between ray and normal below 0.05) are left out of the difference
+    # quotient: dt/dparameter grows like 1/cos there, and the O(h^2) error of the central
+    # difference with it.
+    dn = R.directions / np.linalg.norm(R.directions, axis=1, keepdims=True)
+    well = np.abs(np.einsum("ij,ij->i", dn, f["normal"])) >= 0.05
 
     def fd(kind, key, index):
         specs = []
@@ -80,12 +86,12 @@ def test_adjoint_scene_analytic_and_finite_differences():
                 getattr(s2, "add_" + k)(*arrs.values())
             specs.append(s2)
         outs = [to_numpy(product_scene(x).intersectN(to, td)) for x in specs]
-        stable = np.ones(len(wt), bool)
+        stable = well.copy()
         for out in outs:
             stable &= (out["prim"] == f["prim"]) & (out["geom"] == f["geom"])
-        lp, _ = loss(specs[0], stable)
-        lm, _ = loss(specs[1], stable)
-        return (lp - lm) / (2 * H), stable
+        tp, tm = (np.where(o_["hit"][stable].astype(bool), o_["t"][stable], 0.0) for o_ in outs)
+        # per-ray differences first: rays the perturbation leaves alone contribute exactly 0
+        return float(np.sum(wt[stable] * (tp * tp - tm * tm))) / (2 * H), stable
 
     used = 0
     vert_candidates = np.unique(f["prim"][hit & (f["geom"] == 0)])
@@ -138,5 +144,4 @@ def test_autograd_wrapper():
     ref = adjoint_ref.gradients(spec, o, d, {k: v for k, v in f.items()}, gt, guv, gn)
     for got, k in ((to.grad, "origins"), (td.grad, "directions"), (verts.grad, "vertices"),
                    (cen.grad, "centers"), (rad.grad, "radii")):
-        g = got.cpu().numpy()
-        assert np.abs(g - ref[k]).max() <= 1e-9 * (np.abs(ref[k]).max() + 1e-300), k
+        assert_close(got.cpu().numpy(), ref[k], k)

@@ -1,0 +1,47 @@
+"""The batching form (bzr_batch_*): many scenes of uneven sizes in one launch per kind,
+replayed from a CUDA graph; every scene's results equal the oracle's for that scene."""
+import numpy as np
+import pytest
+
+import blazert_b200 as B
+from blazert_b200 import workloads as W
+from oracle.oracle import Oracle
+from tests.helpers import mismatches, product_scene, to_numpy
+
+pytestmark = pytest.mark.gpu
+
+
+def _batch_case(n_scenes=24, scale=0.02, seed=4):
+    wls = W.batched_icospheres(n_scenes=n_scenes, seed=seed, scale=scale)
+    extra = W.mixed_primitives(n_rays=3000, n_spheres=500, n_cylinders=50, n_planes=20, seed=9)
+    wls.insert(3, extra)                                  # a scene with three kinds
+    wls.insert(5, W.Workload("empty", W.SceneSpec().add_spheres(np.zeros((0, 3)), np.zeros(0)),
+                             W.RayBatch(np.zeros((50, 3)), np.ones((50, 3)))))  # nothing to hit
+    wls.insert(7, W.Workload("no_rays", wls[0].scene, W.RayBatch(np.zeros((0, 3)), np.zeros((0, 3)))))
+    return wls
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_batch_matches_per_scene_oracle(mode):
+    import torch
+
+    wls = _batch_case()
+    scenes = [product_scene(w.scene) for w in wls]
+    batch = B.Batch(scenes)
+    offs = np.concatenate([[0], np.cumsum([w.rays.n for w in wls])])
+    o = torch.from_numpy(np.concatenate([w.rays.origins for w in wls])).cuda()
+    d = torch.from_numpy(np.concatenate([w.rays.directions for w in wls])).cuda()
+    ts = torch.zeros(len(wls) + 1, dtype=torch.int64, device="cuda")
+    for _ in range(3):  # first call captures the graph, later calls replay it
+        out = batch.intersect(offs, o, d, timestamps=ts, mode=mode)
+        assert batch.check() == 0
+        got = to_numpy(out)
+        for s, w in enumerate(wls):
+            a, b = offs[s], offs[s + 1]
+            ref = Oracle(w.scene).intersect(w.rays.origins, w.rays.directions)
+            assert mismatches({k: v[a:b] for k, v in got.items()}, ref) == [], (s, w.name)
+    t = ts.cpu().numpy()
+    start = t[-1]
+    for s, w in enumerate(wls):
+        if w.rays.n and any(len(next(iter(getattr(w.scene, k).values()))) for k in w.scene.order):
+            assert t[s] >= start > 0
