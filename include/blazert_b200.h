@@ -114,6 +114,20 @@ int bzr_intersectN(const bzr_scene *scene, size_t n, const double *origins,
                    double *hit_distance, double *uv, double *normal, uint32_t *prim_id,
                    uint32_t *geom_id, uint8_t *hit, int mode, void *stream);
 
+/* bzr_intersectN for callers that cannot allocate device memory while they trace (no
+ * counterpart in the reference) -- for example a renderer plugin traced from its host
+ * application's frame loop, where a cudaMalloc/cudaFree would synchronise the whole device, or
+ * a service whose device memory budget is handed out up front.  Same arguments and results as
+ * bzr_intersectN, but device arrays only, at most 1,048,576 rays per call (larger batches get
+ * BZR_EINVAL), and no coherence sort.  The call allocates nothing: its scratch is one 8 MiB
+ * static device array per GPU, held until the process exits.  All calls on a device share that
+ * array; calls whose GPU work overlaps race -- order them on one stream.  The first call on each
+ * device looks up the array's address; make it before any stream capture. */
+int bzr_intersectN_noalloc(const bzr_scene *scene, size_t n, const double *origins,
+                           const double *directions, const double *tmin, const double *tmax,
+                           double *hit_distance, double *uv, double *normal, uint32_t *prim_id,
+                           uint32_t *geom_id, uint8_t *hit, int mode, void *stream);
+
 /* Batching form (no counterpart in the reference): many committed scenes of one device, each
  * with its own batch of rays, traced together -- one persistent kernel per primitive kind for
  * all scenes -- with the launch sequence captured in a CUDA graph and replayed while the
