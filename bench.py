@@ -38,7 +38,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 RAY_IO_BYTES = 24 + 24 + 8 + 8 + 8 + 16 + 24 + 4 + 4 + 1  # o, d, tmin, tmax | t, uv, n, ids, hit
-PRIM_RECORD_BYTES = {0: 96 + 4, 1: 32 + 4, 2: 112 + 4, 3: 128 + 4}
+# bytes a primitive test consumes: triangle = {i0, i1, i2, id} + three 24-byte vertex positions;
+# the other kinds read their record and 4-byte id word
+PRIM_RECORD_BYTES = {0: 16 + 3 * 24, 1: 32 + 4, 2: 112 + 4, 3: 128 + 4}
 BOX_TEST_BYTES = 64
 METRIC = "Mrays/s closest-hit on 1 B200: FP64 vs mixed FP32/FP64, same hits; vs CPU"
 

@@ -252,12 +252,14 @@ int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
     total = align_up(total + std::max<size_t>(bytes, 1), 256);
     return off;
   };
-  size_t off_nodes64[4], off_nodes32[4], off_payload[4], off_ids[4];
+  size_t off_nodes64[4], off_nodes32[4], off_payload[4], off_ids[4], off_tri[4], off_tv[4];
   for (int k = 0; k < bzr::kNumKinds; ++k) {
     off_nodes64[k] = place(img[k].nodes64.data(), img[k].nodes64.size() * sizeof(double));
     off_nodes32[k] = place(img[k].nodes32.data(), img[k].nodes32.size() * sizeof(float));
     off_payload[k] = place(img[k].payload.data(), img[k].payload.size() * sizeof(double));
     off_ids[k] = place(img[k].prim_ids.data(), img[k].prim_ids.size() * sizeof(uint32_t));
+    off_tri[k] = place(img[k].tri.data(), img[k].tri.size() * sizeof(uint32_t));
+    off_tv[k] = place(img[k].verts.data(), img[k].verts.size() * sizeof(double));
   }
   const size_t off_faces = place(s->host.faces.data(), s->host.faces.size() * sizeof(uint32_t));
   const size_t off_vn = place(s->host.vert_n.data(), s->host.vert_n.size() * sizeof(double));
@@ -287,6 +289,8 @@ int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
     v.nodes32 = reinterpret_cast<const float *>(base + off_nodes32[k]);
     v.payload = reinterpret_cast<const double *>(base + off_payload[k]);
     v.prim_ids = reinterpret_cast<const uint32_t *>(base + off_ids[k]);
+    v.tri = reinterpret_cast<const uint32_t *>(base + off_tri[k]);
+    v.verts = reinterpret_cast<const double *>(base + off_tv[k]);
     v.n_internal = img[k].n_internal;
     v.n_prims = static_cast<uint32_t>(img[k].prim_ids.size());
     v.root_ref = img[k].root_ref;

@@ -36,17 +36,26 @@ constexpr int kNode64Doubles = 16;
 constexpr int kNode32Floats = 16;
 
 // Leaf-ordered primitive payload, doubles per primitive:
-//   mesh       12: v0(3), e1 = v0 - v1 (3), e2 = v2 - v0 (3), n = cross(e1, e2) (3)
-//                  (the Triangle of blazert/primitives/trimesh.h:19-31 plus its face normal)
 //   spheres     4: center(3), radius
 //   planes     14: center(3), dx, dy, rotation(9, row-major)
 //   cylinders  16: center(3), semi_axis_a, semi_axis_b, height, rotation(9), pad
-constexpr int kPayloadDoubles[kNumKinds] = {12, 4, 14, 16};
+// Triangles are indexed instead (the reference's TriangleMesh keeps vertices and faces,
+// blazert/primitives/trimesh.h:78-90, and builds v0, e1 = v0 - v1, e2 = v2 - v0 per test,
+// trimesh.h:153-160): per leaf-ordered triangle one 16-byte word group {i0, i1, i2, id word}
+// indexing a vertex array of 32-byte {x, y, z, 0} entries, the vertices numbered in order of
+// first use by the leaf-ordered triangles (so a leaf's vertices sit together) and each shared
+// vertex stored once.  That is 16 B + 3 x 32 B per test against 96 B for a precomputed
+// record, but the distinct data of a mesh is 16 B per triangle + 32 B per vertex: a 2M-triangle
+// grid needs 67 MB instead of 201 MB, which keeps far more of it in L2.
+constexpr int kPayloadDoubles[kNumKinds] = {0, 4, 14, 16};
+constexpr int kVertexDoubles = 4;
 
 struct KindView {
   const double *nodes64 = nullptr;  // n_internal * kNode64Doubles
   const float *nodes32 = nullptr;   // n_internal * kNode32Floats
-  const double *payload = nullptr;  // n_prims * kPayloadDoubles[kind]
+  const double *payload = nullptr;  // n_prims * kPayloadDoubles[kind] (spheres, planes, cylinders)
+  const uint32_t *tri = nullptr;    // triangles: n_prims * 4 {i0, i1, i2, id word}
+  const double *verts = nullptr;    // triangles: kVertexDoubles per vertex {x, y, z, 0}
   const uint32_t *prim_ids = nullptr;  // n_prims: id | kLastBit on a leaf's last primitive
   uint32_t n_internal = 0;
   uint32_t n_prims = 0;

@@ -405,6 +405,11 @@ KindImage flatten(const HostScene &s, int kind) {
   const int stride = kPayloadDoubles[kind];
   img.prim_ids.resize(np);
   img.payload.assign(np * stride, 0.0);
+  std::vector<uint32_t> remap;
+  if (kind == kMesh) {
+    img.tri.resize(4 * np);
+    remap.assign(s.vertices.size() / 3, 0xFFFFFFFFu);
+  }
   for (size_t i = 0; i < nn; ++i) {
     const TreeNode &nd = t.nodes[i];
     if (nd.leaf != 1) continue;
@@ -412,17 +417,20 @@ KindImage flatten(const HostScene &s, int kind) {
       const uint32_t at = leaf_pos[i] + q;
       const uint32_t id = t.leaf_prims[nd.prim_off + q];
       img.prim_ids[at] = id | (q + 1 == nd.prim_cnt ? kLastBit : 0u);
-      double *p = &img.payload[size_t(at) * stride];
+      double *p = img.payload.data() + size_t(at) * stride;
       switch (kind) {
         case kMesh: {
           const uint32_t *F = &s.faces[3 * id];
-          const V3 v0 = load3(&s.vertices[3 * F[0]]), v1 = load3(&s.vertices[3 * F[1]]),
-                   v2 = load3(&s.vertices[3 * F[2]]);
-          const V3 e1 = v0 - v1, e2 = v2 - v0;  // the reference Triangle's c and b
-          store3(p, v0);
-          store3(p + 3, e1);
-          store3(p + 6, e2);
-          store3(p + 9, cross(e1, e2));
+          for (int j = 0; j < 3; ++j) {
+            uint32_t &r = remap[F[j]];
+            if (r == 0xFFFFFFFFu) {
+              r = static_cast<uint32_t>(img.verts.size() / kVertexDoubles);
+              const double *v = &s.vertices[3 * size_t(F[j])];
+              img.verts.insert(img.verts.end(), {v[0], v[1], v[2], 0.0});
+            }
+            img.tri[4 * size_t(at) + j] = r;
+          }
+          img.tri[4 * size_t(at) + 3] = img.prim_ids[at];
           break;
         }
         case kSpheres:

@@ -157,13 +157,20 @@ BZR_HD double2 ld2(const double *p) {
   return ldg(reinterpret_cast<const double2 *>(p));
 }
 
-// blazert/primitives/trimesh.h:153-181 with the precomputed n = cross(e1, e2)
-BZR_HD bool isect_triangle(const double *P, uint32_t pos, const Ray &r,
-                                               KState &st) {
-  const double2 q0 = ld2(P), q1 = ld2(P + 2), q2 = ld2(P + 4), q3 = ld2(P + 6), q4 = ld2(P + 8),
-                q5 = ld2(P + 10);
-  const D3 v0 = d3(q0.x, q0.y, q1.x), e1 = d3(q1.y, q2.x, q2.y), e2 = d3(q3.x, q3.y, q4.x),
-           n = d3(q4.y, q5.x, q5.y);
+BZR_HD D3 ld_vertex(const double *verts, uint32_t i) {
+  const double *p = verts + size_t(i) * kVertexDoubles;
+  const double2 xy = ld2(p), z0 = ld2(p + 2);
+  return d3(xy.x, xy.y, z0.x);
+}
+
+// blazert/primitives/trimesh.h:153-181.  F holds the triangle's three vertex indices; v0,
+// e1 = v0 - v1, e2 = v2 - v0 (the reference Triangle's members, trimesh.h:19-31) and
+// n = cross(e1, e2) are formed here with the reference's operations, hence the same bits.
+BZR_HD bool isect_triangle(const double *verts, uint4 F, uint32_t pos, const Ray &r,
+                           KState &st) {
+  const D3 v0 = ld_vertex(verts, F.x), v1 = ld_vertex(verts, F.y), v2 = ld_vertex(verts, F.z);
+  const D3 e1 = sub(v0, v1), e2 = sub(v2, v0);
+  const D3 n = cross(e1, e2);
   const D3 c = sub(v0, r.o);
   const D3 rr = cross(r.d, c);
   const double det = dot(n, r.d);
@@ -349,14 +356,21 @@ BZR_NOINLINE bool isect_cylinder(const double *P, uint32_t pos, const Ray &r,
   return false;
 }
 
+// Tests the primitive at leaf position pos and returns its id word (id | kLastBit on the
+// leaf's last primitive).
 template <int KIND>
-BZR_HD bool isect(const double *payload, uint32_t pos, const Ray &r,
-                                      KState &st) {
-  const double *P = payload + size_t(pos) * kPayloadDoubles[KIND];
-  if (KIND == kMesh) return isect_triangle(P, pos, r, st);
-  if (KIND == kSpheres) return isect_sphere(P, pos, r, st);
-  if (KIND == kPlanes) return isect_plane(P, pos, r, st);
-  return isect_cylinder(P, pos, r, st);
+BZR_HD uint32_t isect(const KindView &K, uint32_t pos, const Ray &r, KState &st) {
+  if (KIND == kMesh) {
+    const uint4 F = ldg(reinterpret_cast<const uint4 *>(K.tri) + pos);
+    isect_triangle(K.verts, F, pos, r, st);
+    return F.w;
+  }
+  const uint32_t id = ldg(K.prim_ids + pos);
+  const double *P = K.payload + size_t(pos) * kPayloadDoubles[KIND];
+  if (KIND == kSpheres) isect_sphere(P, pos, r, st);
+  else if (KIND == kPlanes) isect_plane(P, pos, r, st);
+  else isect_cylinder(P, pos, r, st);
+  return id;
 }
 
 // Traversal stack in shared memory, entry j of thread t at [j * blockDim.x + t].
@@ -461,9 +475,8 @@ BZR_HD void trav_leaf(const KindView &K, const Ray &r, KState &st, Trav &tv, con
       tv.live = false;
       return;
     }
-    const uint32_t id = ldg(K.prim_ids + pos);
     if (COUNT) cnt->prim[KIND] += 1;
-    isect<KIND>(K.payload, pos, r, st);
+    const uint32_t id = isect<KIND>(K, pos, r, st);
     if (id & kLastBit) break;
     ++pos;
   }
@@ -689,9 +702,8 @@ BZR_HD void trav_leaf32(const KindView &K, const Ray &r, const RayF &f, KState &
       tv.live = false;
       return;
     }
-    const uint32_t id = ldg(K.prim_ids + pos);
     if (COUNT) cnt->prim[KIND] += 1;
-    isect<KIND>(K.payload, pos, r, st);
+    const uint32_t id = isect<KIND>(K, pos, r, st);
     if (id & kLastBit) break;
     ++pos;
   }

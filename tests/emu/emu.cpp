@@ -63,6 +63,8 @@ void *emu_scene_create(const int *order, int n_order, const double *verts, long 
     v.nodes32 = im.nodes32.data();
     v.payload = im.payload.data();
     v.prim_ids = im.prim_ids.data();
+    v.tri = im.tri.data();
+    v.verts = im.verts.data();
     v.n_internal = im.n_internal;
     v.n_prims = static_cast<uint32_t>(im.prim_ids.size());
     v.root_ref = im.root_ref;
