@@ -40,23 +40,45 @@ namespace {
 constexpr uint32_t kChunk = 64;  // rays taken from the global counter per warp fetch
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
+// Traversal stack storage.  LOCAL: a thread-local array of kLocalStack entries (local memory,
+// cached in L1; the host picks it when the tree's stack fits, and it leaves the SM's shared
+// memory to L1 and the occupancy to the register count).  Otherwise shared memory sized from
+// the tree, entry j of thread t at [j * blockDim.x + t].  The capacity is clamped to the
+// storage, so a mismatch is reported as kErrStack, never written past.
+template <bool LOCAL>
+__device__ __forceinline__ void init_stack(Stack &sk, uint32_t &tid, uint32_t cap,
+                                           unsigned char *smem, double *lkey, uint32_t *lref) {
+  if (LOCAL) {
+    sk.stride = 1;
+    sk.cap = cap < kLocalStack ? cap : kLocalStack;
+    sk.key = lkey;
+    sk.ref = lref;
+    tid = 0;
+  } else {
+    sk.stride = blockDim.x;
+    sk.cap = cap;
+    sk.key = reinterpret_cast<double *>(smem);
+    sk.ref = reinterpret_cast<uint32_t *>(sk.key + size_t(sk.cap) * sk.stride);
+    tid = threadIdx.x;
+  }
+}
+
 // One kind over the whole batch.  first: this pass writes the whole output record.
 // COUNT: also sums the work counters into totals[8] (box tests per kind, then primitive
 // tests per kind).
-template <int KIND, bool COUNT, bool MIXED>
+template <int KIND, bool COUNT, bool MIXED, bool LOCAL>
 __global__ void __launch_bounds__(kTraceThreads)
     trace_kind_kernel(SceneView S, RayIO io, int first, uint32_t *work_counter,
                       unsigned long long *totals) {
   extern __shared__ __align__(16) unsigned char smem[];
+  double lkey[LOCAL ? kLocalStack : 1];
+  uint32_t lref[LOCAL ? kLocalStack : 1];
   Stack sk;
-  sk.stride = blockDim.x;
-  sk.cap = S.stack_cap;
-  sk.key = reinterpret_cast<double *>(smem);
-  sk.ref = reinterpret_cast<uint32_t *>(sk.key + size_t(sk.cap) * sk.stride);
+  uint32_t tid;
+  init_stack<LOCAL>(sk, tid, S.stack_cap, smem, lkey, lref);
   const KindView &K = S.k[KIND];
   const unsigned lane = threadIdx.x & 31u;
   const unsigned below = (1u << lane) - 1u;
-  const uint32_t tid = threadIdx.x;
   uint32_t pool_next = 0, pool_end = 0;  // warp-uniform
   bool exhausted = false;                // warp-uniform
   bool active = false;
@@ -134,18 +156,17 @@ __global__ void __launch_bounds__(kTraceThreads)
 // keeps its own ray's scene, so a warp may finish rays of one scene while starting another's.
 // The pass of a scene's first kind writes its whole record; the pass of its last kind
 // completes it and stamps the scene's completion time.
-template <int KIND, bool MIXED>
+template <int KIND, bool MIXED, bool LOCAL>
 __global__ void __launch_bounds__(kTraceThreads)
     trace_batch_kernel(BatchView B, RayIO io, uint32_t *chunk_counter, uint32_t stack_cap) {
   extern __shared__ __align__(16) unsigned char smem[];
+  double lkey[LOCAL ? kLocalStack : 1];
+  uint32_t lref[LOCAL ? kLocalStack : 1];
   Stack sk;
-  sk.stride = blockDim.x;
-  sk.cap = stack_cap;
-  sk.key = reinterpret_cast<double *>(smem);
-  sk.ref = reinterpret_cast<uint32_t *>(sk.key + size_t(sk.cap) * sk.stride);
+  uint32_t tid;
+  init_stack<LOCAL>(sk, tid, stack_cap, smem, lkey, lref);
   const unsigned lane = threadIdx.x & 31u;
   const unsigned below = (1u << lane) - 1u;
-  const uint32_t tid = threadIdx.x;
   uint32_t pool_next = 0, pool_end = 0, pool_scene = 0;  // warp-uniform
   bool exhausted = false;
   bool active = false;
@@ -333,39 +354,66 @@ __global__ void sort_scatter_kernel(uint32_t n, const uint32_t *keys, uint32_t *
   }
 }
 
+// The counting kernels (measurement only) always keep the stack in shared memory; the
+// tracing kernels use the thread-local stack whenever the tree's stack fits it.
 template <int KIND, bool COUNT>
 cudaError_t launch_kind(const SceneView &S, const RayIO &io, int mode, int first, int blocks,
                         cudaStream_t stream, uint32_t *counter, unsigned long long *totals) {
-  const size_t smem = trace_smem_bytes(S.stack_cap, kTraceThreads);
-  if (mode == kModeMixed)
-    trace_kind_kernel<KIND, COUNT, true><<<blocks, kTraceThreads, smem, stream>>>(
-        S, io, first, counter, totals);
-  else
-    trace_kind_kernel<KIND, COUNT, false><<<blocks, kTraceThreads, smem, stream>>>(
-        S, io, first, counter, totals);
+  const bool mixed = mode == kModeMixed;
+  if (!COUNT && S.stack_cap <= kLocalStack) {
+    if (mixed)
+      trace_kind_kernel<KIND, false, true, true><<<blocks, kTraceThreads, 0, stream>>>(
+          S, io, first, counter, totals);
+    else
+      trace_kind_kernel<KIND, false, false, true><<<blocks, kTraceThreads, 0, stream>>>(
+          S, io, first, counter, totals);
+  } else {
+    const size_t smem = trace_smem_bytes(S.stack_cap, kTraceThreads);
+    if (mixed)
+      trace_kind_kernel<KIND, COUNT, true, false><<<blocks, kTraceThreads, smem, stream>>>(
+          S, io, first, counter, totals);
+    else
+      trace_kind_kernel<KIND, COUNT, false, false><<<blocks, kTraceThreads, smem, stream>>>(
+          S, io, first, counter, totals);
+  }
   return cudaGetLastError();
+}
+
+// Resident blocks per SM of `fn` with `smem` bytes of dynamic shared memory, times the SMs.
+cudaError_t grid_for(const void *fn, size_t smem, int sms, int *blocks) {
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTraceThreads, smem);
+  if (e != cudaSuccess) return e;
+  *blocks = sms * (per_sm > 0 ? per_sm : 1);
+  return cudaSuccess;
 }
 
 template <int KIND>
 cudaError_t prepare_kind(uint32_t stack_cap, int sms, int *blocks, int *blocks32) {
   const size_t smem = trace_smem_bytes(stack_cap, kTraceThreads);
-  const void *fns[4] = {reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, false>),
-                        reinterpret_cast<const void *>(trace_kind_kernel<KIND, true, false>),
-                        reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, true>),
-                        reinterpret_cast<const void *>(trace_kind_kernel<KIND, true, true>)};
-  for (const void *fn : fns) {
-    const cudaError_t e =
-        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  const void *shared_fns[4] = {
+      reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, false, false>),
+      reinterpret_cast<const void *>(trace_kind_kernel<KIND, true, false, false>),
+      reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, true, false>),
+      reinterpret_cast<const void *>(trace_kind_kernel<KIND, true, true, false>)};
+  int counting = 0;
+  for (const void *fn : shared_fns) {
+    const cudaError_t e = grid_for(fn, smem, sms, &counting);
     if (e != cudaSuccess) return e;
   }
-  int per_sm = 0, per_sm32 = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fns[0], kTraceThreads, smem);
+  if (stack_cap <= kLocalStack) {
+    const cudaError_t e = grid_for(
+        reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, false, true>), 0, sms,
+        blocks);
+    if (e != cudaSuccess) return e;
+    return grid_for(reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, true, true>), 0,
+                    sms, blocks32);
+  }
+  const cudaError_t e = grid_for(shared_fns[0], smem, sms, blocks);
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm32, fns[2], kTraceThreads, smem);
-  if (e != cudaSuccess) return e;
-  *blocks = sms * (per_sm > 0 ? per_sm : 1);
-  *blocks32 = sms * (per_sm32 > 0 ? per_sm32 : 1);
-  return cudaSuccess;
+  return grid_for(shared_fns[2], smem, sms, blocks32);
 }
 
 }  // namespace
@@ -473,20 +521,15 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
 namespace {
 template <int KIND>
 cudaError_t prepare_batch_kind(uint32_t stack_cap, int sms, int *blocks, int *blocks32) {
-  const size_t smem = trace_smem_bytes(stack_cap, kTraceThreads);
-  const void *fns[2] = {reinterpret_cast<const void *>(trace_batch_kernel<KIND, false>),
-                        reinterpret_cast<const void *>(trace_batch_kernel<KIND, true>)};
-  int per[2] = {0, 0};
-  for (int j = 0; j < 2; ++j) {
-    cudaError_t e =
-        cudaFuncSetAttribute(fns[j], cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[j], fns[j], kTraceThreads, smem);
-    if (e != cudaSuccess) return e;
-  }
-  *blocks = sms * (per[0] > 0 ? per[0] : 1);
-  *blocks32 = sms * (per[1] > 0 ? per[1] : 1);
-  return cudaSuccess;
+  const bool local = stack_cap <= kLocalStack;
+  const size_t smem = local ? 0 : trace_smem_bytes(stack_cap, kTraceThreads);
+  const void *fp64 = local ? reinterpret_cast<const void *>(trace_batch_kernel<KIND, false, true>)
+                           : reinterpret_cast<const void *>(trace_batch_kernel<KIND, false, false>);
+  const void *mixed = local ? reinterpret_cast<const void *>(trace_batch_kernel<KIND, true, true>)
+                            : reinterpret_cast<const void *>(trace_batch_kernel<KIND, true, false>);
+  const cudaError_t e = grid_for(fp64, smem, sms, blocks);
+  if (e != cudaSuccess) return e;
+  return grid_for(mixed, smem, sms, blocks32);
 }
 }  // namespace
 
@@ -517,17 +560,26 @@ cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const Ba
   if (e != cudaSuccess) return e;
   batch_start_kernel<<<1, 256, 0, stream>>>(B, B.n_scenes);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const size_t smem = trace_smem_bytes(plan.stack_cap, kTraceThreads);
+  const bool local = plan.stack_cap <= kLocalStack;
+  const size_t smem = local ? 0 : trace_smem_bytes(plan.stack_cap, kTraceThreads);
   for (int k = 0; k < kNumKinds; ++k) {
     if (!(plan.kinds_present & (1 << k))) continue;
     const bool m = mode == kModeMixed;
     const int b = m ? plan.blocks32[k] : plan.blocks[k];
     uint32_t *c = counters + k;
-#define BZR_BATCH_LAUNCH(KK)                                                                  \
-  if (m)                                                                                      \
-    trace_batch_kernel<KK, true><<<b, kTraceThreads, smem, stream>>>(B, io, c, plan.stack_cap); \
-  else                                                                                        \
-    trace_batch_kernel<KK, false><<<b, kTraceThreads, smem, stream>>>(B, io, c, plan.stack_cap);
+#define BZR_BATCH_LAUNCH(KK)                                                                 \
+  if (local && m)                                                                            \
+    trace_batch_kernel<KK, true, true><<<b, kTraceThreads, 0, stream>>>(B, io, c,            \
+                                                                        plan.stack_cap);     \
+  else if (local)                                                                            \
+    trace_batch_kernel<KK, false, true><<<b, kTraceThreads, 0, stream>>>(B, io, c,           \
+                                                                         plan.stack_cap);    \
+  else if (m)                                                                                \
+    trace_batch_kernel<KK, true, false><<<b, kTraceThreads, smem, stream>>>(B, io, c,        \
+                                                                            plan.stack_cap); \
+  else                                                                                       \
+    trace_batch_kernel<KK, false, false><<<b, kTraceThreads, smem, stream>>>(B, io, c,       \
+                                                                             plan.stack_cap);
     switch (k) {
       case kMesh: BZR_BATCH_LAUNCH(kMesh); break;
       case kSpheres: BZR_BATCH_LAUNCH(kSpheres); break;

@@ -39,6 +39,40 @@ def test_workload_bit_exact(name, mode):
     assert mismatches(out_host, ref) == []
 
 
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+@pytest.mark.parametrize("max_depth", [62, 100])
+def test_deep_tree_stack_storage(mode, max_depth):
+    """150 spheres at x = 8^i (up to 3.6e134) with leaves of one sphere build a chain-like tree
+    of depth 70 when max_tree_depth allows it.  Then the traversal stack (depth + 2 entries)
+    exceeds the kernels' 64-entry thread-local stack and lives in shared memory; capped at
+    depth 62 it fits the local stack.  Both must match the oracle built with the same
+    options."""
+    import torch
+
+    import blazert_b200 as B
+
+    n = 150
+    c = np.zeros((n, 3))
+    c[:, 0] = 8.0 ** np.arange(n)
+    c[:, 1] = np.linspace(-0.05, 0.05, n)
+    spec = W.SceneSpec().add_spheres(c, np.full(n, 0.1))
+    rng = np.random.Generator(np.random.PCG64(71))
+    k = rng.integers(0, n, 4096)
+    o = np.stack([c[k, 0] - 1.0, rng.uniform(-0.2, 0.2, 4096), rng.uniform(-0.2, 0.2, 4096)], 1)
+    d = np.stack([np.ones(4096), rng.uniform(-0.05, 0.05, 4096), rng.uniform(-0.05, 0.05, 4096)], 1)
+    opts = B.BuildOptions(min_leaf_primitives=1, max_tree_depth=max_depth)
+    s = product_scene(spec, opts)
+    depth = s.stats("spheres")["max_depth"]
+    assert (depth + 2 > 64) == (max_depth == 100), depth
+    ref = Oracle(spec, min_leaf=1, max_depth=max_depth).intersect(o, d)
+    assert ref["hit"].sum() > 500
+    dev = torch.device("cuda", 0)
+    out = s.intersectN(torch.from_numpy(o).to(dev), torch.from_numpy(d).to(dev), mode=mode)
+    torch.cuda.synchronize()
+    assert s.check() == 0
+    assert mismatches(out, ref) == []
+
+
 def test_intersect1_matches_batch():
     import blazert_b200 as B
 
