@@ -285,11 +285,12 @@ def run_ours(args):
     import blazert_b200 as B
     from blazert_b200 import workloads as W
 
+    from blazert_b200 import multi
+
     wl = W.WORKLOADS[args.workload](**({"n_rays": args.rays} if args.rays else {}))
     R = wl.rays
-    if rank > 0:  # each rank traces its own batch: rotate the rays so ranks differ
-        sh = (rank * 7919) % R.n
-        R = W.RayBatch(np.roll(R.origins, sh, 0), np.roll(R.directions, sh, 0), R.tmin, R.tmax)
+    if rank > 0:  # weak scaling: each rank traces its own full-size batch
+        R = W.RayBatch(*multi.rank_batch(R.origins, R.directions, R.tmin, R.tmax, rank))
     scene = B.Scene()
     for kind in wl.scene.order:
         d = getattr(wl.scene, kind)
@@ -351,9 +352,7 @@ def run_ours(args):
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = sum(step_ms)
     if pg:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = multi.max_over_ranks(total_ms)
     value = world * n * args.steps / (total_ms / 1e3) / 1e6
     hits = float(out["hit"].float().mean().item())
     # one traversal kernel per primitive kind present, per step
@@ -391,9 +390,7 @@ def run_ours(args):
             scene.intersectN(ho, hd, htmn, htmx, mode=args.mode, out=hout)
         el = time.perf_counter() - t0
         if pg:
-            t = torch.tensor([el], dtype=torch.float64, device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            el = float(t.item())
+            el = multi.max_over_ranks(el)
         e2e = {"value": world * n * args.steps / el / 1e6, "unit": "Mrays/s",
                "h2d_bytes_per_step": n * (24 + 24 + 8 + 8),
                "d2h_bytes_per_step": n * (8 + 16 + 24 + 4 + 4 + 1)}
