@@ -40,6 +40,23 @@ def test_workload_bit_exact(name, mode):
 
 
 @pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_four_kinds_merge(mode):
+    """All four kinds overlapping in space, so that every rule of the merge across kind passes
+    (triangles first, strict '<' for later kinds, misses) decides some rays; device arrays and
+    host arrays (in chunks) both equal the oracle."""
+    wl = W.mixed_primitives(n_rays=400_000, n_spheres=2000, n_cylinders=400, n_planes=60, seed=31)
+    v, f = W.icosphere(3)
+    spec = W.SceneSpec().add_mesh(v * 60.0, f)
+    for k in wl.scene.order:
+        getattr(spec, "add_" + k)(*getattr(wl.scene, k).values())
+    wl4 = W.Workload("four_kinds", spec, wl.rays, {})
+    ref, out_dev, out_host = _run_both(wl4, mode)
+    assert len(set(ref["geom"][ref["hit"] == 1].tolist())) == 4
+    assert mismatches(out_dev, ref) == []
+    assert mismatches(out_host, ref) == []
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
 @pytest.mark.parametrize("max_depth", [62, 100])
 def test_deep_tree_stack_storage(mode, max_depth):
     """150 spheres at x = 8^i (up to 3.6e134) with leaves of one sphere build a chain-like tree
