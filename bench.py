@@ -259,7 +259,9 @@ def run_batched(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)",
             "config": {"workload": "batched_icospheres", "scenes": len(wls), "rays_per_gpu": n,
-                       "levels": [w.meta["level"] for w in wls], "mode": args.mode,
+                       "scenes_per_level": {str(lv): sum(1 for w in wls if w.meta["level"] == lv)
+                                            for lv in sorted({w.meta["level"] for w in wls})},
+                       "mode": args.mode,
                        "graph": "CUDA graph replay", "l2": "flushed between timed steps"},
             "gpu_launches": args.steps * 2,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
@@ -426,12 +428,154 @@ def run_ours(args):
     return 0
 
 
+# bytes the adjoint reads and writes per ray hit: rays (48), forward record t/prim/geom/hit
+# (17), dL/dt (8), dL/d(origin, direction) out (48), three vertices or one sphere (72) read and
+# their gradient accumulated (72)
+ADJOINT_BYTES_PER_RAY = 48 + 17 + 8 + 48 + 72 + 72
+
+
+def run_adjoint(args):
+    """Differentiation form: one step = the forward closest-hit pass over the batch, dL/dt of
+    L = sum w_i t_i^2 (w ~ N(0, 1), misses contribute 0), and the adjoint kernels giving
+    dL/d(vertices, sphere centres and radii, ray origins and directions).  Mrays/s of the whole
+    step; the adjoint's own time is reported beside it."""
+    import numpy as np
+    import torch
+
+    import blazert_b200 as B
+    from blazert_b200 import multi
+    from blazert_b200 import workloads as W
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    wl = W.adjoint_scene(**({"n_rays": args.rays} if args.rays else {}))
+    R = wl.rays
+    if rank > 0:
+        R = W.RayBatch(*multi.rank_batch(R.origins, R.directions, R.tmin, R.tmax, rank))
+    spec = wl.scene
+    scene = B.Scene()
+    for kind in spec.order:
+        getattr(scene, "add_" + kind)(*getattr(spec, kind).values())
+    scene.commit()
+    n = R.n
+    nv, ns = len(spec.mesh["vertices"]), len(spec.spheres["radii"])
+    o = torch.from_numpy(R.origins).to(dev)
+    d = torch.from_numpy(R.directions).to(dev)
+    w = torch.from_numpy(np.asarray(wl.meta["weights"])[:n]).to(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(ev=None):
+        fwd = scene.intersectN(o, d, stream=stream)
+        gt = torch.where(fwd["hit"].bool(), 2.0 * w * fwd["t"], torch.zeros_like(w))
+        if ev is not None:
+            ev.record(stream)
+        return scene.adjoint(o, d, fwd, grad_t=gt, n_vertices=nv, n_spheres=ns, stream=stream)
+
+    for i in range(args.warmup):
+        flush.fill_(i & 0xFF)
+        step()
+    torch.cuda.synchronize(dev)
+    scene.check()
+    if pg:
+        pg.barrier()
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.fill_((i + 1) & 0xFF)
+        evs[i][0].record(stream)
+        step(evs[i][1])
+        evs[i][2].record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop() if sampler else None
+    scene.check()
+    total_ms = sum(a.elapsed_time(c) for a, _, c in evs)
+    adj_ms = sum(b.elapsed_time(c) for _, b, c in evs)
+    if pg:
+        total_ms = multi.max_over_ranks(total_ms)
+        adj_ms = multi.max_over_ranks(adj_ms)
+    value = world * n * args.steps / (total_ms / 1e3) / 1e6
+    fwd = scene.intersectN(o, d, stream=stream)
+    hit_frac = float(fwd["hit"].float().mean().item())
+    counts = scene.work_counts(o, d, stream=stream)
+    fwd_bytes = n * RAY_IO_BYTES + BOX_TEST_BYTES * sum(counts["box"]) + \
+        sum(PRIM_RECORD_BYTES[k] * counts["prim"][k] for k in range(4))
+    alg_bytes = fwd_bytes + hit_frac * n * ADJOINT_BYTES_PER_RAY
+    achieved = alg_bytes / (total_ms / args.steps / 1e3) / 1e9
+    peak, peak_src = load_peaks()
+
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+        ho, hd = pin(R.origins), pin(R.directions)
+        hw = pin(np.asarray(wl.meta["weights"])[:n])
+        host_out = {k: torch.empty(shape, dtype=torch.float64).pin_memory()
+                    for k, shape in (("vertices", (nv, 3)), ("centers", (ns, 3)),
+                                     ("radii", (ns,)), ("origins", (n, 3)),
+                                     ("directions", (n, 3)))}
+
+        def e2e_step():
+            o.copy_(ho, non_blocking=True)
+            d.copy_(hd, non_blocking=True)
+            w.copy_(hw, non_blocking=True)
+            g = step()
+            for k, t in host_out.items():
+                t.copy_(g[k], non_blocking=True)
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        torch.cuda.synchronize(dev)
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        torch.cuda.synchronize(dev)
+        el = time.perf_counter() - t0
+        if pg:
+            el = multi.max_over_ranks(el)
+        e2e = {"value": world * n * args.steps / el / 1e6, "unit": "Mrays/s",
+               "h2d_bytes_per_step": n * (24 + 24 + 8),
+               "d2h_bytes_per_step": 8 * (3 * nv + 3 * ns + ns + 6 * n)}
+
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC + " (forward + adjoint)", "value": value, "unit": "Mrays/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "adjoint_scene", "rays_per_gpu": n, "triangles": len(spec.mesh["faces"]),
+                       "spheres": ns, "loss": "sum w t^2, w ~ N(0,1)",
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "adjoint_ms_per_step": adj_ms / args.steps, "hit_fraction": hit_frac,
+            "e2e": e2e,
+            "gpu_launches": args.steps * 4,  # two kind passes, the ray and face adjoint kernels
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_source": peak_src},
+            "clocks": clocks}), flush=True)
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
 def main(argv=None):
     args = parse(argv)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batched_icospheres":
         return run_batched(args)
+    if args.workload == "adjoint_scene":
+        return run_adjoint(args)
     return run_ours(args)
 
 

@@ -8,12 +8,16 @@
 #include "scene.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <future>
 #include <limits>
 #include <numeric>
 #include <queue>
+#include <system_error>
+#include <thread>
 
 namespace bzr {
 namespace {
@@ -92,10 +96,13 @@ inline double surface(const double *mn, const double *mx) {
   return 2.0 * ((e0 * e1 + e1 * e2) + e2 * e0);
 }
 
+// Subtrees of at least this many primitives may be built on another thread.
+constexpr uint32_t kParallelPrims = 1u << 15;
+
 class SahBuilder {
  public:
-  SahBuilder(const PrimBoxes &p, const BuildOptions &o, Tree &t)
-      : p_(p), o_(o), t_(t), bins_(3 * size_t(o.bins)) {}
+  SahBuilder(const PrimBoxes &p, const BuildOptions &o, Tree &t, std::atomic<int> *threads)
+      : p_(p), o_(o), t_(t), bins_(3 * size_t(o.bins)), threads_(threads) {}
 
   // Returns the index of the node created for [begin, end) (blazert/bvh/builder.h:84-115).
   uint32_t node(uint32_t *begin, uint32_t *end, uint32_t depth) {
@@ -124,10 +131,36 @@ class SahBuilder {
     nd.axis = split(begin, end, nd.mn, nd.mx, mid);
     nd.prim_off = nd.prim_cnt = 0;
     t_.nodes[self] = nd;
+    // The two halves of the id range are disjoint, so a large right subtree can be built on
+    // another thread into its own fragment while this thread builds the left one; splicing
+    // the fragment after the left subtree gives the same DFS pre-order node numbering and leaf
+    // order as the sequential recursion.
+    std::future<Tree> right;
+    if (threads_ && static_cast<uint32_t>(end - mid) >= kParallelPrims) {
+      if (threads_->fetch_sub(1) > 0) {
+        try {
+          right = std::async(std::launch::async, [this, mid, end, depth] {
+            Tree frag;
+            SahBuilder b(p_, o_, frag, threads_);
+            b.node(mid, end, depth + 1);
+            threads_->fetch_add(1);
+            return frag;
+          });
+        } catch (const std::system_error &) {  // no thread available: build it here
+          threads_->fetch_add(1);
+        }
+      } else {
+        threads_->fetch_add(1);  // no thread left: undo the claim
+      }
+    }
     const uint32_t c0 = node(begin, mid, depth + 1);
     t_.nodes[self].child[0] = c0;
-    const uint32_t c1 = node(mid, end, depth + 1);
-    t_.nodes[self].child[1] = c1;
+    if (right.valid()) {
+      t_.nodes[self].child[1] = splice(right.get());
+    } else {
+      const uint32_t c1 = node(mid, end, depth + 1);
+      t_.nodes[self].child[1] = c1;
+    }
     return self;
   }
 
@@ -203,10 +236,30 @@ class SahBuilder {
     return axis;
   }
 
+  // Appends a subtree built as its own fragment (root at index 0); returns its root index.
+  uint32_t splice(Tree &&f) {
+    const auto base = static_cast<uint32_t>(t_.nodes.size());
+    const auto pbase = static_cast<uint32_t>(t_.leaf_prims.size());
+    for (TreeNode nd : f.nodes) {
+      if (nd.leaf == 1) {
+        nd.prim_off += pbase;
+      } else {
+        nd.child[0] += base;
+        nd.child[1] += base;
+      }
+      t_.nodes.push_back(nd);
+    }
+    t_.leaf_prims.insert(t_.leaf_prims.end(), f.leaf_prims.begin(), f.leaf_prims.end());
+    t_.max_depth = std::max(t_.max_depth, f.max_depth);
+    t_.bad_splits += f.bad_splits;
+    return base;
+  }
+
   const PrimBoxes &p_;
   const BuildOptions &o_;
   Tree &t_;
   std::vector<Bin> bins_;
+  std::atomic<int> *threads_;  // threads that may still be started
 };
 
 // Outward rounding of a double bound to float.
@@ -231,7 +284,9 @@ Tree build_tree(const PrimBoxes &boxes, const BuildOptions &opt) {
   std::iota(ids.begin(), ids.end(), 0u);
   t.nodes.reserve(2 * boxes.n + 1);
   t.leaf_prims.reserve(boxes.n);
-  SahBuilder b(boxes, opt, t);
+  const unsigned hw = std::thread::hardware_concurrency();
+  std::atomic<int> threads{hw > 1 ? static_cast<int>(hw) - 1 : 0};
+  SahBuilder b(boxes, opt, t, &threads);
   b.node(ids.data(), ids.data() + ids.size(), 0);
   t.build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return t;

@@ -63,6 +63,17 @@ def test_product_builder_matches_reference(case):
 
 
 @needs_ref
+def test_parallel_builder_matches_reference_on_large_mesh():
+    """A 293,046-triangle grid: the product builder builds subtrees of 32,768 primitives or
+    more on other threads and splices them back; the tree must still be the reference's node
+    for node (DFS numbering, leaf order, boxes)."""
+    wl = W.heightfield(n_rays=16, grid=384)
+    ref = RefScene(wl.scene)
+    emu = EmuScene(wl.scene)
+    assert same_tree(emu.tree("mesh"), ref.tree("mesh")) is None
+
+
+@needs_ref
 @pytest.mark.parametrize("opts", [dict(min_leaf=1, max_depth=28, bins=64),
                                   dict(min_leaf=8, max_depth=6, bins=16),
                                   dict(min_leaf=2, max_depth=40, bins=3),
