@@ -357,6 +357,24 @@ def run_ours(args):
         total_ms = multi.max_over_ranks(total_ms)
     value = world * n * args.steps / (total_ms / 1e3) / 1e6
     hits = float(out["hit"].float().mean().item())
+    precision = None
+    if args.mode == "mixed":  # the precision form's report: its results against the FP64 path's
+        ref = scene.intersectN(o, d, tmn, tmx, mode="fp64", stream=stream)
+        torch.cuda.synchronize(dev)
+        hm = out["hit"] == ref["hit"]
+        same = hm & (out["prim"] == ref["prim"]) & (out["geom"] == ref["geom"])
+        both = (out["hit"] == 1) & (ref["hit"] == 1)
+        rel = ((out["t"] - ref["t"]).abs() / ref["t"].abs().clamp_min(1e-300))[both]
+        precision = {"vs": "FP64 GPU path (bit-identical to the oracle in the parity tests)",
+                     "hit_mismatches": int((~same).sum().item()),
+                     "t_max_rel_err": float(rel.max().item()) if rel.numel() else 0.0,
+                     "t_mean_rel_err": float(rel.mean().item()) if rel.numel() else 0.0,
+                     "bit_identical": bool(torch.equal(out["t"].view(torch.int64),
+                                                       ref["t"].view(torch.int64))
+                                           and torch.equal(out["normal"].view(torch.int64),
+                                                           ref["normal"].view(torch.int64))
+                                           and torch.equal(out["uv"].view(torch.int64),
+                                                           ref["uv"].view(torch.int64)))}
     # one traversal kernel per primitive kind present, per step
     n_passes = sum(1 for k in wl.scene.order if len(next(iter(getattr(wl.scene, k).values()))))
 
@@ -417,7 +435,7 @@ def run_ours(args):
                          "alg_bytes_per_ray": alg_bytes / n,
                          "box_tests_per_ray": [c / n for c in counts["box"]],
                          "prim_tests_per_ray": [c / n for c in counts["prim"]]},
-            "cpu_baseline": cpu, "clocks": clocks, "hit_fraction": hits,
+            "cpu_baseline": cpu, "clocks": clocks, "hit_fraction": hits, "precision": precision,
             "commit_seconds": commit_s, "wall_seconds_timed": wall, "tuning": tuning,
             "step_ms_min_max": [min(step_ms), max(step_ms)],
         }

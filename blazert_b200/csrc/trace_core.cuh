@@ -13,7 +13,6 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 #define BZR_HD __host__ __device__ __forceinline__
-#define BZR_NOINLINE __host__ __device__ __noinline__
 #define BZR_INF (__builtin_inf())
 #else
 #include <vector_types.h>
@@ -21,7 +20,6 @@
 using std::isfinite;
 using std::isnan;
 #define BZR_HD inline
-#define BZR_NOINLINE inline
 #define BZR_INF (__builtin_inf())
 #endif
 
@@ -268,16 +266,21 @@ BZR_HD bool isect_plane(const double *P, uint32_t pos, const Ray &r,
   return true;
 }
 
-BZR_HD bool cyl_hit(KState &st, uint32_t pos, D3 n, double t, D3 dir) {
-  st.n = n;
-  st.hit = norm(mul(dir, t));
-  st.pos = pos;
-  return true;
-}
+// Result of one cylinder test: the reference's post-hit state (the normal as computed at hit
+// time and norm(t * dir) as the hit distance).
+struct CylHit {
+  bool hit;
+  double dist;
+  D3 n;
+};
 
-// blazert/primitives/cylinder.h:181-495 (no hit-distance test; unrotated normal in one branch)
-BZR_NOINLINE bool isect_cylinder(const double *P, uint32_t pos, const Ray &r,
-                                            KState &st) {
+BZR_HD CylHit cyl_hit(D3 n, double t, D3 dir) { return CylHit{true, norm(mul(dir, t)), n}; }
+BZR_HD CylHit cyl_miss() { return CylHit{false, 0.0, d3(0.0, 0.0, 0.0)}; }
+
+// blazert/primitives/cylinder.h:181-495 (no hit-distance test; unrotated normal in one branch).
+// Takes the ray's origin and direction and returns its result by value, so that nothing of the
+// caller's ray or state has to live in memory around the test.
+BZR_HD CylHit isect_cylinder(const double *P, D3 ro, D3 rd) {
   double R[9];
   const double2 q0 = ld2(P), q1 = ld2(P + 2), q2 = ld2(P + 4), q3 = ld2(P + 6), q4 = ld2(P + 8),
                 q5 = ld2(P + 10), q6 = ld2(P + 12), q7 = ld2(P + 14);
@@ -285,8 +288,8 @@ BZR_NOINLINE bool isect_cylinder(const double *P, uint32_t pos, const Ray &r,
   const double a = q1.y, b = q2.x, h = q2.y;
   R[0] = q3.x; R[1] = q3.y; R[2] = q4.x; R[3] = q4.y; R[4] = q5.x;
   R[5] = q5.y; R[6] = q6.x; R[7] = q6.y; R[8] = q7.x;
-  const D3 org = rot_t(R, sub(r.o, center));
-  const D3 dir = rot_t(R, r.d);
+  const D3 org = rot_t(R, sub(ro, center));
+  const D3 dir = rot_t(R, rd);
   const double x0 = org.x, y0 = org.y, z0 = org.z;
   const double j = dir.x, k = dir.y, l = dir.z;
   const double h2 = h / 2.0, mh2 = -h / 2.0;
@@ -299,8 +302,10 @@ BZR_NOINLINE bool isect_cylinder(const double *P, uint32_t pos, const Ray &r,
     const double C = a * a * k * k + b * b * j * j - j * j * y0 * y0 + 2 * j * k * x0 * y0 -
                      k * k * x0 * x0;
     if (C < 0) return false;
-    t0 = 1.0 / A * (-B + a * b * sqrt(C));
-    t1 = -1.0 / A * (B + a * b * sqrt(C));
+    const double rA = 1.0 / A;  // -1.0 / A is -(1.0 / A) exactly
+    const double s = a * b * sqrt(C);
+    t0 = rA * (-B + s);
+    t1 = -rA * (B + s);
     i0 = add(org, mul(dir, t0));
     i1 = add(org, mul(dir, t1));
     return true;
@@ -308,52 +313,52 @@ BZR_NOINLINE bool isect_cylinder(const double *P, uint32_t pos, const Ray &r,
   double t0, t1;
   D3 i0, i1;
   if (z0 > h2 || z0 < mh2) {  // areas 1 and 2: origin above or below the caps
-    if (l == 0) return false;
+    if (l == 0) return cyl_miss();
     const double zc = z0 > h2 ? h2 : mh2;
     const double tc = (zc - z0) / l;
-    if (tc < 0) return false;
+    if (tc < 0) return cyl_miss();
     const D3 ic = add(org, mul(dir, tc));
     if (b * b * ic.x * ic.x + a * a * ic.y * ic.y <= a * a * b * b)
-      return cyl_hit(st, pos, ng(d3(0.0, 0.0, z0 > h2 ? 1.0 : -1.0)), tc, dir);
-    if (!quad(t0, t1, i0, i1)) return false;
+      return cyl_hit(ng(d3(0.0, 0.0, z0 > h2 ? 1.0 : -1.0)), tc, dir);
+    if (!quad(t0, t1, i0, i1)) return cyl_miss();
     if ((t1 > 0) && (t1 < t0) && (i1.z <= h2) && (i1.z >= mh2))
-      return cyl_hit(st, pos, ng(shell_n(i1)), t1, dir);
+      return cyl_hit(ng(shell_n(i1)), t1, dir);
     if ((t0 > 0) && (t0 < t1) && (i0.z <= h2) && (i0.z >= mh2))
-      return cyl_hit(st, pos, ng(shell_n(i0)), t0, dir);
-    return false;  // area 4 cannot hold when z0 is outside [-h/2, h/2]
+      return cyl_hit(ng(shell_n(i0)), t0, dir);
+    return cyl_miss();  // area 4 cannot hold when z0 is outside [-h/2, h/2]
   }
   const double ell = x0 * x0 * b * b + y0 * y0 * a * a;
   if ((z0 > mh2) && (z0 < h2) && (ell > a * a * b * b)) {  // area 3: beside the shell
-    if (!quad(t0, t1, i0, i1)) return false;
+    if (!quad(t0, t1, i0, i1)) return cyl_miss();
     if ((t1 > 0) && (t1 < t0) && (i1.z <= h2) && (i1.z >= mh2))
-      return cyl_hit(st, pos, ng(shell_n(i1)), t1, dir);
+      return cyl_hit(ng(shell_n(i1)), t1, dir);
     if ((t0 > 0) && (t0 < t1) && (i0.z <= h2) && (i0.z >= mh2))
-      return cyl_hit(st, pos, ng(shell_n(i0)), t0, dir);
-    return false;
+      return cyl_hit(ng(shell_n(i0)), t0, dir);
+    return cyl_miss();
   }
   if ((z0 >= mh2) && (z0 <= h2) && (ell <= a * a * b * b)) {  // area 4: inside
     if (l == 0) {
-      if ((z0 == mh2) || (z0 == h2)) return false;
-      if (!quad(t0, t1, i0, i1)) return false;
+      if ((z0 == mh2) || (z0 == h2)) return cyl_miss();
+      if (!quad(t0, t1, i0, i1)) return cyl_miss();
       if ((t1 > 0) && (i1.z <= h2) && (i1.z >= mh2))
-        return cyl_hit(st, pos, ng(shell_n(i1)), t1, dir);
+        return cyl_hit(ng(shell_n(i1)), t1, dir);
       if ((t0 > 0) && (i0.z <= h2) && (i0.z >= mh2))
-        return cyl_hit(st, pos, ng(shell_n(i0)), t0, dir);
+        return cyl_hit(ng(shell_n(i0)), t0, dir);
     } else if ((j == 0.0) && (k == 0)) {
-      if (b * b * x0 * x0 + a * a * y0 * y0 == a * a * b * b) return false;
-      if (l < 0) return cyl_hit(st, pos, ng(d3(0.0, 0.0, -1.0)), (mh2 - z0) / l, dir);
-      if (l > 0) return cyl_hit(st, pos, ng(d3(0.0, 0.0, 1.0)), (h2 - z0) / l, dir);
+      if (b * b * x0 * x0 + a * a * y0 * y0 == a * a * b * b) return cyl_miss();
+      if (l < 0) return cyl_hit(ng(d3(0.0, 0.0, -1.0)), (mh2 - z0) / l, dir);
+      if (l > 0) return cyl_hit(ng(d3(0.0, 0.0, 1.0)), (h2 - z0) / l, dir);
     } else {
-      if (!quad(t0, t1, i0, i1)) return false;
+      if (!quad(t0, t1, i0, i1)) return cyl_miss();
       if ((t1 > 0) && (i1.z <= h2) && (i1.z >= mh2))
-        return cyl_hit(st, pos, ng(shell_n(i1)), t1, dir);
+        return cyl_hit(ng(shell_n(i1)), t1, dir);
       if ((t0 > 0) && (i0.z <= h2) && (i0.z >= mh2))
-        return cyl_hit(st, pos, shell_n(i0), t0, dir);  // unrotated (cylinder.h:462-463)
-      if (l < 0) return cyl_hit(st, pos, ng(d3(0.0, 0.0, -1.0)), (mh2 - z0) / l, dir);
-      if (l > 0) return cyl_hit(st, pos, ng(d3(0.0, 0.0, 1.0)), (h2 - z0) / l, dir);
+        return cyl_hit(shell_n(i0), t0, dir);  // unrotated (cylinder.h:462-463)
+      if (l < 0) return cyl_hit(ng(d3(0.0, 0.0, -1.0)), (mh2 - z0) / l, dir);
+      if (l > 0) return cyl_hit(ng(d3(0.0, 0.0, 1.0)), (h2 - z0) / l, dir);
     }
   }
-  return false;
+  return cyl_miss();
 }
 
 // Tests the primitive at leaf position pos and returns its id word (id | kLastBit on the
@@ -369,7 +374,14 @@ BZR_HD uint32_t isect(const KindView &K, uint32_t pos, const Ray &r, KState &st)
   const double *P = K.payload + size_t(pos) * kPayloadDoubles[KIND];
   if (KIND == kSpheres) isect_sphere(P, pos, r, st);
   else if (KIND == kPlanes) isect_plane(P, pos, r, st);
-  else isect_cylinder(P, pos, r, st);
+  else {
+    const CylHit c = isect_cylinder(P, r.o, r.d);
+    if (c.hit) {  // no closest-hit test (blazert/primitives/cylinder.h:181-495)
+      st.n = c.n;
+      st.hit = c.dist;
+      st.pos = pos;
+    }
+  }
   return id;
 }
 
