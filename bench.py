@@ -58,6 +58,8 @@ def parse(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--rays", type=int, default=0,
                     help="override the workload's ray count (smaller cases for profiling)")
+    ap.add_argument("--any-hit", action="store_true",
+                    help="every ray with Ray::AnyHit::yes (shadow rays)")
     ap.add_argument("--sort", default="auto", choices=["auto", "on", "off"],
                     help="coherence sort of each batch; auto = chosen by blazert_b200.autotune")
     return ap.parse_args(argv)
@@ -151,6 +153,7 @@ def config_of(args, wl, world):
     return {"workload": args.workload, "rays_per_gpu": wl.rays.n,
             "scene": {k: v for k, v in m.items() if k != "seed"},
             "seed": m.get("seed"), "mode": args.mode, "parallelism": f"replicated-scene x{world}",
+            "rays": "any-hit (shadow)" if getattr(args, "any_hit", False) else "closest-hit",
             "l2": "flushed between timed steps (256 MiB write)"}
 
 
@@ -322,7 +325,8 @@ def run_ours(args):
         scene.tune(sort=args.sort == "on")
 
     def step():
-        scene.intersectN(o, d, tmn, tmx, mode=args.mode, out=out, stream=stream)
+        scene.intersectN(o, d, tmn, tmx, mode=args.mode, out=out, stream=stream,
+                         any_hit=args.any_hit)
 
     for i in range(args.warmup):
         flush.fill_(i & 0xFF)
@@ -359,7 +363,7 @@ def run_ours(args):
     hits = float(out["hit"].float().mean().item())
     precision = None
     if args.mode == "mixed":  # the precision form's report: its results against the FP64 path's
-        ref = scene.intersectN(o, d, tmn, tmx, mode="fp64", stream=stream)
+        ref = scene.intersectN(o, d, tmn, tmx, mode="fp64", stream=stream, any_hit=args.any_hit)
         torch.cuda.synchronize(dev)
         hm = out["hit"] == ref["hit"]
         same = hm & (out["prim"] == ref["prim"]) & (out["geom"] == ref["geom"])
@@ -387,7 +391,7 @@ def run_ours(args):
     peak, peak_src = load_peaks()
     traffic = None
     tf = os.path.join(ROOT, "profiles", f"trace_fp64_{args.workload}.json")
-    if os.path.exists(tf):
+    if os.path.exists(tf) and not args.any_hit:
         with open(tf) as f:
             traffic = json.load(f).get("dram_bytes_per_launch")
 
@@ -402,12 +406,12 @@ def run_ours(args):
                     geom=torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
                     hit=torch.empty(n, dtype=torch.uint8).pin_memory().numpy())
         for _ in range(max(1, args.warmup)):
-            scene.intersectN(ho, hd, htmn, htmx, mode=args.mode, out=hout)
+            scene.intersectN(ho, hd, htmn, htmx, mode=args.mode, out=hout, any_hit=args.any_hit)
         if pg:
             pg.barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            scene.intersectN(ho, hd, htmn, htmx, mode=args.mode, out=hout)
+            scene.intersectN(ho, hd, htmn, htmx, mode=args.mode, out=hout, any_hit=args.any_hit)
         el = time.perf_counter() - t0
         if pg:
             el = multi.max_over_ranks(el)
@@ -434,7 +438,9 @@ def run_ours(args):
                          "peak_source": peak_src,
                          "alg_bytes_per_ray": alg_bytes / n,
                          "box_tests_per_ray": [c / n for c in counts["box"]],
-                         "prim_tests_per_ray": [c / n for c in counts["prim"]]},
+                         "prim_tests_per_ray": [c / n for c in counts["prim"]],
+                         "note": ("work counts are the closest-hit traversal's; any-hit rays do "
+                                  "less, so achieved is an upper bound") if args.any_hit else None},
             "cpu_baseline": cpu, "clocks": clocks, "hit_fraction": hits, "precision": precision,
             "commit_seconds": commit_s, "wall_seconds_timed": wall, "tuning": tuning,
             "step_ms_min_max": [min(step_ms), max(step_ms)],

@@ -32,6 +32,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libblazert_b200.so")
 INVALID_ID = 0xFFFFFFFF
 DBL_MAX = float(np.finfo(np.float64).max)
 MODES = {"fp64": 0, "mixed": 1}
+RAY_ANY_HIT = 1  # BZR_RAY_ANY_HIT
 
 OK, EINVAL, ESTATE, ENOMEM, ECUDA, ETIMEOUT, EDEVICE_FLAG, ENODEV = 0, -1, -2, -3, -4, -5, -6, -7
 
@@ -78,6 +79,10 @@ def library():
         lib.bzr_intersect1.argtypes = [P, _dp, _dp, C.c_double, C.c_double,
                                        C.POINTER(_RayHitC), C.POINTER(C.c_int)]
         lib.bzr_intersectN.argtypes = [P, C.c_size_t, P, P, P, P, P, P, P, P, P, P, C.c_int, P]
+        lib.bzr_intersect1_ex.argtypes = [P, _dp, _dp, C.c_double, C.c_double, C.c_uint32,
+                                          C.POINTER(_RayHitC), C.POINTER(C.c_int)]
+        lib.bzr_intersectN_ex.argtypes = [P, C.c_size_t, P, P, P, P, P, P, P, P, P, P, C.c_int,
+                                          C.c_uint32, P]
         lib.bzr_scene_check.argtypes = [P, P, C.c_int, _u32p]
         lib.bzr_work_counts.argtypes = [P, C.c_size_t, P, P, P, P, C.POINTER(C.c_uint64), P]
         lib.bzr_scene_tune.argtypes = [P, C.c_int, C.c_int64]
@@ -105,12 +110,14 @@ def _f64(a, cols=None):
 
 @dataclass
 class Ray:
-    """blazert/ray.h:56-65.  The direction need not be unit length."""
+    """blazert/ray.h:56-65.  The direction need not be unit length.  any_hit is the reference's
+    Ray::AnyHit::yes: each kind's traversal stops at its first accepted hit (shadow rays)."""
 
     origin: np.ndarray
     direction: np.ndarray
     min_hit_distance: float = 0.0
     max_hit_distance: float = DBL_MAX
+    any_hit: bool = False
 
 
 @dataclass
@@ -225,9 +232,11 @@ class Scene:
         o, d = _f64(ray.origin), _f64(ray.direction)
         rh = _RayHitC()
         hit = C.c_int()
-        _check(self._lib.bzr_intersect1(self._h, o.ctypes.data_as(_dp), d.ctypes.data_as(_dp),
-                                        float(ray.min_hit_distance), float(ray.max_hit_distance),
-                                        C.byref(rh), C.byref(hit)))
+        _check(self._lib.bzr_intersect1_ex(self._h, o.ctypes.data_as(_dp), d.ctypes.data_as(_dp),
+                                           float(ray.min_hit_distance),
+                                           float(ray.max_hit_distance),
+                                           RAY_ANY_HIT if ray.any_hit else 0, C.byref(rh),
+                                           C.byref(hit)))
         if rayhit is None:
             rayhit = RayHit()
         if hit.value:  # on a miss the rayhit is left untouched, as in the reference
@@ -239,17 +248,20 @@ class Scene:
         return bool(hit.value), rayhit
 
     def intersectN(self, origins, directions, tmin=None, tmax=None, mode="fp64", out=None,
-                   stream=None):
+                   stream=None, any_hit=False):
         """intersect1 over a batch.  numpy inputs: host path, returns numpy arrays when the
         results are in place.  torch CUDA tensors: device path, queued on ``stream`` (default:
-        torch's current stream), returns torch tensors without waiting."""
+        torch's current stream), returns torch tensors without waiting.  any_hit: every ray
+        with Ray::AnyHit::yes."""
+        flags = RAY_ANY_HIT if any_hit else 0
         try:
             import torch
             is_torch = isinstance(origins, torch.Tensor)
         except ImportError:
             is_torch = False
         if is_torch and origins.is_cuda:
-            return self._intersect_device(origins, directions, tmin, tmax, mode, out, stream)
+            return self._intersect_device(origins, directions, tmin, tmax, mode, out, stream,
+                                          flags)
         o, d = _f64(origins, 3), _f64(directions, 3)
         n = o.shape[0]
         tmn = None if tmin is None else np.ascontiguousarray(np.broadcast_to(tmin, (n,)), np.float64)
@@ -259,14 +271,14 @@ class Scene:
                        prim=np.empty(n, np.uint32), geom=np.empty(n, np.uint32),
                        hit=np.empty(n, np.uint8))
         ptr = lambda a: None if a is None else a.ctypes.data
-        _check(self._lib.bzr_intersectN(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
-                                        ptr(out.get("t")), ptr(out.get("uv")),
-                                        ptr(out.get("normal")), ptr(out.get("prim")),
-                                        ptr(out.get("geom")), ptr(out.get("hit")),
-                                        MODES[mode], None))
+        _check(self._lib.bzr_intersectN_ex(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
+                                           ptr(out.get("t")), ptr(out.get("uv")),
+                                           ptr(out.get("normal")), ptr(out.get("prim")),
+                                           ptr(out.get("geom")), ptr(out.get("hit")),
+                                           MODES[mode], flags, None))
         return out
 
-    def _intersect_device(self, o, d, tmin, tmax, mode, out, stream):
+    def _intersect_device(self, o, d, tmin, tmax, mode, out, stream, flags=0):
         import torch
         n = o.shape[0]
         dev = o.device
@@ -284,11 +296,11 @@ class Scene:
                        hit=torch.empty(n, dtype=torch.uint8, device=dev))
         st = (stream or torch.cuda.current_stream(dev)).cuda_stream
         ptr = lambda a: None if a is None else a.data_ptr()
-        _check(self._lib.bzr_intersectN(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
-                                        ptr(out.get("t")), ptr(out.get("uv")),
-                                        ptr(out.get("normal")), ptr(out.get("prim")),
-                                        ptr(out.get("geom")), ptr(out.get("hit")),
-                                        MODES[mode], C.c_void_p(st)))
+        _check(self._lib.bzr_intersectN_ex(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
+                                           ptr(out.get("t")), ptr(out.get("uv")),
+                                           ptr(out.get("normal")), ptr(out.get("prim")),
+                                           ptr(out.get("geom")), ptr(out.get("hit")),
+                                           MODES[mode], flags, C.c_void_p(st)))
         out["_keep"] = (o, d, tmn, tmx)
         return out
 
@@ -425,4 +437,4 @@ def intersect1(scene: Scene, ray: Ray, rayhit: RayHit) -> bool:
 
 
 __all__ = ["Scene", "Batch", "Ray", "RayHit", "BuildOptions", "intersect1", "BlazertError", "INVALID_ID",
-           "DBL_MAX", "library"]
+           "DBL_MAX", "RAY_ANY_HIT", "library"]

@@ -372,11 +372,12 @@ static bool is_device_ptr(const void *p) { return bzr::is_device_pointer(p); }
 static int run_batch(const bzr_scene *cs, size_t n, const double *org, const double *dir,
                      const double *tmin, const double *tmax, double *t, double *uv,
                      double *normal, uint32_t *prim, uint32_t *geom, uint8_t *hit, int mode,
-                     void *stream, unsigned long long *totals) {
+                     uint32_t ray_flags, void *stream, unsigned long long *totals) {
   bzr_scene *s = const_cast<bzr_scene *>(cs);
   if (!s) return fail(BZR_EINVAL, "scene is null");
   if (!s->host.committed) return fail(BZR_ESTATE, "scene is not committed");
   if (mode != BZR_MODE_FP64 && mode != BZR_MODE_MIXED) return fail(BZR_EINVAL, "bad mode");
+  if (ray_flags & ~uint32_t(BZR_RAY_ANY_HIT)) return fail(BZR_EINVAL, "unknown ray flags");
   if (n == 0) return BZR_OK;
   if (!org || !dir) return fail(BZR_EINVAL, "origins and directions are required");
   if (n > 0x7FFFFFC0u) return fail(BZR_EINVAL, "batch too large (at most 2^31 - 64 rays)");
@@ -399,6 +400,7 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
   uint32_t *counters = s->slots + kSlotWords * slot;
   bzr::RayIO io;
   io.n = static_cast<uint32_t>(n);
+  io.any_hit = (ray_flags & BZR_RAY_ANY_HIT) ? 1 : 0;
 
   if (n_dev == n_given) {  // device arrays: queue on the caller's stream and return
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -469,6 +471,7 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
     h2d(d_tmax, tmax, 1);
     bzr::RayIO ci;
     ci.n = static_cast<uint32_t>(m);
+    ci.any_hit = io.any_hit;
     ci.org = d_org + 3 * a;
     ci.dir = d_dir + 3 * a;
     ci.tmin = d_tmin ? d_tmin + a : nullptr;
@@ -509,8 +512,16 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
 int bzr_intersectN(const bzr_scene *s, size_t n, const double *org, const double *dir,
                    const double *tmin, const double *tmax, double *t, double *uv, double *normal,
                    uint32_t *prim, uint32_t *geom, uint8_t *hit, int mode, void *stream) {
-  return run_batch(s, n, org, dir, tmin, tmax, t, uv, normal, prim, geom, hit, mode, stream,
+  return run_batch(s, n, org, dir, tmin, tmax, t, uv, normal, prim, geom, hit, mode, 0u, stream,
                    nullptr);
+}
+
+int bzr_intersectN_ex(const bzr_scene *s, size_t n, const double *org, const double *dir,
+                      const double *tmin, const double *tmax, double *t, double *uv,
+                      double *normal, uint32_t *prim, uint32_t *geom, uint8_t *hit, int mode,
+                      uint32_t ray_flags, void *stream) {
+  return run_batch(s, n, org, dir, tmin, tmax, t, uv, normal, prim, geom, hit, mode, ray_flags,
+                   stream, nullptr);
 }
 
 int bzr_work_counts(const bzr_scene *cs, size_t n, const double *org, const double *dir,
@@ -535,7 +546,7 @@ int bzr_work_counts(const bzr_scene *cs, size_t n, const double *org, const doub
   cudaSetDevice(cur);
   if (rc == BZR_OK)
     rc = run_batch(s, n, org, dir, tmin, tmax, nullptr, nullptr, nullptr, nullptr, nullptr,
-                   nullptr, BZR_MODE_FP64, stream, dev);
+                   nullptr, BZR_MODE_FP64, 0u, stream, dev);
   cudaSetDevice(s->device);
   // the host path ran on the scene's streams; make the counter copy wait for all of them
   for (cudaStream_t q : s->streams)
@@ -611,11 +622,16 @@ int bzr_adjoint_hit(const bzr_scene *cs, size_t n, const double *origins,
 
 int bzr_intersect1(const bzr_scene *s, const double origin[3], const double direction[3],
                    double tmin, double tmax, bzr_rayhit *rayhit, int *hit) {
+  return bzr_intersect1_ex(s, origin, direction, tmin, tmax, 0u, rayhit, hit);
+}
+
+int bzr_intersect1_ex(const bzr_scene *s, const double origin[3], const double direction[3],
+                      double tmin, double tmax, uint32_t ray_flags, bzr_rayhit *rayhit, int *hit) {
   if (!origin || !direction || !rayhit) return fail(BZR_EINVAL, "null argument");
   uint8_t h = 0;
-  const int rc = bzr_intersectN(s, 1, origin, direction, &tmin, &tmax, &rayhit->hit_distance,
-                                rayhit->uv, rayhit->normal, &rayhit->prim_id, &rayhit->geom_id,
-                                &h, BZR_MODE_FP64, nullptr);
+  const int rc = bzr_intersectN_ex(s, 1, origin, direction, &tmin, &tmax, &rayhit->hit_distance,
+                                   rayhit->uv, rayhit->normal, &rayhit->prim_id,
+                                   &rayhit->geom_id, &h, BZR_MODE_FP64, ray_flags, nullptr);
   if (hit) *hit = h;
   return rc;
 }

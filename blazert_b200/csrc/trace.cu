@@ -106,6 +106,7 @@ __global__ void __launch_bounds__(kTraceThreads)
           active = true;
           r = make_ray(io.org + 3 * size_t(i), io.dir + 3 * size_t(i), io.tmin ? io.tmin[i] : 0.0,
                        io.tmax ? io.tmax[i] : kDblMax);
+          r.any_hit = io.any_hit != 0;
           if (MIXED) {
             f = make_ray_f(r, K.coord_max);
             use32 = K.mixed_ok && f.ok;
@@ -224,6 +225,7 @@ __global__ void __launch_bounds__(kTraceThreads)
           K = &B.views[sc].k[KIND];
           r = make_ray(io.org + 3 * size_t(i), io.dir + 3 * size_t(i), io.tmin ? io.tmin[i] : 0.0,
                        io.tmax ? io.tmax[i] : kDblMax);
+          r.any_hit = io.any_hit != 0;
           if (MIXED) {
             f = make_ray_f(r, K->coord_max);
             use32 = K->mixed_ok && f.ok;

@@ -32,6 +32,7 @@ struct RayIO {
   uint32_t n = 0;
   uint32_t *error_word = nullptr;
   const uint32_t *perm = nullptr;  // optional processing order (ray indices), see RaySort
+  int any_hit = 0;                 // every ray is Ray::AnyHit::yes (blazert/ray.h:24-34)
 };
 
 // Coherence sort of a batch: rays are processed in the order of a 32-bit key -- the direction

@@ -99,6 +99,7 @@ struct Ray {
   D3 o, d, inv;  // origin, normalized direction, 1 / raw direction
   unsigned sx, sy, sz;
   double tmin, tmax;
+  bool any_hit;  // Ray::AnyHit::yes (blazert/ray.h:24-34)
 };
 
 // blazert/ray.h:56-65
@@ -114,6 +115,7 @@ BZR_HD Ray make_ray(const double *o, const double *raw, double tmin,
   r.sz = w.z < 0.0;
   r.tmin = tmin;
   r.tmax = tmax;
+  r.any_hit = false;
   return r;
 }
 
@@ -362,20 +364,23 @@ BZR_HD CylHit isect_cylinder(const double *P, D3 ro, D3 rd) {
 }
 
 // Tests the primitive at leaf position pos and returns its id word (id | kLastBit on the
-// leaf's last primitive).
+// leaf's last primitive); hit receives intersect_primitive's result.
 template <int KIND>
-BZR_HD uint32_t isect(const KindView &K, uint32_t pos, const Ray &r, KState &st) {
+BZR_HD uint32_t isect(const KindView &K, uint32_t pos, const Ray &r, KState &st, bool &hit) {
   if (KIND == kMesh) {
     const uint4 F = ldg(reinterpret_cast<const uint4 *>(K.tri) + pos);
-    isect_triangle(K.verts, F, pos, r, st);
+    hit = isect_triangle(K.verts, F, pos, r, st);
     return F.w;
   }
   const uint32_t id = ldg(K.prim_ids + pos);
   const double *P = K.payload + size_t(pos) * kPayloadDoubles[KIND];
-  if (KIND == kSpheres) isect_sphere(P, pos, r, st);
-  else if (KIND == kPlanes) isect_plane(P, pos, r, st);
-  else {
+  if (KIND == kSpheres) {
+    hit = isect_sphere(P, pos, r, st);
+  } else if (KIND == kPlanes) {
+    hit = isect_plane(P, pos, r, st);
+  } else {
     const CylHit c = isect_cylinder(P, r.o, r.d);
+    hit = c.hit;
     if (c.hit) {  // no closest-hit test (blazert/primitives/cylinder.h:181-495)
       st.n = c.n;
       st.hit = c.dist;
@@ -488,7 +493,12 @@ BZR_HD void trav_leaf(const KindView &K, const Ray &r, KState &st, Trav &tv, con
       return;
     }
     if (COUNT) cnt->prim[KIND] += 1;
-    const uint32_t id = isect<KIND>(K, pos, r, st);
+    bool h;
+    const uint32_t id = isect<KIND>(K, pos, r, st, h);
+    if (h && r.any_hit) {  // the first hit ends the leaf and the traversal (intersect.h:73-75,
+      tv.live = false;     // accel.h:109-110)
+      return;
+    }
     if (id & kLastBit) break;
     ++pos;
   }
@@ -715,7 +725,12 @@ BZR_HD void trav_leaf32(const KindView &K, const Ray &r, const RayF &f, KState &
       return;
     }
     if (COUNT) cnt->prim[KIND] += 1;
-    const uint32_t id = isect<KIND>(K, pos, r, st);
+    bool h;
+    const uint32_t id = isect<KIND>(K, pos, r, st, h);
+    if (h && r.any_hit) {
+      tv.live = false;
+      return;
+    }
     if (id & kLastBit) break;
     ++pos;
   }

@@ -16,6 +16,9 @@
  *   bzr_intersect1                intersect1(scene, ray, rayhit)    blazert/scene.h:161-210
  *                                 with Ray / RayHit                 blazert/ray.h:56-85
  *   bzr_intersectN                new: intersect1 over a batch of rays, one GPU launch
+ *   bzr_intersect1_ex / _ex       the two above with ray flags: BZR_RAY_ANY_HIT for
+ *                                 Ray::AnyHit::yes              blazert/ray.h:24-65,
+ *                                 blazert/bvh/intersect.h:67-78, blazert/bvh/accel.h:105-111
  *   bzr_adjoint_hit               new: gradients of the outputs (differentiation form)
  *   bzr_batch_*                   new: many scenes per launch, CUDA graph (batching form)
  *   bzr_work_counts, bzr_scene_check, bzr_scene_stats, bzr_scene_tune
@@ -102,6 +105,19 @@ int bzr_commit(bzr_scene *scene, const bzr_build_options *options);
 int bzr_intersect1(const bzr_scene *scene, const double origin[3], const double direction[3],
                    double tmin, double tmax, bzr_rayhit *rayhit, int *hit);
 
+/* Ray flags (the reference's per-ray enums, blazert/ray.h:24-34).  BZR_RAY_ANY_HIT is
+ * Ray::AnyHit::yes: in each kind's traversal the first primitive hit a leaf accepts ends the
+ * leaf and the traversal (blazert/bvh/intersect.h:73-75, blazert/bvh/accel.h:109-110); the
+ * kinds are still merged as intersect1 does.  Used for shadow rays, where only hit / miss
+ * matters (the reported hit need not be the closest).  CullBackFace has no flag: the reference
+ * does not implement it (blazert/ray.h:52). */
+#define BZR_RAY_ANY_HIT 1u
+
+/* bzr_intersect1 with ray flags (0 or BZR_RAY_ANY_HIT). */
+int bzr_intersect1_ex(const bzr_scene *scene, const double origin[3], const double direction[3],
+                      double tmin, double tmax, uint32_t ray_flags, bzr_rayhit *rayhit,
+                      int *hit);
+
 /* A batch of n rays, structure-of-arrays.  Inputs: origins, directions (n x 3); tmin, tmax (n,
  * or NULL for 0 and DBL_MAX).  Outputs (each may be NULL to skip it): hit_distance (n), uv
  * (n x 2), normal (n x 3), prim_id, geom_id (n), hit (n, 0/1).
@@ -113,6 +129,13 @@ int bzr_intersectN(const bzr_scene *scene, size_t n, const double *origins,
                    const double *directions, const double *tmin, const double *tmax,
                    double *hit_distance, double *uv, double *normal, uint32_t *prim_id,
                    uint32_t *geom_id, uint8_t *hit, int mode, void *stream);
+
+/* bzr_intersectN with ray flags applied to every ray of the batch (0 or BZR_RAY_ANY_HIT). */
+int bzr_intersectN_ex(const bzr_scene *scene, size_t n, const double *origins,
+                      const double *directions, const double *tmin, const double *tmax,
+                      double *hit_distance, double *uv, double *normal, uint32_t *prim_id,
+                      uint32_t *geom_id, uint8_t *hit, int mode, uint32_t ray_flags,
+                      void *stream);
 
 /* bzr_intersectN for callers that cannot allocate device memory while they trace (no
  * counterpart in the reference) -- for example a renderer plugin traced from its host

@@ -49,16 +49,24 @@ struct Mat3r {
 template <typename T>
 using Mat3rList = std::vector<Mat3r<T>>;
 
-// blazert/ray.h:56-65: the direction need not be unit length.
+// blazert/ray.h:19-65: the direction need not be unit length.  AnyHit::yes ends each kind's
+// traversal at its first accepted hit; CullBackFace is accepted and, as in the reference
+// (ray.h:52), has no effect.
 template <typename T>
 struct Ray {
+  enum class CullBackFace { yes, no };
+  enum class AnyHit { yes, no };
   Vec3r<T> origin;
   Vec3r<T> direction;
   T min_hit_distance = T(0);
   T max_hit_distance = std::numeric_limits<T>::max();
+  CullBackFace cull_back_face = CullBackFace::no;
+  AnyHit any_hit = AnyHit::no;
   Ray(const Vec3r<T> &o, const Vec3r<T> &d, T tmin = T(0),
-      T tmax = std::numeric_limits<T>::max())
-      : origin(o), direction(d), min_hit_distance(tmin), max_hit_distance(tmax) {}
+      T tmax = std::numeric_limits<T>::max(), CullBackFace cull = CullBackFace::no,
+      AnyHit any = AnyHit::no)
+      : origin(o), direction(d), min_hit_distance(tmin), max_hit_distance(tmax),
+        cull_back_face(cull), any_hit(any) {}
 };
 
 // blazert/ray.h:72-85, with the reference's defaults.
@@ -105,35 +113,39 @@ class Scene {
   // Each returns the geom id, or static_cast<unsigned>(-1) for a second add of a kind or an
   // add after commit (as the reference does); other errors throw blazert_b200::Error.
   unsigned int add_mesh(const Vec3rList<T> &vertices, const Vec3iList &triangles) {
-    uint32_t id;
-    return added(bzr_add_mesh(s_, flat(vertices), vertices.size(),
-                              reinterpret_cast<const uint32_t *>(triangles.data()),
-                              triangles.size(), &id), id);
+    uint32_t id = 0;
+    const int rc = bzr_add_mesh(s_, flat(vertices), vertices.size(),
+                                reinterpret_cast<const uint32_t *>(triangles.data()),
+                                triangles.size(), &id);
+    return added(rc, id);
   }
   unsigned int add_spheres(const Vec3rList<T> &centers, const std::vector<T> &radii) {
-    uint32_t id;
+    uint32_t id = 0;
     if (centers.size() != radii.size()) throw Error(BZR_EINVAL, "centers and radii differ");
-    return added(bzr_add_spheres(s_, flat(centers), radii.data(), radii.size(), &id), id);
+    const int rc = bzr_add_spheres(s_, flat(centers), radii.data(), radii.size(), &id);
+    return added(rc, id);
   }
   unsigned int add_planes(const Vec3rList<T> &centers, const std::vector<T> &dxs,
                           const std::vector<T> &dys, const Mat3rList<T> &rotations) {
-    uint32_t id;
+    uint32_t id = 0;
     const size_t n = centers.size();
     if (dxs.size() != n || dys.size() != n || rotations.size() != n)
       throw Error(BZR_EINVAL, "plane arrays differ in length");
-    return added(bzr_add_planes(s_, flat(centers), dxs.data(), dys.data(), flat(rotations), n,
-                                &id), id);
+    const int rc =
+        bzr_add_planes(s_, flat(centers), dxs.data(), dys.data(), flat(rotations), n, &id);
+    return added(rc, id);
   }
   unsigned int add_cylinders(const Vec3rList<T> &centers, const std::vector<T> &semi_axes_a,
                              const std::vector<T> &semi_axes_b, const std::vector<T> &heights,
                              const Mat3rList<T> &rotations) {
-    uint32_t id;
+    uint32_t id = 0;
     const size_t n = centers.size();
     if (semi_axes_a.size() != n || semi_axes_b.size() != n || heights.size() != n ||
         rotations.size() != n)
       throw Error(BZR_EINVAL, "cylinder arrays differ in length");
-    return added(bzr_add_cylinders(s_, flat(centers), semi_axes_a.data(), semi_axes_b.data(),
-                                   heights.data(), flat(rotations), n, &id), id);
+    const int rc = bzr_add_cylinders(s_, flat(centers), semi_axes_a.data(), semi_axes_b.data(),
+                                     heights.data(), flat(rotations), n, &id);
+    return added(rc, id);
   }
 
   bool commit() {
@@ -143,13 +155,14 @@ class Scene {
     return true;
   }
 
-  // Batched query, structure of arrays (see bzr_intersectN); returns nothing, fills outputs.
+  // Batched query, structure of arrays (see bzr_intersectN_ex); returns nothing, fills
+  // outputs.  ray_flags: 0 or BZR_RAY_ANY_HIT for every ray.
   void intersectN(size_t n, const T *origins, const T *directions, const T *tmin,
                   const T *tmax, T *hit_distance, T *uv, T *normal, uint32_t *prim_id,
                   uint32_t *geom_id, uint8_t *hit, int mode = BZR_MODE_FP64,
-                  void *stream = nullptr) const {
-    check(bzr_intersectN(s_, n, origins, directions, tmin, tmax, hit_distance, uv, normal,
-                         prim_id, geom_id, hit, mode, stream));
+                  void *stream = nullptr, uint32_t ray_flags = 0) const {
+    check(bzr_intersectN_ex(s_, n, origins, directions, tmin, tmax, hit_distance, uv, normal,
+                            prim_id, geom_id, hit, mode, ray_flags, stream));
   }
 
   const bzr_scene *handle() const { return s_; }
@@ -175,8 +188,9 @@ template <typename T>
 inline bool intersect1(const Scene<T> &scene, const Ray<T> &ray, RayHit<T> &rayhit) {
   bzr_rayhit rh;
   int hit = 0;
-  check(bzr_intersect1(scene.handle(), ray.origin.data(), ray.direction.data(),
-                       ray.min_hit_distance, ray.max_hit_distance, &rh, &hit));
+  const uint32_t flags = ray.any_hit == Ray<T>::AnyHit::yes ? BZR_RAY_ANY_HIT : 0u;
+  check(bzr_intersect1_ex(scene.handle(), ray.origin.data(), ray.direction.data(),
+                          ray.min_hit_distance, ray.max_hit_distance, flags, &rh, &hit));
   if (hit) {
     rayhit.normal = {rh.normal[0], rh.normal[1], rh.normal[2]};
     rayhit.uv = {rh.uv[0], rh.uv[1]};

@@ -524,6 +524,7 @@ typedef struct {
   v3 org, dir, inv;
   unsigned sign[3];
   double tmin, tmax;
+  int any_hit; /* Ray::AnyHit::yes (blazert/ray.h:24-34) */
 } ora_ray;
 
 /* blazert/ray.h:56-65: direction normalized, inverse and sign from the RAW direction. */
@@ -536,6 +537,7 @@ static ora_ray make_ray(const double *o, const double *d, double tmin, double tm
   for (int i = 0; i < 3; i++) r.sign[i] = raw.e[i] < 0.0 ? 1u : 0u;
   r.tmin = tmin;
   r.tmax = tmax;
+  r.any_hit = 0;
   return r;
 }
 
@@ -851,12 +853,18 @@ static int traverse_kind(const ora_scene *s, int kind, const ora_ray *r, ora_hit
         stack[ss++] = nd->child[near];
         if (peak && ss > *peak) *peak = ss;
       } else {
+        /* intersect_leaf: with any_hit the leaf stops at its first hit, and the traversal
+         * with it (intersect.h:73-75, accel.h:109-110) */
         int hit = 0;
         for (uint32_t q = 0; q < nd->prim_cnt; q++) {
           if (cnt_prims) (*cnt_prims)++;
           hit += isect_prim(s, kind, &st, k->leaf_prims[nd->prim_off + q], r);
+          if (hit && r->any_hit) break;
         }
-        if (hit) hit_distance = st.hit;
+        if (hit) {
+          hit_distance = st.hit;
+          if (r->any_hit) break;
+        }
       }
     }
   }
@@ -894,6 +902,15 @@ void ora_scene_intersect(const ora_scene *s, long n, const double *org, const do
                          const double *tmin, const double *tmax, double *t, double *uv,
                          double *normal, uint32_t *prim, uint32_t *geom, uint8_t *hit,
                          uint32_t *counters, uint32_t *stack_peak, int nthreads) {
+  ora_scene_intersect_ex(s, n, org, dir, tmin, tmax, 0, t, uv, normal, prim, geom, hit, counters,
+                         stack_peak, nthreads);
+}
+
+void ora_scene_intersect_ex(const ora_scene *s, long n, const double *org, const double *dir,
+                            const double *tmin, const double *tmax, int any_hit, double *t,
+                            double *uv, double *normal, uint32_t *prim, uint32_t *geom,
+                            uint8_t *hit, uint32_t *counters, uint32_t *stack_peak,
+                            int nthreads) {
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 256)
@@ -901,8 +918,9 @@ void ora_scene_intersect(const ora_scene *s, long n, const double *org, const do
   (void)nthreads;
 #endif
   for (long i = 0; i < n; i++) {
-    const ora_ray r = make_ray(org + 3 * i, dir + 3 * i, tmin ? tmin[i] : 0.0,
-                               tmax ? tmax[i] : DBL_MAX);
+    ora_ray r = make_ray(org + 3 * i, dir + 3 * i, tmin ? tmin[i] : 0.0,
+                         tmax ? tmax[i] : DBL_MAX);
+    r.any_hit = any_hit != 0;
     ora_hit rh;
     rh.t = DBL_MAX; /* RayHit defaults, blazert/ray.h:80-84 */
     rh.uv[0] = rh.uv[1] = 0.0;

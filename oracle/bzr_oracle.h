@@ -38,6 +38,14 @@ void ora_scene_intersect(const ora_scene *s, long n, const double *org, const do
                          double *normal, uint32_t *prim, uint32_t *geom, uint8_t *hit,
                          uint32_t *counters, uint32_t *stack_peak, int nthreads);
 
+/* ora_scene_intersect with every ray's any_hit flag set to `any_hit` (Ray::AnyHit::yes,
+ * blazert/ray.h:24-34): each kind's traversal stops at the first leaf hit it accepts. */
+void ora_scene_intersect_ex(const ora_scene *s, long n, const double *org, const double *dir,
+                            const double *tmin, const double *tmax, int any_hit, double *t,
+                            double *uv, double *normal, uint32_t *prim, uint32_t *geom,
+                            uint8_t *hit, uint32_t *counters, uint32_t *stack_peak,
+                            int nthreads);
+
 /* Node dump with the same layout as oracle/ref_driver.cpp's ref_scene_tree. */
 long ora_scene_tree(const ora_scene *s, int kind, double *bmin, double *bmax, uint32_t *leaf,
                     uint32_t *axis, uint32_t *children, uint32_t *prim_off, uint32_t *prim_cnt,

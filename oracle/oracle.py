@@ -166,6 +166,9 @@ class Oracle(_Base):
             lib.ora_scene_destroy.argtypes = [C.c_void_p]
             lib.ora_scene_intersect.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _dp, _dp, _dp, _dp,
                                                 _dp, _u32p, _u32p, _u8p, _u32p, _u32p, C.c_int]
+            lib.ora_scene_intersect_ex.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _dp, _dp,
+                                                   C.c_int, _dp, _dp, _dp, _u32p, _u32p, _u8p,
+                                                   _u32p, _u32p, C.c_int]
             lib.ora_scene_tree.restype = C.c_long
             lib.ora_scene_tree.argtypes = _TREE_ARGS
             lib.ora_intersect_node.restype = C.c_int
@@ -183,16 +186,18 @@ class Oracle(_Base):
         self.load()
         super().__init__(spec, **kw)
 
-    def intersect(self, org, dirs, tmin=None, tmax=None, counters=False, nthreads=0):
+    def intersect(self, org, dirs, tmin=None, tmax=None, counters=False, nthreads=0,
+                  any_hit=False):
+        """intersect1 over the rays; any_hit: every ray with Ray::AnyHit::yes."""
         org, dirs, tmin, tmax, n = _rays(org, dirs, tmin, tmax)
         out = _outputs(n)
         cnt = np.zeros((n, 8), np.uint32) if counters else None
         peak = np.zeros(n, np.uint32) if counters else None
-        self._lib.ora_scene_intersect(
+        self._lib.ora_scene_intersect_ex(
             self._h, n, _ptr(org, _dp), _ptr(dirs, _dp), _ptr(tmin, _dp), _ptr(tmax, _dp),
-            _ptr(out["t"], _dp), _ptr(out["uv"], _dp), _ptr(out["normal"], _dp),
-            _ptr(out["prim"], _u32p), _ptr(out["geom"], _u32p), _ptr(out["hit"], _u8p),
-            _ptr(cnt, _u32p), _ptr(peak, _u32p), nthreads)
+            1 if any_hit else 0, _ptr(out["t"], _dp), _ptr(out["uv"], _dp),
+            _ptr(out["normal"], _dp), _ptr(out["prim"], _u32p), _ptr(out["geom"], _u32p),
+            _ptr(out["hit"], _u8p), _ptr(cnt, _u32p), _ptr(peak, _u32p), nthreads)
         if counters:
             out["counters"] = cnt
             out["stack_peak"] = peak
@@ -248,6 +253,10 @@ class RefScene(_Base):
             lib.ref_scene_intersect.restype = C.c_double
             lib.ref_scene_intersect.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _dp, _dp, _dp,
                                                 _dp, _dp, _u32p, _u32p, _u8p, C.c_int]
+            lib.ref_scene_intersect_ex.restype = C.c_double
+            lib.ref_scene_intersect_ex.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _dp, _dp,
+                                                   C.c_int, _dp, _dp, _dp, _u32p, _u32p, _u8p,
+                                                   C.c_int]
             lib.ref_scene_tree.restype = C.c_long
             lib.ref_scene_tree.argtypes = _TREE_ARGS
             lib.ref_scene_traverse_kind.restype = C.c_double
@@ -261,12 +270,14 @@ class RefScene(_Base):
     def commit_seconds(self):
         return self._lib.ref_scene_commit_seconds(self._h)
 
-    def intersect(self, org, dirs, tmin=None, tmax=None, nthreads=0):
+    def intersect(self, org, dirs, tmin=None, tmax=None, nthreads=0, any_hit=False):
+        """intersect1 over the rays; any_hit builds them with Ray::AnyHit::yes."""
         org, dirs, tmin, tmax, n = _rays(org, dirs, tmin, tmax)
         out = _outputs(n)
-        secs = self._lib.ref_scene_intersect(
+        secs = self._lib.ref_scene_intersect_ex(
             self._h, n, _ptr(org, _dp), _ptr(dirs, _dp), _ptr(tmin, _dp), _ptr(tmax, _dp),
-            _ptr(out["t"], _dp), _ptr(out["uv"], _dp), _ptr(out["normal"], _dp),
-            _ptr(out["prim"], _u32p), _ptr(out["geom"], _u32p), _ptr(out["hit"], _u8p), nthreads)
+            1 if any_hit else 0, _ptr(out["t"], _dp), _ptr(out["uv"], _dp),
+            _ptr(out["normal"], _dp), _ptr(out["prim"], _u32p), _ptr(out["geom"], _u32p),
+            _ptr(out["hit"], _u8p), nthreads)
         out["seconds"] = secs
         return out

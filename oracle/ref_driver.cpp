@@ -160,10 +160,24 @@ void ref_scene_destroy(void *h) { delete static_cast<RefScene *>(h); }
 
 // intersect1 over n rays.  Misses leave the default RayHit (blazert/ray.h:80-84).
 // nthreads <= 0 uses the OpenMP default.  Returns wall seconds of the ray loop.
+double ref_scene_intersect_ex(void *h, long n, const double *org, const double *dir,
+                              const double *tmin, const double *tmax, int any_hit, double *t,
+                              double *uv, double *normal, uint32_t *prim, uint32_t *geom,
+                              uint8_t *hit, int nthreads);
+
 double ref_scene_intersect(void *h, long n, const double *org, const double *dir,
                            const double *tmin, const double *tmax, double *t, double *uv,
                            double *normal, uint32_t *prim, uint32_t *geom, uint8_t *hit,
                            int nthreads) {
+  return ref_scene_intersect_ex(h, n, org, dir, tmin, tmax, 0, t, uv, normal, prim, geom, hit,
+                                nthreads);
+}
+
+// As ref_scene_intersect, every ray built with Ray::AnyHit::yes when any_hit is non-zero.
+double ref_scene_intersect_ex(void *h, long n, const double *org, const double *dir,
+                              const double *tmin, const double *tmax, int any_hit, double *t,
+                              double *uv, double *normal, uint32_t *prim, uint32_t *geom,
+                              uint8_t *hit, int nthreads) {
   const RefScene *s = static_cast<RefScene *>(h);
   const BlazertScene<double> &scene = *s->scene;
   const long row = 512;
@@ -182,7 +196,9 @@ double ref_scene_intersect(void *h, long n, const double *org, const double *dir
     for (long i = r * row; i < end; ++i) {
       const Ray<double> ray{v3(org + 3 * i), v3(dir + 3 * i),
                             tmin ? tmin[i] : 0.0,
-                            tmax ? tmax[i] : std::numeric_limits<double>::max()};
+                            tmax ? tmax[i] : std::numeric_limits<double>::max(),
+                            Ray<double>::CullBackFace::no,
+                            any_hit ? Ray<double>::AnyHit::yes : Ray<double>::AnyHit::no};
       RayHit<double> rh;
       const bool hh = intersect1(scene, ray, rh);
       if (t) t[i] = rh.hit_distance;

@@ -129,10 +129,11 @@ static void emu_pass(const bzr::SceneView &view, long n, const double *org, cons
     sk.stride = 1;
 #pragma omp for schedule(dynamic, 256)
     for (long i = 0; i < n; ++i) {
-      const bzr::Ray r = bzr::make_ray(org + 3 * i, dir + 3 * i, tmin ? tmin[i] : 0.0,
-                                       tmax ? tmax[i] : 1.7976931348623157e308);
+      bzr::Ray r = bzr::make_ray(org + 3 * i, dir + 3 * i, tmin ? tmin[i] : 0.0,
+                                 tmax ? tmax[i] : 1.7976931348623157e308);
+      r.any_hit = (mode & 2) != 0;
       bzr::KState st;
-      if (mode == 1)
+      if (mode & 1)
         bzr::traverse_mixed<KIND, false>(view.k[KIND], r, st, sk, 0, &e, nullptr);
       else
         bzr::traverse<KIND, false>(view.k[KIND], r, st, sk, 0, &e, nullptr);

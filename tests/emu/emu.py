@@ -68,12 +68,13 @@ class EmuScene(_Base):
         assert rc == 0
         return mn, mx, c
 
-    def intersect(self, org, dirs, tmin=None, tmax=None, stack_cap=0, mode="fp64"):
+    def intersect(self, org, dirs, tmin=None, tmax=None, stack_cap=0, mode="fp64", any_hit=False):
+        """mode fp64 | mixed; any_hit: every ray with Ray::AnyHit::yes."""
         org, dirs, tmin, tmax, n = _rays(org, dirs, tmin, tmax)
         out = _outputs(n)
         out["error_word"] = int(self._lib.emu_scene_intersect(
             self._h, n, _ptr(org, _dp), _ptr(dirs, _dp), _ptr(tmin, _dp), _ptr(tmax, _dp),
             _ptr(out["t"], _dp), _ptr(out["uv"], _dp), _ptr(out["normal"], _dp),
             _ptr(out["prim"], _u32p), _ptr(out["geom"], _u32p), _ptr(out["hit"], _u8p), stack_cap,
-            1 if mode == "mixed" else 0))
+            (1 if mode == "mixed" else 0) | (2 if any_hit else 0)))
         return out

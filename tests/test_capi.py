@@ -66,3 +66,52 @@ def test_commit_without_device_fails_loudly():
         s.commit()
     assert e.value.code == B.ENODEV
     s.close()
+
+
+FACADE_APP = r"""
+#include <blazert_b200/scene.hpp>
+#include <cstdio>
+using namespace blazert_b200;
+
+int main(int argc, char **) {
+  // reference-style call sites (blazert/scene.h, blazert/ray.h)
+  Vec3rList<double> centers{{0.0, 0.0, 0.0}, {3.0, 0.0, 0.0}};
+  std::vector<double> radii{1.0, 0.5};
+  Vec3rList<double> vertices{{0.0, 0.0, 2.0}, {1.0, 0.0, 2.0}, {0.0, 1.0, 2.0}};
+  Vec3iList triangles{{0, 1, 2}};
+  Mat3rList<double> rot{Mat3r<double>::identity()};
+  Scene<double> scene;
+  const unsigned mesh_id = scene.add_mesh(vertices, triangles);
+  const unsigned sph_id = scene.add_spheres(centers, radii);
+  scene.add_cylinders(Vec3rList<double>{{0.0, 5.0, 0.0}}, {0.5}, {0.5}, {2.0}, rot);
+  scene.add_planes(Vec3rList<double>{{0.0, -5.0, 0.0}}, {2.0}, {2.0}, rot);
+  if (scene.add_spheres(centers, radii) != static_cast<unsigned>(-1)) return 2;
+  if (argc > 1) {  // needs a GPU
+    scene.commit();
+    Ray<double> ray{{0.2, 0.2, 5.0}, {0.0, 0.0, -1.0}};
+    Ray<double> shadow{{0.2, 0.2, 5.0}, {0.0, 0.0, -1.0}, 0.0, 10.0,
+                       Ray<double>::CullBackFace::no, Ray<double>::AnyHit::yes};
+    RayHit<double> rh, rh2;
+    const bool hit = intersect1(scene, ray, rh);
+    const bool hit2 = intersect1(scene, shadow, rh2);
+    std::printf("%d %u %u %.17g %d\n", hit, rh.geom_id, rh.prim_id, rh.hit_distance, hit2);
+  }
+  return mesh_id == 0 && sph_id == 1 ? 0 : 1;
+}
+"""
+
+
+def test_cpp_facade_compiles_links_and_keeps_add_rules(tmp_path):
+    """include/blazert_b200/scene.hpp: reference-style C++ (Scene<double>, add_*, Ray with the
+    reference's CullBackFace / AnyHit enums, RayHit, intersect1) compiles against the header,
+    links against the library, and runs the add rules without a GPU."""
+    import subprocess
+
+    src = tmp_path / "app.cpp"
+    src.write_text(FACADE_APP)
+    exe = tmp_path / "app"
+    lib = os.path.join(ROOT, "blazert_b200", "_lib")
+    cxx = os.environ.get("BZR_CXX", "g++")
+    subprocess.run([cxx, "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), str(src),
+                    "-L", lib, "-lblazert_b200", f"-Wl,-rpath,{lib}", "-o", str(exe)], check=True)
+    subprocess.run([str(exe)], check=True)

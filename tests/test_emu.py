@@ -31,6 +31,27 @@ def test_workloads(name, mode):
 
 
 @pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("name", ["icosphere_pinhole", "mixed_primitives", "heightfield"])
+def test_any_hit(name, mode):
+    """Rays with Ray::AnyHit::yes: the kernels' leaf step ends the traversal at the first hit,
+    as the oracle (pinned to the reference) does."""
+    if name == "mixed_primitives":
+        wl = W.mixed_primitives(n_rays=100_000)
+    elif name == "heightfield":
+        wl = W.heightfield(n_rays=50_000, grid=256)
+    else:
+        wl = W.WORKLOADS[name]()
+    R = wl.rays
+    ref = Oracle(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax, any_hit=True)
+    closest = Oracle(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax)
+    assert (ref["prim"] != closest["prim"]).any()  # the flag changes which hit is reported
+    got = EmuScene(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax, mode=mode,
+                                       any_hit=True)
+    assert got["error_word"] == 0
+    assert mismatches(got, ref) == []
+
+
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("case", edge_case_scenes(), ids=lambda c: c[0])
 def test_edge_cases(case, mode):
     _, spec, R = case

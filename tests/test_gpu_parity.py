@@ -90,6 +90,50 @@ def test_deep_tree_stack_storage(mode, max_depth):
     assert mismatches(out, ref) == []
 
 
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["icosphere_pinhole", "mixed_primitives"])
+def test_any_hit_bit_exact(name, mode):
+    """Ray::AnyHit::yes for the whole batch (BZR_RAY_ANY_HIT): device and host arrays against
+    the oracle's any-hit traversal (pinned to the reference in test_oracle_pin.py)."""
+    import torch
+
+    wl = W.WORKLOADS[name]()
+    R = wl.rays
+    ref = Oracle(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax, any_hit=True)
+    s = product_scene(wl.scene)
+    dev = torch.device("cuda", 0)
+    out_dev = s.intersectN(torch.from_numpy(R.origins).to(dev),
+                           torch.from_numpy(R.directions).to(dev),
+                           torch.from_numpy(R.tmin).to(dev), torch.from_numpy(R.tmax).to(dev),
+                           mode=mode, any_hit=True)
+    torch.cuda.synchronize()
+    assert s.check() == 0
+    out_host = s.intersectN(R.origins, R.directions, R.tmin, R.tmax, mode=mode, any_hit=True)
+    assert mismatches(out_dev, ref) == []
+    assert mismatches(out_host, ref) == []
+
+
+def test_cpp_facade_runs_on_gpu(tmp_path):
+    """The C++ facade end to end: reference-style code commits a four-kind scene and traces a
+    closest-hit and an any-hit (shadow) ray through intersect1."""
+    import os
+    import subprocess
+
+    from tests.test_capi import FACADE_APP, ROOT
+
+    src = tmp_path / "app.cpp"
+    src.write_text(FACADE_APP)
+    exe = tmp_path / "app"
+    lib = os.path.join(ROOT, "blazert_b200", "_lib")
+    subprocess.run([os.environ.get("BZR_CXX", "g++"), "-std=c++17", "-O1", "-I",
+                    os.path.join(ROOT, "include"), str(src), "-L", lib, "-lblazert_b200",
+                    f"-Wl,-rpath,{lib}", "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe), "gpu"], check=True, capture_output=True, text=True)
+    hit, geom, prim, t, hit2 = r.stdout.split()
+    # the ray from (0.2, 0.2, 5) down -z meets the triangle at z = 2 first (t = 3), then sphere 0
+    assert (hit, geom, prim, float(t), hit2) == ("1", "0", "0", 3.0, "1")
+
+
 def test_intersect1_matches_batch():
     import blazert_b200 as B
 

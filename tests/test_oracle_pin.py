@@ -53,6 +53,22 @@ def test_oracle_matches_reference(case):
 
 @needs_ref
 @pytest.mark.parametrize("case", _cases(), ids=lambda c: c[0])
+def test_oracle_any_hit_matches_reference(case):
+    """Rays built with Ray::AnyHit::yes: each kind's traversal stops at the first leaf hit it
+    accepts (blazert/bvh/intersect.h:73-75, accel.h:109-110); intersect1 still merges the kinds."""
+    _, spec, R = case
+    ref = RefScene(spec)
+    ora = Oracle(spec)
+    a = ora.intersect(R.origins, R.directions, R.tmin, R.tmax, any_hit=True)
+    b = ref.intersect(R.origins, R.directions, R.tmin, R.tmax, any_hit=True)
+    assert mismatches(a, b) == []
+    # any-hit finds the same hit/miss set as closest-hit (only which hit is reported differs)
+    c = ora.intersect(R.origins, R.directions, R.tmin, R.tmax)
+    assert np.array_equal(a["hit"], c["hit"])
+
+
+@needs_ref
+@pytest.mark.parametrize("case", _cases(), ids=lambda c: c[0])
 def test_product_builder_matches_reference(case):
     _, spec, _ = case
     ref = RefScene(spec)
