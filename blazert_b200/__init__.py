@@ -304,12 +304,21 @@ class Scene:
         out["_keep"] = (o, d, tmn, tmx)
         return out
 
-    def tune(self, sort=None, sort_min_rays=None):
-        """Speed knobs (bzr_scene_tune); results do not depend on them."""
+    def tune(self, sort=None, sort_min_rays=None, threads=None, shared_stack=None, chunk=None):
+        """Speed knobs (bzr_scene_tune); results do not depend on them.  sort: coherence sort
+        of each batch; threads: 64 / 128 / 256 per block; shared_stack: traversal stack in
+        shared memory instead of thread-local; chunk: rays per warp fetch (32 / 64 / 128, or 0
+        for exactly the idle lanes)."""
         if sort is not None:
             _check(self._lib.bzr_scene_tune(self._h, 1, int(bool(sort))))
         if sort_min_rays is not None:
             _check(self._lib.bzr_scene_tune(self._h, 2, int(sort_min_rays)))
+        if threads is not None:
+            _check(self._lib.bzr_scene_tune(self._h, 3, int(threads)))
+        if shared_stack is not None:
+            _check(self._lib.bzr_scene_tune(self._h, 4, int(bool(shared_stack))))
+        if chunk is not None:
+            _check(self._lib.bzr_scene_tune(self._h, 5, int(chunk)))
 
     def work_counts(self, origins, directions, tmin=None, tmax=None, stream=None):
         """Box tests and primitive tests per kind for a batch (counting kernel; see

@@ -1,31 +1,56 @@
 """Picks a scene's speed knobs by timing them on a sample of the caller's rays.
 
-The knobs (bzr_scene_tune) never change results, only the processing order and launch
-shape, so tuning is safe to run on live data.  Each candidate is timed with CUDA events on
-the caller's stream over `reps` repetitions after one warm-up; the fastest is kept.
+The knobs (bzr_scene_tune) never change results, only the processing order and the launch
+shape, so tuning is safe to run on live data:
+
+  sort          coherence sort of each batch (octant + origin Morton order) or caller order
+  threads       threads per block of the traversal kernels: 64, 128, 256
+  shared_stack  traversal stack in shared memory (sized from the tree) or thread-local
+  chunk         rays a warp takes from the work counter per fetch: 32, 64, 128, or 0 for
+                exactly the lanes that are idle
+
+The search is coordinate-wise: starting from the defaults, each knob in turn is set to the
+value with the lowest time while the others stay at their current best; two sweeps.  Each
+candidate is timed with CUDA events on the caller's stream, the minimum over `reps`
+repetitions after one warm-up.  The tree's node width stays binary: the reference's visit
+order, and so its tie-breaking, is defined on its binary tree.
 """
 from __future__ import annotations
 
-import itertools
+KNOBS = {"sort": (False, True), "threads": (128, 64, 256), "shared_stack": (False, True),
+         "chunk": (32, 0, 64, 128)}
 
 
 def autotune(scene, origins, directions, tmin=None, tmax=None, mode="fp64", reps=3,
-             sample=1 << 20, stream=None):
-    """origins/directions: torch CUDA tensors (n x 3 float64).  Returns the chosen settings
-    and the per-candidate timings (ms)."""
+             sample=1 << 20, stream=None, knobs=None, sweeps=2):
+    """origins/directions: torch CUDA tensors (n x 3 float64).  Applies and returns the chosen
+    settings with the per-candidate timings (ms)."""
     import torch
 
+    knobs = dict(KNOBS if knobs is None else knobs)
     n = origins.shape[0]
     m = min(n, sample)
     o, d = origins[:m], directions[:m]
     tmn = None if tmin is None else tmin[:m]
     tmx = None if tmax is None else tmax[:m]
     st = stream or torch.cuda.current_stream(origins.device)
-    candidates = [dict(sort=s) for s in (True, False)]
-    timings = []
     out = None
-    for cand in candidates:
-        scene.tune(sort=cand["sort"], sort_min_rays=0 if cand["sort"] else None)
+    timings = {}
+
+    def apply(cfg):
+        scene.tune(sort=cfg["sort"], sort_min_rays=0 if cfg["sort"] else 1 << 16,
+                   threads=cfg["threads"], shared_stack=cfg["shared_stack"], chunk=cfg["chunk"])
+
+    def timed(cfg):
+        nonlocal out
+        key = str(sorted(cfg.items()))
+        if key in timings:
+            return timings[key]
+        try:
+            apply(cfg)
+        except Exception:  # e.g. the stack does not fit shared memory at this block size
+            timings[key] = float("inf")
+            return timings[key]
         out = scene.intersectN(o, d, tmn, tmx, mode=mode, out=out, stream=st)  # warm-up
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(reps)]
@@ -34,9 +59,14 @@ def autotune(scene, origins, directions, tmin=None, tmax=None, mode="fp64", reps
             scene.intersectN(o, d, tmn, tmx, mode=mode, out=out, stream=st)
             b.record(st)
         torch.cuda.synchronize(origins.device)
-        timings.append(min(a.elapsed_time(b) for a, b in evs))
-    best = min(range(len(candidates)), key=lambda i: timings[i])
-    choice = candidates[best]
-    scene.tune(sort=choice["sort"], sort_min_rays=1 << 16)
-    return dict(choice=choice, timings_ms={str(c): t for c, t in zip(candidates, timings)},
-                sample_rays=m)
+        timings[key] = min(a.elapsed_time(b) for a, b in evs)
+        return timings[key]
+
+    best = {k: v[0] for k, v in knobs.items()}
+    for _ in range(sweeps):
+        for k, values in knobs.items():
+            scores = {v: timed({**best, k: v}) for v in values}
+            best[k] = min(scores, key=scores.get)
+    apply(best)
+    return dict(choice=best, best_ms=timings[str(sorted(best.items()))],
+                timings_ms=timings, sample_rays=m)

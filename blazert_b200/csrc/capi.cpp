@@ -668,6 +668,34 @@ int bzr_scene_tune(bzr_scene *s, int option, int64_t value) {
       if (value < 0 || value > 0x7FFFFFFF) return fail(BZR_EINVAL, "bad sort threshold");
       s->plan.sort_min_rays = static_cast<uint32_t>(value);
       return BZR_OK;
+    case BZR_TUNE_CHUNK:
+      if (value != 0 && value != 32 && value != 64 && value != 128)
+        return fail(BZR_EINVAL, "rays per warp fetch must be 0 (the idle lanes), 32, 64 or 128");
+      s->plan.chunk = static_cast<uint32_t>(value);
+      return BZR_OK;
+    case BZR_TUNE_BLOCK:
+    case BZR_TUNE_STACK: {
+      bzr::LaunchPlan p = s->plan;
+      if (option == BZR_TUNE_BLOCK) {
+        if (value != 64 && value != 128 && value != 256)
+          return fail(BZR_EINVAL, "threads per block must be 64, 128 or 256");
+        p.threads = static_cast<int>(value);
+      } else {
+        if (value != 0 && value != 1) return fail(BZR_EINVAL, "stack storage must be 0 or 1");
+        p.shared_stack = value == 1;
+      }
+      if ((p.shared_stack || s->view.stack_cap > bzr::kLocalStack) &&
+          bzr::trace_smem_bytes(s->view.stack_cap, p.threads) > 227 * 1024)
+        return fail(BZR_EINVAL, "the traversal stack does not fit shared memory at this block size");
+      int cur = 0;
+      cudaGetDevice(&cur);
+      cudaSetDevice(s->device);
+      const cudaError_t e = bzr::trace_prepare(s->view, &p);
+      cudaSetDevice(cur);
+      if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+      s->plan = p;
+      return BZR_OK;
+    }
   }
   return fail(BZR_EINVAL, "unknown tuning option");
 }

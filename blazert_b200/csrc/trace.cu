@@ -37,7 +37,6 @@
 namespace bzr {
 namespace {
 
-constexpr uint32_t kChunk = 64;  // rays taken from the global counter per warp fetch
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 // Traversal stack storage.  LOCAL: a thread-local array of kLocalStack entries (local memory,
@@ -67,7 +66,7 @@ __device__ __forceinline__ void init_stack(Stack &sk, uint32_t &tid, uint32_t ca
 // COUNT: also sums the work counters into totals[8] (box tests per kind, then primitive
 // tests per kind).
 template <int KIND, bool COUNT, bool MIXED, bool LOCAL>
-__global__ void __launch_bounds__(kTraceThreads)
+__global__ void __launch_bounds__(kMaxTraceThreads)
     trace_kind_kernel(SceneView S, RayIO io, int first, uint32_t *work_counter,
                       unsigned long long *totals) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -93,9 +92,12 @@ __global__ void __launch_bounds__(kTraceThreads)
     const unsigned idle = __ballot_sync(kFull, !active);
     if (idle && !exhausted) {
       const uint32_t want = __popc(idle), avail = pool_end - pool_next;
+      // rays taken per fetch: io.chunk (>= 32, so one fetch serves every idle lane), or with
+      // io.chunk == 0 exactly the number of idle lanes the pool cannot serve
+      const uint32_t take = io.chunk ? io.chunk : want - avail;
       uint32_t base = 0;
       if (want > avail) {
-        if (lane == 0) base = atomicAdd(work_counter, kChunk);
+        if (lane == 0) base = atomicAdd(work_counter, take);
         base = __shfl_sync(kFull, base, 0);
       }
       if (!active) {
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(kTraceThreads)
       }
       if (want > avail) {
         pool_next = base + (want - avail);
-        pool_end = base + kChunk;
+        pool_end = base + take;
         if (base >= io.n) exhausted = true;
       } else {
         pool_next += want;
@@ -158,7 +160,7 @@ __global__ void __launch_bounds__(kTraceThreads)
 // The pass of a scene's first kind writes its whole record; the pass of its last kind
 // completes it and stamps the scene's completion time.
 template <int KIND, bool MIXED, bool LOCAL>
-__global__ void __launch_bounds__(kTraceThreads)
+__global__ void __launch_bounds__(kMaxTraceThreads)
     trace_batch_kernel(BatchView B, RayIO io, uint32_t *chunk_counter, uint32_t stack_cap) {
   extern __shared__ __align__(16) unsigned char smem[];
   double lkey[LOCAL ? kLocalStack : 1];
@@ -357,65 +359,75 @@ __global__ void sort_scatter_kernel(uint32_t n, const uint32_t *keys, uint32_t *
 }
 
 // The counting kernels (measurement only) always keep the stack in shared memory; the
-// tracing kernels use the thread-local stack whenever the tree's stack fits it.
+// tracing kernels use the thread-local stack whenever the tree's stack fits it, unless the
+// plan asks for shared memory.
+inline bool use_local(const SceneView &S, const LaunchPlan &plan) {
+  return !plan.shared_stack && S.stack_cap <= kLocalStack;
+}
+
 template <int KIND, bool COUNT>
 cudaError_t launch_kind(const SceneView &S, const RayIO &io, int mode, int first, int blocks,
-                        cudaStream_t stream, uint32_t *counter, unsigned long long *totals) {
+                        const LaunchPlan &plan, cudaStream_t stream, uint32_t *counter,
+                        unsigned long long *totals) {
   const bool mixed = mode == kModeMixed;
-  if (!COUNT && S.stack_cap <= kLocalStack) {
+  const int th = plan.threads;
+  if (!COUNT && use_local(S, plan)) {
     if (mixed)
-      trace_kind_kernel<KIND, false, true, true><<<blocks, kTraceThreads, 0, stream>>>(
-          S, io, first, counter, totals);
+      trace_kind_kernel<KIND, false, true, true><<<blocks, th, 0, stream>>>(S, io, first, counter,
+                                                                           totals);
     else
-      trace_kind_kernel<KIND, false, false, true><<<blocks, kTraceThreads, 0, stream>>>(
-          S, io, first, counter, totals);
+      trace_kind_kernel<KIND, false, false, true><<<blocks, th, 0, stream>>>(S, io, first,
+                                                                            counter, totals);
   } else {
-    const size_t smem = trace_smem_bytes(S.stack_cap, kTraceThreads);
+    const size_t smem = trace_smem_bytes(S.stack_cap, th);
     if (mixed)
-      trace_kind_kernel<KIND, COUNT, true, false><<<blocks, kTraceThreads, smem, stream>>>(
-          S, io, first, counter, totals);
+      trace_kind_kernel<KIND, COUNT, true, false><<<blocks, th, smem, stream>>>(S, io, first,
+                                                                               counter, totals);
     else
-      trace_kind_kernel<KIND, COUNT, false, false><<<blocks, kTraceThreads, smem, stream>>>(
-          S, io, first, counter, totals);
+      trace_kind_kernel<KIND, COUNT, false, false><<<blocks, th, smem, stream>>>(S, io, first,
+                                                                                counter, totals);
   }
   return cudaGetLastError();
 }
 
-// Resident blocks per SM of `fn` with `smem` bytes of dynamic shared memory, times the SMs.
-cudaError_t grid_for(const void *fn, size_t smem, int sms, int *blocks) {
+// Resident blocks per SM of `fn` with `threads` per block and `smem` bytes of dynamic shared
+// memory, times the SMs.
+cudaError_t grid_for(const void *fn, int threads, size_t smem, int sms, int *blocks) {
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTraceThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
   if (e != cudaSuccess) return e;
   *blocks = sms * (per_sm > 0 ? per_sm : 1);
   return cudaSuccess;
 }
 
 template <int KIND>
-cudaError_t prepare_kind(uint32_t stack_cap, int sms, int *blocks, int *blocks32) {
-  const size_t smem = trace_smem_bytes(stack_cap, kTraceThreads);
+cudaError_t prepare_kind(const SceneView &S, LaunchPlan *plan) {
+  const int th = plan->threads;
+  const size_t smem = trace_smem_bytes(S.stack_cap, th);
   const void *shared_fns[4] = {
       reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, false, false>),
       reinterpret_cast<const void *>(trace_kind_kernel<KIND, true, false, false>),
       reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, true, false>),
       reinterpret_cast<const void *>(trace_kind_kernel<KIND, true, true, false>)};
-  int counting = 0;
+  int ignored = 0;
   for (const void *fn : shared_fns) {
-    const cudaError_t e = grid_for(fn, smem, sms, &counting);
+    const cudaError_t e = grid_for(fn, th, smem, plan->sms, &ignored);
     if (e != cudaSuccess) return e;
   }
-  if (stack_cap <= kLocalStack) {
+  int *blocks = &plan->blocks[KIND], *blocks32 = &plan->blocks32[KIND];
+  if (use_local(S, *plan)) {
     const cudaError_t e = grid_for(
-        reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, false, true>), 0, sms,
-        blocks);
+        reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, false, true>), th, 0,
+        plan->sms, blocks);
     if (e != cudaSuccess) return e;
-    return grid_for(reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, true, true>), 0,
-                    sms, blocks32);
+    return grid_for(reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, true, true>), th,
+                    0, plan->sms, blocks32);
   }
-  const cudaError_t e = grid_for(shared_fns[0], smem, sms, blocks);
+  const cudaError_t e = grid_for(shared_fns[0], th, smem, plan->sms, blocks);
   if (e != cudaSuccess) return e;
-  return grid_for(shared_fns[2], smem, sms, blocks32);
+  return grid_for(shared_fns[2], th, smem, plan->sms, blocks32);
 }
 
 }  // namespace
@@ -439,17 +451,10 @@ cudaError_t trace_prepare(const SceneView &S, LaunchPlan *plan) {
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
   plan->sms = sms;
-  if ((e = prepare_kind<kMesh>(S.stack_cap, sms, &plan->blocks[kMesh],
-                               &plan->blocks32[kMesh])) != cudaSuccess)
-    return e;
-  if ((e = prepare_kind<kSpheres>(S.stack_cap, sms, &plan->blocks[kSpheres],
-                                  &plan->blocks32[kSpheres])) != cudaSuccess)
-    return e;
-  if ((e = prepare_kind<kPlanes>(S.stack_cap, sms, &plan->blocks[kPlanes],
-                                 &plan->blocks32[kPlanes])) != cudaSuccess)
-    return e;
-  return prepare_kind<kCylinders>(S.stack_cap, sms, &plan->blocks[kCylinders],
-                                  &plan->blocks32[kCylinders]);
+  if ((e = prepare_kind<kMesh>(S, plan)) != cudaSuccess) return e;
+  if ((e = prepare_kind<kSpheres>(S, plan)) != cudaSuccess) return e;
+  if ((e = prepare_kind<kPlanes>(S, plan)) != cudaSuccess) return e;
+  return prepare_kind<kCylinders>(S, plan);
 }
 
 int trace_passes(const SceneView &S) {
@@ -463,6 +468,7 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
   cudaError_t e = cudaMemsetAsync(counters, 0, kNumKinds * sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
   RayIO sorted = io;
+  sorted.chunk = plan.chunk;
   uint32_t *scratch = nullptr;
   if (plan.sort.enabled && io.n >= plan.sort_min_rays && trace_passes(S) > 0) {
     const size_t nb = size_t(1) << kSortBits;
@@ -487,20 +493,24 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
     uint32_t *c = counters + k;
     switch (k) {
       case kMesh:
-        e = totals ? launch_kind<kMesh, true>(S, run, mode, first, b, stream, c, totals)
-                   : launch_kind<kMesh, false>(S, run, mode, first, b, stream, c, nullptr);
+        e = totals ? launch_kind<kMesh, true>(S, run, mode, first, b, plan, stream, c, totals)
+                   : launch_kind<kMesh, false>(S, run, mode, first, b, plan, stream, c, nullptr);
         break;
       case kSpheres:
-        e = totals ? launch_kind<kSpheres, true>(S, run, mode, first, b, stream, c, totals)
-                   : launch_kind<kSpheres, false>(S, run, mode, first, b, stream, c, nullptr);
+        e = totals
+                ? launch_kind<kSpheres, true>(S, run, mode, first, b, plan, stream, c, totals)
+                : launch_kind<kSpheres, false>(S, run, mode, first, b, plan, stream, c, nullptr);
         break;
       case kPlanes:
-        e = totals ? launch_kind<kPlanes, true>(S, run, mode, first, b, stream, c, totals)
-                   : launch_kind<kPlanes, false>(S, run, mode, first, b, stream, c, nullptr);
+        e = totals
+                ? launch_kind<kPlanes, true>(S, run, mode, first, b, plan, stream, c, totals)
+                : launch_kind<kPlanes, false>(S, run, mode, first, b, plan, stream, c, nullptr);
         break;
       default:
-        e = totals ? launch_kind<kCylinders, true>(S, run, mode, first, b, stream, c, totals)
-                   : launch_kind<kCylinders, false>(S, run, mode, first, b, stream, c, nullptr);
+        e = totals
+                ? launch_kind<kCylinders, true>(S, run, mode, first, b, plan, stream, c, totals)
+                : launch_kind<kCylinders, false>(S, run, mode, first, b, plan, stream, c,
+                                                 nullptr);
         break;
     }
     if (e != cudaSuccess) return e;
@@ -529,9 +539,9 @@ cudaError_t prepare_batch_kind(uint32_t stack_cap, int sms, int *blocks, int *bl
                            : reinterpret_cast<const void *>(trace_batch_kernel<KIND, false, false>);
   const void *mixed = local ? reinterpret_cast<const void *>(trace_batch_kernel<KIND, true, true>)
                             : reinterpret_cast<const void *>(trace_batch_kernel<KIND, true, false>);
-  const cudaError_t e = grid_for(fp64, smem, sms, blocks);
+  const cudaError_t e = grid_for(fp64, kTraceThreads, smem, sms, blocks);
   if (e != cudaSuccess) return e;
-  return grid_for(mixed, smem, sms, blocks32);
+  return grid_for(mixed, kTraceThreads, smem, sms, blocks32);
 }
 }  // namespace
 

@@ -9,7 +9,9 @@
 
 namespace bzr {
 
-constexpr int kTraceThreads = 128;
+constexpr int kTraceThreads = 128;     // default threads per block of the trace kernels
+constexpr int kMaxTraceThreads = 256;  // largest block the trace kernels are compiled for
+constexpr uint32_t kRayChunk = 32;     // default rays a warp takes from the global counter
 // Entries of the thread-local traversal stack; trees whose stack needs more (depth > 62,
 // reachable only with max_tree_depth above 62) trace with the stack in shared memory.
 constexpr uint32_t kLocalStack = 64;
@@ -33,6 +35,8 @@ struct RayIO {
   uint32_t *error_word = nullptr;
   const uint32_t *perm = nullptr;  // optional processing order (ray indices), see RaySort
   int any_hit = 0;                 // every ray is Ray::AnyHit::yes (blazert/ray.h:24-34)
+  uint32_t chunk = kRayChunk;      // rays a warp takes per fetch: 32, 64, 128, or 0 for
+                                   // exactly the lanes that are idle
 };
 
 // Coherence sort of a batch: rays are processed in the order of a 32-bit key -- the direction
@@ -46,9 +50,13 @@ struct RaySort {
   float scale[3] = {0, 0, 0};  // 512 / extent per axis
 };
 
-// Grid of each per-kind persistent kernel: SMs x resident blocks per SM.
+// Grid of each per-kind persistent kernel: SMs x resident blocks per SM, and the launch
+// shape the tuning knobs select (none of them changes results).
 struct LaunchPlan {
   int sms = 0;
+  int threads = kTraceThreads;     // threads per block: 64, 128 or 256
+  bool shared_stack = false;       // traversal stack in shared memory even when it fits locally
+  uint32_t chunk = kRayChunk;      // rays per warp fetch: 32, 64, 128 or 0 (exactly the idle lanes)
   int blocks[kNumKinds] = {0, 0, 0, 0};    // FP64 kernels
   int blocks32[kNumKinds] = {0, 0, 0, 0};  // mixed-precision kernels
   RaySort sort;
@@ -92,6 +100,7 @@ cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const Ba
 cudaError_t launch_defaults(const RayIO &io, int sms, cudaStream_t stream);
 
 size_t trace_smem_bytes(uint32_t stack_cap, int threads);
+// Fills plan->sms and the per-kind grids for plan->threads and plan->shared_stack.
 cudaError_t trace_prepare(const SceneView &S, LaunchPlan *plan);
 // Number of per-kind passes a batch runs (kinds present with at least one primitive).
 int trace_passes(const SceneView &S);

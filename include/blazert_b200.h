@@ -207,6 +207,13 @@ int bzr_scene_check(const bzr_scene *scene, void *stream, int timeout_ms, uint32
  * caller's order. */
 #define BZR_TUNE_SORT 1
 #define BZR_TUNE_SORT_MIN_RAYS 2
+/* Launch shape of the traversal kernels: threads per block (64, 128 -- the default -- or 256);
+ * traversal-stack storage (0: a thread-local array when the tree's stack fits its 64 entries,
+ * the default; 1: shared memory sized from the tree); rays a warp takes from the work counter
+ * per fetch (32 -- the default --, 64, 128, or 0 for exactly the lanes that are idle). */
+#define BZR_TUNE_BLOCK 3
+#define BZR_TUNE_STACK 4
+#define BZR_TUNE_CHUNK 5
 int bzr_scene_tune(bzr_scene *scene, int option, int64_t value);
 
 /* Statistics of the last commit: per kind (0 mesh, 1 spheres, 2 planes, 3 cylinders) the

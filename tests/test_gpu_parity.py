@@ -149,21 +149,34 @@ def test_intersect1_matches_batch():
         assert np.float64(rh.hit_distance).view(np.uint64) == ref["t"][i].view(np.uint64)
 
 
-def test_sort_changes_speed_not_results():
+def test_tuning_changes_speed_not_results():
+    """Every tuning knob (coherence sort, threads per block, stack storage, rays per warp
+    fetch) and the autotuner's choice give the oracle's results."""
     import torch
+
+    from blazert_b200.autotune import autotune
 
     wl = W.mixed_primitives(n_rays=300_000, seed=8)
     R = wl.rays
+    ref = Oracle(wl.scene).intersect(R.origins, R.directions)
     s = product_scene(wl.scene)
     dev = torch.device("cuda", 0)
     o, d = torch.from_numpy(R.origins).to(dev), torch.from_numpy(R.directions).to(dev)
-    outs = []
-    for sort in (False, True):
-        s.tune(sort=sort, sort_min_rays=0)
-        outs.append({k: v.cpu().numpy() for k, v in s.intersectN(o, d).items() if not k.startswith("_")})
-    s.check()
-    ref = Oracle(wl.scene).intersect(R.origins, R.directions)
-    assert mismatches(outs[0], ref) == [] and mismatches(outs[1], ref) == []
+    configs = [dict(sort=True), dict(sort=False), dict(threads=64), dict(threads=256),
+               dict(shared_stack=True), dict(shared_stack=True, threads=256), dict(chunk=0),
+               dict(chunk=64), dict(chunk=128), dict(threads=128, shared_stack=False, chunk=32)]
+    for cfg in configs:
+        s.tune(sort_min_rays=0, **cfg)
+        for mode in ("fp64", "mixed"):
+            out = s.intersectN(o, d, mode=mode)
+            torch.cuda.synchronize()
+            assert s.check() == 0
+            assert mismatches(out, ref) == [], (cfg, mode)
+    res = autotune(s, o, d, sample=100_000)
+    assert set(res["choice"]) == {"sort", "threads", "shared_stack", "chunk"}
+    out = s.intersectN(o, d)
+    torch.cuda.synchronize()
+    assert mismatches(out, ref) == []
 
 
 @pytest.fixture(scope="module")
