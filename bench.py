@@ -215,6 +215,7 @@ def run_batched(args):
     commit_s = time.perf_counter() - t0
     batch = B.Batch(scenes)
     offs = np.concatenate([[0], np.cumsum([w.rays.n for w in wls])]).astype(np.int64)
+    tuning = None
     n = int(offs[-1])
     o = torch.from_numpy(np.concatenate([w.rays.origins for w in wls])).to(dev)
     d = torch.from_numpy(np.concatenate([w.rays.directions for w in wls])).to(dev)
@@ -229,6 +230,9 @@ def run_batched(args):
                hit=torch.empty(n, dtype=torch.uint8, device=dev))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
+    if args.sort == "auto":  # the batch kernels' launch shape, chosen on this batch
+        from blazert_b200.autotune import autotune_batch
+        tuning = autotune_batch(batch, offs, o, d, tmn, tmx, mode=args.mode, stream=stream)
     for i in range(args.warmup):
         flush.fill_(i & 0xFF)
         batch.intersect(offs, o, d, tmn, tmx, out=out, timestamps=ts, mode=args.mode, stream=stream)
@@ -269,7 +273,7 @@ def run_batched(args):
             "gpu_launches": args.steps * 2,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "max": float(lat.max())},
-            "clocks": clocks, "commit_seconds": commit_s}), flush=True)
+            "clocks": clocks, "commit_seconds": commit_s, "tuning": tuning}), flush=True)
     return 0
 
 

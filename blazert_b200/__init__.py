@@ -91,6 +91,10 @@ def library():
         lib.bzr_batch_destroy.argtypes = [P]
         lib.bzr_batch_intersect.argtypes = [P, C.POINTER(C.c_uint64)] + [P] * 11 + [C.c_int, P]
         lib.bzr_batch_check.argtypes = [P, P, _u32p]
+        lib.bzr_batch_tune.argtypes = [P, C.c_int, C.c_int64]
+        lib.bzr_commit_ex.argtypes = [P, C.POINTER(_OptsC), C.c_uint32]
+        lib.bzr_scene_tree.restype = C.c_long
+        lib.bzr_scene_tree.argtypes = [P, C.c_int] + [P] * 7 + [C.c_long]
         lib.bzr_scene_stats.argtypes = [P, C.c_int, C.POINTER(C.c_uint64), _u32p,
                                         C.POINTER(C.c_double)]
         lib.bzr_last_error_string.restype = C.c_char_p
@@ -213,12 +217,33 @@ class Scene:
                                                      h.ctypes.data_as(_dp), rot.ctypes.data_as(_dp),
                                                      n, C.byref(gid)), gid)
 
-    def commit(self, build_options: Optional[BuildOptions] = None):
+    def commit(self, build_options: Optional[BuildOptions] = None, gpu_build: bool = False):
+        """blazert/scene.h:91-115.  gpu_build: build the BVHs on the GPU (the same trees;
+        bzr_commit_ex with BZR_COMMIT_GPU_BUILD)."""
         o = build_options or BuildOptions()
         opts = _OptsC(o.min_leaf_primitives, o.max_tree_depth, o.bin_size)
-        _check(self._lib.bzr_commit(self._h, C.byref(opts)))
+        _check(self._lib.bzr_commit_ex(self._h, C.byref(opts), 1 if gpu_build else 0))
         self.committed = True
         return True
+
+    def tree(self, kind):
+        """Node arrays of one kind's BVH in the reference's node order (bzr_scene_tree):
+        bmin, bmax (n x 3), leaf, axis, children (n x 2), prim_cnt, prim_ids."""
+        k = ("mesh", "spheres", "planes", "cylinders").index(kind)
+        f = self._lib.bzr_scene_tree
+        n = f(self._h, k, None, None, None, None, None, None, None, 0)
+        if n < 0:
+            _check(int(n))
+        bmin, bmax = np.zeros((n, 3)), np.zeros((n, 3))
+        leaf, axis = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+        ch, cnt = np.zeros((n, 2), np.uint32), np.zeros(n, np.uint32)
+        f(self._h, k, bmin.ctypes.data, bmax.ctypes.data, leaf.ctypes.data, axis.ctypes.data,
+          ch.ctypes.data, cnt.ctypes.data, None, 0)
+        prims = np.zeros(max(int(cnt.sum()), 1), np.uint32)
+        f(self._h, k, bmin.ctypes.data, bmax.ctypes.data, leaf.ctypes.data, axis.ctypes.data,
+          ch.ctypes.data, cnt.ctypes.data, prims.ctypes.data, int(cnt.sum()))
+        return dict(bmin=bmin, bmax=bmax, leaf=leaf, axis=axis, children=ch, prim_cnt=cnt,
+                    prim_ids=prims[:int(cnt.sum())])
 
     def stats(self, kind):
         kinds = ("mesh", "spheres", "planes", "cylinders")
@@ -406,6 +431,13 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+    def tune(self, threads=None, shared_stack=None):
+        """Launch shape of the batch kernels (bzr_batch_tune); results do not depend on it."""
+        if threads is not None:
+            _check(self._lib.bzr_batch_tune(self._h, 3, int(threads)))
+        if shared_stack is not None:
+            _check(self._lib.bzr_batch_tune(self._h, 4, int(bool(shared_stack))))
 
     def intersect(self, ray_offsets, origins, directions, tmin=None, tmax=None, out=None,
                   timestamps=None, mode="fp64", stream=None):

@@ -70,3 +70,49 @@ def autotune(scene, origins, directions, tmin=None, tmax=None, mode="fp64", reps
     apply(best)
     return dict(choice=best, best_ms=timings[str(sorted(best.items()))],
                 timings_ms=timings, sample_rays=m)
+
+
+BATCH_KNOBS = {"threads": (128, 64, 256), "shared_stack": (False, True)}
+
+
+def autotune_batch(batch, ray_offsets, origins, directions, tmin=None, tmax=None, mode="fp64",
+                   reps=3, stream=None, knobs=None):
+    """The batching form's knobs (threads per block, stack storage), timed on the caller's
+    whole batch (each candidate captures its own graph, then replays it `reps` times).
+    Applies and returns the choice with the per-candidate timings (ms)."""
+    import torch
+
+    knobs = dict(BATCH_KNOBS if knobs is None else knobs)
+    st = stream or torch.cuda.current_stream(origins.device)
+    out = None
+    timings = {}
+
+    def timed(cfg):
+        nonlocal out
+        key = str(sorted(cfg.items()))
+        if key in timings:
+            return timings[key]
+        try:
+            batch.tune(**cfg)
+        except Exception:  # e.g. the stack does not fit shared memory at this block size
+            timings[key] = float("inf")
+            return timings[key]
+        out = batch.intersect(ray_offsets, origins, directions, tmin, tmax, out=out, mode=mode,
+                              stream=st)  # capture + warm-up
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(reps)]
+        for a, b in evs:
+            a.record(st)
+            batch.intersect(ray_offsets, origins, directions, tmin, tmax, out=out, mode=mode,
+                            stream=st)
+            b.record(st)
+        torch.cuda.synchronize(origins.device)
+        timings[key] = min(a.elapsed_time(b) for a, b in evs)
+        return timings[key]
+
+    best = {k: v[0] for k, v in knobs.items()}
+    for k, values in knobs.items():
+        scores = {v: timed({**best, k: v}) for v in values}
+        best[k] = min(scores, key=scores.get)
+    batch.tune(**best)
+    return dict(choice=best, best_ms=timings[str(sorted(best.items()))], timings_ms=timings)

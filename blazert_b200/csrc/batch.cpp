@@ -232,6 +232,39 @@ int bzr_batch_intersect(bzr_batch *b, const uint64_t *ray_offsets, const double 
   return e == cudaSuccess ? BZR_OK : cuda_fail(e);
 }
 
+int bzr_batch_tune(bzr_batch *b, int option, int64_t value) {
+  if (!b) return fail(BZR_EINVAL, "batch is null");
+  std::lock_guard<std::mutex> lock(b->mu);
+  bzr::BatchPlan p = b->plan;
+  if (option == BZR_TUNE_BLOCK) {
+    if (value != 64 && value != 128 && value != 256)
+      return fail(BZR_EINVAL, "threads per block must be 64, 128 or 256");
+    p.threads = static_cast<int>(value);
+  } else if (option == BZR_TUNE_STACK) {
+    if (value != 0 && value != 1) return fail(BZR_EINVAL, "stack storage must be 0 or 1");
+    p.shared_stack = value == 1;
+  } else {
+    return fail(BZR_EINVAL, "unknown tuning option for a batch");
+  }
+  if ((p.shared_stack || p.stack_cap > bzr::kLocalStack) &&
+      bzr::trace_smem_bytes(p.stack_cap, p.threads) > 227 * 1024)
+    return fail(BZR_EINVAL, "the traversal stack does not fit shared memory at this block size");
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(b->device);
+  cudaError_t e = bzr::batch_prepare(p.stack_cap, &p);
+  if (e == cudaSuccess && b->exec) {  // the cached graph holds the old launch shape
+    e = cudaStreamSynchronize(b->capture);
+    cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    b->key.clear();
+  }
+  cudaSetDevice(cur);
+  if (e != cudaSuccess) return cuda_fail(e);
+  b->plan = p;
+  return BZR_OK;
+}
+
 int bzr_batch_check(bzr_batch *b, void *stream, uint32_t *flags) {
   if (!b) return fail(BZR_EINVAL, "batch is null");
   int cur = 0;

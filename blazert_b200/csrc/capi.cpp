@@ -213,7 +213,12 @@ int bzr_add_cylinders(bzr_scene *s, const double *c, const double *a, const doub
 }
 
 int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
+  return bzr_commit_ex(s, options, 0u);
+}
+
+int bzr_commit_ex(bzr_scene *s, const bzr_build_options *options, uint32_t flags) {
   if (!s) return fail(BZR_EINVAL, "scene is null");
+  if (flags & ~uint32_t(BZR_COMMIT_GPU_BUILD)) return fail(BZR_EINVAL, "unknown commit flags");
   if (s->host.committed) return fail(BZR_ESTATE, "scene already committed");
   if (options) {
     if (options->bin_size < 2 || options->max_tree_depth > 1000)
@@ -231,7 +236,20 @@ int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
     for (int k = 0; k < bzr::kNumKinds; ++k) {
       bzr::Collection &c = s->host.kind[k];
       if (!c.present) continue;
-      c.tree = bzr::build_tree(c.boxes, s->host.opt);
+      bool built = false;
+      if ((flags & BZR_COMMIT_GPU_BUILD) && bzr::gpu_build_possible(c.boxes, s->host.opt)) {
+        const auto t0 = std::chrono::steady_clock::now();
+        bzr::Tree t;
+        if (bzr::gpu_build_tree(c.boxes, s->host.opt, &t) == cudaSuccess) {
+          t.build_seconds =
+              std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+          c.tree = std::move(t);
+          built = true;
+        } else {
+          cudaGetLastError();  // clear a launch error; the host builds the same tree
+        }
+      }
+      if (!built) c.tree = bzr::build_tree(c.boxes, s->host.opt);
       depth = std::max(depth, c.tree.max_depth);
       img[k] = bzr::flatten(s->host, k);
     }
@@ -698,6 +716,32 @@ int bzr_scene_tune(bzr_scene *s, int option, int64_t value) {
     }
   }
   return fail(BZR_EINVAL, "unknown tuning option");
+}
+
+long bzr_scene_tree(const bzr_scene *s, int kind, double *bmin, double *bmax, uint32_t *leaf,
+                    uint32_t *axis, uint32_t *children, uint32_t *prim_cnt, uint32_t *prim_ids,
+                    long prim_cap) {
+  if (!s || kind < 0 || kind >= bzr::kNumKinds) return fail(BZR_EINVAL, "bad argument");
+  if (!s->host.committed) return fail(BZR_ESTATE, "scene is not committed");
+  const bzr::Collection &c = s->host.kind[kind];
+  if (!c.present) return fail(BZR_EINVAL, "kind not in the scene");
+  const bzr::Tree &t = c.tree;
+  const long n = static_cast<long>(t.nodes.size());
+  if (!bmin || !bmax || !leaf || !axis || !children || !prim_cnt) return n;
+  for (long i = 0; i < n; ++i) {
+    const bzr::TreeNode &nd = t.nodes[i];
+    std::memcpy(bmin + 3 * i, nd.mn, sizeof nd.mn);
+    std::memcpy(bmax + 3 * i, nd.mx, sizeof nd.mx);
+    leaf[i] = nd.leaf;
+    axis[i] = nd.axis;
+    children[2 * i] = nd.child[0];
+    children[2 * i + 1] = nd.child[1];
+    prim_cnt[i] = nd.leaf == 1 ? nd.prim_cnt : 0;
+  }
+  if (prim_ids)
+    for (long i = 0; i < static_cast<long>(t.leaf_prims.size()) && i < prim_cap; ++i)
+      prim_ids[i] = t.leaf_prims[i];
+  return n;
 }
 
 int bzr_scene_stats(const bzr_scene *s, int kind, uint64_t *n_nodes, uint32_t *max_depth,

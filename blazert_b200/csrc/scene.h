@@ -2,6 +2,8 @@
 // the binned-SAH builder that reproduces the reference's tree node for node, and the
 // flattening into the device layout of layout.h.
 #pragma once
+#include <cuda_runtime_api.h>
+
 #include <cstddef>
 #include <cstdint>
 #include <vector>
@@ -38,6 +40,12 @@ struct Tree {
 };
 
 Tree build_tree(const PrimBoxes &boxes, const BuildOptions &opt);
+
+// The same tree built on the current CUDA device (gbuild.cu): level by level, one CTA per
+// node.  Possible for finite boxes and centres, at least one primitive and at most 256 bins;
+// returns a CUDA error otherwise or on failure (the caller then builds on the host).
+bool gpu_build_possible(const PrimBoxes &boxes, const BuildOptions &opt);
+cudaError_t gpu_build_tree(const PrimBoxes &boxes, const BuildOptions &opt, Tree *out);
 
 // Host copy of one collection (the caller's arrays are copied at add time).
 struct Collection {

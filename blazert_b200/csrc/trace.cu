@@ -532,16 +532,18 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
 
 namespace {
 template <int KIND>
-cudaError_t prepare_batch_kind(uint32_t stack_cap, int sms, int *blocks, int *blocks32) {
-  const bool local = stack_cap <= kLocalStack;
-  const size_t smem = local ? 0 : trace_smem_bytes(stack_cap, kTraceThreads);
+cudaError_t prepare_batch_kind(uint32_t stack_cap, const BatchPlan &plan, int *blocks,
+                               int *blocks32) {
+  const int sms = plan.sms, th = plan.threads;
+  const bool local = !plan.shared_stack && stack_cap <= kLocalStack;
+  const size_t smem = local ? 0 : trace_smem_bytes(stack_cap, th);
   const void *fp64 = local ? reinterpret_cast<const void *>(trace_batch_kernel<KIND, false, true>)
                            : reinterpret_cast<const void *>(trace_batch_kernel<KIND, false, false>);
   const void *mixed = local ? reinterpret_cast<const void *>(trace_batch_kernel<KIND, true, true>)
                             : reinterpret_cast<const void *>(trace_batch_kernel<KIND, true, false>);
-  const cudaError_t e = grid_for(fp64, kTraceThreads, smem, sms, blocks);
+  const cudaError_t e = grid_for(fp64, th, smem, sms, blocks);
   if (e != cudaSuccess) return e;
-  return grid_for(mixed, kTraceThreads, smem, sms, blocks32);
+  return grid_for(mixed, th, smem, sms, blocks32);
 }
 }  // namespace
 
@@ -553,16 +555,16 @@ cudaError_t batch_prepare(uint32_t stack_cap, BatchPlan *plan) {
   if (e != cudaSuccess) return e;
   plan->sms = sms;
   plan->stack_cap = stack_cap;
-  if ((e = prepare_batch_kind<kMesh>(stack_cap, sms, &plan->blocks[kMesh],
+  if ((e = prepare_batch_kind<kMesh>(stack_cap, *plan, &plan->blocks[kMesh],
                                      &plan->blocks32[kMesh])) != cudaSuccess)
     return e;
-  if ((e = prepare_batch_kind<kSpheres>(stack_cap, sms, &plan->blocks[kSpheres],
+  if ((e = prepare_batch_kind<kSpheres>(stack_cap, *plan, &plan->blocks[kSpheres],
                                         &plan->blocks32[kSpheres])) != cudaSuccess)
     return e;
-  if ((e = prepare_batch_kind<kPlanes>(stack_cap, sms, &plan->blocks[kPlanes],
+  if ((e = prepare_batch_kind<kPlanes>(stack_cap, *plan, &plan->blocks[kPlanes],
                                        &plan->blocks32[kPlanes])) != cudaSuccess)
     return e;
-  return prepare_batch_kind<kCylinders>(stack_cap, sms, &plan->blocks[kCylinders],
+  return prepare_batch_kind<kCylinders>(stack_cap, *plan, &plan->blocks[kCylinders],
                                         &plan->blocks32[kCylinders]);
 }
 
@@ -572,8 +574,9 @@ cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const Ba
   if (e != cudaSuccess) return e;
   batch_start_kernel<<<1, 256, 0, stream>>>(B, B.n_scenes);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const bool local = plan.stack_cap <= kLocalStack;
-  const size_t smem = local ? 0 : trace_smem_bytes(plan.stack_cap, kTraceThreads);
+  const bool local = !plan.shared_stack && plan.stack_cap <= kLocalStack;
+  const int th = plan.threads;
+  const size_t smem = local ? 0 : trace_smem_bytes(plan.stack_cap, th);
   for (int k = 0; k < kNumKinds; ++k) {
     if (!(plan.kinds_present & (1 << k))) continue;
     const bool m = mode == kModeMixed;
@@ -581,16 +584,16 @@ cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const Ba
     uint32_t *c = counters + k;
 #define BZR_BATCH_LAUNCH(KK)                                                                 \
   if (local && m)                                                                            \
-    trace_batch_kernel<KK, true, true><<<b, kTraceThreads, 0, stream>>>(B, io, c,            \
+    trace_batch_kernel<KK, true, true><<<b, th, 0, stream>>>(B, io, c,                       \
                                                                         plan.stack_cap);     \
   else if (local)                                                                            \
-    trace_batch_kernel<KK, false, true><<<b, kTraceThreads, 0, stream>>>(B, io, c,           \
+    trace_batch_kernel<KK, false, true><<<b, th, 0, stream>>>(B, io, c,                      \
                                                                          plan.stack_cap);    \
   else if (m)                                                                                \
-    trace_batch_kernel<KK, true, false><<<b, kTraceThreads, smem, stream>>>(B, io, c,        \
+    trace_batch_kernel<KK, true, false><<<b, th, smem, stream>>>(B, io, c,                   \
                                                                             plan.stack_cap); \
   else                                                                                       \
-    trace_batch_kernel<KK, false, false><<<b, kTraceThreads, smem, stream>>>(B, io, c,       \
+    trace_batch_kernel<KK, false, false><<<b, th, smem, stream>>>(B, io, c,                  \
                                                                              plan.stack_cap);
     switch (k) {
       case kMesh: BZR_BATCH_LAUNCH(kMesh); break;

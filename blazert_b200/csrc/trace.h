@@ -86,11 +86,14 @@ struct BatchView {
 };
 struct BatchPlan {
   int sms = 0;
+  int threads = kTraceThreads;  // threads per block: 64, 128 or 256
+  bool shared_stack = false;    // traversal stack in shared memory even when it fits locally
   int blocks[kNumKinds] = {0, 0, 0, 0};
   int blocks32[kNumKinds] = {0, 0, 0, 0};
   uint32_t stack_cap = 32;
   int kinds_present = 0;  // bit k: some scene has kind k
 };
+// Fills plan's grids for stack_cap, plan->threads and plan->shared_stack.
 cudaError_t batch_prepare(uint32_t stack_cap, BatchPlan *plan);
 // counters: kNumKinds device words (chunk counters), zeroed here.
 cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const BatchPlan &plan,

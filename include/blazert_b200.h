@@ -101,6 +101,15 @@ int bzr_add_cylinders(bzr_scene *scene, const double *centers, const double *sem
  * options may be NULL for the defaults. */
 int bzr_commit(bzr_scene *scene, const bzr_build_options *options);
 
+/* bzr_commit with flags (the builder has no counterpart in the reference; the tree it builds
+ * is the reference's).  BZR_COMMIT_GPU_BUILD builds each kind's BVH on the current CUDA device
+ * instead of the host -- the same binned SAH, the same bins and leaf size, the same tree node
+ * for node (node boxes can differ only in the sign of a zero bound) -- when every box and
+ * centre is finite and bin_size <= 256; otherwise, or if the device build fails, the host
+ * builds it. */
+#define BZR_COMMIT_GPU_BUILD 1u
+int bzr_commit_ex(bzr_scene *scene, const bzr_build_options *options, uint32_t flags);
+
 /* One ray (Ray{origin, direction, tmin, tmax}); *hit receives intersect1's return value. */
 int bzr_intersect1(const bzr_scene *scene, const double origin[3], const double direction[3],
                    double tmin, double tmax, bzr_rayhit *rayhit, int *hit);
@@ -170,6 +179,10 @@ int bzr_batch_intersect(bzr_batch *batch, const uint64_t *ray_offsets, const dou
                         void *stream);
 /* Waits for `stream` and reports the batch kernels' error word (as bzr_scene_check). */
 int bzr_batch_check(bzr_batch *batch, void *stream, uint32_t *flags);
+/* Launch shape of the batch's kernels: BZR_TUNE_BLOCK (64, 128, 256 threads per block) or
+ * BZR_TUNE_STACK (0 thread-local, 1 shared memory); see bzr_scene_tune.  Drops the cached
+ * graph; the next bzr_batch_intersect captures a new one.  Results do not change. */
+int bzr_batch_tune(bzr_batch *batch, int option, int64_t value);
 
 /* Adjoint of the closest-hit outputs (no counterpart in the reference): given a batch's
  * forward results (as returned by bzr_intersectN) and upstream gradients dL/dhit_distance (n),
@@ -220,6 +233,16 @@ int bzr_scene_tune(bzr_scene *scene, int option, int64_t value);
  * number of reference BVH nodes, the maximum depth and the host build time in seconds. */
 int bzr_scene_stats(const bzr_scene *scene, int kind, uint64_t *n_nodes, uint32_t *max_depth,
                     double *build_seconds);
+
+/* Node arrays of a committed scene's BVH of one kind (0 triangles, 1 spheres, 2 planes,
+ * 3 cylinders) in the reference's DFS node order (blazert/bvh/node.h:15-41): per node its box
+ * (3 + 3 doubles), leaf flag, split axis, two child indices and, for leaves, its primitive
+ * count; prim_ids receives the leaves' primitives in node order (up to prim_cap).  Returns
+ * the node count (call with NULL arrays to size them) or a negative status.  For tests and
+ * diagnostics: compares a build against the reference's tree. */
+long bzr_scene_tree(const bzr_scene *scene, int kind, double *bmin, double *bmax, uint32_t *leaf,
+                    uint32_t *axis, uint32_t *children, uint32_t *prim_cnt, uint32_t *prim_ids,
+                    long prim_cap);
 
 const char *bzr_last_error_string(void);
 

@@ -45,3 +45,34 @@ def test_batch_matches_per_scene_oracle(mode):
     for s, w in enumerate(wls):
         if w.rays.n and any(len(next(iter(getattr(w.scene, k).values()))) for k in w.scene.order):
             assert t[s] >= start > 0
+
+
+def test_batch_tuning_changes_speed_not_results():
+    """The batch kernels' launch shape (threads per block, stack storage; bzr_batch_tune) and
+    the batch autotuner's choice re-capture the graph and give the same results."""
+    import torch
+
+    from blazert_b200.autotune import autotune_batch
+
+    wls = _batch_case(n_scenes=10)
+    scenes = [product_scene(w.scene) for w in wls]
+    batch = B.Batch(scenes)
+    offs = np.concatenate([[0], np.cumsum([w.rays.n for w in wls])])
+    o = torch.from_numpy(np.concatenate([w.rays.origins for w in wls])).cuda()
+    d = torch.from_numpy(np.concatenate([w.rays.directions for w in wls])).cuda()
+    refs = [Oracle(w.scene).intersect(w.rays.origins, w.rays.directions) for w in wls]
+
+    def check():
+        got = to_numpy(batch.intersect(offs, o, d))
+        assert batch.check() == 0
+        for s, ref in enumerate(refs):
+            a, b = offs[s], offs[s + 1]
+            assert mismatches({k: v[a:b] for k, v in got.items()}, ref) == [], s
+
+    for cfg in (dict(threads=64), dict(threads=256), dict(shared_stack=True),
+                dict(threads=128, shared_stack=False)):
+        batch.tune(**cfg)
+        check()
+    res = autotune_batch(batch, offs, o, d)
+    assert set(res["choice"]) == {"threads", "shared_stack"}
+    check()
