@@ -217,12 +217,14 @@ class Scene:
                                                      h.ctypes.data_as(_dp), rot.ctypes.data_as(_dp),
                                                      n, C.byref(gid)), gid)
 
-    def commit(self, build_options: Optional[BuildOptions] = None, gpu_build: bool = False):
-        """blazert/scene.h:91-115.  gpu_build: build the BVHs on the GPU (the same trees;
-        bzr_commit_ex with BZR_COMMIT_GPU_BUILD)."""
+    def commit(self, build_options: Optional[BuildOptions] = None, gpu_build: Optional[bool] = None):
+        """blazert/scene.h:91-115.  gpu_build: None builds kinds of 65,536 primitives or more
+        on the GPU and smaller ones on the host; True / False forces the GPU / the host.  The
+        trees are the same either way (bzr_commit_ex)."""
         o = build_options or BuildOptions()
         opts = _OptsC(o.min_leaf_primitives, o.max_tree_depth, o.bin_size)
-        _check(self._lib.bzr_commit_ex(self._h, C.byref(opts), 1 if gpu_build else 0))
+        flags = 0 if gpu_build is None else (1 if gpu_build else 2)
+        _check(self._lib.bzr_commit_ex(self._h, C.byref(opts), flags))
         self.committed = True
         return True
 

@@ -42,6 +42,8 @@ constexpr int kStickyWord = kSlots * kSlotWords;
 constexpr int kStreams = 3;
 constexpr size_t kMaxChunks = 8;
 constexpr size_t kMinChunk = size_t(1) << 17;
+// Collections of at least this many primitives are built on the device by default.
+constexpr size_t kGpuBuildMin = size_t(1) << 16;
 
 int default_timeout_ms() {
   const char *s = std::getenv("BZR_TIMEOUT_MS");
@@ -218,7 +220,10 @@ int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
 
 int bzr_commit_ex(bzr_scene *s, const bzr_build_options *options, uint32_t flags) {
   if (!s) return fail(BZR_EINVAL, "scene is null");
-  if (flags & ~uint32_t(BZR_COMMIT_GPU_BUILD)) return fail(BZR_EINVAL, "unknown commit flags");
+  if (flags & ~uint32_t(BZR_COMMIT_GPU_BUILD | BZR_COMMIT_HOST_BUILD))
+    return fail(BZR_EINVAL, "unknown commit flags");
+  if ((flags & BZR_COMMIT_GPU_BUILD) && (flags & BZR_COMMIT_HOST_BUILD))
+    return fail(BZR_EINVAL, "BZR_COMMIT_GPU_BUILD and BZR_COMMIT_HOST_BUILD exclude each other");
   if (s->host.committed) return fail(BZR_ESTATE, "scene already committed");
   if (options) {
     if (options->bin_size < 2 || options->max_tree_depth > 1000)
@@ -237,7 +242,11 @@ int bzr_commit_ex(bzr_scene *s, const bzr_build_options *options, uint32_t flags
       bzr::Collection &c = s->host.kind[k];
       if (!c.present) continue;
       bool built = false;
-      if ((flags & BZR_COMMIT_GPU_BUILD) && bzr::gpu_build_possible(c.boxes, s->host.opt)) {
+      // the device build pays for its transfers and per-level launches from about 64k
+      // primitives on; below that the host builds unless asked otherwise
+      const bool want_gpu = (flags & BZR_COMMIT_GPU_BUILD) ||
+                            (!(flags & BZR_COMMIT_HOST_BUILD) && c.boxes.n >= kGpuBuildMin);
+      if (want_gpu && bzr::gpu_build_possible(c.boxes, s->host.opt)) {
         const auto t0 = std::chrono::steady_clock::now();
         bzr::Tree t;
         if (bzr::gpu_build_tree(c.boxes, s->host.opt, &t) == cudaSuccess) {

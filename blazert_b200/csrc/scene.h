@@ -42,7 +42,8 @@ struct Tree {
 Tree build_tree(const PrimBoxes &boxes, const BuildOptions &opt);
 
 // The same tree built on the current CUDA device (gbuild.cu): level by level, one CTA per
-// node.  Possible for finite boxes and centres, at least one primitive and at most 256 bins;
+// node.  Possible for finite boxes and centres, at least one primitive, min_leaf >= 1 and at
+// most 256 bins;
 // returns a CUDA error otherwise or on failure (the caller then builds on the host).
 bool gpu_build_possible(const PrimBoxes &boxes, const BuildOptions &opt);
 cudaError_t gpu_build_tree(const PrimBoxes &boxes, const BuildOptions &opt, Tree *out);

@@ -96,18 +96,22 @@ int bzr_add_cylinders(bzr_scene *scene, const double *centers, const double *sem
                       const double *semi_axes_b, const double *heights, const double *rotations,
                       size_t n, uint32_t *geom_id);
 
-/* Builds the per-kind binned-SAH BVHs on the host (the reference's tree, node for node),
- * flattens them into the device layout and uploads them to the current CUDA device.
- * options may be NULL for the defaults. */
+/* Builds the per-kind binned-SAH BVHs (the reference's tree, node for node; on the device for
+ * kinds of at least 65,536 primitives, see bzr_commit_ex), flattens them into the device
+ * layout and uploads them to the current CUDA device.  options may be NULL for the
+ * defaults. */
 int bzr_commit(bzr_scene *scene, const bzr_build_options *options);
 
-/* bzr_commit with flags (the builder has no counterpart in the reference; the tree it builds
- * is the reference's).  BZR_COMMIT_GPU_BUILD builds each kind's BVH on the current CUDA device
- * instead of the host -- the same binned SAH, the same bins and leaf size, the same tree node
- * for node (node boxes can differ only in the sign of a zero bound) -- when every box and
- * centre is finite and bin_size <= 256; otherwise, or if the device build fails, the host
- * builds it. */
+/* bzr_commit with flags (the device builder has no counterpart in the reference; the tree it
+ * builds is the reference's).  The device build gives each kind's BVH from the same binned
+ * SAH with the same bins and leaf size, node for node (node boxes can differ only in the sign
+ * of a zero bound), when every box and centre is finite, min_leaf_primitives >= 1 and
+ * bin_size <= 256; otherwise, or if it fails, the host builds.  By default (flags 0, and in
+ * bzr_commit) kinds of at least 65,536 primitives are built on the device;
+ * BZR_COMMIT_GPU_BUILD asks for the device at every size, BZR_COMMIT_HOST_BUILD for the host
+ * at every size. */
 #define BZR_COMMIT_GPU_BUILD 1u
+#define BZR_COMMIT_HOST_BUILD 2u
 int bzr_commit_ex(bzr_scene *scene, const bzr_build_options *options, uint32_t flags);
 
 /* One ray (Ray{origin, direction, tmin, tmax}); *hit receives intersect1's return value. */
