@@ -85,6 +85,10 @@ struct bzr_scene {
   size_t stage_bytes = 0;
   uint32_t *pinned_err = nullptr;  // one error word per chunk
   cudaStream_t streams[kStreams] = {nullptr, nullptr, nullptr};
+  // host-array pipeline: copies in on copy_in, kernels on streams[], copies out on copy_out,
+  // chained per chunk by ev_in / ev_done
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t ev_in[kMaxChunks] = {}, ev_done[kMaxChunks] = {};
 
   ~bzr_scene() {
     if (device >= 0) {
@@ -93,12 +97,20 @@ struct bzr_scene {
       cudaSetDevice(device);
       for (cudaStream_t st : streams)
         if (st) cudaStreamSynchronize(st);
+      if (copy_in) cudaStreamSynchronize(copy_in);
+      if (copy_out) cudaStreamSynchronize(copy_out);
       cudaFree(arena);
       cudaFree(slots);
       cudaFree(stage_dev);
       cudaFreeHost(pinned_err);
       for (cudaStream_t st : streams)
         if (st) cudaStreamDestroy(st);
+      if (copy_in) cudaStreamDestroy(copy_in);
+      if (copy_out) cudaStreamDestroy(copy_out);
+      for (size_t c = 0; c < kMaxChunks; ++c) {
+        if (ev_in[c]) cudaEventDestroy(ev_in[c]);
+        if (ev_done[c]) cudaEventDestroy(ev_done[c]);
+      }
       if (plan.pool) cudaMemPoolDestroy(plan.pool);  // released once pending frees complete
       cudaSetDevice(cur);
     }
@@ -350,6 +362,15 @@ int bzr_commit_ex(bzr_scene *s, const bzr_build_options *options, uint32_t flags
     e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
   }
+  for (cudaStream_t *st : {&s->copy_in, &s->copy_out}) {
+    e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+  }
+  for (size_t c = 0; c < kMaxChunks; ++c) {
+    e = cudaEventCreateWithFlags(&s->ev_in[c], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_done[c], cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
+  }
   e = bzr::trace_prepare(s->view, &s->plan);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   {  // per-scene memory pool for per-call scratch; it keeps freed memory for reuse
@@ -479,8 +500,10 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
   uint32_t *d_prim = prim ? reinterpret_cast<uint32_t *>(take(4 * n)) : nullptr;
   uint32_t *d_geom = geom ? reinterpret_cast<uint32_t *>(take(4 * n)) : nullptr;
   uint8_t *d_hit = hit ? reinterpret_cast<uint8_t *>(take(n)) : nullptr;
-  // Chunks round-robin over the scene's streams, so that the copies in of one chunk, the
-  // kernels of another and the copies out of a third overlap.
+  // A three-stage pipeline over chunks: the copies in run ahead on copy_in, each chunk's
+  // kernels start on one of the scene's streams (round robin, so that one chunk's slowest rays
+  // overlap the next chunk's kernels) once its copies in are done, and its copies out follow
+  // on copy_out once its kernels are done.
   const size_t chunk = n <= kMinChunk ? n : std::max(kMinChunk, (n + kMaxChunks - 1) / kMaxChunks);
   const size_t nchunks = (n + chunk - 1) / chunk;
   cudaError_t e = cudaSuccess;
@@ -490,7 +513,8 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
     uint32_t *cnt = c == 0 ? counters : s->slots + kSlotWords * (s->next_slot.fetch_add(1) % kSlots);
     auto h2d = [&](double *dst, const double *src, size_t per) {
       if (src && e == cudaSuccess)
-        e = cudaMemcpyAsync(dst + per * a, src + per * a, 8 * per * m, cudaMemcpyHostToDevice, st);
+        e = cudaMemcpyAsync(dst + per * a, src + per * a, 8 * per * m, cudaMemcpyHostToDevice,
+                            s->copy_in);
     };
     h2d(d_org, org, 3);
     h2d(d_dir, dir, 3);
@@ -510,10 +534,15 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
     ci.geom = d_geom ? d_geom + a : nullptr;
     ci.hit = d_hit ? d_hit + a : nullptr;
     ci.error_word = cnt + bzr::kNumKinds;
+    if (e == cudaSuccess) e = cudaEventRecord(s->ev_in[c], s->copy_in);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, s->ev_in[c], 0);
     if (e == cudaSuccess) e = cudaMemsetAsync(ci.error_word, 0, sizeof(uint32_t), st);
     if (e == cudaSuccess) e = bzr::launch_trace(s->view, ci, mode, s->plan, st, cnt, totals);
+    if (e == cudaSuccess) e = cudaEventRecord(s->ev_done[c], st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s->copy_out, s->ev_done[c], 0);
     auto d2h = [&](void *dst, const void *src, size_t bytes) {
-      if (dst && e == cudaSuccess) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+      if (dst && e == cudaSuccess)
+        e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->copy_out);
     };
     d2h(t ? t + a : nullptr, ci.t, 8 * m);
     d2h(uv ? uv + 2 * a : nullptr, ci.uv, 16 * m);
@@ -524,8 +553,8 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
     d2h(s->pinned_err + c, ci.error_word, sizeof(uint32_t));
   }
   if (e != cudaSuccess) return cuda_fail(e, "batch submission");
-  for (int k = 0; k < kStreams; ++k) {
-    const int rc = wait_stream(s->streams[k], default_timeout_ms());
+  for (cudaStream_t q : {s->copy_in, s->streams[0], s->streams[1], s->streams[2], s->copy_out}) {
+    const int rc = wait_stream(q, default_timeout_ms());
     if (rc) return rc;
   }
   uint32_t bits = 0;
