@@ -97,9 +97,22 @@ def library():
         lib.bzr_scene_tree.argtypes = [P, C.c_int] + [P] * 7 + [C.c_long]
         lib.bzr_scene_stats.argtypes = [P, C.c_int, C.POINTER(C.c_uint64), _u32p,
                                         C.POINTER(C.c_double)]
+        lib.bzr_distance_to_surface.argtypes = [P, C.c_int, C.c_size_t, P, P, P, P, P]
+        lib.bzr_closest_surface.argtypes = [P, C.c_size_t, P, P, P, P, P]
         lib.bzr_last_error_string.restype = C.c_char_p
         _lib = lib
     return _lib
+
+
+KIND_NAMES = ("mesh", "spheres", "planes", "cylinders")
+
+
+def _is_cuda_tensor(a):
+    try:
+        import torch
+    except ImportError:
+        return False
+    return isinstance(a, torch.Tensor) and a.is_cuda
 
 
 def _check(rc):
@@ -329,6 +342,67 @@ class Scene:
                                            ptr(out.get("geom")), ptr(out.get("hit")),
                                            MODES[mode], flags, C.c_void_p(st)))
         out["_keep"] = (o, d, tmn, tmx)
+        return out
+
+    def distance_to_surface(self, kind, prim_ids, points, closest=False, stream=None):
+        """distance_to_surface of primitive prim_ids[i] of `kind` ("mesh", "spheres", "planes",
+        "cylinders") and point i (bzr_distance_to_surface).  numpy inputs: returns numpy
+        distances (and, for meshes with closest=True, the n x 3 closest points).  torch CUDA
+        tensors: queued on ``stream`` (default: torch's current stream), returns tensors."""
+        k = KIND_NAMES.index(kind)
+        if closest and kind != "mesh":
+            raise ValueError("closest points are returned for meshes only")
+        if _is_cuda_tensor(points):
+            import torch
+            dev = points.device
+            pts = points.to(torch.float64).contiguous()
+            ids = torch.as_tensor(prim_ids, device=dev).to(torch.int32).contiguous()
+            n = pts.shape[0]
+            dist = torch.empty(n, dtype=torch.float64, device=dev)
+            cl = torch.empty((n, 3), dtype=torch.float64, device=dev) if closest else None
+            st = (stream or torch.cuda.current_stream(dev)).cuda_stream
+            _check(self._lib.bzr_distance_to_surface(
+                self._h, k, n, ids.data_ptr(), pts.data_ptr(), dist.data_ptr(),
+                None if cl is None else cl.data_ptr(), C.c_void_p(st)))
+            return (dist, cl) if closest else dist
+        pts = _f64(points, 3)
+        n = pts.shape[0]
+        ids = np.ascontiguousarray(prim_ids, np.uint32).reshape(-1)
+        if ids.shape[0] != n:
+            raise ValueError("one primitive id per point")
+        dist = np.empty(n)
+        cl = np.empty((n, 3)) if closest else None
+        _check(self._lib.bzr_distance_to_surface(self._h, k, n, ids.ctypes.data, pts.ctypes.data,
+                                                 dist.ctypes.data,
+                                                 None if cl is None else cl.ctypes.data, None))
+        return (dist, cl) if closest else dist
+
+    def closest_surface(self, points, stream=None):
+        """Nearest surface of the scene per point (bzr_closest_surface): dict of distance,
+        prim and geom (numpy for numpy input; torch tensors, queued on ``stream``, for CUDA
+        tensors)."""
+        if _is_cuda_tensor(points):
+            import torch
+            dev = points.device
+            pts = points.to(torch.float64).contiguous()
+            n = pts.shape[0]
+            out = dict(distance=torch.empty(n, dtype=torch.float64, device=dev),
+                       prim=torch.empty(n, dtype=torch.int32, device=dev),
+                       geom=torch.empty(n, dtype=torch.int32, device=dev))
+            st = (stream or torch.cuda.current_stream(dev)).cuda_stream
+            _check(self._lib.bzr_closest_surface(self._h, n, pts.data_ptr(),
+                                                 out["distance"].data_ptr(),
+                                                 out["prim"].data_ptr(), out["geom"].data_ptr(),
+                                                 C.c_void_p(st)))
+            out["_keep"] = pts
+            return out
+        pts = _f64(points, 3)
+        n = pts.shape[0]
+        out = dict(distance=np.empty(n), prim=np.empty(n, np.uint32), geom=np.empty(n, np.uint32))
+        _check(self._lib.bzr_closest_surface(self._h, n, pts.ctypes.data,
+                                             out["distance"].ctypes.data,
+                                             out["prim"].ctypes.data, out["geom"].ctypes.data,
+                                             None))
         return out
 
     def tune(self, sort=None, sort_min_rays=None, threads=None, shared_stack=None, chunk=None):

@@ -18,6 +18,7 @@
 #include "layout.h"
 #include "scene.h"
 #include "adjoint.h"
+#include "distance.h"
 #include "capi_internal.h"
 #include "trace.h"
 
@@ -291,12 +292,14 @@ int bzr_commit_ex(bzr_scene *s, const bzr_build_options *options, uint32_t flags
     total = align_up(total + std::max<size_t>(bytes, 1), 256);
     return off;
   };
-  size_t off_nodes64[4], off_nodes32[4], off_payload[4], off_ids[4], off_tri[4], off_tv[4];
+  size_t off_nodes64[4], off_nodes32[4], off_payload[4], off_ids[4], off_tri[4], off_tv[4],
+      off_pos[4];
   for (int k = 0; k < bzr::kNumKinds; ++k) {
     off_nodes64[k] = place(img[k].nodes64.data(), img[k].nodes64.size() * sizeof(double));
     off_nodes32[k] = place(img[k].nodes32.data(), img[k].nodes32.size() * sizeof(float));
     off_payload[k] = place(img[k].payload.data(), img[k].payload.size() * sizeof(double));
     off_ids[k] = place(img[k].prim_ids.data(), img[k].prim_ids.size() * sizeof(uint32_t));
+    off_pos[k] = place(img[k].pos_of.data(), img[k].pos_of.size() * sizeof(uint32_t));
     off_tri[k] = place(img[k].tri.data(), img[k].tri.size() * sizeof(uint32_t));
     off_tv[k] = place(img[k].verts.data(), img[k].verts.size() * sizeof(double));
   }
@@ -328,6 +331,7 @@ int bzr_commit_ex(bzr_scene *s, const bzr_build_options *options, uint32_t flags
     v.nodes32 = reinterpret_cast<const float *>(base + off_nodes32[k]);
     v.payload = reinterpret_cast<const double *>(base + off_payload[k]);
     v.prim_ids = reinterpret_cast<const uint32_t *>(base + off_ids[k]);
+    v.pos_of = reinterpret_cast<const uint32_t *>(base + off_pos[k]);
     v.tri = reinterpret_cast<const uint32_t *>(base + off_tri[k]);
     v.verts = reinterpret_cast<const double *>(base + off_tv[k]);
     v.n_internal = img[k].n_internal;
@@ -358,19 +362,6 @@ int bzr_commit_ex(bzr_scene *s, const bzr_build_options *options, uint32_t flags
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemset");
   e = cudaMallocHost(&s->pinned_err, kMaxChunks * sizeof(uint32_t));
   if (e != cudaSuccess) return fail(BZR_ENOMEM, "pinned allocation failed");
-  for (cudaStream_t &st : s->streams) {
-    e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
-  }
-  for (cudaStream_t *st : {&s->copy_in, &s->copy_out}) {
-    e = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
-  }
-  for (size_t c = 0; c < kMaxChunks; ++c) {
-    e = cudaEventCreateWithFlags(&s->ev_in[c], cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_done[c], cudaEventDisableTiming);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
-  }
   e = bzr::trace_prepare(s->view, &s->plan);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   {  // per-scene memory pool for per-call scratch; it keeps freed memory for reuse
@@ -468,6 +459,23 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
 
   // Host arrays: stage through device buffers on the scene's stream.
   std::lock_guard<std::mutex> lock(s->stage_mu);
+  // the pipeline's streams and events are made on the first host-array call: scenes that are
+  // only queried with device arrays (or through a batch) never need them
+  if (!s->copy_out) {
+    cudaError_t ce = cudaSuccess;
+    for (cudaStream_t &st : s->streams)
+      if (ce == cudaSuccess && !st) ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    for (size_t c = 0; c < kMaxChunks && ce == cudaSuccess; ++c) {
+      if (!s->ev_in[c]) ce = cudaEventCreateWithFlags(&s->ev_in[c], cudaEventDisableTiming);
+      if (ce == cudaSuccess && !s->ev_done[c])
+        ce = cudaEventCreateWithFlags(&s->ev_done[c], cudaEventDisableTiming);
+    }
+    if (ce == cudaSuccess && !s->copy_in)
+      ce = cudaStreamCreateWithFlags(&s->copy_in, cudaStreamNonBlocking);
+    // copy_out last: its presence marks the whole set as made
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&s->copy_out, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamCreate");
+  }
   // every staged array starts on a 256-byte boundary (see take() below)
   const size_t piece_bytes[10] = {24 * n, 24 * n, tmin ? 8 * n : 0, tmax ? 8 * n : 0,
                                   8 * n, uv ? 16 * n : 0, normal ? 24 * n : 0,
@@ -674,6 +682,100 @@ int bzr_adjoint_hit(const bzr_scene *cs, size_t n, const double *origins,
   if (gvn) cudaFreeAsync(gvn, st);
   cudaSetDevice(cur);
   return e == cudaSuccess ? BZR_OK : cuda_fail(e, "adjoint launch");
+}
+
+// Shared body of the two distance queries: kind >= 0 is the per-primitive form, -1 the scene
+// form.  Device arrays are queued on the caller's stream; host arrays are staged through
+// stream-ordered scratch from the scene's pool and the call waits for the results.
+static int run_distance(const bzr_scene *cs, int kind, size_t n, const uint32_t *ids,
+                        const double *points, double *distance, double *closest, uint32_t *prim,
+                        uint32_t *geom, void *stream) {
+  bzr_scene *s = const_cast<bzr_scene *>(cs);
+  if (!s) return fail(BZR_EINVAL, "scene is null");
+  if (!s->host.committed) return fail(BZR_ESTATE, "scene is not committed");
+  if (kind >= bzr::kNumKinds || kind < -1) return fail(BZR_EINVAL, "bad primitive kind");
+  if (kind >= 0 && !s->host.kind[kind].present)
+    return fail(BZR_EINVAL, "the scene has no primitives of this kind");
+  if (closest && kind != bzr::kMesh)
+    return fail(BZR_EINVAL, "closest points are returned for triangles only");
+  if (n == 0) return BZR_OK;
+  if (!points || !distance || (kind >= 0 && !ids)) return fail(BZR_EINVAL, "null argument");
+  if (n > (size_t(1) << 40)) return fail(BZR_EINVAL, "batch too large");
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != s->device) cudaSetDevice(s->device);
+  struct DevGuard {
+    int d;
+    ~DevGuard() { cudaSetDevice(d); }
+  } guard{cur};
+  const void *ptrs[6] = {ids, points, distance, closest, prim, geom};
+  int n_dev = 0, n_given = 0;
+  for (const void *p : ptrs)
+    if (p) {
+      ++n_given;
+      n_dev += is_device_ptr(p) ? 1 : 0;
+    }
+  if (n_dev != 0 && n_dev != n_given)
+    return fail(BZR_EINVAL, "arrays must be all host or all device memory");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  bzr::DistanceIO io;
+  io.n = n;
+  io.error_word = s->slots + kStickyWord;
+  auto launch = [&]() {
+    return kind >= 0 ? bzr::launch_distance(s->view, kind, io, s->plan.sms, st)
+                     : bzr::launch_nearest(s->view, io, s->plan.sms, st);
+  };
+  if (n_dev == n_given) {
+    io.ids = ids; io.points = points; io.distance = distance; io.closest = closest;
+    io.prim = prim; io.geom = geom;
+    const cudaError_t e = launch();
+    return e == cudaSuccess ? BZR_OK : cuda_fail(e, "distance launch");
+  }
+  if (kind >= 0) {
+    const size_t count = s->host.kind[kind].n;
+    for (size_t i = 0; i < n; ++i)
+      if (ids[i] >= count) return fail(BZR_EINVAL, "primitive id outside the kind");
+  }
+  const size_t piece[6] = {kind >= 0 ? 4 * n : 0, 24 * n, 8 * n, closest ? 24 * n : 0,
+                           prim ? 4 * n : 0, geom ? 4 * n : 0};
+  size_t total = 0;
+  for (size_t b : piece) total += align_up(b, 256);
+  char *dev = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&dev), total, s->plan.pool, st);
+  if (e != cudaSuccess) return fail(BZR_ENOMEM, "distance staging allocation failed");
+  char *at[6];
+  for (size_t j = 0, off = 0; j < 6; ++j) {
+    at[j] = piece[j] ? dev + off : nullptr;
+    off += align_up(piece[j], 256);
+  }
+  io.ids = reinterpret_cast<const uint32_t *>(at[0]);
+  io.points = reinterpret_cast<const double *>(at[1]);
+  io.distance = reinterpret_cast<double *>(at[2]);
+  io.closest = reinterpret_cast<double *>(at[3]);
+  io.prim = reinterpret_cast<uint32_t *>(at[4]);
+  io.geom = reinterpret_cast<uint32_t *>(at[5]);
+  if (kind >= 0) e = cudaMemcpyAsync(at[0], ids, piece[0], cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(at[1], points, piece[1], cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = launch();
+  void *outs[4] = {distance, closest, prim, geom};
+  for (int j = 0; j < 4 && e == cudaSuccess; ++j)
+    if (outs[j])
+      e = cudaMemcpyAsync(outs[j], at[2 + j], piece[2 + j], cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(dev, st);
+  if (e != cudaSuccess) return cuda_fail(e, "distance staging");
+  return wait_stream(st, default_timeout_ms());
+}
+
+int bzr_distance_to_surface(const bzr_scene *s, int kind, size_t n, const uint32_t *prim_ids,
+                            const double *points, double *distance, double *closest,
+                            void *stream) {
+  if (kind < 0) return fail(BZR_EINVAL, "bad primitive kind");
+  return run_distance(s, kind, n, prim_ids, points, distance, closest, nullptr, nullptr, stream);
+}
+
+int bzr_closest_surface(const bzr_scene *s, size_t n, const double *points, double *distance,
+                        uint32_t *prim, uint32_t *geom, void *stream) {
+  return run_distance(s, -1, n, nullptr, points, distance, nullptr, prim, geom, stream);
 }
 
 int bzr_intersect1(const bzr_scene *s, const double origin[3], const double direction[3],

@@ -31,6 +31,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "scene.h"
@@ -572,6 +573,21 @@ __global__ void scatter_kernel(const GNode *g, const uint32_t *dfs, TreeNode *ou
   }
 }
 
+// Device scratch of the builder, one per device, kept from build to build and grown on demand.
+// A mesh of 3 x 10^5 triangles builds its levels in about 5 ms, while allocating and releasing
+// its scratch (about 420 bytes per primitive) took about 40 ms; a workspace above kKeepBytes is
+// released after its build.  The mutex serialises device builds of one process.
+constexpr size_t kKeepBytes = size_t(2) << 30;
+constexpr int kMaxDevices = 64;
+struct Workspace {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+};
+std::mutex g_workspace_mutex;
+Workspace g_workspace[kMaxDevices];
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
 bool finite_boxes(const PrimBoxes &b) {
   for (size_t i = 0; i < 3 * b.n; ++i)
     if (!std::isfinite(b.bmin[i]) || !std::isfinite(b.bmax[i]) || !std::isfinite(b.center[i]))
@@ -592,27 +608,47 @@ cudaError_t gpu_build_tree(const PrimBoxes &boxes, const BuildOptions &opt, Tree
   const size_t n = boxes.n;
   const size_t max_nodes = 2 * n;  // 2n - 1 nodes at most with min_leaf >= 1
   const size_t max_wide = n / kWidePrims + 2;
-  double *d_box = nullptr;  // bmin, bmax, centre: n x 3 each
-  uint32_t *d_u32 = nullptr;  // ids, L, R, counts[8], size, dfs
-  Seg *d_seg = nullptr;       // narrow ranges x 2, wide ranges x 2
-  GNode *d_nodes = nullptr;
-  TreeNode *d_tree = nullptr;
-  cudaError_t e = cudaSuccess;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  // bmin, bmax, centre (n x 3 each); ids, L, R, counts[8], size, dfs; narrow ranges x 2 and
+  // wide ranges x 2; level-order nodes; DFS-ordered nodes
+  const size_t sz_box = align256(72 * n);
+  const size_t sz_u32 = align256(sizeof(uint32_t) * (3 * n + 8 + 2 * max_nodes));
+  const size_t sz_seg = align256(sizeof(Seg) * 2 * (n + 1 + max_wide));
+  const size_t sz_nodes = align256(sizeof(GNode) * max_nodes);
+  const size_t need = sz_box + sz_u32 + sz_seg + sz_nodes + sizeof(TreeNode) * max_nodes;
+  std::vector<uint32_t> ids(n);
+  for (size_t i = 0; i < n; ++i) ids[i] = static_cast<uint32_t>(i);
+  Tree &t = *out;
+  uint32_t h[8];
+  std::unique_lock<std::mutex> lock(g_workspace_mutex);
+  Workspace &ws = g_workspace[dev];
+  if (ws.bytes < need) {
+    if (ws.ptr) cudaFree(ws.ptr);
+    ws = Workspace{};
+    e = cudaMalloc(&ws.ptr, need);
+    if (e != cudaSuccess) {
+      ws.ptr = nullptr;
+      return e;
+    }
+    ws.bytes = need;
+  }
+  char *base = static_cast<char *>(ws.ptr);
+  double *d_box = reinterpret_cast<double *>(base);
+  uint32_t *d_u32 = reinterpret_cast<uint32_t *>(base + sz_box);
+  Seg *d_seg = reinterpret_cast<Seg *>(base + sz_box + sz_u32);
+  GNode *d_nodes = reinterpret_cast<GNode *>(base + sz_box + sz_u32 + sz_seg);
+  TreeNode *d_tree = reinterpret_cast<TreeNode *>(base + sz_box + sz_u32 + sz_seg + sz_nodes);
   auto ok = [&](cudaError_t r) {
     if (e == cudaSuccess) e = r;
     return e == cudaSuccess;
   };
-  ok(cudaMalloc(&d_box, 72 * n));
-  ok(cudaMalloc(&d_u32, sizeof(uint32_t) * (3 * n + 8 + 2 * max_nodes)));
-  ok(cudaMalloc(&d_seg, sizeof(Seg) * 2 * (n + 1 + max_wide)));
-  ok(cudaMalloc(&d_nodes, sizeof(GNode) * max_nodes));
-  ok(cudaMalloc(&d_tree, sizeof(TreeNode) * max_nodes));
   uint32_t *d_ids = d_u32, *d_L = d_u32 + n, *d_R = d_u32 + 2 * n, *d_counts = d_u32 + 3 * n;
   uint32_t *d_size = d_counts + 8, *d_dfs = d_size + max_nodes;
   Seg *narrow[2] = {d_seg, d_seg + (n + 1)};
   Seg *wide[2] = {d_seg + 2 * (n + 1), d_seg + 2 * (n + 1) + max_wide};
-  std::vector<uint32_t> ids(n);
-  for (size_t i = 0; i < n; ++i) ids[i] = static_cast<uint32_t>(i);
   ok(cudaMemcpy(d_box, boxes.bmin.data(), 24 * n, cudaMemcpyHostToDevice));
   ok(cudaMemcpy(d_box + 3 * n, boxes.bmax.data(), 24 * n, cudaMemcpyHostToDevice));
   ok(cudaMemcpy(d_box + 6 * n, boxes.center.data(), 24 * n, cudaMemcpyHostToDevice));
@@ -641,7 +677,8 @@ cudaError_t gpu_build_tree(const PrimBoxes &boxes, const BuildOptions &opt, Tree
   A.max_depth = opt.max_depth;
   A.nb = nb;
   // counts: [0] next narrow ranges, [1] nodes, [2] max depth, [3] bad splits, [4] next wide
-  uint32_t h[8] = {root_wide ? 0u : 1u, 1u, 0u, 0u, root_wide ? 1u : 0u, 0u, 0u, 0u};
+  const uint32_t h0[8] = {root_wide ? 0u : 1u, 1u, 0u, 0u, root_wide ? 1u : 0u, 0u, 0u, 0u};
+  std::memcpy(h, h0, sizeof h);
   std::vector<uint32_t> level_start{0u, 1u};  // node index ranges of the levels
   int cur = 0;
   uint32_t n_narrow = h[0], n_wide = h[4];
@@ -693,15 +730,18 @@ cudaError_t gpu_build_tree(const PrimBoxes &boxes, const BuildOptions &opt, Tree
   }
   if (e == cudaSuccess) scatter_kernel<<<grid, 256>>>(d_nodes, d_dfs, d_tree, count);
   ok(cudaGetLastError());
-  Tree &t = *out;
-  t.nodes.resize(count);
-  ok(cudaMemcpy(t.nodes.data(), d_tree, sizeof(TreeNode) * count, cudaMemcpyDeviceToHost));
-  ok(cudaMemcpy(ids.data(), d_ids, 4 * n, cudaMemcpyDeviceToHost));
-  cudaFree(d_box);
-  cudaFree(d_u32);
-  cudaFree(d_seg);
-  cudaFree(d_nodes);
-  cudaFree(d_tree);
+  if (e == cudaSuccess) {
+    t.nodes.resize(count);
+    ok(cudaMemcpy(t.nodes.data(), d_tree, sizeof(TreeNode) * count, cudaMemcpyDeviceToHost));
+    ok(cudaMemcpy(ids.data(), d_ids, 4 * n, cudaMemcpyDeviceToHost));
+  }
+  // nothing of this build may still run on the workspace when the next build takes it
+  if (e != cudaSuccess) cudaStreamSynchronize(0);
+  if (ws.bytes > kKeepBytes) {
+    cudaFree(ws.ptr);
+    ws = Workspace{};
+  }
+  lock.unlock();
   if (e != cudaSuccess) return e;
   // structural check before anything walks the tree: DFS pre-order (left child right after its
   // parent, right child after that), leaf ranges tiling [0, n) left to right

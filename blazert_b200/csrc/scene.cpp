@@ -459,6 +459,7 @@ KindImage flatten(const HostScene &s, int kind) {
   const size_t np = t.leaf_prims.size();
   const int stride = kPayloadDoubles[kind];
   img.prim_ids.resize(np);
+  img.pos_of.assign(np, 0u);
   img.payload.assign(np * stride, 0.0);
   std::vector<uint32_t> remap;
   if (kind == kMesh) {
@@ -472,6 +473,7 @@ KindImage flatten(const HostScene &s, int kind) {
       const uint32_t at = leaf_pos[i] + q;
       const uint32_t id = t.leaf_prims[nd.prim_off + q];
       img.prim_ids[at] = id | (q + 1 == nd.prim_cnt ? kLastBit : 0u);
+      img.pos_of[id] = at;
       double *p = img.payload.data() + size_t(at) * stride;
       switch (kind) {
         case kMesh: {

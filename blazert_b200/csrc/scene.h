@@ -82,6 +82,7 @@ struct KindImage {
   std::vector<float> nodes32;
   std::vector<double> payload;
   std::vector<uint32_t> prim_ids;
+  std::vector<uint32_t> pos_of;  // leaf-ordered position of each primitive id
   std::vector<uint32_t> tri;     // triangles: {i0, i1, i2, id word} per leaf-ordered triangle
   std::vector<double> verts;     // triangles: {x, y, z, 0} per vertex, in order of first use
   uint32_t n_internal = 0;

@@ -248,6 +248,32 @@ long bzr_scene_tree(const bzr_scene *scene, int kind, double *bmin, double *bmax
                     uint32_t *axis, uint32_t *children, uint32_t *prim_cnt, uint32_t *prim_ids,
                     long prim_cap);
 
+/* Distance from points to given primitives of one kind (0 triangles, 1 spheres, 2 planes,
+ * 3 cylinders): distance[i] = distance_to_surface(primitive prim_ids[i], points[3i..3i+2]),
+ * bit for bit the reference's per-primitive function
+ *   spheres    blazert/primitives/sphere.h:179-182    |norm(center - p) - radius|
+ *   planes     blazert/primitives/plane.h:272-284     |local z| inside the rectangle test,
+ *                                                     DBL_MAX outside it
+ *   cylinders  blazert/primitives/cylinder.h:677-759  shell (Newton search on the ellipse), caps
+ * and for triangles closest_point_on_triangle (blazert/primitives/trimesh_distance.h:177-218)
+ * on the face's vertices with distance norm(closest - p); closest (n x 3, triangles only, may
+ * be NULL) receives those points.  All arrays host memory (the call returns when the results
+ * are written; an id outside the kind is BZR_EINVAL) or all device memory (queued on stream;
+ * an id outside the kind gives NaN and sets the error word bzr_scene_check reads). */
+int bzr_distance_to_surface(const bzr_scene *scene, int kind, size_t n, const uint32_t *prim_ids,
+                            const double *points, double *distance, double *closest,
+                            void *stream);
+
+/* Nearest surface of the whole scene per point: distance[i] = the smallest
+ * bzr_distance_to_surface value over every primitive of every kind, prim[i] / geom[i] (may be
+ * NULL) the primitive that gives it -- the first in the order triangles, spheres, planes,
+ * cylinders and, within a kind, the lowest id among equal distances; +inf and BZR_INVALID_ID
+ * when no primitive gives a number.  Triangles and spheres are searched through their BVHs
+ * (a subtree is skipped only when its box is farther than the best distance), planes and
+ * cylinders are evaluated one by one.  Arrays all host or all device memory, as above. */
+int bzr_closest_surface(const bzr_scene *scene, size_t n, const double *points, double *distance,
+                        uint32_t *prim, uint32_t *geom, void *stream);
+
 const char *bzr_last_error_string(void);
 
 #ifdef __cplusplus

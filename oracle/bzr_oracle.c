@@ -990,3 +990,264 @@ int ora_traverse_kind(const ora_scene *s, int kind, const double org[3], const d
   *prim = rh.prim;
   return h;
 }
+
+/* ------------------------------------------------------------------------------------------
+ * Distance to surface (blazert/primitives/sphere.h:179-182, plane.h:272-284,
+ * cylinder.h:498-759; triangles through trimesh_distance.h:37-218). */
+
+/* cylinder.h:508-513 */
+static double ellipse_equation(double a, double b, double x, double y) {
+  return (x * x) / (a * a) + (y * y) / (b * b) - 1;
+}
+
+/* the conditional square root every branch of cylinder.h:516-590 starts with */
+static double gap_sqrt(double val, double s) {
+  return (val * val > s * s) ? sqrt(val * val - s * s) : sqrt(s * s - val * val);
+}
+
+/* branch: 0 upper/x, 1 lower/x, 2 upper/y, 3 lower/y (cylinder.h:516-547) */
+static double distance_derivative(int branch, double a, double b, double xq, double yq,
+                                  double val) {
+  switch (branch) {
+    case 0: {
+      const double sq = gap_sqrt(val, a);
+      return -2 * (xq - val) - 2 * b * val * (b / a * sq - yq) / (a * sq);
+    }
+    case 1: {
+      const double sq = gap_sqrt(val, a);
+      return -2 * (xq - val) - 2 * b * val * (b / a * sq + yq) / (a * sq);
+    }
+    case 2: {
+      const double sq = gap_sqrt(val, b);
+      return -2 * (yq - val) - 2 * a * val * (a / b * sq + xq) / (b * sq);
+    }
+    default: {
+      const double sq = gap_sqrt(val, b);
+      return -2 * (yq - val) - 2 * a * val * (a / b * sq - xq) / (b * sq);
+    }
+  }
+}
+
+/* cylinder.h:551-590 */
+static double single_newton_iteration(int branch, double a, double b, double xq, double yq,
+                                      double val) {
+  switch (branch) {
+    case 0: {
+      const double sq = gap_sqrt(val, a);
+      return ((a * a * a * xq - a * val * val * xq) * sq + b * val * val * val * yq) /
+             ((a * a * a - a * b * b - a * val * val + b * b * val * val / a) * sq + a * a * b * yq);
+    }
+    case 1: {
+      const double sq = gap_sqrt(val, a);
+      return ((-a * a * a * xq + a * val * val * xq) * sq + b * val * val * val * yq) /
+             ((-a * a * a + a * b * b + a * val * val - b * b * val * val / a) * sq + a * a * b * yq);
+    }
+    case 2: {
+      const double sq = gap_sqrt(val, b);
+      return ((b * b * b * yq - b * val * val * yq) * sq + a * val * val * val * xq) /
+             ((b * b * b - b * a * a - b * val * val + a * a * val * val / b) * sq + b * b * a * xq);
+    }
+    default: {
+      const double sq = gap_sqrt(val, b);
+      return ((-b * b * b * yq + b * val * val * yq) * sq + a * val * val * val * xq) /
+             ((-b * b * b + b * a * a + b * val * val - a * a * val * val / b) * sq + b * b * a * xq);
+    }
+  }
+}
+
+/* cylinder.h:594-614: epsilon 1e-7 for double, at most 100 iterations */
+static double newton_iteration(int branch, double a, double b, double xq, double yq, double x0) {
+  double val0 = x0, cnt = 0;
+  while ((fabs(distance_derivative(branch, a, b, xq, yq, val0)) >= 1e-7) && (cnt < 100)) {
+    const double val = single_newton_iteration(branch, a, b, xq, yq, val0);
+    val0 = val;
+    cnt++;
+    if (fabs(val0) == a) val0 += DBL_EPSILON;
+  }
+  return val0;
+}
+
+/* cylinder.h:622-673 (the distance of the returned pair) */
+static double min_distance_to_ellipse(double a, double b, double xq, double yq) {
+  const double percentage = 0.95;
+  if (((xq >= 0) && (yq >= (b / a) * xq)) || ((xq <= 0) && (yq >= (-b / a) * xq))) {
+    const double x0 = xq > 0 ? percentage * a : -percentage * a;
+    const double x_min = newton_iteration(0, a, b, xq, yq, x0);
+    const double sq = sqrt(a * a - x_min * x_min);
+    const double y_min = b / a * sq;
+    return sqrt((xq - x_min) * (xq - x_min) + (yq - y_min) * (yq - y_min));
+  }
+  if (((xq >= 0) && (yq <= (-b / a) * xq)) || ((xq <= 0) && (yq <= (b / a) * xq))) {
+    const double x0 = xq > 0 ? percentage * a : -percentage * a;
+    const double x_min = newton_iteration(1, a, b, xq, yq, x0);
+    const double sq = sqrt(a * a - x_min * x_min);
+    const double y_min = -b / a * sq;
+    return sqrt((xq - x_min) * (xq - x_min) + (yq - y_min) * (yq - y_min));
+  }
+  if ((xq >= 0) && (yq <= (b / a) * xq) && (yq >= (-b / a) * xq)) {
+    const double y0 = yq > 0 ? percentage * b : -percentage * b;
+    const double y_min = newton_iteration(2, a, b, xq, yq, y0);
+    const double sq = sqrt(b * b - y_min * y_min);
+    const double x_min = a / b * sq;
+    return sqrt((yq - y_min) * (yq - y_min) + (xq - x_min) * (xq - x_min));
+  }
+  {
+    const double y0 = yq > 0 ? percentage * b : -percentage * b;
+    const double y_min = newton_iteration(3, a, b, xq, yq, y0);
+    const double sq = sqrt(b * b - y_min * y_min);
+    const double x_min = -a / b * sq;
+    return sqrt((yq - y_min) * (yq - y_min) + (xq - x_min) * (xq - x_min));
+  }
+}
+
+/* cylinder.h:677-759 */
+static double cylinder_distance(const ora_scene *s, uint32_t id, v3 p) {
+  const double *R = s->cy_rot + 9 * id;
+  const v3 lp = mattvec(R, sub(p, ld(s->cy_c + 3 * id)));
+  const double h = s->cy_h[id];
+  const double dist_top = fabs(lp.e[2] - h / 2);
+  const double dist_bottom = fabs(lp.e[2] + h / 2);
+  const double x_q = lp.e[0], y_q = lp.e[1], z_q = lp.e[2];
+  const double a = s->cy_a[id], b = s->cy_b[id];
+  if (x_q == 0 && y_q == 0) {
+    if ((z_q > h / 2) || (z_q < -h / 2)) return std_min(dist_top, dist_bottom);
+    return std_min(std_min(std_min(a, b), dist_top), dist_bottom);
+  }
+  const double ellipse = ellipse_equation(a, b, x_q, y_q);
+  if (fabs(ellipse) < DBL_EPSILON) {
+    if ((z_q > h / 2) || (z_q < -h / 2)) return std_min(dist_top, dist_bottom);
+    return 0.0;
+  }
+  if (ellipse < 0) {
+    if (z_q >= h / 2) return dist_top;
+    if (z_q <= -h / 2) return dist_bottom;
+    return std_min(std_min(min_distance_to_ellipse(a, b, x_q, y_q), dist_bottom), dist_top);
+  }
+  if (ellipse > 0) {
+    const double shell = min_distance_to_ellipse(a, b, x_q, y_q);
+    if ((z_q < h / 2) && (z_q > -h / 2)) return shell;
+    return std_min(sqrt(shell * shell + dist_top * dist_top),
+                   sqrt(shell * shell + dist_bottom * dist_bottom));
+  }
+  return -1;
+}
+
+/* trimesh_distance.h:177-218 with r0..r6 (:37-163) */
+static v3 closest_point_on_triangle(v3 v0, v3 v1, v3 v2, v3 p) {
+  const v3 E0 = sub(v1, v0), E1 = sub(v2, v0), D = sub(v0, p);
+  const double a = dot(E0, E0), b = dot(E0, E1), c = dot(E1, E1);
+  const double d = dot(E0, D), e = dot(E1, D);
+  const double det = a * c - b * b;
+  double sv = b * e - c * d, tv = b * d - a * e;
+  if (sv + tv <= det) {
+    if (sv < 0) {
+      if (tv < 0) { /* r4 */
+        if (d < 0) {
+          tv = 0;
+          sv = (-d >= a) ? 1 : -d / a;
+        } else {
+          sv = 0;
+          tv = (e >= 0) ? 0 : ((-e >= c) ? 1 : -e / c);
+        }
+      } else { /* r3 */
+        sv = 0;
+        tv = (e >= 0) ? 0 : ((-e >= c) ? 1 : -e / c);
+      }
+    } else if (tv < 0) { /* r5 */
+      tv = 0;
+      sv = (d >= 0) ? 0 : ((-d >= a) ? 1 : -d / a);
+    } else { /* r0 */
+      const double inv_det = 1.0 / det;
+      sv *= inv_det;
+      tv *= inv_det;
+    }
+  } else if (sv < 0) { /* r2 */
+    const double tmp0 = b + d, tmp1 = c + e;
+    if (tmp1 > tmp0) {
+      const double numer = tmp1 - tmp0, denom = a - 2.0 * b + c;
+      sv = (numer >= denom) ? 1 : numer / denom;
+      tv = 1.0 - sv;
+    } else {
+      sv = 0;
+      tv = (tmp1 <= 0) ? 1 : ((e >= 0) ? 0 : -e / c);
+    }
+  } else if (tv < 0) { /* r6 */
+    const double tmp0 = b + e, tmp1 = a + d;
+    if (tmp1 > tmp0) {
+      const double numer = tmp1 - tmp0, denom = a - 2.0 * b + c;
+      tv = (numer >= denom) ? 1 : numer / denom;
+      sv = 1.0 - tv;
+    } else {
+      tv = 0;
+      sv = (tmp1 <= 0) ? 1 : ((d >= 0) ? 0 : -d / a);
+    }
+  } else { /* r1 */
+    const double numer = c + e - b - d;
+    if (numer <= 0) {
+      sv = 0;
+    } else {
+      const double denom = a - 2.0 * b + c;
+      sv = (numer >= denom) ? 1 : numer / denom;
+    }
+    tv = 1.0 - sv;
+  }
+  return add(add(v0, mul_sv(sv, E0)), mul_sv(tv, E1));
+}
+
+double ora_distance_one(const ora_scene *s, int kind, uint32_t id, const double point[3],
+                        double closest[3]) {
+  const v3 p = ld(point);
+  switch (kind) {
+    case 0: {
+      const uint32_t *F = s->faces + 3 * id;
+      const v3 c = closest_point_on_triangle(ld(s->verts + 3 * F[0]), ld(s->verts + 3 * F[1]),
+                                             ld(s->verts + 3 * F[2]), p);
+      if (closest) memcpy(closest, c.e, 24);
+      return norm(sub(c, p));
+    }
+    case 1: /* sphere.h:179-182 */
+      return fabs(norm(sub(ld(s->sph_c + 3 * id), p)) - s->sph_r[id]);
+    case 2: { /* plane.h:272-284 */
+      const v3 c = ld(s->pl_c + 3 * id);
+      const v3 lp = mattvec(s->pl_rot + 9 * id, sub(p, c));
+      const double dx = s->pl_dx[id] / 2, dy = s->pl_dy[id] / 2;
+      if ((lp.e[0] >= c.e[0] - dx) && (lp.e[0] <= c.e[0] + dx) && (lp.e[1] >= c.e[1] - dy) &&
+          (lp.e[1] <= c.e[1] + dy))
+        return fabs(lp.e[2]);
+      return DBL_MAX;
+    }
+    default:
+      return cylinder_distance(s, id, p);
+  }
+}
+
+void ora_distance_to_surface(const ora_scene *s, int kind, long n, const uint32_t *ids,
+                             const double *points, double *distance, double *closest) {
+  for (long i = 0; i < n; i++)
+    distance[i] = ora_distance_one(s, kind, ids[i], points + 3 * i,
+                                   closest ? closest + 3 * i : NULL);
+}
+
+/* The scene-level nearest surface by exhaustion: kinds in the order triangles, spheres, planes,
+ * cylinders, primitives by increasing id, the first strictly smaller distance kept. */
+void ora_closest_surface(const ora_scene *s, long n, const double *points, double *distance,
+                         uint32_t *prim, uint32_t *geom) {
+  for (long i = 0; i < n; i++) {
+    double best = INFINITY;
+    uint32_t bp = 0xFFFFFFFFu, bg = 0xFFFFFFFFu;
+    for (int kind = 0; kind < 4; kind++) {
+      if (!s->k[kind].present) continue;
+      for (long id = 0; id < s->k[kind].n; id++) {
+        const double d = ora_distance_one(s, kind, (uint32_t)id, points + 3 * i, NULL);
+        if (d < best) {
+          best = d;
+          bp = (uint32_t)id;
+          bg = s->k[kind].geom_id;
+        }
+      }
+    }
+    distance[i] = best;
+    if (prim) prim[i] = bp;
+    if (geom) geom[i] = bg;
+  }
+}

@@ -67,6 +67,21 @@ int ora_traverse_kind(const ora_scene *s, int kind, const double org[3], const d
                       double tmin, double tmax, double *t, double *uv, double *normal,
                       uint32_t *prim);
 
+/* distance_to_surface of primitive ids[i] of one kind for n points (blazert/primitives/
+ * sphere.h:179-182, plane.h:272-284, cylinder.h:677-759); triangles: closest_point_on_triangle
+ * (trimesh_distance.h:177-218) on the face's vertices, distance norm(closest - p), closest
+ * (n x 3 or NULL) receives the points. */
+void ora_distance_to_surface(const ora_scene *s, int kind, long n, const uint32_t *ids,
+                             const double *points, double *distance, double *closest);
+double ora_distance_one(const ora_scene *s, int kind, uint32_t id, const double point[3],
+                        double closest[3]);
+
+/* Nearest surface over the whole scene by exhaustion: kinds in the order triangles, spheres,
+ * planes, cylinders, primitives by increasing id, the first strictly smaller distance kept
+ * (+inf and 0xFFFFFFFF when none). */
+void ora_closest_surface(const ora_scene *s, long n, const double *points, double *distance,
+                         uint32_t *prim, uint32_t *geom);
+
 #ifdef __cplusplus
 }
 #endif

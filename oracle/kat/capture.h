@@ -4,8 +4,9 @@
 // compiles.  It includes the reference headers and the reference's assert helpers
 // (test/test_primitives/assert_helper.h) first and then declares explicit specialisations of
 // those helpers for T = double.  Each specialisation
-//   * records the collection, the ray and the values the test asserts (expected hit, prim id,
-//     distance, normal, box, centre) as one JSON line, and
+//   * records the collection, the ray (or query point) and the values the test asserts
+//     (expected hit, prim id, distance, normal, box, centre, distance to surface) as one JSON
+//     line, and
 //   * evaluates the reference exactly as the helper does -- prepare_traversal +
 //     intersect_primitive + post_traversal on primitive 0, or SAHBinnedBuilder + traverse --
 //     and records those outputs too, then runs the helper's CHECKs.
@@ -233,6 +234,18 @@ struct Node {
   blazert::Vec3r<double> min, max;
 };
 
+// assert_distance_to_surface (test/test_primitives/assert_helper.h:102-106): the reference's
+// distance_to_surface of one primitive and the test's expected value.
+template <template <typename> class Coll>
+void distance(const Coll<double> &collection, unsigned prim_id, const blazert::Vec3r<double> &p,
+              double true_distance) {
+  const double got = distance_to_surface(primitive_from_collection(collection, prim_id), p);
+  emit("distance_to_surface", geometry(collection) + ",\"prim_id\":" + std::to_string(prim_id) +
+                                  ",\"point\":" + vec(p, 3) + ",\"expected\":" +
+                                  num(true_distance) + ",\"reference\":" + num(got));
+  CHECK(got == doctest::Approx(true_distance));
+}
+
 }  // namespace kat
 
 #define KAT_SPECIALISE(COLL)                                                                      \
@@ -283,6 +296,20 @@ KAT_SPECIALISE(SphereCollection)
 KAT_SPECIALISE(PlaneCollection)
 KAT_SPECIALISE(CylinderCollection)
 #undef KAT_SPECIALISE
+
+// The reference's tests assert distances for spheres, planes and cylinders (its triangle
+// distance_to_surface cannot be instantiated, and no test calls it).
+#define KAT_SPECIALISE_DISTANCE(COLL)                                                             \
+  template <>                                                                                     \
+  inline void assert_distance_to_surface<double, blazert::COLL>(                                  \
+      const blazert::COLL<double> &c, const unsigned int p, const blazert::Vec3r<double> &pt,   \
+      const double d) {                                                                           \
+    kat::distance<blazert::COLL>(c, p, pt, d);                                                    \
+  }
+KAT_SPECIALISE_DISTANCE(SphereCollection)
+KAT_SPECIALISE_DISTANCE(PlaneCollection)
+KAT_SPECIALISE_DISTANCE(CylinderCollection)
+#undef KAT_SPECIALISE_DISTANCE
 
 // test/test_bvh/test_intersect.cpp tests intersect_node on BVHNode<T, PlaneCollection>.
 template <>

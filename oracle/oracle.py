@@ -134,6 +134,36 @@ class _Base:
                     prim_cnt=cnt, prim_ids=prims[:total])
 
 
+_DIST_ARGS = [C.c_void_p, C.c_int, C.c_long, _u32p, _dp, _dp, _dp]
+_NEAREST_ARGS = [C.c_void_p, C.c_long, _dp, _dp, _u32p, _u32p]
+
+
+def _distance_to_surface(obj, kind, ids, points):
+    ids = np.ascontiguousarray(ids, np.uint32).reshape(-1)
+    pts = _f64(points).reshape(-1, 3)
+    n = pts.shape[0]
+    if ids.shape[0] != n:
+        raise ValueError("one primitive id per point")
+    dist = np.empty(n)
+    closest = np.full((n, 3), np.nan)
+    getattr(obj._lib, obj._prefix + "distance_to_surface")(
+        obj._h, KINDS.index(kind), n, _ptr(ids, _u32p), _ptr(pts, _dp), _ptr(dist, _dp),
+        _ptr(closest, _dp) if kind == "mesh" else None)
+    return (dist, closest) if kind == "mesh" else (dist, None)
+
+
+def _closest_surface(obj, points):
+    pts = _f64(points).reshape(-1, 3)
+    n = pts.shape[0]
+    dist = np.empty(n)
+    prim = np.empty(n, np.uint32)
+    geom = np.empty(n, np.uint32)
+    getattr(obj._lib, obj._prefix + "closest_surface")(obj._h, n, _ptr(pts, _dp),
+                                                       _ptr(dist, _dp), _ptr(prim, _u32p),
+                                                       _ptr(geom, _u32p))
+    return dict(distance=dist, prim=prim, geom=geom)
+
+
 def _outputs(n):
     return dict(t=np.empty(n), uv=np.empty((n, 2)), normal=np.empty((n, 3)),
                 prim=np.empty(n, np.uint32), geom=np.empty(n, np.uint32),
@@ -179,6 +209,8 @@ class Oracle(_Base):
             lib.ora_traverse_kind.restype = C.c_int
             lib.ora_traverse_kind.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_double,
                                               C.c_double, _dp, _dp, _dp, _u32p]
+            lib.ora_distance_to_surface.argtypes = _DIST_ARGS
+            lib.ora_closest_surface.argtypes = _NEAREST_ARGS
             cls._lib = lib
         return cls._lib
 
@@ -218,6 +250,14 @@ class Oracle(_Base):
                                         tmin, tmax, _ptr(t, _dp), _ptr(uv, _dp), _ptr(nrm, _dp),
                                         _ptr(prim, _u32p))
         return dict(hit=bool(h), t=float(t[0]), uv=uv, normal=nrm, prim=int(prim[0]))
+
+    def distance_to_surface(self, kind, ids, points):
+        """(distances, closest points for meshes else None) of primitive ids[i] and point i."""
+        return _distance_to_surface(self, kind, ids, points)
+
+    def closest_surface(self, points):
+        """Nearest surface over the whole scene, by exhaustion."""
+        return _closest_surface(self, points)
 
     @classmethod
     def intersect_node(cls, tmin, tmax, bmin, bmax, org, raw_dir):
@@ -262,9 +302,15 @@ class RefScene(_Base):
             lib.ref_scene_traverse_kind.restype = C.c_double
             lib.ref_scene_traverse_kind.argtypes = [C.c_void_p, C.c_int, C.c_long, _dp, _dp, _dp,
                                                     _u32p, _u8p, C.c_int]
+            if hasattr(lib, "ref_distance_to_surface"):
+                lib.ref_distance_to_surface.argtypes = _DIST_ARGS
             RefScene._libs[flavour] = lib
         self._lib = RefScene._libs[flavour]
         super().__init__(spec, **kw)
+
+    def distance_to_surface(self, kind, ids, points):
+        """The reference's own distance_to_surface (closest_point_on_triangle for meshes)."""
+        return _distance_to_surface(self, kind, ids, points)
 
     @property
     def commit_seconds(self):

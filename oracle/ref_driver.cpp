@@ -239,6 +239,43 @@ long ref_scene_tree(void *h, int kind, double *bmin, double *bmax, uint32_t *lea
   return -1;
 }
 
+// The reference's own per-primitive distance_to_surface (blazert/primitives/sphere.h:179-182,
+// plane.h:272-284, cylinder.h:677-759) on primitive ids[i] of one kind for n points.  For
+// triangles, whose distance_to_surface (trimesh.h:183-192) cannot be instantiated, the
+// reference's closest_point_on_triangle (trimesh_distance.h:177-218) on the face's vertices,
+// norm(closest - p) as the distance and the point in closest (n x 3, may be NULL).
+void ref_distance_to_surface(void *h, int kind, long n, const uint32_t *ids, const double *points,
+                             double *distance, double *closest) {
+  const RefScene *s = static_cast<RefScene *>(h);
+  for (long i = 0; i < n; ++i) {
+    const Vec3r<double> p = v3(points + 3 * i);
+    const unsigned id = ids[i];
+    switch (kind) {
+      case 0: {
+        const Vec3ui &f = s->faces[id];
+        const Vec3r<double> c =
+            closest_point_on_triangle(s->verts[f[0]], s->verts[f[1]], s->verts[f[2]], p);
+        distance[i] = norm(c - p);
+        if (closest)
+          for (int k = 0; k < 3; ++k) closest[3 * i + k] = c[k];
+        break;
+      }
+      case 1:
+        distance[i] = distance_to_surface(
+            primitive_from_collection(bvh_of<SphereCollection>(s)->collection, id), p);
+        break;
+      case 2:
+        distance[i] = distance_to_surface(
+            primitive_from_collection(bvh_of<PlaneCollection>(s)->collection, id), p);
+        break;
+      case 3:
+        distance[i] = distance_to_surface(
+            primitive_from_collection(bvh_of<CylinderCollection>(s)->collection, id), p);
+        break;
+    }
+  }
+}
+
 // Traversal of ONE per-type BVH (blazert/bvh/accel.h:60-120) for n rays, as the reference's
 // benchmarks time it (benchmarks/benchmark_BVH/realistic/benchmark_BVH_traverse.cpp:33-60).
 double ref_scene_traverse_kind(void *h, int kind, long n, const double *org, const double *dir,

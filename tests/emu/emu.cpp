@@ -10,6 +10,7 @@
 #include "../../blazert_b200/csrc/layout.h"
 #include "../../blazert_b200/csrc/scene.h"
 #include "../../blazert_b200/csrc/trace_core.cuh"
+#include "../../blazert_b200/csrc/distance_core.cuh"
 
 namespace {
 struct Emu {
@@ -63,6 +64,7 @@ void *emu_scene_create(const int *order, int n_order, const double *verts, long 
     v.nodes32 = im.nodes32.data();
     v.payload = im.payload.data();
     v.prim_ids = im.prim_ids.data();
+    v.pos_of = im.pos_of.data();
     v.tri = im.tri.data();
     v.verts = im.verts.data();
     v.n_internal = im.n_internal;
@@ -195,6 +197,41 @@ int emu_box_accept(const double *bmin, const double *bmax, const double *org, co
   const bool p = bzr::box_test(make_double2(bmin[0], bmax[0]), make_double2(bmin[1], bmax[1]),
                                make_double2(bmin[2], bmax[2]), r, key);
   return (p && !(key > tmax)) ? 1 : 0;
+}
+
+// The distance kernels' per-point code (distance_core.cuh): per-primitive form and the
+// scene-level nearest surface with its BVH pruning.  Returns the error bits.
+uint32_t emu_distance_to_surface(void *h, int kind, long n, const uint32_t *ids,
+                                 const double *points, double *distance, double *closest) {
+  const Emu *e = static_cast<Emu *>(h);
+  uint32_t err = 0;
+  for (long i = 0; i < n; ++i) {
+    bzr::D3 c;
+    bool bad = false;
+    const bzr::D3 p = bzr::d3(points[3 * i], points[3 * i + 1], points[3 * i + 2]);
+    distance[i] = bzr::distance_query(e->view, kind, ids[i], p, &c, &bad);
+    if (closest) {
+      closest[3 * i] = c.x;
+      closest[3 * i + 1] = c.y;
+      closest[3 * i + 2] = c.z;
+    }
+    if (bad) err |= bzr::kErrPrimIndex;
+  }
+  return err;
+}
+
+void emu_closest_surface(void *h, long n, const double *points, double *distance, uint32_t *prim,
+                         uint32_t *geom) {
+  const Emu *e = static_cast<Emu *>(h);
+  uint32_t stack_ref[64];
+  double stack_key[64];
+  for (long i = 0; i < n; ++i) {
+    const bzr::D3 p = bzr::d3(points[3 * i], points[3 * i + 1], points[3 * i + 2]);
+    const bzr::NearestState st = bzr::nearest_surface(e->view, p, stack_ref, stack_key, 64);
+    distance[i] = st.best;
+    if (prim) prim[i] = st.prim;
+    if (geom) geom[i] = st.geom;
+  }
 }
 
 }  // extern "C"

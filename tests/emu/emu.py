@@ -7,7 +7,9 @@ import subprocess
 
 import numpy as np
 
-from oracle.oracle import _Base, _CREATE_ARGS, _TREE_ARGS, _dp, _outputs, _ptr, _rays, _u32p, _u8p
+from oracle.oracle import (_Base, _CREATE_ARGS, _DIST_ARGS, _NEAREST_ARGS, _TREE_ARGS,
+                           _closest_surface, _distance_to_surface, _dp, _outputs, _ptr, _rays,
+                           _u32p, _u8p)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libbzr_emu.so")
@@ -20,7 +22,7 @@ def build(force=False):
     root = os.path.dirname(os.path.dirname(HERE))
     srcs = [os.path.join(HERE, "emu.cpp"), os.path.join(root, "blazert_b200", "csrc", "scene.cpp")]
     deps = srcs + [os.path.join(root, "blazert_b200", "csrc", f)
-                   for f in ("layout.h", "scene.h", "trace_core.cuh")]
+                   for f in ("layout.h", "scene.h", "trace_core.cuh", "distance_core.cuh")]
     if not force and os.path.exists(LIB) and all(os.path.getmtime(d) <= os.path.getmtime(LIB) for d in deps):
         return LIB
     cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
@@ -43,6 +45,9 @@ def load():
                                             _dp, _u32p, _u32p, _u8p, C.c_uint32, C.c_int]
         lib.emu_prim_box.argtypes = [C.c_void_p, C.c_int, C.c_uint32, _dp, _dp, _dp]
         lib.emu_box_accept.argtypes = [_dp, _dp, _dp, _dp, C.c_double, C.c_double]
+        lib.emu_distance_to_surface.restype = C.c_uint32
+        lib.emu_distance_to_surface.argtypes = _DIST_ARGS
+        lib.emu_closest_surface.argtypes = _NEAREST_ARGS
         _lib = lib
     return _lib
 
@@ -67,6 +72,14 @@ class EmuScene(_Base):
                                     _ptr(mx, _dp), _ptr(c, _dp))
         assert rc == 0
         return mn, mx, c
+
+    def distance_to_surface(self, kind, ids, points):
+        """The distance kernel's per-point code on the CPU."""
+        return _distance_to_surface(self, kind, ids, points)
+
+    def closest_surface(self, points):
+        """The nearest-surface kernel's per-point code (BVH pruning included) on the CPU."""
+        return _closest_surface(self, points)
 
     def intersect(self, org, dirs, tmin=None, tmax=None, stack_cap=0, mode="fp64", any_hit=False):
         """mode fp64 | mixed; any_hit: every ray with Ray::AnyHit::yes."""

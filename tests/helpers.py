@@ -72,9 +72,12 @@ def kat_spec(rec):
         s.add_planes(np.array(rec["centers"], float), np.array(rec["dxs"], float),
                      np.array(rec["dys"], float), np.array(rec["rotations"], float).reshape(-1, 3, 3))
     else:
-        s.add_cylinders(np.array(rec["centers"], float), np.array(rec["semi_axes_a"], float),
-                        np.array(rec["semi_axes_b"], float), np.array(rec["heights"], float),
-                        np.array(rec["rotations"], float).reshape(-1, 3, 3))
+        # a few cylinder tests push a rotation more than they push cylinders; the collection
+        # reads rotations[prim_id], so the first len(centers) entries are the ones in use
+        n = len(rec["centers"])
+        s.add_cylinders(np.array(rec["centers"], float), np.array(rec["semi_axes_a"], float)[:n],
+                        np.array(rec["semi_axes_b"], float)[:n], np.array(rec["heights"], float)[:n],
+                        np.array(rec["rotations"], float).reshape(-1, 3, 3)[:n])
     return s
 
 
