@@ -20,6 +20,11 @@ isotropic directions), float64, seeded.  A step is one intersectN over the whole
   cpu_baseline  the reference's own intersect1 loop (its headers, release flags, OpenMP over
              all host cores) on the same rays, rank 0 at N = 1.
 
+Other forms: --workload heightfield | icosphere_pinhole (same line), batched_icospheres
+(batching), adjoint_scene (differentiation), distance_queries (the reference's per-primitive
+distance_to_surface over 4M (primitive, point) pairs per kind, Mqueries/s) and closest_surface
+(nearest surface over the scene for 1M points, Mqueries/s).
+
 Multi-GPU: one process per GPU (torchrun); every rank holds the scene and traces its own batch
 (weak scaling, no data-path collective); the time is the max over ranks.
 """
@@ -163,8 +168,30 @@ def run_reference(args):
         return 0
     from blazert_b200 import workloads as W
     from oracle.oracle import Oracle, RefScene
-    wl = W.WORKLOADS[args.workload](**({"n_rays": args.rays} if args.rays else {}))
     threads = os.cpu_count() or 1
+    if args.workload in W.DISTANCE_WORKLOADS:
+        # the reference's distance functions on every host core; steps of the closest-surface
+        # workload are bounded samples (the reference has no scene-level query: every point
+        # is checked against every primitive)
+        from oracle.cpu_baseline import measure_distance
+        m = measure_distance(args.workload, seconds=0.0, threads=threads,
+                             max_queries=0 if args.workload == "distance_queries" else 2048,
+                             min_reps=args.warmup + args.steps)
+        print(json.dumps({
+            "metric": ("Mqueries/s distance_to_surface (per-primitive, bit-exact) on 1 B200"
+                       if args.workload == "distance_queries" else
+                       "Mqueries/s nearest surface over the scene (bit-exact) on 1 B200"),
+            "value": m["value"], "unit": "Mqueries/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * m["seconds_per_batch"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": args.workload,
+                                                     "queries_per_step": m["queries"]},
+            "impl": "reference",
+            "cpu_baseline": {k: m[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": m["value"], "unit": "Mqueries/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
+    wl = W.WORKLOADS[args.workload](**({"n_rays": args.rays} if args.rays else {}))
     kind = "reference" if RefScene.available("bench") else "port"
     sc = RefScene(wl.scene, flavour="bench") if kind == "reference" else Oracle(wl.scene)
     R = wl.rays
@@ -596,6 +623,185 @@ def run_adjoint(args):
     return 0
 
 
+DIST_RECORD_BYTES = {"mesh": 16 + 3 * 24, "spheres": 32, "planes": 112, "cylinders": 128}
+
+
+def run_distance(args):
+    """Distance form.  distance_queries: one step = bzr_distance_to_surface over 4,194,304
+    (primitive, point) pairs of each kind of the mixed-primitive scene (one launch per kind).
+    closest_surface: one step = bzr_closest_surface over 1,048,576 points in the box of the
+    differentiation scene (91,920 triangles, 500 spheres).  Mqueries/s, device time, the L2
+    flushed between steps; e2e through Scene.distance_to_surface / closest_surface with pinned
+    host arrays."""
+    import numpy as np
+    import torch
+
+    import blazert_b200 as B
+    from blazert_b200 import multi
+    from blazert_b200 import workloads as W
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    wl = W.DISTANCE_WORKLOADS[args.workload]()
+    spec = wl.scene
+    scene = B.Scene()
+    for kind in spec.order:
+        getattr(scene, "add_" + kind)(*getattr(spec, kind).values())
+    scene.commit()
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    per_query = 24 + 8  # point in, distance out
+    if args.workload == "distance_queries":
+        qs = {}
+        for k, (ids, pts) in wl.meta["queries"].items():
+            if rank > 0:  # weak scaling: each rank its own rotation of the queries
+                sh = (rank * 7919) % len(ids)
+                ids, pts = np.roll(ids, sh), np.roll(pts, sh, 0)
+            qs[k] = (torch.from_numpy(ids.astype(np.int32)).to(dev), torch.from_numpy(pts).to(dev))
+        n = sum(int(i.shape[0]) for i, _ in qs.values())
+        outs = {k: torch.empty(i.shape[0], dtype=torch.float64, device=dev)
+                for k, (i, _) in qs.items()}
+        lib = scene._lib
+
+        def launch(k, ev=None):
+            ids, pts = qs[k]
+            B._check(lib.bzr_distance_to_surface(scene._h, B.KIND_NAMES.index(k), ids.shape[0],
+                                                 ids.data_ptr(), pts.data_ptr(),
+                                                 outs[k].data_ptr(), None,
+                                                 B.C.c_void_p(stream.cuda_stream)))
+
+        kinds = list(qs)
+        launches = len(kinds)
+        alg = {k: int(qs[k][0].shape[0]) * (4 + 4 + per_query + DIST_RECORD_BYTES[k]) for k in kinds}
+    else:
+        pts_np = wl.meta["points"]
+        if rank > 0:
+            pts_np = np.roll(pts_np, (rank * 7919) % len(pts_np), 0)
+        pts = torch.from_numpy(pts_np).to(dev)
+        n = int(pts.shape[0])
+        out = dict(distance=torch.empty(n, dtype=torch.float64, device=dev),
+                   prim=torch.empty(n, dtype=torch.int32, device=dev),
+                   geom=torch.empty(n, dtype=torch.int32, device=dev))
+        lib = scene._lib
+
+        def launch(k, ev=None):
+            B._check(lib.bzr_closest_surface(scene._h, n, pts.data_ptr(),
+                                             out["distance"].data_ptr(), out["prim"].data_ptr(),
+                                             out["geom"].data_ptr(),
+                                             B.C.c_void_p(stream.cuda_stream)))
+
+        kinds = ["scene"]
+        launches = 1
+        alg = {"scene": n * (per_query + 8)}
+
+    def step(evs=None):
+        for j, k in enumerate(kinds):
+            if evs is not None:
+                evs[j].record(stream)
+            launch(k)
+        if evs is not None:
+            evs[-1].record(stream)
+
+    for i in range(args.warmup):
+        flush.fill_(i & 0xFF)
+        step()
+    torch.cuda.synchronize(dev)
+    scene.check()
+    if pg:
+        pg.barrier()
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(len(kinds) + 1)]
+           for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.fill_((i + 1) & 0xFF)
+        step(evs[i])
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop() if sampler else None
+    scene.check()
+    per_kind_ms = {k: sum(e[j].elapsed_time(e[j + 1]) for e in evs) / args.steps
+                   for j, k in enumerate(kinds)}
+    total_ms = sum(per_kind_ms.values()) * args.steps
+    if pg:
+        total_ms = multi.max_over_ranks(total_ms)
+    value = world * n * args.steps / (total_ms / 1e3) / 1e6
+    top = max(per_kind_ms, key=per_kind_ms.get)
+    achieved = alg[top] / (per_kind_ms[top] / 1e3) / 1e9
+    peak, peak_src = load_peaks()
+
+    e2e = None
+    if not args.no_e2e:
+        if args.workload == "distance_queries":
+            host = {k: (torch.from_numpy(ids.cpu().numpy().view(np.uint32)).pin_memory(),
+                        torch.from_numpy(p.cpu().numpy()).pin_memory()) for k, (ids, p) in qs.items()}
+            hout = {k: torch.empty(i.shape[0], dtype=torch.float64).pin_memory() for k, (i, _) in host.items()}
+
+            def e2e_step():
+                for k, (ids, p) in host.items():
+                    B._check(lib.bzr_distance_to_surface(
+                        scene._h, B.KIND_NAMES.index(k), ids.shape[0], ids.data_ptr(),
+                        p.data_ptr(), hout[k].data_ptr(), None, None))
+            h2d, d2h = n * 28, n * 8
+        else:
+            hp = torch.from_numpy(pts.cpu().numpy()).pin_memory()
+            hd = torch.empty(n, dtype=torch.float64).pin_memory()
+            hpr = torch.empty(n, dtype=torch.int32).pin_memory()
+            hg = torch.empty(n, dtype=torch.int32).pin_memory()
+
+            def e2e_step():
+                B._check(lib.bzr_closest_surface(scene._h, n, hp.data_ptr(), hd.data_ptr(),
+                                                 hpr.data_ptr(), hg.data_ptr(), None))
+            h2d, d2h = n * 24, n * 16
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        el = time.perf_counter() - t0
+        if pg:
+            el = multi.max_over_ranks(el)
+        e2e = {"value": world * n * args.steps / el / 1e6, "unit": "Mqueries/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.workload, args.cpu_seconds)
+        if "value" in cpu:
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        cfg = {"workload": args.workload, "queries_per_gpu": n,
+               "scene": {k: len(next(iter(getattr(spec, k).values()))) for k in spec.order},
+               "parallelism": f"replicated-scene x{world}",
+               "l2": "flushed between timed steps (256 MiB write)"}
+        print(json.dumps({
+            "metric": ("Mqueries/s distance_to_surface (per-primitive, bit-exact) on 1 B200"
+                       if args.workload == "distance_queries" else
+                       "Mqueries/s nearest surface over the scene (bit-exact) on 1 B200"),
+            "value": value, "unit": "Mqueries/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": cfg,
+            "ms_per_kind": per_kind_ms, "e2e": e2e, "gpu_launches": args.steps * launches,
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": peak_src},
+            "cpu_baseline": cpu, "clocks": clocks}), flush=True)
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
 def main(argv=None):
     args = parse(argv)
     if args.impl == "reference":
@@ -604,6 +810,8 @@ def main(argv=None):
         return run_batched(args)
     if args.workload == "adjoint_scene":
         return run_adjoint(args)
+    if args.workload in ("distance_queries", "closest_surface"):
+        return run_distance(args)
     return run_ours(args)
 
 

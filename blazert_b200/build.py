@@ -30,7 +30,7 @@ CU_FLAGS = ARCH + ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler
 SOURCES = [("scene.cpp", "cxx"), ("capi.cpp", "cxx"), ("trace.cu", "cu"), ("adjoint.cu", "cu"),
            ("noalloc.cu", "cu"), ("batch.cpp", "cxx"), ("gbuild.cu", "cu"), ("distance.cu", "cu")]
 HEADERS = ["layout.h", "scene.h", "trace.h", "trace_core.cuh", "adjoint.h", "capi_internal.h",
-           "distance.h", "distance_core.cuh"]
+           "distance.h", "distance_core.cuh", "bucket_sort.cuh"]
 
 
 def _cuda_home():

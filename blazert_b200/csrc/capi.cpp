@@ -723,7 +723,7 @@ static int run_distance(const bzr_scene *cs, int kind, size_t n, const uint32_t 
   io.error_word = s->slots + kStickyWord;
   auto launch = [&]() {
     return kind >= 0 ? bzr::launch_distance(s->view, kind, io, s->plan.sms, st)
-                     : bzr::launch_nearest(s->view, io, s->plan.sms, st);
+                     : bzr::launch_nearest(s->view, io, s->plan.sms, s->plan.pool, st);
   };
   if (n_dev == n_given) {
     io.ids = ids; io.points = points; io.distance = distance; io.closest = closest;

@@ -52,130 +52,189 @@ BZR_HD double plane_distance(D3 c, double dxs, double dys, const double *R, D3 p
   return kDblMax;
 }
 
-// The four branches of the ellipse search (cylinder.h:512-599).  UPPER/LOWER half plane,
-// iterating over X or Y.
-enum EllipseBranch : int { kUpperX = 0, kLowerX = 1, kUpperY = 2, kLowerY = 3 };
+// The ellipse search (cylinder.h:498-673).  The reference has four branches -- the point's
+// sector selects the upper or lower half plane and whether the iteration runs over x or y --
+// each with its own derivative (distance_derivative, :516-547) and Newton step
+// (single_newton_iteration, :551-590).  All four are the same expressions under a renaming,
+// and are evaluated here by ONE loop so that the lanes of a warp in different sectors iterate
+// together:
+//   A, B   the semi-axis of the iterated coordinate and the other one (a, b over x; b, a over y)
+//   X, Y   the point's iterated coordinate and the other one
+//   sg     +1 upper / -1 lower: the sign of the A^3 terms of the step and of the final other
+//          coordinate (-b / a * sqrt in the lower branches)
+//   tg     the sign of Y in the derivative's bracket: (B / A * s - tg * Y) -- +1 for upper-x
+//          and lower-y, -1 for lower-x and upper-y
+// Each operation is the reference's with a sign applied exactly where its expression has one
+// (x - (-y) and x + y, (-a) * a and -(a * a) are the same bits), so every branch's values are
+// reproduced bit for bit.
 
 // sqrt(|val^2 - s^2|) as the reference forms it: the larger square first
 BZR_HD double root_gap(double val, double s) {
   return (val * val > s * s) ? sqrt(val * val - s * s) : sqrt(s * s - val * val);
 }
 
-// distance_derivative (cylinder.h:516-547): R'(val)
-template <int BR>
-BZR_HD double ellipse_derivative(double a, double b, double xq, double yq, double val) {
-  if (BR == kUpperX) {
-    const double s = root_gap(val, a);
-    return -2 * (xq - val) - 2 * b * val * (b / a * s - yq) / (a * s);
-  } else if (BR == kLowerX) {
-    const double s = root_gap(val, a);
-    return -2 * (xq - val) - 2 * b * val * (b / a * s + yq) / (a * s);
-  } else if (BR == kUpperY) {
-    const double s = root_gap(val, b);
-    return -2 * (yq - val) - 2 * a * val * (a / b * s + xq) / (b * s);
-  } else {
-    const double s = root_gap(val, b);
-    return -2 * (yq - val) - 2 * a * val * (a / b * s - xq) / (b * s);
-  }
+struct EllipseBranch {
+  double A, B, X, Y, sg, tg;
+};
+
+// The search's loop-invariant sub-expressions, each formed exactly as the reference's
+// expression forms it (left to right), so that using them gives the same bits.
+struct EllipseSearch {
+  EllipseBranch e;
+  double BA = 0.0;    // B / A
+  double B2 = 0.0;    // 2 * B
+  double A3X = 0.0;   // (+-A) * A * A * X
+  double D0 = 0.0;    // (+-A) * A * A -+ A * B * B
+  double BB = 0.0;    // B * B
+  double AABY = 0.0;  // A * A * B * Y
+};
+
+BZR_HD EllipseSearch ellipse_search(const EllipseBranch &e) {
+  EllipseSearch S;
+  S.e = e;
+  S.BA = e.B / e.A;
+  S.B2 = 2 * e.B;
+  S.A3X = (e.sg * e.A) * e.A * e.A * e.X;
+  S.D0 = (e.sg * e.A) * e.A * e.A - e.sg * (e.A * e.B * e.B);
+  S.BB = e.B * e.B;
+  S.AABY = e.A * e.A * e.B * e.Y;
+  return S;
 }
 
-// single_newton_iteration (cylinder.h:551-590): val - R'(val) / R''(val) in closed form
-template <int BR>
-BZR_HD double ellipse_newton_step(double a, double b, double xq, double yq, double val) {
-  if (BR == kUpperX) {
-    const double s = root_gap(val, a);
-    return ((a * a * a * xq - a * val * val * xq) * s + b * val * val * val * yq) /
-           ((a * a * a - a * b * b - a * val * val + b * b * val * val / a) * s + a * a * b * yq);
-  } else if (BR == kLowerX) {
-    const double s = root_gap(val, a);
-    return ((-a * a * a * xq + a * val * val * xq) * s + b * val * val * val * yq) /
-           ((-a * a * a + a * b * b + a * val * val - b * b * val * val / a) * s + a * a * b * yq);
-  } else if (BR == kUpperY) {
-    const double s = root_gap(val, b);
-    return ((b * b * b * yq - b * val * val * yq) * s + a * val * val * val * xq) /
-           ((b * b * b - b * a * a - b * val * val + a * a * val * val / b) * s + b * b * a * xq);
-  } else {
-    const double s = root_gap(val, b);
-    return ((-b * b * b * yq + b * val * val * yq) * s + a * val * val * val * xq) /
-           ((-b * b * b + b * a * a + b * val * val - a * a * val * val / b) * s + b * b * a * xq);
-  }
+// One pass of newton_iteration's loop (cylinder.h:594-614): the condition -- at most 100
+// steps while |R'(v)| >= 1e-7, R' being distance_derivative (:516-547),
+//   -2 * (X - v) - 2 * B * v * (B / A * s -+ Y) / (A * s)
+// -- and, when it holds, the step single_newton_iteration (:551-590),
+//   v <- ((+-A A A X -+ A v v X) s + B v v v Y) / ((+-A A A -+ A B B -+ A v v +- B B v v / A) s
+//         + A A B Y),
+// then the nudge of a value that lands on |v| == a (the cylinder's a in every branch, as the
+// reference).  The derivative and the step take the same s = sqrt(|v^2 - A^2|), computed once.
+// Returns false when the loop ends (v is then final).
+BZR_HD bool ellipse_search_step(const EllipseSearch &S, double a, double &v, int &steps) {
+  const EllipseBranch &e = S.e;
+  const double s = root_gap(v, e.A);
+  const double d = -2 * (e.X - v) - S.B2 * v * (S.BA * s - e.tg * e.Y) / (e.A * s);
+  if (!((fabs(d) >= 1e-7) && (steps < 100))) return false;
+  const double num = (S.A3X - e.sg * (e.A * v * v * e.X)) * s + e.B * v * v * v * e.Y;
+  const double den = (S.D0 - e.sg * (e.A * v * v) + e.sg * (S.BB * v * v / e.A)) * s + S.AABY;
+  v = num / den;
+  ++steps;
+  if (fabs(v) == a) v += kDblEps;
+  return true;
 }
 
-// newton_iteration (cylinder.h:594-614): at most 100 steps while |R'| >= 1e-7; a value that
-// lands on |val| == a is nudged by one epsilon (against a in every branch, as the reference).
-template <int BR>
-BZR_HD double ellipse_newton(double a, double b, double xq, double yq, double val0) {
-  double cnt = 0;
-  while ((fabs(ellipse_derivative<BR>(a, b, xq, yq, val0)) >= 1e-7) && (cnt < 100)) {
-    const double val = ellipse_newton_step<BR>(a, b, xq, yq, val0);
-    val0 = val;
-    cnt++;
-    if (fabs(val0) == a) val0 += kDblEps;
-  }
-  return val0;
+// The sector test of find_minimum_distance_to_ellipse (cylinder.h:622-673) as branch
+// parameters.
+BZR_HD EllipseBranch ellipse_branch(double a, double b, double xq, double yq) {
+  if (((xq >= 0) && (yq >= (b / a) * xq)) || ((xq <= 0) && (yq >= (-b / a) * xq)))
+    return {a, b, xq, yq, 1.0, 1.0};    // upper half, over x
+  if (((xq >= 0) && (yq <= (-b / a) * xq)) || ((xq <= 0) && (yq <= (b / a) * xq)))
+    return {a, b, xq, yq, -1.0, -1.0};  // lower half, over x
+  if ((xq >= 0) && (yq <= (b / a) * xq) && (yq >= (-b / a) * xq))
+    return {b, a, yq, xq, 1.0, -1.0};   // right sector, over y
+  return {b, a, yq, xq, -1.0, 1.0};     // left sector, over y
 }
 
-// find_minimum_distance_to_ellipse (cylinder.h:622-673): the shortest distance from (xq, yq)
-// to the ellipse x^2/a^2 + y^2/b^2 = 1, by the branch the point's sector selects.
+// find_minimum_distance_to_ellipse after its search: the other coordinate
+// +-(B / A) sqrt(A^2 - v^2) and the distance from the point.
+BZR_HD double ellipse_finish(const EllipseBranch &e, double v) {
+  const double s = sqrt(e.A * e.A - v * v);
+  const double w = (e.sg * e.B) / e.A * s;
+  return sqrt((e.X - v) * (e.X - v) + (e.Y - w) * (e.Y - w));
+}
+
+// find_minimum_distance_to_ellipse: the start at +-0.95 A, the search, the finish.
 BZR_HD double ellipse_distance(double a, double b, double xq, double yq) {
+  const EllipseSearch S = ellipse_search(ellipse_branch(a, b, xq, yq));
   const double percentage = 0.95;
-  if (((xq >= 0) && (yq >= (b / a) * xq)) || ((xq <= 0) && (yq >= (-b / a) * xq))) {
-    const double x0 = xq > 0 ? percentage * a : -percentage * a;
-    const double x_min = ellipse_newton<kUpperX>(a, b, xq, yq, x0);
-    const double s = sqrt(a * a - x_min * x_min);
-    const double y_min = b / a * s;
-    return sqrt((xq - x_min) * (xq - x_min) + (yq - y_min) * (yq - y_min));
-  } else if (((xq >= 0) && (yq <= (-b / a) * xq)) || ((xq <= 0) && (yq <= (b / a) * xq))) {
-    const double x0 = xq > 0 ? percentage * a : -percentage * a;
-    const double x_min = ellipse_newton<kLowerX>(a, b, xq, yq, x0);
-    const double s = sqrt(a * a - x_min * x_min);
-    const double y_min = -b / a * s;
-    return sqrt((xq - x_min) * (xq - x_min) + (yq - y_min) * (yq - y_min));
-  } else if ((xq >= 0) && (yq <= (b / a) * xq) && (yq >= (-b / a) * xq)) {
-    const double y0 = yq > 0 ? percentage * b : -percentage * b;
-    const double y_min = ellipse_newton<kUpperY>(a, b, xq, yq, y0);
-    const double s = sqrt(b * b - y_min * y_min);
-    const double x_min = a / b * s;
-    return sqrt((yq - y_min) * (yq - y_min) + (xq - x_min) * (xq - x_min));
-  } else {
-    const double y0 = yq > 0 ? percentage * b : -percentage * b;
-    const double y_min = ellipse_newton<kLowerY>(a, b, xq, yq, y0);
-    const double s = sqrt(b * b - y_min * y_min);
-    const double x_min = -a / b * s;
-    return sqrt((yq - y_min) * (yq - y_min) + (xq - x_min) * (xq - x_min));
+  double v = S.e.X > 0 ? percentage * S.e.A : -percentage * S.e.A;
+  int steps = 0;
+  while (ellipse_search_step(S, a, v, steps)) {
   }
+  return ellipse_finish(S.e, v);
+}
+
+// cylinder.h:677-759 split around its ellipse search, so that a kernel can run the searches
+// of many points in lockstep: cylinder_setup takes every decision before the search (and
+// returns the result when no search is needed), cylinder_finish combines the shell distance
+// with the caps as the reference's region does.
+struct CylinderQuery {
+  EllipseSearch S;
+  double a = 0.0;       // the cylinder's semi_axis_a (the search's nudge compares with it)
+  double v = 0.0;       // the search's value (start: +-0.95 A)
+  double top = 0.0, bottom = 0.0;
+  int region = 0;       // 0 result ready; 1 inside; 2 beside the shell; 3 outside above/below
+  int steps = 0;        // search steps taken
+  double result = 0.0;
+};
+
+BZR_HD CylinderQuery cylinder_setup(D3 c, double a, double b, double height, const double *R,
+                                    D3 p) {
+  CylinderQuery q;
+  const D3 lp = to_local(R, c, p);
+  const double dist_top = fabs(lp.z - height / 2);
+  const double dist_bottom = fabs(lp.z + height / 2);
+  const double x_q = lp.x, y_q = lp.y, z_q = lp.z;
+  q.top = dist_top;
+  q.bottom = dist_bottom;
+  q.a = a;
+  if (x_q == 0 && y_q == 0) {  // isZero(point_xy)
+    if ((z_q > height / 2) || (z_q < -height / 2))
+      q.result = min_first(dist_top, dist_bottom);
+    else
+      q.result = min_first(min_first(min_first(a, b), dist_top), dist_bottom);
+    return q;
+  }
+  const double ellipse = (x_q * x_q) / (a * a) + (y_q * y_q) / (b * b) - 1;
+  if (fabs(ellipse) < kDblEps) {
+    q.result = ((z_q > height / 2) || (z_q < -height / 2)) ? min_first(dist_top, dist_bottom)
+                                                          : 0.0;
+    return q;
+  }
+  if (ellipse < 0) {
+    if (z_q >= height / 2) {
+      q.result = dist_top;
+      return q;
+    }
+    if (z_q <= -height / 2) {
+      q.result = dist_bottom;
+      return q;
+    }
+    q.region = 1;
+  } else if (ellipse > 0) {
+    q.region = ((z_q < height / 2) && (z_q > -height / 2)) ? 2 : 3;
+  } else {
+    q.result = -1.0;  // a NaN ellipse value (degenerate semi-axes)
+    return q;
+  }
+  q.S = ellipse_search(ellipse_branch(a, b, x_q, y_q));
+  const double percentage = 0.95;
+  q.v = q.S.e.X > 0 ? percentage * q.S.e.A : -percentage * q.S.e.A;
+  return q;
+}
+
+BZR_HD double cylinder_finish(const CylinderQuery &q, double v) {
+  const double dist_shell = ellipse_finish(q.S.e, v);
+  if (q.region == 1) return min_first(min_first(dist_shell, q.bottom), q.top);
+  if (q.region == 2) return dist_shell;
+  const double dist1 = sqrt(dist_shell * dist_shell + q.top * q.top);
+  const double dist2 = sqrt(dist_shell * dist_shell + q.bottom * q.bottom);
+  return min_first(dist1, dist2);
+}
+
+// One pass of the search's loop for a query in its search: false when it has ended.
+BZR_HD bool cylinder_search_step(CylinderQuery &q) {
+  return ellipse_search_step(q.S, q.a, q.v, q.steps);
 }
 
 // cylinder.h:677-759
 BZR_HD double cylinder_distance(D3 c, double a, double b, double height, const double *R,
                                 D3 p) {
-  const D3 lp = to_local(R, c, p);
-  const double dist_top = fabs(lp.z - height / 2);
-  const double dist_bottom = fabs(lp.z + height / 2);
-  const double x_q = lp.x, y_q = lp.y, z_q = lp.z;
-  if (x_q == 0 && y_q == 0) {  // isZero(point_xy)
-    if ((z_q > height / 2) || (z_q < -height / 2)) return min_first(dist_top, dist_bottom);
-    return min_first(min_first(min_first(a, b), dist_top), dist_bottom);
+  CylinderQuery q = cylinder_setup(c, a, b, height, R, p);
+  if (q.region == 0) return q.result;
+  while (cylinder_search_step(q)) {
   }
-  const double ellipse = (x_q * x_q) / (a * a) + (y_q * y_q) / (b * b) - 1;
-  if (fabs(ellipse) < kDblEps) {
-    if ((z_q > height / 2) || (z_q < -height / 2)) return min_first(dist_top, dist_bottom);
-    return 0.0;
-  }
-  if (ellipse < 0) {
-    if (z_q >= height / 2) return dist_top;
-    if (z_q <= -height / 2) return dist_bottom;
-    const double dist_shell = ellipse_distance(a, b, x_q, y_q);
-    return min_first(min_first(dist_shell, dist_bottom), dist_top);
-  }
-  if (ellipse > 0) {
-    const double dist_shell = ellipse_distance(a, b, x_q, y_q);
-    if ((z_q < height / 2) && (z_q > -height / 2)) return dist_shell;
-    const double dist1 = sqrt(dist_shell * dist_shell + dist_top * dist_top);
-    const double dist2 = sqrt(dist_shell * dist_shell + dist_bottom * dist_bottom);
-    return min_first(dist1, dist2);
-  }
-  return -1.0;  // a NaN ellipse value (degenerate semi-axes)
+  return cylinder_finish(q, q.v);
 }
 
 // trimesh_distance.h:177-218 with the region helpers r0..r6 (:37-163)
@@ -306,8 +365,11 @@ struct NearestState {
 
 BZR_HD double distance_margin(double scale, double best) { return 1e-12 * (scale + best); }
 
+// The smallest (distance, kind, id) wins, so the order in which kinds and primitives are
+// searched does not change the result.
 BZR_HD void nearest_offer(NearestState &st, int kind, uint32_t geom, uint32_t id, double d) {
-  if (d < st.best || (d == st.best && st.kind == kind && id < st.prim)) {
+  if (d < st.best || (d == st.best && st.prim != 0xFFFFFFFFu &&
+                      (kind < st.kind || (kind == st.kind && id < st.prim)))) {
     st.best = d;
     st.prim = id;
     st.geom = geom;
@@ -404,12 +466,18 @@ BZR_HD void nearest_bvh(const SceneView &S, int kind, D3 p, double scale, Neares
   }
 }
 
+// Search order: the smaller of the two BVH kinds first (a cheap early bound prunes the larger
+// one), then the other, then cylinders (whose skip test uses the bound) and planes.
 BZR_HD NearestState nearest_surface(const SceneView &S, D3 p, uint32_t *stack_ref,
                                     double *stack_key, uint32_t cap) {
   NearestState st;
   st.best = BZR_INF;
   const double ps = fmax(fmax(fabs(p.x), fabs(p.y)), fabs(p.z));
-  for (int kind = 0; kind < kNumKinds; ++kind) {
+  const bool spheres_first = S.k[kSpheres].n_prims < S.k[kMesh].n_prims;
+  const int order[kNumKinds] = {spheres_first ? kSpheres : kMesh,
+                                spheres_first ? kMesh : kSpheres, kCylinders, kPlanes};
+  for (int j = 0; j < kNumKinds; ++j) {
+    const int kind = order[j];
     const KindView &K = S.k[kind];
     if (!K.present || K.n_prims == 0) continue;
     const double scale = ps + double(K.coord_max);

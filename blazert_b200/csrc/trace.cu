@@ -31,6 +31,7 @@
 #include <cstdint>
 
 #include "layout.h"
+#include "bucket_sort.cuh"
 #include "trace.h"
 #include "trace_core.cuh"
 
@@ -298,15 +299,6 @@ __global__ void fill_defaults_kernel(RayIO io) {
 }
 
 // -------------------------------------------------------------------------- coherence sort
-__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 9 bits -> every third bit
-  v &= 0x1FFu;
-  v = (v | (v << 16)) & 0x030000FFu;
-  v = (v | (v << 8)) & 0x0300F00Fu;
-  v = (v | (v << 4)) & 0x030C30C3u;
-  v = (v | (v << 2)) & 0x09249249u;
-  return v;
-}
-
 __device__ __forceinline__ uint32_t ray_key(const RayIO &io, const RaySort &rs, uint32_t i) {
   const double *o = io.org + 3 * size_t(i), *d = io.dir + 3 * size_t(i);
   uint32_t q[3];
@@ -324,37 +316,6 @@ __global__ void sort_histogram_kernel(RayIO io, RaySort rs, uint32_t *keys, uint
     const uint32_t k = ray_key(io, rs, i);
     keys[i] = k;
     atomicAdd(counts + (k >> (32 - kSortBits)), 1u);
-  }
-}
-
-// In-place exclusive scan of 2^kSortBits counts; one block of 1024 threads.
-__global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t *counts) {
-  constexpr int kPer = (1 << kSortBits) / 1024;
-  __shared__ uint32_t part[1024];
-  uint32_t *c = counts + threadIdx.x * kPer;
-  uint32_t sum = 0;
-  for (int j = 0; j < kPer; ++j) sum += c[j];
-  part[threadIdx.x] = sum;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scan
-    const uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
-  }
-  uint32_t run = part[threadIdx.x] - sum;
-  for (int j = 0; j < kPer; ++j) {
-    const uint32_t v = c[j];
-    c[j] = run;
-    run += v;
-  }
-}
-
-__global__ void sort_scatter_kernel(uint32_t n, const uint32_t *keys, uint32_t *offsets,
-                                    uint32_t *perm) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t pos = atomicAdd(offsets + (keys[i] >> (32 - kSortBits)), 1u);
-    if (pos < n) perm[pos] = i;
   }
 }
 
@@ -480,8 +441,8 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
     if (e != cudaSuccess) return e;
     const int blocks = plan.sms * 8;
     sort_histogram_kernel<<<blocks, 256, 0, stream>>>(io, plan.sort, keys, counts);
-    sort_scan_kernel<<<1, 1024, 0, stream>>>(counts);
-    sort_scatter_kernel<<<blocks, 256, 0, stream>>>(io.n, keys, counts, perm);
+    bucket_scan_kernel<<<1, 1024, 0, stream>>>(counts);
+    bucket_scatter_kernel<<<blocks, 256, 0, stream>>>(io.n, keys, counts, perm);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     sorted.perm = perm;
   }

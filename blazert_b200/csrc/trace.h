@@ -43,7 +43,6 @@ struct RayIO {
 // octant (3 bits) over a Morton code of the origin quantised inside the scene bounds (9 bits
 // per axis) -- bucketed on the key's top kSortBits bits by a device counting sort.  The order
 // affects only speed: every ray's result is written to its own index.
-constexpr int kSortBits = 16;
 struct RaySort {
   bool enabled = false;
   float lo[3] = {0, 0, 0};     // origin quantisation box

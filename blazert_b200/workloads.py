@@ -355,9 +355,91 @@ def adjoint_scene(n_rays=1 << 22, seed=5, level=6, n_split=10_000, n_spheres=500
                     dict(triangles=int(f.shape[0]), spheres=n_spheres, seed=seed, weights=w))
 
 
+def distance_points(spec, kind, rng, n):
+    """(ids, points) of distance queries on one kind: random points around random primitives at
+    several scales, plus special points -- centres, axis points, shell and cap points of
+    cylinders (in the cylinder's frame), surface points of spheres, vertices, edge midpoints
+    and centroids of triangles."""
+    col = getattr(spec, kind)
+    if kind == "mesh":
+        v, f = col["vertices"], col["faces"]
+        m = len(f)
+        ids = rng.integers(0, m, n).astype(np.uint32)
+        tri = v[f[ids]]  # n x 3 x 3
+        w = rng.dirichlet([1.0, 1.0, 1.0], n)
+        base = np.einsum("ni,nij->nj", w, tri)
+        scale = rng.choice([0.0, 1e-3, 0.1, 1.0, 10.0], (n, 1))
+        pts = base + rng.standard_normal((n, 3)) * scale
+        k = n // 8
+        pts[:k] = tri[:k, 0]                                   # vertices
+        pts[k:2 * k] = 0.5 * (tri[k:2 * k, 0] + tri[k:2 * k, 1])  # edge midpoints
+        pts[2 * k:3 * k] = tri[2 * k:3 * k].mean(1)            # centroids
+        return ids, pts
+    c = col["centers"]
+    m = len(c)
+    ids = rng.integers(0, m, n).astype(np.uint32)
+    scale = rng.choice([0.01, 0.3, 1.0, 5.0, 50.0], (n, 1))
+    pts = c[ids] + rng.standard_normal((n, 3)) * scale
+    k = n // 10
+    pts[:k] = c[ids[:k]]  # centres
+    if kind == "spheres":
+        u = rng.standard_normal((k, 3))
+        u /= np.linalg.norm(u, axis=1, keepdims=True)
+        r = col["radii"][ids[k:2 * k]]
+        pts[k:2 * k] = c[ids[k:2 * k]] + u * r[:, None]
+    if kind == "cylinders":
+        R = col["rotations"].reshape(-1, 3, 3)
+        a, b, h = col["semi_axes_a"], col["semi_axes_b"], col["heights"]
+        for j in range(k, min(n, 6 * k)):
+            i = ids[j]
+            th = rng.uniform(0, 2 * np.pi)
+            sel = j % 5
+            if sel == 0:    # on the axis at several heights
+                loc = np.array([0.0, 0.0, rng.choice([0.0, h[i] / 2, -h[i] / 2, h[i], 0.3 * h[i]])])
+            elif sel == 1:  # on the shell
+                loc = np.array([a[i] * np.cos(th), b[i] * np.sin(th), rng.uniform(-h[i], h[i])])
+            elif sel == 2:  # on a cap
+                rr = rng.uniform(0, 1)
+                loc = np.array([rr * a[i] * np.cos(th), rr * b[i] * np.sin(th), h[i] / 2])
+            elif sel == 3:  # inside, near the shell
+                loc = np.array([0.9 * a[i] * np.cos(th), 0.9 * b[i] * np.sin(th), 0.1 * h[i]])
+            else:           # outside beside and above
+                loc = np.array([2 * a[i] * np.cos(th), 2 * b[i] * np.sin(th), rng.choice([0.0, h[i]])])
+            pts[j] = c[i] + R[i] @ loc
+    return ids, pts
+
+
+def distance_queries(n_per_kind=1 << 22, seed=6):
+    """Per-primitive distance queries on the mixed-primitive scene (10,000 spheres, 1,000
+    cylinders, 100 planes): n_per_kind (primitive id, point) pairs for each kind, from
+    distance_points (points around random primitives at scales 0.01 to 50 plus centres, axis,
+    shell and cap points)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    scene = mixed_primitives(n_rays=1).scene
+    queries = {k: distance_points(scene, k, rng, n_per_kind) for k in scene.order}
+    return Workload("distance_queries", scene, RayBatch(np.zeros((1, 3)), np.ones((1, 3))),
+                    dict(queries=queries, n_per_kind=n_per_kind, seed=seed))
+
+
+def closest_surface_points(n_points=1 << 20, seed=7):
+    """Nearest-surface queries on the differentiation scene (91,920 triangles and 500 spheres):
+    points uniform in [-2.5, 2.5]^3."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    scene = adjoint_scene(n_rays=1).scene
+    pts = rng.uniform(-2.5, 2.5, (n_points, 3))
+    return Workload("closest_surface", scene, RayBatch(np.zeros((1, 3)), np.ones((1, 3))),
+                    dict(points=pts, seed=seed))
+
+
 WORKLOADS = {
     "icosphere_pinhole": icosphere_pinhole,
     "mixed_primitives": mixed_primitives,
     "heightfield": heightfield,
     "adjoint_scene": adjoint_scene,
+}
+
+# query workloads of the distance kernels (not ray batches)
+DISTANCE_WORKLOADS = {
+    "distance_queries": distance_queries,
+    "closest_surface": closest_surface_points,
 }

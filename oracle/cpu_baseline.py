@@ -55,6 +55,63 @@ def measure(workload="mixed_primitives", seconds=10.0, threads=0, max_rays=0, mi
                 seconds_per_batch=med, rays=rays.n, repetitions=len(times))
 
 
+def measure_distance(workload="distance_queries", seconds=10.0, threads=0, max_queries=0,
+                     min_reps=3, flavour="bench"):
+    """The reference's distance_to_surface over the per-primitive queries of each kind
+    (distance_queries), or the nearest surface by a loop over every primitive with the
+    reference's distance functions (closest_surface; the reference has no scene-level query),
+    OpenMP over the queries.  Queries per second over the sample."""
+    import ctypes as C
+
+    import numpy as np
+
+    from oracle.oracle import _dp, _ptr, _u32p
+
+    wl = W.DISTANCE_WORKLOADS[workload]()
+    threads = threads or os.cpu_count() or 1
+    sc = RefScene(wl.scene, flavour=flavour)
+    lib = sc._lib
+    lib.ref_distance_to_surface_timed.restype = C.c_double
+    lib.ref_distance_to_surface_timed.argtypes = [C.c_void_p, C.c_int, C.c_long, _u32p, _dp,
+                                                  _dp, C.c_int]
+    lib.ref_closest_surface_timed.restype = C.c_double
+    lib.ref_closest_surface_timed.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _u32p, _u32p,
+                                              C.c_int]
+    kinds = ("mesh", "spheres", "planes", "cylinders")
+    if workload == "distance_queries":
+        qs = {k: (ids[:max_queries or None], np.ascontiguousarray(pts[:max_queries or None]))
+              for k, (ids, pts) in wl.meta["queries"].items()}
+        n = sum(len(i) for i, _ in qs.values())
+        outs = {k: np.empty(len(i)) for k, (i, _) in qs.items()}
+
+        def run():
+            return sum(lib.ref_distance_to_surface_timed(
+                sc._h, kinds.index(k), len(ids), _ptr(np.ascontiguousarray(ids, np.uint32), _u32p),
+                _ptr(pts, _dp), _ptr(outs[k], _dp), threads) for k, (ids, pts) in qs.items())
+        what = f"{workload}: {n} (primitive, point) pairs over {len(qs)} kinds"
+    else:
+        pts = np.ascontiguousarray(wl.meta["points"][:max_queries or 2048])
+        n = len(pts)
+        d, p_, g = np.empty(n), np.empty(n, np.uint32), np.empty(n, np.uint32)
+
+        def run():
+            return lib.ref_closest_surface_timed(sc._h, n, _ptr(pts, _dp), _ptr(d, _dp),
+                                                 _ptr(p_, _u32p), _ptr(g, _u32p), threads)
+        what = (f"{workload}: {n} points, each against every primitive with the reference's "
+                "distance functions")
+    run()
+    times = []
+    t_end = time.perf_counter() + seconds
+    while len(times) < min_reps or time.perf_counter() < t_end:
+        times.append(run())
+        if len(times) >= 1000:
+            break
+    med = statistics.median(times)
+    return dict(value=n / med / 1e6, unit="Mqueries/s", cores=threads, kind="reference",
+                sample=f"{what} x {len(times)} repetitions ({sum(times):.1f} s), median",
+                seconds_per_batch=med, queries=n, repetitions=len(times))
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="mixed_primitives")
@@ -63,7 +120,11 @@ def main(argv=None):
     ap.add_argument("--max-rays", type=int, default=0)
     ap.add_argument("--min-reps", type=int, default=3)
     a = ap.parse_args(argv)
-    print(json.dumps(measure(a.workload, a.seconds, a.threads, a.max_rays, a.min_reps)))
+    if a.workload in W.DISTANCE_WORKLOADS:
+        print(json.dumps(measure_distance(a.workload, a.seconds, a.threads, a.max_rays,
+                                          a.min_reps)))
+    else:
+        print(json.dumps(measure(a.workload, a.seconds, a.threads, a.max_rays, a.min_reps)))
 
 
 if __name__ == "__main__":

@@ -13,9 +13,11 @@
 // owned here) and copies RayHit fields out (blazert/ray.h:72-85).
 #include <blazert/blazert.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <vector>
 
@@ -274,6 +276,74 @@ void ref_distance_to_surface(void *h, int kind, long n, const uint32_t *ids, con
         break;
     }
   }
+}
+
+// ref_distance_to_surface over n pairs with OpenMP over the pairs: the CPU baseline of the
+// distance kernel.  Returns the seconds of the loop.
+double ref_distance_to_surface_timed(void *h, int kind, long n, const uint32_t *ids,
+                                     const double *points, double *distance, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+  const long chunk = 4096;
+  const auto t0 = std::chrono::steady_clock::now();
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+  for (long b = 0; b < n; b += chunk) {
+    const long m = std::min(chunk, n - b);
+    ref_distance_to_surface(h, kind, m, ids + b, points + 3 * b, distance + b, nullptr);
+  }
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// The nearest surface of the scene by a loop over every primitive with the reference's own
+// distance functions (kinds in the order triangles, spheres, planes, cylinders, ids increasing,
+// the first strictly smaller value kept): what a caller of the reference computes without a
+// scene-level query.  OpenMP over the points; returns the seconds of the loop.
+double ref_closest_surface_timed(void *h, long n, const double *points, double *distance,
+                                 uint32_t *prim, uint32_t *geom, int nthreads) {
+  const RefScene *s = static_cast<RefScene *>(h);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+  const long counts[4] = {long(s->faces.size()), long(s->sph_r.size()), long(s->pl_dx.size()),
+                          long(s->cy_a.size())};
+  const bool present[4] = {s->scene->has_triangles, s->scene->has_spheres, s->scene->has_planes,
+                           s->scene->has_cylinders};
+  const uint32_t geom_ids[4] = {present[0] ? s->scene->triangles_geom_id : UINT32_MAX,
+                                present[1] ? s->scene->spheres_geom_id : UINT32_MAX,
+                                present[2] ? s->scene->planes_geom_id : UINT32_MAX,
+                                present[3] ? s->scene->cylinders_geom_id : UINT32_MAX};
+  const auto t0 = std::chrono::steady_clock::now();
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16)
+#endif
+  for (long i = 0; i < n; ++i) {
+    double best = std::numeric_limits<double>::infinity();
+    uint32_t bp = UINT32_MAX, bg = UINT32_MAX;
+    for (int kind = 0; kind < 4; ++kind) {
+      if (!present[kind]) continue;
+      for (long id = 0; id < counts[kind]; ++id) {
+        const uint32_t u = uint32_t(id);
+        double d = 0.0;
+        ref_distance_to_surface(h, kind, 1, &u, points + 3 * i, &d, nullptr);
+        if (d < best) {
+          best = d;
+          bp = u;
+          bg = geom_ids[kind];
+        }
+      }
+    }
+    distance[i] = best;
+    if (prim) prim[i] = bp;
+    if (geom) geom[i] = bg;
+  }
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 // Traversal of ONE per-type BVH (blazert/bvh/accel.h:60-120) for n rays, as the reference's

@@ -111,55 +111,4 @@ def edge_case_scenes(seed=11):
     return out
 
 
-def distance_queries(spec, kind, rng, n):
-    """(ids, points) for distance tests of one kind: random points around random primitives at
-    several scales, plus special points -- centres, axis points, shell and cap points of
-    cylinders (in the cylinder's frame), surface points of spheres, vertices, edge midpoints
-    and centroids of triangles."""
-    col = getattr(spec, kind)
-    if kind == "mesh":
-        v, f = col["vertices"], col["faces"]
-        m = len(f)
-        ids = rng.integers(0, m, n).astype(np.uint32)
-        tri = v[f[ids]]  # n x 3 x 3
-        w = rng.dirichlet([1.0, 1.0, 1.0], n)
-        base = np.einsum("ni,nij->nj", w, tri)
-        scale = rng.choice([0.0, 1e-3, 0.1, 1.0, 10.0], (n, 1))
-        pts = base + rng.standard_normal((n, 3)) * scale
-        k = n // 8
-        pts[:k] = tri[:k, 0]                                   # vertices
-        pts[k:2 * k] = 0.5 * (tri[k:2 * k, 0] + tri[k:2 * k, 1])  # edge midpoints
-        pts[2 * k:3 * k] = tri[2 * k:3 * k].mean(1)            # centroids
-        return ids, pts
-    c = col["centers"]
-    m = len(c)
-    ids = rng.integers(0, m, n).astype(np.uint32)
-    scale = rng.choice([0.01, 0.3, 1.0, 5.0, 50.0], (n, 1))
-    pts = c[ids] + rng.standard_normal((n, 3)) * scale
-    k = n // 10
-    pts[:k] = c[ids[:k]]  # centres
-    if kind == "spheres":
-        u = rng.standard_normal((k, 3))
-        u /= np.linalg.norm(u, axis=1, keepdims=True)
-        r = col["radii"][ids[k:2 * k]]
-        pts[k:2 * k] = c[ids[k:2 * k]] + u * r[:, None]
-    if kind == "cylinders":
-        R = col["rotations"].reshape(-1, 3, 3)
-        a, b, h = col["semi_axes_a"], col["semi_axes_b"], col["heights"]
-        for j in range(k, min(n, 6 * k)):
-            i = ids[j]
-            th = rng.uniform(0, 2 * np.pi)
-            sel = j % 5
-            if sel == 0:    # on the axis at several heights
-                loc = np.array([0.0, 0.0, rng.choice([0.0, h[i] / 2, -h[i] / 2, h[i], 0.3 * h[i]])])
-            elif sel == 1:  # on the shell
-                loc = np.array([a[i] * np.cos(th), b[i] * np.sin(th), rng.uniform(-h[i], h[i])])
-            elif sel == 2:  # on a cap
-                rr = rng.uniform(0, 1)
-                loc = np.array([rr * a[i] * np.cos(th), rr * b[i] * np.sin(th), h[i] / 2])
-            elif sel == 3:  # inside, near the shell
-                loc = np.array([0.9 * a[i] * np.cos(th), 0.9 * b[i] * np.sin(th), 0.1 * h[i]])
-            else:           # outside beside and above
-                loc = np.array([2 * a[i] * np.cos(th), 2 * b[i] * np.sin(th), rng.choice([0.0, h[i]])])
-            pts[j] = c[i] + R[i] @ loc
-    return ids, pts
+from blazert_b200.workloads import distance_points as distance_queries  # noqa: E402,F401
