@@ -99,6 +99,15 @@ def library():
                                         C.POINTER(C.c_double)]
         lib.bzr_distance_to_surface.argtypes = [P, C.c_int, C.c_size_t, P, P, P, P, P]
         lib.bzr_closest_surface.argtypes = [P, C.c_size_t, P, P, P, P, P]
+        lib.bzr_scene_serialize.restype = C.c_long
+        lib.bzr_scene_serialize.argtypes = [P, P, C.c_size_t]
+        lib.bzr_scene_deserialize.argtypes = [C.POINTER(P), P, C.c_size_t]
+        lib.bzr_scene_save.argtypes = [P, C.c_char_p]
+        lib.bzr_scene_load.argtypes = [C.POINTER(P), C.c_char_p]
+        lib.bzr_obj_load.argtypes = [C.c_char_p, C.POINTER(C.POINTER(C.c_double)),
+                                     C.POINTER(C.c_size_t), C.POINTER(C.POINTER(C.c_uint32)),
+                                     C.POINTER(C.c_size_t)]
+        lib.bzr_obj_free.argtypes = [P]
         lib.bzr_last_error_string.restype = C.c_char_p
         _lib = lib
     return _lib
@@ -157,6 +166,22 @@ class BuildOptions:
     bin_size: int = 64
 
 
+def load_obj(path):
+    """(vertices n x 3 float64, faces m x 3 uint32) of a Wavefront OBJ file, as the reference's
+    examples build the mesh (bzr_obj_load); ready for Scene.add_mesh."""
+    lib = library()
+    pv, pf = C.POINTER(C.c_double)(), C.POINTER(C.c_uint32)()
+    nv, nf = C.c_size_t(), C.c_size_t()
+    _check(lib.bzr_obj_load(os.fsencode(path), C.byref(pv), C.byref(nv), C.byref(pf), C.byref(nf)))
+    try:
+        v = np.ctypeslib.as_array(pv, (max(1, nv.value) * 3,))[: 3 * nv.value].reshape(-1, 3).copy()
+        f = np.ctypeslib.as_array(pf, (max(1, nf.value) * 3,))[: 3 * nf.value].reshape(-1, 3).copy()
+    finally:
+        lib.bzr_obj_free(C.cast(pv, C.c_void_p))
+        lib.bzr_obj_free(C.cast(pf, C.c_void_p))
+    return v, f
+
+
 class Scene:
     """BlazertScene<double> on the GPU (blazert/scene.h:38-115)."""
 
@@ -176,6 +201,41 @@ class Scene:
             self.close()
         except Exception:
             pass
+
+    # -- persistent format (bzr_scene_serialize / bzr_scene_deserialize) ---------------------
+    def to_bytes(self) -> bytes:
+        """The committed scene in the persistent format (inputs, build options, trees)."""
+        n = self._lib.bzr_scene_serialize(self._h, None, 0)
+        if n < 0:
+            _check(int(n))
+        buf = (C.c_uint8 * n)()
+        m = self._lib.bzr_scene_serialize(self._h, buf, n)
+        if m < 0:
+            _check(int(m))
+        return bytes(buf)
+
+    @classmethod
+    def from_bytes(cls, data: bytes) -> "Scene":
+        """A committed scene from the persistent format, without rebuilding its trees."""
+        self = cls.__new__(cls)
+        self._lib = library()
+        self._h = C.c_void_p()
+        buf = (C.c_uint8 * len(data)).from_buffer_copy(data)
+        _check(self._lib.bzr_scene_deserialize(C.byref(self._h), buf, len(data)))
+        self.committed = True
+        return self
+
+    def save(self, path):
+        _check(self._lib.bzr_scene_save(self._h, os.fsencode(path)))
+
+    @classmethod
+    def load(cls, path) -> "Scene":
+        self = cls.__new__(cls)
+        self._lib = library()
+        self._h = C.c_void_p()
+        _check(self._lib.bzr_scene_load(C.byref(self._h), os.fsencode(path)))
+        self.committed = True
+        return self
 
     def __enter__(self):
         return self

@@ -28,7 +28,8 @@ CU_FLAGS = ARCH + ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler
                    "-fPIC,-ffp-contract=off", "-ccbin", CXX]
 
 SOURCES = [("scene.cpp", "cxx"), ("capi.cpp", "cxx"), ("trace.cu", "cu"), ("adjoint.cu", "cu"),
-           ("noalloc.cu", "cu"), ("batch.cpp", "cxx"), ("gbuild.cu", "cu"), ("distance.cu", "cu")]
+           ("noalloc.cu", "cu"), ("batch.cpp", "cxx"), ("gbuild.cu", "cu"), ("distance.cu", "cu"),
+           ("scene_io.cpp", "cxx"), ("obj.cpp", "cxx")]
 HEADERS = ["layout.h", "scene.h", "trace.h", "trace_core.cuh", "adjoint.h", "capi_internal.h",
            "distance.h", "distance_core.cuh", "bucket_sort.cuh"]
 

@@ -23,27 +23,41 @@ __device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 9 bits -> every th
 
 namespace {
 
-// In-place exclusive scan of 2^kSortBits counts; one block of 1024 threads.
+// In-place exclusive scan of the 2^kSortBits counts; one block of 1024 threads (32 warps).
+// Each warp scans its contiguous 2,048 counts in coalesced rounds of 32 (shuffle scan, running
+// carry), the 32 warp totals are scanned by one warp, and a second coalesced pass adds each
+// warp's offset.
 __global__ void __launch_bounds__(1024) bucket_scan_kernel(uint32_t *counts) {
-  constexpr int kPer = (1 << kSortBits) / 1024;
-  __shared__ uint32_t part[1024];
-  uint32_t *c = counts + threadIdx.x * kPer;
-  uint32_t sum = 0;
-  for (int j = 0; j < kPer; ++j) sum += c[j];
-  part[threadIdx.x] = sum;
+  constexpr int kPerWarp = (1 << kSortBits) / 32;
+  constexpr unsigned kFull = 0xFFFFFFFFu;
+  __shared__ uint32_t warp_offset[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *c = counts + warp * kPerWarp;
+  uint32_t carry = 0;
+  for (int r = 0; r < kPerWarp; r += 32) {
+    const uint32_t v = c[r + lane];
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, x, o);
+      if (lane >= o) x += y;
+    }
+    c[r + lane] = carry + x - v;
+    carry += __shfl_sync(kFull, x, 31);
+  }
+  if (lane == 0) warp_offset[warp] = carry;
   __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scan
-    const uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
+  if (warp == 0) {
+    const uint32_t t = warp_offset[lane];
+    uint32_t x = t;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, x, o);
+      if (lane >= o) x += y;
+    }
+    warp_offset[lane] = x - t;
   }
-  uint32_t run = part[threadIdx.x] - sum;
-  for (int j = 0; j < kPer; ++j) {
-    const uint32_t v = c[j];
-    c[j] = run;
-    run += v;
-  }
+  __syncthreads();
+  const uint32_t off = warp_offset[warp];
+  for (int r = 0; r < kPerWarp; r += 32) c[r + lane] += off;
 }
 
 __global__ void bucket_scatter_kernel(uint32_t n, const uint32_t *keys, uint32_t *offsets,

@@ -5,6 +5,7 @@
 #include <atomic>
 #include <cmath>
 #include <chrono>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <limits>
@@ -231,6 +232,8 @@ int bzr_commit(bzr_scene *s, const bzr_build_options *options) {
   return bzr_commit_ex(s, options, 0u);
 }
 
+static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given);
+
 int bzr_commit_ex(bzr_scene *s, const bzr_build_options *options, uint32_t flags) {
   if (!s) return fail(BZR_EINVAL, "scene is null");
   if (flags & ~uint32_t(BZR_COMMIT_GPU_BUILD | BZR_COMMIT_HOST_BUILD))
@@ -245,6 +248,12 @@ int bzr_commit_ex(bzr_scene *s, const bzr_build_options *options, uint32_t flags
     s->host.opt.max_depth = options->max_tree_depth;
     s->host.opt.bins = options->bin_size;
   }
+  return commit_scene(s, flags, false);
+}
+
+// Builds the trees (unless trees_given: a scene read from the persistent format), flattens
+// and uploads them and prepares the launch plan.
+static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(BZR_ENODEV, "no CUDA device");
@@ -254,12 +263,12 @@ int bzr_commit_ex(bzr_scene *s, const bzr_build_options *options, uint32_t flags
     for (int k = 0; k < bzr::kNumKinds; ++k) {
       bzr::Collection &c = s->host.kind[k];
       if (!c.present) continue;
-      bool built = false;
+      bool built = trees_given;
       // the device build pays for its transfers and per-level launches from about 64k
       // primitives on; below that the host builds unless asked otherwise
       const bool want_gpu = (flags & BZR_COMMIT_GPU_BUILD) ||
                             (!(flags & BZR_COMMIT_HOST_BUILD) && c.boxes.n >= kGpuBuildMin);
-      if (want_gpu && bzr::gpu_build_possible(c.boxes, s->host.opt)) {
+      if (!built && want_gpu && bzr::gpu_build_possible(c.boxes, s->host.opt)) {
         const auto t0 = std::chrono::steady_clock::now();
         bzr::Tree t;
         if (bzr::gpu_build_tree(c.boxes, s->host.opt, &t) == cudaSuccess) {
@@ -777,6 +786,110 @@ int bzr_closest_surface(const bzr_scene *s, size_t n, const double *points, doub
                         uint32_t *prim, uint32_t *geom, void *stream) {
   return run_distance(s, -1, n, nullptr, points, distance, nullptr, prim, geom, stream);
 }
+
+long bzr_scene_serialize(const bzr_scene *s, uint8_t *buffer, size_t capacity) {
+  if (!s) return fail(BZR_EINVAL, "scene is null");
+  if (!s->host.committed) return fail(BZR_ESTATE, "scene is not committed");
+  std::vector<uint8_t> b;
+  try {
+    b = bzr::encode_scene(s->host);
+  } catch (const std::bad_alloc &) {
+    return fail(BZR_ENOMEM, "host allocation failed while writing the scene");
+  }
+  if (buffer) {
+    if (capacity < b.size()) return fail(BZR_EINVAL, "buffer too small for the scene");
+    std::memcpy(buffer, b.data(), b.size());
+  }
+  return static_cast<long>(b.size());
+}
+
+int bzr_scene_deserialize(bzr_scene **out, const uint8_t *buffer, size_t size) {
+  if (!out || !buffer) return fail(BZR_EINVAL, "null argument");
+  *out = nullptr;
+  auto *s = new (std::nothrow) bzr_scene();
+  if (!s) return fail(BZR_ENOMEM, "host allocation failed");
+  std::string why;
+  try {
+    why = bzr::decode_scene(buffer, size, &s->host);
+  } catch (const std::bad_alloc &) {
+    why = "host allocation failed while reading the scene";
+  }
+  if (!why.empty()) {
+    delete s;
+    return fail(BZR_EINVAL, "scene data refused: " + why);
+  }
+  const int rc = commit_scene(s, 0u, true);
+  if (rc != BZR_OK) {
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return BZR_OK;
+}
+
+int bzr_scene_save(const bzr_scene *s, const char *path) {
+  if (!path) return fail(BZR_EINVAL, "path is null");
+  const long n = bzr_scene_serialize(s, nullptr, 0);
+  if (n < 0) return static_cast<int>(n);
+  std::vector<uint8_t> b(static_cast<size_t>(n));
+  const long m = bzr_scene_serialize(s, b.data(), b.size());
+  if (m < 0) return static_cast<int>(m);
+  std::FILE *f = std::fopen(path, "wb");
+  if (!f) return fail(BZR_EINVAL, std::string("cannot open for writing: ") + path);
+  const bool ok = std::fwrite(b.data(), 1, b.size(), f) == b.size();
+  const bool closed = std::fclose(f) == 0;
+  if (!ok || !closed) return fail(BZR_EINVAL, std::string("write failed: ") + path);
+  return BZR_OK;
+}
+
+int bzr_scene_load(bzr_scene **out, const char *path) {
+  if (!out || !path) return fail(BZR_EINVAL, "null argument");
+  *out = nullptr;
+  std::FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(BZR_EINVAL, std::string("cannot open: ") + path);
+  std::vector<uint8_t> b;
+  uint8_t chunk[1 << 16];
+  size_t got;
+  while ((got = std::fread(chunk, 1, sizeof chunk, f)) > 0) b.insert(b.end(), chunk, chunk + got);
+  const bool err = std::ferror(f) != 0;
+  std::fclose(f);
+  if (err) return fail(BZR_EINVAL, std::string("read failed: ") + path);
+  return bzr_scene_deserialize(out, b.data(), b.size());
+}
+
+int bzr_obj_load(const char *path, double **vertices, size_t *n_vertices, uint32_t **faces,
+                 size_t *n_faces) {
+  if (!path || !vertices || !n_vertices || !faces || !n_faces)
+    return fail(BZR_EINVAL, "null argument");
+  *vertices = nullptr;
+  *faces = nullptr;
+  *n_vertices = *n_faces = 0;
+  std::vector<double> v;
+  std::vector<uint32_t> f;
+  std::string why;
+  try {
+    why = bzr::load_obj(path, &v, &f);
+  } catch (const std::bad_alloc &) {
+    return fail(BZR_ENOMEM, "host allocation failed while reading the OBJ file");
+  }
+  if (!why.empty()) return fail(BZR_EINVAL, why);
+  auto *pv = static_cast<double *>(std::malloc(std::max<size_t>(1, v.size()) * sizeof(double)));
+  auto *pf = static_cast<uint32_t *>(std::malloc(std::max<size_t>(1, f.size()) * sizeof(uint32_t)));
+  if (!pv || !pf) {
+    std::free(pv);
+    std::free(pf);
+    return fail(BZR_ENOMEM, "host allocation failed");
+  }
+  if (!v.empty()) std::memcpy(pv, v.data(), v.size() * sizeof(double));
+  if (!f.empty()) std::memcpy(pf, f.data(), f.size() * sizeof(uint32_t));
+  *vertices = pv;
+  *faces = pf;
+  *n_vertices = v.size() / 3;
+  *n_faces = f.size() / 3;
+  return BZR_OK;
+}
+
+void bzr_obj_free(void *p) { std::free(p); }
 
 int bzr_intersect1(const bzr_scene *s, const double origin[3], const double direction[3],
                    double tmin, double tmax, bzr_rayhit *rayhit, int *hit) {

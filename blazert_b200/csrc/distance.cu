@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(kDistanceThreads)
 // it: every trip of the loop gives new queries to the idle lanes (their decisions before the
 // search, cylinder_setup) and one search step to the lanes in a search, all four sectors in
 // the same instructions.
-__global__ void __launch_bounds__(kDistanceThreads)
+__global__ void __launch_bounds__(kDistanceThreads, 4)
     cylinder_distance_kernel(const SceneView S, const DistanceIO io) {
   const KindView &K = S.k[kCylinders];
   const unsigned full = 0xFFFFFFFFu;

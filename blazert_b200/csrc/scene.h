@@ -6,6 +6,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "layout.h"
@@ -93,5 +94,16 @@ struct KindImage {
 };
 
 KindImage flatten(const HostScene &s, int kind);
+
+// Persistent scene format (scene_io.cpp): a committed scene's inputs, build options and trees
+// as bytes, and back.  decode_scene fills a fresh HostScene (primitives added, trees checked
+// and attached, not committed) or returns why the bytes were refused.
+std::vector<uint8_t> encode_scene(const HostScene &s);
+std::string decode_scene(const uint8_t *data, size_t size, HostScene *out);
+
+// Wavefront OBJ mesh as the reference's examples build it (obj.cpp): vertices n x 3, faces
+// m x 3; returns "" or the reason the file was refused.
+std::string load_obj(const std::string &path, std::vector<double> *vertices,
+                     std::vector<uint32_t> *faces);
 
 }  // namespace bzr

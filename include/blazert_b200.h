@@ -274,6 +274,31 @@ int bzr_distance_to_surface(const bzr_scene *scene, int kind, size_t n, const ui
 int bzr_closest_surface(const bzr_scene *scene, size_t n, const double *points, double *distance,
                         uint32_t *prim, uint32_t *geom, void *stream);
 
+/* Persistent scene format: a committed scene -- its inputs as added, build options and every
+ * kind's BVH in the reference's node order -- as bytes, and a committed scene made from them
+ * WITHOUT rebuilding the trees (the primitives' precompute is re-run; the trees are checked:
+ * DFS structure, leaf lists a permutation of the primitives, node boxes equal to the unions of
+ * their primitives' boxes; the bytes carry a checksum).  A loaded scene answers every query bit
+ * for bit as the saved one.  The reference has no scene file (blazert/scene.h builds at every
+ * commit).  bzr_scene_serialize returns the byte count (call with NULL to size the buffer) or a
+ * negative status; damaged or inconsistent data is BZR_EINVAL with the reason in
+ * bzr_last_error_string. */
+long bzr_scene_serialize(const bzr_scene *scene, uint8_t *buffer, size_t capacity);
+int bzr_scene_deserialize(bzr_scene **scene, const uint8_t *buffer, size_t size);
+int bzr_scene_save(const bzr_scene *scene, const char *path);
+int bzr_scene_load(bzr_scene **scene, const char *path);
+
+/* Mesh ingestion: the vertices (n x 3) and triangles (m x 3) the reference's examples build
+ * from a Wavefront OBJ file (examples/scene_mesh/main.cc:15-43 over the vendored
+ * tiny_obj_loader 0.9.14, examples/common/tiny_obj_loader.cc:911-1081): the loader's own
+ * number parser rounded to float, shapes ended by "g" and "o", vertices numbered per shape in
+ * order of first use by (position, texcoord, normal) index triple, polygons split into fans,
+ * shapes concatenated.  Ready for bzr_add_mesh.  The arrays are allocated here; release each
+ * with bzr_obj_free.  A missing file or a face index outside the vertices is BZR_EINVAL. */
+int bzr_obj_load(const char *path, double **vertices, size_t *n_vertices, uint32_t **faces,
+                 size_t *n_faces);
+void bzr_obj_free(void *p);
+
 const char *bzr_last_error_string(void);
 
 #ifdef __cplusplus

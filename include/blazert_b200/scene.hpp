@@ -12,6 +12,7 @@
 #include <cstdint>
 #include <initializer_list>
 #include <limits>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -165,9 +166,31 @@ class Scene {
                             prim_id, geom_id, hit, mode, ray_flags, stream));
   }
 
+  // Distances (bzr_distance_to_surface): kind 0 triangles, 1 spheres, 2 planes, 3 cylinders;
+  // closest (triangles only) may be null.
+  void distance_to_surface(int kind, size_t n, const uint32_t *prim_ids, const T *points,
+                           T *distance, T *closest = nullptr, void *stream = nullptr) const {
+    check(bzr_distance_to_surface(s_, kind, n, prim_ids, points, distance, closest, stream));
+  }
+  // Nearest surface of the scene per point (bzr_closest_surface).
+  void closest_surface(size_t n, const T *points, T *distance, uint32_t *prim_id,
+                       uint32_t *geom_id, void *stream = nullptr) const {
+    check(bzr_closest_surface(s_, n, points, distance, prim_id, geom_id, stream));
+  }
+
+  // Persistent format (bzr_scene_save / bzr_scene_load): a loaded scene is committed and
+  // answers as the saved one, without rebuilding its trees.
+  void save(const std::string &path) const { check(bzr_scene_save(s_, path.c_str())); }
+  static std::unique_ptr<Scene> load(const std::string &path) {
+    bzr_scene *h = nullptr;
+    check(bzr_scene_load(&h, path.c_str()));
+    return std::unique_ptr<Scene>(new Scene(h));
+  }
+
   const bzr_scene *handle() const { return s_; }
 
  private:
+  explicit Scene(bzr_scene *h) : s_(h) {}
   template <typename V>
   static const T *flat(const std::vector<V> &v) {
     static_assert(sizeof(V) % sizeof(T) == 0, "contiguous scalar storage");

@@ -327,3 +327,27 @@ class RefScene(_Base):
             _ptr(out["hit"], _u8p), nthreads)
         out["seconds"] = secs
         return out
+
+
+def ref_load_obj(path):
+    """(vertices, faces) of an OBJ file through the reference's vendored loader and the
+    scene_mesh example's assembly (oracle/_ref/libref_obj.so); ValueError with the loader's
+    message when it reports an error."""
+    lib = C.CDLL(os.path.join(HERE, "_ref", "libref_obj.so"))
+    lib.ref_obj_load.argtypes = [C.c_char_p, C.POINTER(C.POINTER(C.c_double)),
+                                 C.POINTER(C.c_long), C.POINTER(C.POINTER(C.c_uint32)),
+                                 C.POINTER(C.c_long), C.c_char_p, C.c_long]
+    lib.ref_obj_free.argtypes = [C.c_void_p]
+    pv, pf = C.POINTER(C.c_double)(), C.POINTER(C.c_uint32)()
+    nv, nf = C.c_long(), C.c_long()
+    why = C.create_string_buffer(512)
+    if lib.ref_obj_load(os.fsencode(path), C.byref(pv), C.byref(nv), C.byref(pf), C.byref(nf),
+                        why, 512):
+        raise ValueError(why.value.decode(errors="replace"))
+    try:
+        v = np.ctypeslib.as_array(pv, (3 * nv.value + 1,))[: 3 * nv.value].reshape(-1, 3).copy()
+        f = np.ctypeslib.as_array(pf, (3 * nf.value + 1,))[: 3 * nf.value].reshape(-1, 3).copy()
+    finally:
+        lib.ref_obj_free(C.cast(pv, C.c_void_p))
+        lib.ref_obj_free(C.cast(pf, C.c_void_p))
+    return v, f

@@ -20,6 +20,42 @@ struct Emu {
 };
 }  // namespace
 
+// Builds (or, for a loaded scene, keeps) every kind's tree, flattens it and fills the view.
+static void commit(Emu *e, bool build) {
+  bzr::HostScene &s = e->host;
+  e->img.resize(4);
+  uint32_t depth = 0;
+  for (int k = 0; k < 4; ++k) {
+    bzr::Collection &c = s.kind[k];
+    bzr::KindView &v = e->view.k[k];
+    v.present = c.present;
+    v.geom_id = c.geom_id;
+    if (!c.present) continue;
+    if (build) c.tree = bzr::build_tree(c.boxes, s.opt);
+    depth = depth > c.tree.max_depth ? depth : c.tree.max_depth;
+    e->img[k] = bzr::flatten(s, k);
+    const bzr::KindImage &im = e->img[k];
+    v.nodes64 = im.nodes64.data();
+    v.nodes32 = im.nodes32.data();
+    v.payload = im.payload.data();
+    v.prim_ids = im.prim_ids.data();
+    v.pos_of = im.pos_of.data();
+    v.tri = im.tri.data();
+    v.verts = im.verts.data();
+    v.n_internal = im.n_internal;
+    v.n_prims = static_cast<uint32_t>(im.prim_ids.size());
+    v.root_ref = im.root_ref;
+    v.mixed_ok = im.mixed_ok;
+    std::memcpy(v.root_box, im.root_box, sizeof v.root_box);
+    v.coord_max = im.coord_max;
+  }
+  e->view.faces = s.faces.data();
+  e->view.vert_n = s.vert_n.data();
+  e->view.stack_cap = (depth + 2) < 8 ? 8 : depth + 2;
+  s.committed = true;
+}
+
+
 extern "C" {
 
 void *emu_scene_create(const int *order, int n_order, const double *verts, long n_verts,
@@ -48,35 +84,30 @@ void *emu_scene_create(const int *order, int n_order, const double *verts, long 
   s.opt.min_leaf = min_leaf;
   s.opt.max_depth = max_depth;
   s.opt.bins = bins;
-  e->img.resize(4);
-  uint32_t depth = 0;
-  for (int k = 0; k < 4; ++k) {
-    bzr::Collection &c = s.kind[k];
-    bzr::KindView &v = e->view.k[k];
-    v.present = c.present;
-    v.geom_id = c.geom_id;
-    if (!c.present) continue;
-    c.tree = bzr::build_tree(c.boxes, s.opt);
-    depth = depth > c.tree.max_depth ? depth : c.tree.max_depth;
-    e->img[k] = bzr::flatten(s, k);
-    const bzr::KindImage &im = e->img[k];
-    v.nodes64 = im.nodes64.data();
-    v.nodes32 = im.nodes32.data();
-    v.payload = im.payload.data();
-    v.prim_ids = im.prim_ids.data();
-    v.pos_of = im.pos_of.data();
-    v.tri = im.tri.data();
-    v.verts = im.verts.data();
-    v.n_internal = im.n_internal;
-    v.n_prims = static_cast<uint32_t>(im.prim_ids.size());
-    v.root_ref = im.root_ref;
-    v.mixed_ok = im.mixed_ok;
-    std::memcpy(v.root_box, im.root_box, sizeof v.root_box);
-    v.coord_max = im.coord_max;
+  commit(e, true);
+  return e;
+}
+
+// The persistent scene format (scene_io.cpp) on the CPU: bytes of a scene, and a scene from
+// bytes (NULL and the reason in `why` when they are refused).
+long emu_scene_encode(void *h, uint8_t *out, long cap) {
+  const std::vector<uint8_t> b = bzr::encode_scene(static_cast<Emu *>(h)->host);
+  if (out && cap >= static_cast<long>(b.size())) std::memcpy(out, b.data(), b.size());
+  return static_cast<long>(b.size());
+}
+
+void *emu_scene_decode(const uint8_t *data, long size, char *why, long why_cap) {
+  auto *e = new Emu();
+  const std::string err = bzr::decode_scene(data, static_cast<size_t>(size), &e->host);
+  if (!err.empty()) {
+    if (why && why_cap > 0) {
+      std::strncpy(why, err.c_str(), static_cast<size_t>(why_cap) - 1);
+      why[why_cap - 1] = 0;
+    }
+    delete e;
+    return nullptr;
   }
-  e->view.faces = s.faces.data();
-  e->view.vert_n = s.vert_n.data();
-  e->view.stack_cap = (depth + 2) < 8 ? 8 : depth + 2;
+  commit(e, false);
   return e;
 }
 

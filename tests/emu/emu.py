@@ -20,7 +20,8 @@ _lib = None
 def build(force=False):
     """Compiles the emulator with the host compiler (no GPU or nvcc needed)."""
     root = os.path.dirname(os.path.dirname(HERE))
-    srcs = [os.path.join(HERE, "emu.cpp"), os.path.join(root, "blazert_b200", "csrc", "scene.cpp")]
+    srcs = [os.path.join(HERE, "emu.cpp"), os.path.join(root, "blazert_b200", "csrc", "scene.cpp"),
+            os.path.join(root, "blazert_b200", "csrc", "scene_io.cpp")]
     deps = srcs + [os.path.join(root, "blazert_b200", "csrc", f)
                    for f in ("layout.h", "scene.h", "trace_core.cuh", "distance_core.cuh")]
     if not force and os.path.exists(LIB) and all(os.path.getmtime(d) <= os.path.getmtime(LIB) for d in deps):
@@ -45,6 +46,10 @@ def load():
                                             _dp, _u32p, _u32p, _u8p, C.c_uint32, C.c_int]
         lib.emu_prim_box.argtypes = [C.c_void_p, C.c_int, C.c_uint32, _dp, _dp, _dp]
         lib.emu_box_accept.argtypes = [_dp, _dp, _dp, _dp, C.c_double, C.c_double]
+        lib.emu_scene_encode.restype = C.c_long
+        lib.emu_scene_encode.argtypes = [C.c_void_p, C.c_void_p, C.c_long]
+        lib.emu_scene_decode.restype = C.c_void_p
+        lib.emu_scene_decode.argtypes = [C.c_void_p, C.c_long, C.c_char_p, C.c_long]
         lib.emu_distance_to_surface.restype = C.c_uint32
         lib.emu_distance_to_surface.argtypes = _DIST_ARGS
         lib.emu_closest_surface.argtypes = _NEAREST_ARGS
@@ -72,6 +77,28 @@ class EmuScene(_Base):
                                     _ptr(mx, _dp), _ptr(c, _dp))
         assert rc == 0
         return mn, mx, c
+
+    def encode(self) -> bytes:
+        """The scene in the persistent format (scene_io.cpp)."""
+        n = self._lib.emu_scene_encode(self._h, None, 0)
+        buf = (C.c_uint8 * n)()
+        self._lib.emu_scene_encode(self._h, buf, n)
+        return bytes(buf)
+
+    @classmethod
+    def decode(cls, data: bytes) -> "EmuScene":
+        """A scene from the persistent format; ValueError with the reason when refused."""
+        self = cls.__new__(cls)
+        self._lib = load()
+        why = C.create_string_buffer(256)
+        buf = (C.c_uint8 * max(1, len(data))).from_buffer_copy(data or b"\0")
+        h = self._lib.emu_scene_decode(buf, len(data), why, 256)
+        if not h:
+            raise ValueError(why.value.decode())
+        self._h = h
+        self._keep = None
+        self.geom_ids = {}
+        return self
 
     def distance_to_surface(self, kind, ids, points):
         """The distance kernel's per-point code on the CPU."""

@@ -101,6 +101,64 @@ int main(int argc, char **) {
 """
 
 
+EMBREE_APP = r"""
+#include <blazert_b200/embree_scene.hpp>
+#include <cstdio>
+using namespace blazert_b200;
+
+int main(int argc, char **argv) {
+  // call sites written for the reference's Embree backend (blazert/embree/scene.h)
+  EmbreeScene<float> fs;
+  EmbreeScene<double> ds;
+  const unsigned a = fs.add_spheres(Vec3rList<float>{{0.f, 0.f, 0.f}, {3.f, 0.f, 0.f}}, {1.f, 0.5f});
+  const unsigned b = ds.add_spheres(Vec3rList<double>{{0.0, 0.0, 0.0}, {3.0, 0.0, 0.0}}, {1.0, 0.5});
+  if (a != 0 || b != 0) return 1;
+  if (argc > 1) {  // needs a GPU; argv[1]: a scene file to write
+    fs.commit();
+    ds.commit();
+    Ray<float> rf{{3.f, 0.f, 5.f}, {0.f, 0.f, -1.f}};
+    RayHit<float> hf;
+    const bool h1 = intersect1(fs, rf, hf);
+    Ray<double> rd{{3.0, 0.0, 5.0}, {0.0, 0.0, -1.0}};
+    RayHit<double> hd;
+    const bool h2 = intersect1(ds, rd, hd);
+    const std::vector<uint32_t> ids{0, 1};
+    const std::vector<double> pts{0.0, 0.0, 3.0, 3.0, 0.0, 3.0};
+    std::vector<double> dist(2);
+    ds.blazertscene.distance_to_surface(1, 2, ids.data(), pts.data(), dist.data());
+    ds.blazertscene.save(argv[1]);
+    auto loaded = Scene<double>::load(argv[1]);
+    RayHit<double> h3;
+    const bool h3hit = intersect1(*loaded, rd, h3);
+    std::printf("%d %u %.9g %d %u %.17g %.17g %.17g %d %.17g\n", h1, hf.prim_id, hf.hit_distance,
+                h2, hd.prim_id, hd.hit_distance, dist[0], dist[1], h3hit, h3.hit_distance);
+  }
+  return 0;
+}
+"""
+
+
+def _compile(src_text, tmp_path, name):
+    import subprocess
+
+    src = tmp_path / f"{name}.cpp"
+    src.write_text(src_text)
+    exe = tmp_path / name
+    lib = os.path.join(ROOT, "blazert_b200", "_lib")
+    cxx = os.environ.get("BZR_CXX", "g++")
+    subprocess.run([cxx, "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), str(src),
+                    "-L", lib, "-lblazert_b200", f"-Wl,-rpath,{lib}", "-o", str(exe)], check=True)
+    return exe
+
+
+def test_embree_facade_compiles_and_links(tmp_path):
+    """include/blazert_b200/embree_scene.hpp: EmbreeScene<float> / <double> call sites, the
+    distance and save/load members compile and link; the add rules run without a GPU."""
+    import subprocess
+
+    subprocess.run([str(_compile(EMBREE_APP, tmp_path, "embree_app"))], check=True)
+
+
 def test_cpp_facade_compiles_links_and_keeps_add_rules(tmp_path):
     """include/blazert_b200/scene.hpp: reference-style C++ (Scene<double>, add_*, Ray with the
     reference's CullBackFace / AnyHit enums, RayHit, intersect1) compiles against the header,

@@ -99,3 +99,17 @@ def test_distance_errors():
     with pytest.raises(B.BlazertError) as e:
         s.check()
     assert e.value.code == B.EDEVICE_FLAG
+
+
+def test_closest_surface_large_batch_is_sorted_and_exact():
+    """From 65,536 points on, the batch is processed in Morton order (a device counting sort);
+    every point's result is still its own, equal to the CPU copy of the kernels' search."""
+    from tests.emu.emu import EmuScene
+
+    wl = W.closest_surface_points(n_points=70_000)
+    pts = wl.meta["points"]
+    s = product_scene(wl.scene)
+    got = s.closest_surface(pts)
+    want = EmuScene(wl.scene).closest_surface(pts)
+    assert bits_equal(got["distance"], want["distance"])
+    assert np.array_equal(got["prim"], want["prim"]) and np.array_equal(got["geom"], want["geom"])

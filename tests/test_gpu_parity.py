@@ -134,6 +134,24 @@ def test_cpp_facade_runs_on_gpu(tmp_path):
     assert (hit, geom, prim, float(t), hit2) == ("1", "0", "0", 3.0, "1")
 
 
+def test_embree_facade_runs_on_gpu(tmp_path):
+    """EmbreeScene<float> and <double> (the reference's Embree-backend API) trace through the
+    GPU path; the double scene's distance query, save and load work from C++."""
+    import subprocess
+
+    from tests.test_capi import EMBREE_APP, _compile
+
+    exe = _compile(EMBREE_APP, tmp_path, "embree_app")
+    r = subprocess.run([str(exe), str(tmp_path / "s.bzrscene")], check=True, capture_output=True,
+                       text=True)
+    f = r.stdout.split()
+    # the ray from (3, 0, 5) down -z meets sphere 1 (centre (3, 0, 0), radius 0.5) at t = 4.5
+    assert f[0] == "1" and f[1] == "1" and float(f[2]) == 4.5
+    assert f[3] == "1" and f[4] == "1" and float(f[5]) == 4.5
+    assert float(f[6]) == 2.0 and float(f[7]) == 2.5
+    assert f[8] == "1" and float(f[9]) == 4.5
+
+
 def test_intersect1_matches_batch():
     import blazert_b200 as B
 
