@@ -40,9 +40,11 @@ int cuda_fail(cudaError_t e, const char *what) {
 constexpr int kSlots = 256;
 constexpr int kSlotWords = 8;
 constexpr int kStickyWord = kSlots * kSlotWords;
-// Host-array batches: split into at most kMaxChunks chunks of at least kMinChunk rays.
+// Host-array batches: split into at most host_chunks (default kHostChunks, at most kMaxChunks)
+// chunks of at least host_min_chunk (default kMinChunk) rays.
 constexpr int kStreams = 3;
-constexpr size_t kMaxChunks = 8;
+constexpr size_t kMaxChunks = 40;  // host_chunks (at most 32) plus the two edge chunks
+constexpr size_t kHostChunks = 8;
 constexpr size_t kMinChunk = size_t(1) << 17;
 // Collections of at least this many primitives are built on the device by default.
 constexpr size_t kGpuBuildMin = size_t(1) << 16;
@@ -91,6 +93,8 @@ struct bzr_scene {
   // chained per chunk by ev_in / ev_done
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t ev_in[kMaxChunks] = {}, ev_done[kMaxChunks] = {};
+  size_t host_chunks = kHostChunks, host_min_chunk = kMinChunk;  // bzr_scene_tune
+  size_t host_edge = 0;  // rays of the first and last chunk (0: all chunks the same size)
 
   ~bzr_scene() {
     if (device >= 0) {
@@ -521,11 +525,25 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
   // kernels start on one of the scene's streams (round robin, so that one chunk's slowest rays
   // overlap the next chunk's kernels) once its copies in are done, and its copies out follow
   // on copy_out once its kernels are done.
-  const size_t chunk = n <= kMinChunk ? n : std::max(kMinChunk, (n + kMaxChunks - 1) / kMaxChunks);
-  const size_t nchunks = (n + chunk - 1) / chunk;
+  // The kernels are the slowest stage, so a step takes about the first chunk's copy in, the
+  // kernels of every chunk and the last chunk's copy out: optional small edge chunks shorten
+  // the exposed copies, a few large middle chunks keep the kernels' per-launch tails few.
+  size_t bounds[kMaxChunks + 1];
+  size_t nchunks = 0;
+  {
+    const size_t edge = s->host_edge, min_chunk = s->host_min_chunk, max_chunks = s->host_chunks;
+    const bool edges = edge > 0 && n > 4 * edge;
+    const size_t first = edges ? edge : 0, mid = n - 2 * first;
+    const size_t chunk =
+        mid <= min_chunk ? mid : std::max(min_chunk, (mid + max_chunks - 1) / max_chunks);
+    bounds[0] = 0;
+    if (edges) bounds[++nchunks] = first;
+    for (size_t a = first; a < first + mid; a += chunk) bounds[++nchunks] = std::min(first + mid, a + chunk);
+    if (edges) bounds[++nchunks] = n;
+  }
   cudaError_t e = cudaSuccess;
   for (size_t c = 0; c < nchunks && e == cudaSuccess; ++c) {
-    const size_t a = c * chunk, m = std::min(n, a + chunk) - a;
+    const size_t a = bounds[c], m = bounds[c + 1] - a;
     cudaStream_t st = s->streams[c % kStreams];
     uint32_t *cnt = c == 0 ? counters : s->slots + kSlotWords * (s->next_slot.fetch_add(1) % kSlots);
     auto h2d = [&](double *dst, const double *src, size_t per) {
@@ -939,6 +957,26 @@ int bzr_scene_tune(bzr_scene *s, int option, int64_t value) {
       if (value < 0 || value > 0x7FFFFFFF) return fail(BZR_EINVAL, "bad sort threshold");
       s->plan.sort_min_rays = static_cast<uint32_t>(value);
       return BZR_OK;
+    case BZR_TUNE_HOST_CHUNKS: {
+      if (value < 1 || value > static_cast<int64_t>(kMaxChunks))
+        return fail(BZR_EINVAL, "host-array chunks must be 1 to 32");
+      std::lock_guard<std::mutex> lock(s->stage_mu);
+      s->host_chunks = static_cast<size_t>(value);
+      return BZR_OK;
+    }
+    case BZR_TUNE_HOST_EDGE: {
+      if (value < 0 || value > 0x7FFFFFFF) return fail(BZR_EINVAL, "bad edge chunk size");
+      std::lock_guard<std::mutex> lock(s->stage_mu);
+      s->host_edge = static_cast<size_t>(value);
+      return BZR_OK;
+    }
+    case BZR_TUNE_HOST_MIN_CHUNK: {
+      if (value < 1024 || value > 0x7FFFFFFF)
+        return fail(BZR_EINVAL, "host-array chunk size must be 1024 to 2^31 - 1 rays");
+      std::lock_guard<std::mutex> lock(s->stage_mu);
+      s->host_min_chunk = static_cast<size_t>(value);
+      return BZR_OK;
+    }
     case BZR_TUNE_CHUNK:
       if (value != 0 && value != 32 && value != 64 && value != 128)
         return fail(BZR_EINVAL, "rays per warp fetch must be 0 (the idle lanes), 32, 64 or 128");

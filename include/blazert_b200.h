@@ -231,6 +231,14 @@ int bzr_scene_check(const bzr_scene *scene, void *stream, int timeout_ms, uint32
 #define BZR_TUNE_BLOCK 3
 #define BZR_TUNE_STACK 4
 #define BZR_TUNE_CHUNK 5
+/* Host-array calls: the batch is split into at most this many chunks (1 to 32, default 8) of
+ * at least BZR_TUNE_HOST_MIN_CHUNK rays (default 131,072), pipelined as copies in, kernels and
+ * copies out. */
+#define BZR_TUNE_HOST_CHUNKS 6
+#define BZR_TUNE_HOST_MIN_CHUNK 7
+/* Rays of an extra first and last chunk of host-array calls (0, the default: none), which
+ * shortens the copies that do not overlap a kernel; used when the batch exceeds 4x it. */
+#define BZR_TUNE_HOST_EDGE 8
 int bzr_scene_tune(bzr_scene *scene, int option, int64_t value);
 
 /* Statistics of the last commit: per kind (0 mesh, 1 spheres, 2 planes, 3 cylinders) the
