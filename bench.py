@@ -436,6 +436,11 @@ def run_ours(args):
                     prim=torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
                     geom=torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
                     hit=torch.empty(n, dtype=torch.uint8).pin_memory().numpy())
+        host_tuning = None
+        if args.sort == "auto" and not args.any_hit:
+            from blazert_b200.autotune import autotune_host
+            host_tuning = autotune_host(scene, ho, hd, htmn, htmx, out=hout, mode=args.mode)
+            host_tuning = {"choice": host_tuning["choice"], "best_ms": host_tuning["best_ms"]}
         for _ in range(max(1, args.warmup)):
             scene.intersectN(ho, hd, htmn, htmx, mode=args.mode, out=hout, any_hit=args.any_hit)
         if pg:
@@ -448,7 +453,7 @@ def run_ours(args):
             el = multi.max_over_ranks(el)
         e2e = {"value": world * n * args.steps / el / 1e6, "unit": "Mrays/s",
                "h2d_bytes_per_step": n * (24 + 24 + 8 + 8),
-               "d2h_bytes_per_step": n * (8 + 16 + 24 + 4 + 4 + 1)}
+               "d2h_bytes_per_step": n * (8 + 16 + 24 + 4 + 4 + 1), "host_tuning": host_tuning}
         ok = np.array_equal(hout["prim"], out["prim"].cpu().numpy().view(np.uint32))
         if not ok:
             e2e["warning"] = "host-path results differ from the device path"

@@ -466,13 +466,15 @@ class Scene:
         return out
 
     def tune(self, sort=None, sort_min_rays=None, threads=None, shared_stack=None, chunk=None,
-             host_chunks=None, host_min_chunk=None, host_edge=None):
+             host_chunks=None, host_min_chunk=None, host_edge=None, host_grid_div=None):
         """Speed knobs (bzr_scene_tune); results do not depend on them.  sort: coherence sort
         of each batch; threads: 64 / 128 / 256 per block; shared_stack: traversal stack in
         shared memory instead of thread-local; chunk: rays per warp fetch (32 / 64 / 128, or 0
         for exactly the idle lanes); host_chunks / host_min_chunk: the pipeline of host-array
         calls (at most this many chunks, 1 to 32, of at least this many rays) and host_edge,
         the rays of an extra small first and last chunk (0: none)."""
+        if host_grid_div is not None:
+            _check(self._lib.bzr_scene_tune(self._h, 9, int(host_grid_div)))
         if host_edge is not None:
             _check(self._lib.bzr_scene_tune(self._h, 8, int(host_edge)))
         if host_chunks is not None:

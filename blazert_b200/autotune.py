@@ -116,3 +116,41 @@ def autotune_batch(batch, ray_offsets, origins, directions, tmin=None, tmax=None
         best[k] = min(scores, key=scores.get)
     batch.tune(**best)
     return dict(choice=best, best_ms=timings[str(sorted(best.items()))], timings_ms=timings)
+
+
+HOST_KNOBS = {"host_chunks": (8, 4, 6, 12, 16), "host_grid_div": (1, 2, 3)}
+
+
+def autotune_host(scene, origins, directions, tmin=None, tmax=None, out=None, mode="fp64",
+                  reps=3, knobs=None, sweeps=2):
+    """The pipeline of host-array calls (bzr_scene_tune HOST_CHUNKS / HOST_GRID_DIV): how many
+    chunks the batch is split into and what share of the grid each chunk's kernels take, timed
+    end to end (wall clock, host arrays, copies included) on the caller's whole batch.  The
+    device-path knobs stay as they are.  Applies and returns the choice with the timings (ms)."""
+    import time
+
+    knobs = dict(HOST_KNOBS if knobs is None else knobs)
+    timings = {}
+
+    def timed(cfg):
+        nonlocal out
+        key = str(sorted(cfg.items()))
+        if key in timings:
+            return timings[key]
+        scene.tune(**cfg)
+        out = scene.intersectN(origins, directions, tmin, tmax, mode=mode, out=out)  # warm-up
+        best = float("inf")
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            scene.intersectN(origins, directions, tmin, tmax, mode=mode, out=out)
+            best = min(best, (time.perf_counter() - t0) * 1e3)
+        timings[key] = best
+        return best
+
+    best = {k: v[0] for k, v in knobs.items()}
+    for _ in range(sweeps):
+        for k, values in knobs.items():
+            scores = {v: timed({**best, k: v}) for v in values}
+            best[k] = min(scores, key=scores.get)
+    scene.tune(**best)
+    return dict(choice=best, best_ms=timings[str(sorted(best.items()))], timings_ms=timings)

@@ -43,7 +43,8 @@ constexpr int kStickyWord = kSlots * kSlotWords;
 // Host-array batches: split into at most host_chunks (default kHostChunks, at most kMaxChunks)
 // chunks of at least host_min_chunk (default kMinChunk) rays.
 constexpr int kStreams = 3;
-constexpr size_t kMaxChunks = 40;  // host_chunks (at most 32) plus the two edge chunks
+constexpr size_t kMaxHostChunks = 32;
+constexpr size_t kMaxChunks = kMaxHostChunks + 2;  // plus the two edge chunks
 constexpr size_t kHostChunks = 8;
 constexpr size_t kMinChunk = size_t(1) << 17;
 // Collections of at least this many primitives are built on the device by default.
@@ -95,6 +96,7 @@ struct bzr_scene {
   cudaEvent_t ev_in[kMaxChunks] = {}, ev_done[kMaxChunks] = {};
   size_t host_chunks = kHostChunks, host_min_chunk = kMinChunk;  // bzr_scene_tune
   size_t host_edge = 0;  // rays of the first and last chunk (0: all chunks the same size)
+  int host_grid_div = 1;  // host-array chunks launch 1/host_grid_div of each kind's grid
 
   ~bzr_scene() {
     if (device >= 0) {
@@ -541,6 +543,13 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
     for (size_t a = first; a < first + mid; a += chunk) bounds[++nchunks] = std::min(first + mid, a + chunk);
     if (edges) bounds[++nchunks] = n;
   }
+  // chunks on the round-robin streams may run side by side on smaller grids, so that one
+  // chunk's tail idles only its share of the SMs
+  bzr::LaunchPlan chunk_plan = s->plan;
+  for (int k = 0; k < bzr::kNumKinds; ++k) {
+    chunk_plan.blocks[k] = std::max(1, chunk_plan.blocks[k] / s->host_grid_div);
+    chunk_plan.blocks32[k] = std::max(1, chunk_plan.blocks32[k] / s->host_grid_div);
+  }
   cudaError_t e = cudaSuccess;
   for (size_t c = 0; c < nchunks && e == cudaSuccess; ++c) {
     const size_t a = bounds[c], m = bounds[c + 1] - a;
@@ -572,7 +581,7 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
     if (e == cudaSuccess) e = cudaEventRecord(s->ev_in[c], s->copy_in);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(st, s->ev_in[c], 0);
     if (e == cudaSuccess) e = cudaMemsetAsync(ci.error_word, 0, sizeof(uint32_t), st);
-    if (e == cudaSuccess) e = bzr::launch_trace(s->view, ci, mode, s->plan, st, cnt, totals);
+    if (e == cudaSuccess) e = bzr::launch_trace(s->view, ci, mode, chunk_plan, st, cnt, totals);
     if (e == cudaSuccess) e = cudaEventRecord(s->ev_done[c], st);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s->copy_out, s->ev_done[c], 0);
     auto d2h = [&](void *dst, const void *src, size_t bytes) {
@@ -958,10 +967,16 @@ int bzr_scene_tune(bzr_scene *s, int option, int64_t value) {
       s->plan.sort_min_rays = static_cast<uint32_t>(value);
       return BZR_OK;
     case BZR_TUNE_HOST_CHUNKS: {
-      if (value < 1 || value > static_cast<int64_t>(kMaxChunks))
+      if (value < 1 || value > static_cast<int64_t>(kMaxHostChunks))
         return fail(BZR_EINVAL, "host-array chunks must be 1 to 32");
       std::lock_guard<std::mutex> lock(s->stage_mu);
       s->host_chunks = static_cast<size_t>(value);
+      return BZR_OK;
+    }
+    case BZR_TUNE_HOST_GRID_DIV: {
+      if (value < 1 || value > 8) return fail(BZR_EINVAL, "grid divisor must be 1 to 8");
+      std::lock_guard<std::mutex> lock(s->stage_mu);
+      s->host_grid_div = static_cast<int>(value);
       return BZR_OK;
     }
     case BZR_TUNE_HOST_EDGE: {

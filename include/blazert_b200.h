@@ -239,6 +239,9 @@ int bzr_scene_check(const bzr_scene *scene, void *stream, int timeout_ms, uint32
 /* Rays of an extra first and last chunk of host-array calls (0, the default: none), which
  * shortens the copies that do not overlap a kernel; used when the batch exceeds 4x it. */
 #define BZR_TUNE_HOST_EDGE 8
+/* Host-array calls: each chunk's kernels use 1/value (1 to 8, default 1) of the grid, so that
+ * chunks on the pipeline's three streams can run side by side. */
+#define BZR_TUNE_HOST_GRID_DIV 9
 int bzr_scene_tune(bzr_scene *scene, int option, int64_t value);
 
 /* Statistics of the last commit: per kind (0 mesh, 1 spheres, 2 planes, 3 cylinders) the

@@ -197,6 +197,32 @@ def test_tuning_changes_speed_not_results():
     assert mismatches(out, ref) == []
 
 
+def test_host_pipeline_knobs_change_speed_not_results():
+    """Host-array calls with every pipeline shape (chunk count and size, edge chunks, grid
+    share per chunk) and the host autotuner's choice give the oracle's results."""
+    from blazert_b200.autotune import autotune_host
+
+    wl = W.mixed_primitives(n_rays=700_000, seed=10)
+    R = wl.rays
+    ref = Oracle(wl.scene).intersect(R.origins, R.directions, R.tmin, R.tmax)
+    s = product_scene(wl.scene)
+    configs = [dict(host_chunks=1), dict(host_chunks=3, host_min_chunk=1024),
+               dict(host_chunks=32, host_min_chunk=1024), dict(host_edge=50_000),
+               dict(host_edge=1 << 20), dict(host_grid_div=2), dict(host_grid_div=8, host_chunks=12),
+               dict(host_chunks=8, host_min_chunk=1 << 17, host_edge=0, host_grid_div=1)]
+    for cfg in configs:
+        s.tune(**cfg)
+        out = s.intersectN(R.origins, R.directions, R.tmin, R.tmax)
+        assert mismatches(out, ref) == [], cfg
+    with pytest.raises(Exception):
+        s.tune(host_chunks=33)
+    with pytest.raises(Exception):
+        s.tune(host_grid_div=0)
+    res = autotune_host(s, R.origins, R.directions, R.tmin, R.tmax, reps=1, sweeps=1)
+    assert set(res["choice"]) == {"host_chunks", "host_grid_div"}
+    assert mismatches(s.intersectN(R.origins, R.directions, R.tmin, R.tmax), ref) == []
+
+
 @pytest.fixture(scope="module")
 def heightfield_ref():
     wl = W.heightfield()
