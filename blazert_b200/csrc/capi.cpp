@@ -47,6 +47,9 @@ constexpr size_t kMaxHostChunks = 32;
 constexpr size_t kMaxChunks = kMaxHostChunks + 2;  // plus the two edge chunks
 constexpr size_t kHostChunks = 8;
 constexpr size_t kMinChunk = size_t(1) << 17;
+// Host-array batches of at most kSmallBatch rays (intersect1 included) take a latency path:
+// inputs packed into pinned memory, one copy in, a grid sized to the batch, one copy out.
+constexpr size_t kSmallBatch = 4096;
 // Collections of at least this many primitives are built on the device by default.
 constexpr size_t kGpuBuildMin = size_t(1) << 16;
 
@@ -89,6 +92,7 @@ struct bzr_scene {
   void *stage_dev = nullptr;
   size_t stage_bytes = 0;
   uint32_t *pinned_err = nullptr;  // one error word per chunk
+  unsigned char *small_pin = nullptr;  // small host-array batches: packed inputs and outputs
   cudaStream_t streams[kStreams] = {nullptr, nullptr, nullptr};
   // host-array pipeline: copies in on copy_in, kernels on streams[], copies out on copy_out,
   // chained per chunk by ev_in / ev_done
@@ -111,6 +115,7 @@ struct bzr_scene {
       cudaFree(slots);
       cudaFree(stage_dev);
       cudaFreeHost(pinned_err);
+      cudaFreeHost(small_pin);
       for (cudaStream_t st : streams)
         if (st) cudaStreamDestroy(st);
       if (copy_in) cudaStreamDestroy(copy_in);
@@ -421,6 +426,105 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
 
 static bool is_device_ptr(const void *p) { return bzr::is_device_pointer(p); }
 
+// Waits for a stream: spins on cudaStreamQuery for up to spin_us (a small batch finishes in
+// tens of microseconds, well inside a sleeping wait's granularity), then waits as usual.
+static int wait_stream_spin(cudaStream_t st, int spin_us) {
+  const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(spin_us);
+  do {
+    const cudaError_t e = cudaStreamQuery(st);
+    if (e == cudaSuccess) return BZR_OK;
+    if (e != cudaErrorNotReady) return cuda_fail(e, "stream");
+  } while (std::chrono::steady_clock::now() < until);
+  return wait_stream(st, default_timeout_ms());
+}
+
+// The latency path of small host-array batches (the caller holds stage_mu).  One pinned block
+// mirrors one device block: inputs org, dir, [tmin], [tmax]; then the error word; then the
+// outputs t, [uv], [normal], [prim], [geom], [hit]; each piece 256-byte aligned.  One copy in,
+// the kind passes on a grid sized to the batch, one copy out, the outputs unpacked on the host.
+static int run_small(bzr_scene *s, size_t n, const double *org, const double *dir,
+                     const double *tmin, const double *tmax, double *t, double *uv, double *normal,
+                     uint32_t *prim, uint32_t *geom, uint8_t *hit, int mode, bzr::RayIO io,
+                     uint32_t *counters, unsigned long long *totals) {
+  struct Piece {
+    size_t bytes, off;
+  };
+  size_t total = 0;
+  auto place = [&](size_t bytes) {
+    const Piece p{bytes, total};
+    total += align_up(bytes ? bytes : 0, 256);
+    return p;
+  };
+  const Piece p_org = place(24 * n), p_dir = place(24 * n), p_tmin = place(tmin ? 8 * n : 0),
+              p_tmax = place(tmax ? 8 * n : 0), p_err = place(sizeof(uint32_t));
+  const size_t in_bytes = total;
+  const Piece p_t = place(8 * n), p_uv = place(uv ? 16 * n : 0), p_n = place(normal ? 24 * n : 0),
+              p_prim = place(prim ? 4 * n : 0), p_geom = place(geom ? 4 * n : 0),
+              p_hit = place(hit ? n : 0);
+  const size_t out_begin = p_t.off, out_bytes = total - out_begin;
+  // the block for kSmallBatch rays with every piece bounds what any small batch needs
+  const size_t cap = 8 * align_up(24 * kSmallBatch, 256) + 256;
+  if (!s->small_pin && cudaMallocHost(&s->small_pin, cap) != cudaSuccess) {
+    s->small_pin = nullptr;
+    return fail(BZR_ENOMEM, "pinned staging allocation failed");
+  }
+  if (s->stage_bytes < cap) {
+    cudaFree(s->stage_dev);
+    s->stage_dev = nullptr;
+    s->stage_bytes = 0;
+    if (cudaMalloc(&s->stage_dev, cap) != cudaSuccess)
+      return fail(BZR_ENOMEM, "staging allocation failed");
+    s->stage_bytes = cap;
+  }
+  unsigned char *h = s->small_pin;
+  auto *d = static_cast<unsigned char *>(s->stage_dev);
+  std::memcpy(h + p_org.off, org, p_org.bytes);
+  std::memcpy(h + p_dir.off, dir, p_dir.bytes);
+  if (tmin) std::memcpy(h + p_tmin.off, tmin, p_tmin.bytes);
+  if (tmax) std::memcpy(h + p_tmax.off, tmax, p_tmax.bytes);
+  std::memset(h + p_err.off, 0, sizeof(uint32_t));
+  cudaStream_t st = s->streams[0];
+  bzr::RayIO ci = io;
+  ci.org = reinterpret_cast<const double *>(d + p_org.off);
+  ci.dir = reinterpret_cast<const double *>(d + p_dir.off);
+  ci.tmin = tmin ? reinterpret_cast<const double *>(d + p_tmin.off) : nullptr;
+  ci.tmax = tmax ? reinterpret_cast<const double *>(d + p_tmax.off) : nullptr;
+  ci.error_word = reinterpret_cast<uint32_t *>(d + p_err.off);
+  ci.t = reinterpret_cast<double *>(d + p_t.off);
+  ci.uv = uv ? reinterpret_cast<double *>(d + p_uv.off) : nullptr;
+  ci.normal = normal ? reinterpret_cast<double *>(d + p_n.off) : nullptr;
+  ci.prim = prim ? reinterpret_cast<uint32_t *>(d + p_prim.off) : nullptr;
+  ci.geom = geom ? reinterpret_cast<uint32_t *>(d + p_geom.off) : nullptr;
+  ci.hit = hit ? reinterpret_cast<uint8_t *>(d + p_hit.off) : nullptr;
+  bzr::LaunchPlan plan = s->plan;
+  const int need_blocks = static_cast<int>((n + plan.threads - 1) / plan.threads);
+  for (int k = 0; k < bzr::kNumKinds; ++k) {
+    plan.blocks[k] = std::max(1, std::min(plan.blocks[k], need_blocks));
+    plan.blocks32[k] = std::max(1, std::min(plan.blocks32[k], need_blocks));
+  }
+  cudaError_t e = cudaMemcpyAsync(d, h, in_bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = bzr::launch_trace(s->view, ci, mode, plan, st, counters, totals);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h + out_begin, d + out_begin, out_bytes, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h + p_err.off, d + p_err.off, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess) return cuda_fail(e, "small batch submission");
+  const int rc = wait_stream_spin(st, 2000);
+  if (rc) return rc;
+  if (t) std::memcpy(t, h + p_t.off, p_t.bytes);
+  if (uv) std::memcpy(uv, h + p_uv.off, p_uv.bytes);
+  if (normal) std::memcpy(normal, h + p_n.off, p_n.bytes);
+  if (prim) std::memcpy(prim, h + p_prim.off, p_prim.bytes);
+  if (geom) std::memcpy(geom, h + p_geom.off, p_geom.bytes);
+  if (hit) std::memcpy(hit, h + p_hit.off, p_hit.bytes);
+  uint32_t bits = 0;
+  std::memcpy(&bits, h + p_err.off, sizeof bits);
+  if (bits)
+    return fail(BZR_EDEVICE_FLAG, "kernel bounds check fired (error bits " +
+                                      std::to_string(bits) + ")");
+  return BZR_OK;
+}
+
 // Shared body of bzr_intersectN and bzr_work_counts; totals (device) selects the counting
 // kernel.
 static int run_batch(const bzr_scene *cs, size_t n, const double *org, const double *dir,
@@ -491,6 +595,9 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&s->copy_out, cudaStreamNonBlocking);
     if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamCreate");
   }
+  if (n <= kSmallBatch)
+    return run_small(s, n, org, dir, tmin, tmax, t, uv, normal, prim, geom, hit, mode, io,
+                     counters, totals);
   // every staged array starts on a 256-byte boundary (see take() below)
   const size_t piece_bytes[10] = {24 * n, 24 * n, tmin ? 8 * n : 0, tmax ? 8 * n : 0,
                                   8 * n, uv ? 16 * n : 0, normal ? 24 * n : 0,

@@ -244,3 +244,35 @@ def test_heightfield_full_size(mode, heightfield_ref):
     torch.cuda.synchronize()
     s.check()
     assert mismatches(out, ref) == []
+
+
+def test_small_host_batches():
+    """Host-array batches of up to 4,096 rays take the latency path (one packed copy each way,
+    a grid sized to the batch): every output subset, with and without tmin / tmax, at the
+    boundary sizes, against the oracle."""
+    wl = W.mixed_primitives(n_rays=5000, seed=13)
+    R = wl.rays
+    s = product_scene(wl.scene)
+    ora = Oracle(wl.scene)
+    for n in (1, 2, 31, 4095, 4096, 4097):
+        o, d = R.origins[:n], R.directions[:n]
+        tmin = np.where(np.arange(n) % 3 == 0, 0.5, 0.0)
+        tmax = np.where(np.arange(n) % 5 == 0, 60.0, np.inf)
+        for lo, hi in ((None, None), (tmin, tmax)):
+            ref = ora.intersect(o, d, lo, hi)
+            assert mismatches(s.intersectN(o, d, lo, hi), ref) == [], (n, lo is None)
+    # partial outputs: only the keys given are written
+    import ctypes as C
+
+    n = 100
+    o, d = np.ascontiguousarray(R.origins[:n]), np.ascontiguousarray(R.directions[:n])
+    ref = ora.intersect(o, d)
+    t = np.full(n, -1.0)
+    prim = np.zeros(n, np.uint32)
+    lib = s._lib
+    rc = lib.bzr_intersectN(s._h, n, o.ctypes.data, d.ctypes.data, None, None, t.ctypes.data,
+                            None, None, prim.ctypes.data, None, None, 0, None)
+    assert rc == 0
+    hit = ref["hit"].astype(bool)
+    assert np.array_equal(prim[hit], ref["prim"][hit])
+    assert np.array_equal(t.view(np.uint64), np.asarray(ref["t"]).view(np.uint64))
