@@ -356,6 +356,7 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
     v.verts = reinterpret_cast<const double *>(base + off_tv[k]);
     v.n_internal = img[k].n_internal;
     v.n_prims = static_cast<uint32_t>(img[k].prim_ids.size());
+    v.n_verts = static_cast<uint32_t>(img[k].verts.size() / bzr::kVertexDoubles);
     v.root_ref = img[k].root_ref;
     v.mixed_ok = img[k].mixed_ok ? 1 : 0;
     std::memcpy(v.root_box, img[k].root_box, sizeof v.root_box);

@@ -60,6 +60,7 @@ struct KindView {
   const uint32_t *pos_of = nullptr;    // n_prims: leaf-ordered position of each primitive id
   uint32_t n_internal = 0;
   uint32_t n_prims = 0;
+  uint32_t n_verts = 0;             // triangles: entries of verts
   uint32_t root_ref = 0;
   uint32_t geom_id = 0xFFFFFFFFu;
   int present = 0;

@@ -63,6 +63,38 @@ __device__ __forceinline__ void init_stack(Stack &sk, uint32_t &tid, uint32_t ca
   }
 }
 
+// Cold start: between batches the scene may have left L2 (other work, or the benchmark's L2
+// flush), and then every dependent node fetch of the first rays waits for DRAM.  The grid
+// first asks L2 for the breadth-first prefix of the node array (the top levels every ray
+// visits) and for the leaf-ordered primitive data, at most kPrefetchBytes of each, one
+// 128-byte line per thread per round.  A hint only: nothing waits for it.
+constexpr size_t kPrefetchBytes = size_t(4) << 20;
+
+__device__ __forceinline__ void prefetch_l2(const void *base, size_t bytes) {
+  if (!base) return;
+  bytes = bytes < kPrefetchBytes ? bytes : kPrefetchBytes;
+  const size_t step = size_t(gridDim.x) * blockDim.x * 128;
+  for (size_t off = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) * 128; off < bytes;
+       off += step)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const char *>(base) + off));
+}
+
+template <int KIND, bool MIXED>
+__device__ __forceinline__ void prefetch_kind(const KindView &K) {
+  if (MIXED)
+    prefetch_l2(K.nodes32, size_t(K.n_internal) * kNode32Floats * sizeof(float));
+  else
+    prefetch_l2(K.nodes64, size_t(K.n_internal) * kNode64Doubles * sizeof(double));
+  if (KIND == kMesh) {
+    prefetch_l2(K.tri, size_t(K.n_prims) * 4 * sizeof(uint32_t));
+    prefetch_l2(K.verts, size_t(K.n_verts) * kVertexDoubles * sizeof(double));
+  } else {
+    constexpr int kDoubles = KIND == kSpheres ? 4 : KIND == kPlanes ? 14 : 16;
+    prefetch_l2(K.payload, size_t(K.n_prims) * kDoubles * sizeof(double));
+    prefetch_l2(K.prim_ids, size_t(K.n_prims) * sizeof(uint32_t));
+  }
+}
+
 // One kind over the whole batch.  first: this pass writes the whole output record.
 // COUNT: also sums the work counters into totals[8] (box tests per kind, then primitive
 // tests per kind).
@@ -77,6 +109,7 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
   uint32_t tid;
   init_stack<LOCAL>(sk, tid, S.stack_cap, smem, lkey, lref);
   const KindView &K = S.k[KIND];
+  if (!COUNT) prefetch_kind<KIND, MIXED>(K);
   const unsigned lane = threadIdx.x & 31u;
   const unsigned below = (1u << lane) - 1u;
   uint32_t pool_next = 0, pool_end = 0;  // warp-uniform

@@ -44,6 +44,7 @@ static void commit(Emu *e, bool build) {
     v.verts = im.verts.data();
     v.n_internal = im.n_internal;
     v.n_prims = static_cast<uint32_t>(im.prim_ids.size());
+    v.n_verts = static_cast<uint32_t>(im.verts.size() / bzr::kVertexDoubles);
     v.root_ref = im.root_ref;
     v.mixed_ok = im.mixed_ok;
     std::memcpy(v.root_box, im.root_box, sizeof v.root_box);
