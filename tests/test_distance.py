@@ -129,3 +129,61 @@ def test_bad_primitive_id_gives_nan_and_the_error_bit():
     err = emu._lib.emu_distance_to_surface(emu._h, 1, 2, _ptr(ids, _u32p), _ptr(pts, _dp),
                                            _ptr(out, _dp), None)
     assert out[0] == 1.0 and np.isnan(out[1]) and err == 4
+
+
+def same_or_both_nan(a, b):
+    """Bit-identical, or NaN on both sides (the default NaN's sign differs between x86 and the
+    GPU)."""
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    nan = np.isnan(a) & np.isnan(b)
+    return bool(np.array_equal(np.isnan(a), np.isnan(b))) and bits_equal(a[~nan], b[~nan])
+
+
+def degenerate_scene():
+    """Primitives at the edges of the reference's formulas: zero semi-axes and heights,
+    flat and huge cylinders, zero-size and rotated planes, collinear and repeated-vertex
+    triangles, a zero-radius sphere, coordinates of 1e150."""
+    rot = W.rotation_to(np.array([[0, 0, 1.0], [1.0, 0, 0], [0, 1.0, 1.0], [1, 2, 3.0],
+                                  [0, 0, 1.0], [0, 0, 1.0]]))
+    cyl = dict(c=np.array([[0, 0, 0], [5, 0, 0], [0, 5, 0], [1e150, 0, 0], [0, 0, 5], [9, 9, 9.0]]),
+               a=np.array([0.0, 1.0, 0.5, 2.0, 1.0, 0.0]), b=np.array([0.0, 1.0, 2.0, 2.0, 1e-300, 1.0]),
+               h=np.array([2.0, 0.0, 1.0, 3.0, 1.0, 0.0]))
+    v = np.array([[0, 0, 0], [1, 1, 1], [2, 2, 2], [0, 0, 0], [1, 0, 0], [0, 1, 0.0],
+                  [1e150, 0, 0], [1e150, 1e150, 0], [0, 0, 1e150]])
+    f = np.array([[0, 1, 2], [0, 0, 0], [3, 4, 5], [6, 7, 8], [3, 3, 4]], np.uint32)
+    return (W.SceneSpec().add_mesh(v, f)
+            .add_spheres(np.array([[0, 0, 0], [1e150, 1e150, 1e150], [3, 3, 3.0]]), np.array([0.0, 1.0, 1e-200]))
+            .add_planes(np.array([[0, 0, 0], [2, 2, 2], [1e150, 0, 0.0]]), np.array([0.0, 1.0, 1e150]),
+                        np.array([0.0, 2.0, 3.0]), W.rotation_to(np.array([[0, 0, 1.0], [1, 1, 1.0], [0, 1.0, 0]])))
+            .add_cylinders(cyl["c"], cyl["a"], cyl["b"], cyl["h"], rot))
+
+
+def _degenerate_points(spec, kind, rng):
+    col = getattr(spec, kind)
+    n = len(col["faces"]) if kind == "mesh" else len(col["centers"])
+    special = np.array([[0, 0, 0], [0, 0, 1], [0, 0, -1], [1, 0, 0], [0, 1, 0], [0.5, 0.5, 0.5],
+                        [1e150, 0, 0], [-1e150, 1e150, 0], [5, 0, 0], [5, 0, 1e-300], [9, 9, 9.0],
+                        [np.inf, 0, 0], [0, np.nan, 0], [0, 0, 5.5]])
+    ids = np.repeat(np.arange(n, dtype=np.uint32), len(special))
+    pts = np.tile(special, (n, 1))
+    more_ids, more_pts = distance_queries(spec, kind, rng, 400)
+    return np.concatenate([ids, more_ids]), np.concatenate([pts, more_pts])
+
+
+def test_degenerate_primitives_and_points():
+    spec = degenerate_scene()
+    rng = np.random.default_rng(17)
+    ora, ref, emu = Oracle(spec), RefScene(spec), EmuScene(spec)
+    for kind in spec.order:
+        ids, pts = _degenerate_points(spec, kind, rng)
+        a, ac = ora.distance_to_surface(kind, ids, pts)
+        b, bc = ref.distance_to_surface(kind, ids, pts)
+        c, cc = emu.distance_to_surface(kind, ids, pts)
+        assert same_or_both_nan(a, b), kind
+        assert same_or_both_nan(c, b), kind
+        if kind == "mesh":
+            assert same_or_both_nan(ac, bc) and same_or_both_nan(cc, bc)
+    pts = np.concatenate([_degenerate_points(spec, k, rng)[1] for k in spec.order])
+    want, got = Oracle(spec).closest_surface(pts), emu.closest_surface(pts)
+    assert same_or_both_nan(got["distance"], want["distance"])
+    assert np.array_equal(got["prim"], want["prim"]) and np.array_equal(got["geom"], want["geom"])

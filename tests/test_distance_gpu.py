@@ -113,3 +113,28 @@ def test_closest_surface_large_batch_is_sorted_and_exact():
     want = EmuScene(wl.scene).closest_surface(pts)
     assert bits_equal(got["distance"], want["distance"])
     assert np.array_equal(got["prim"], want["prim"]) and np.array_equal(got["geom"], want["geom"])
+
+
+def test_degenerate_primitives_and_points_on_the_gpu():
+    """The degenerate scene and points of the CPU test through the product: bit for bit, NaN
+    where the oracle gives NaN."""
+    from tests.test_distance import _degenerate_points, degenerate_scene, same_or_both_nan
+
+    spec = degenerate_scene()
+    rng = np.random.default_rng(17)
+    s, ora = product_scene(spec), Oracle(spec)
+    all_pts = []
+    for kind in spec.order:
+        ids, pts = _degenerate_points(spec, kind, rng)
+        all_pts.append(pts)
+        want, want_c = ora.distance_to_surface(kind, ids, pts)
+        got = s.distance_to_surface(kind, ids, pts, closest=kind == "mesh")
+        if kind == "mesh":
+            got, got_c = got
+            assert same_or_both_nan(got_c, want_c)
+        assert same_or_both_nan(got, want), kind
+    pts = np.concatenate(all_pts)
+    want = ora.closest_surface(pts)
+    got = s.closest_surface(pts)
+    assert same_or_both_nan(got["distance"], want["distance"])
+    assert np.array_equal(got["prim"], want["prim"]) and np.array_equal(got["geom"], want["geom"])
