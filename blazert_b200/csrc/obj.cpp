@@ -17,6 +17,7 @@
 //
 // A face index outside the positions read when its shape ends is an error here (the reference
 // asserts, tiny_obj_loader.cc:312, which release builds skip).
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -109,6 +110,13 @@ float read_coordinate(const char *&t) {
 // 1-based, negative relative to n, 0 as the first element
 int resolve(int idx, int n) { return idx > 0 ? idx - 1 : (idx == 0 ? 0 : n + idx); }
 
+// atoi as the loader reads indices (leading blanks, sign, digits), with values outside int
+// clamped instead of atoi's undefined result; the same value for every index that fits.
+int read_int(const char *t) {
+  const long v = std::strtol(t, nullptr, 10);
+  return v > INT_MAX ? INT_MAX : (v < INT_MIN ? INT_MIN : static_cast<int>(v));
+}
+
 struct Corner {
   int v = -1, vt = -1, vn = -1;
   bool operator<(const Corner &o) const {
@@ -118,21 +126,21 @@ struct Corner {
 
 Corner read_corner(const char *&t, int nv, int nvn, int nvt) {
   Corner c;
-  c.v = resolve(std::atoi(t), nv);
+  c.v = resolve(read_int(t), nv);
   t += std::strcspn(t, "/ \t\r");
   if (t[0] != '/') return c;
   ++t;
   if (t[0] == '/') {  // i//k
     ++t;
-    c.vn = resolve(std::atoi(t), nvn);
+    c.vn = resolve(read_int(t), nvn);
     t += std::strcspn(t, "/ \t\r");
     return c;
   }
-  c.vt = resolve(std::atoi(t), nvt);  // i/j or i/j/k
+  c.vt = resolve(read_int(t), nvt);  // i/j or i/j/k
   t += std::strcspn(t, "/ \t\r");
   if (t[0] != '/') return c;
   ++t;
-  c.vn = resolve(std::atoi(t), nvn);
+  c.vn = resolve(read_int(t), nvn);
   t += std::strcspn(t, "/ \t\r");
   return c;
 }

@@ -120,3 +120,33 @@ def test_errors(tmp_path):
         B.load_obj(p)
     v, f = B.load_obj(_write(tmp_path, "empty", "# no geometry\n"))
     assert v.shape == (0, 3) and f.shape == (0, 3)
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_fuzzed_files_load_or_are_refused(tmp_path, seed):
+    """Random edits of valid files (bytes replaced, inserted, lines cut): every one either
+    loads, with faces inside the vertices, or is refused with BZR_EINVAL; never a crash.
+    Where the reference's loader accepts the same file without an out-of-range index, the
+    meshes are equal."""
+    rng = np.random.default_rng(100 + seed)
+    base = _random_obj(np.random.default_rng(seed)).encode()
+    alphabet = np.frombuffer(b"0123456789 -+./eEvfgot\\n#\\t\\r", np.uint8)
+    for k in range(60):
+        b = bytearray(base)
+        for _ in range(int(rng.integers(1, 6))):
+            at = int(rng.integers(len(b)))
+            if rng.random() < 0.5:
+                b[at] = int(alphabet[rng.integers(len(alphabet))])
+            else:
+                b[at:at] = bytes(alphabet[rng.integers(0, len(alphabet), int(rng.integers(1, 8)))])
+        p = tmp_path / f"f{k}.obj"
+        p.write_bytes(bytes(b))
+        try:
+            v, f = B.load_obj(p)
+        except B.BlazertError as e:
+            assert e.code == B.EINVAL
+            continue
+        assert f.size == 0 or int(f.max()) < len(v)
+        if HAVE_REF:
+            rv, rf = ref_load_obj(p)
+            assert np.array_equal(v.view(np.uint64), rv.view(np.uint64)) and np.array_equal(f, rf)

@@ -127,3 +127,40 @@ def test_inconsistent_trees_are_refused():
     struct.pack_into("<I", mb, at, len(v) + 5)
     with pytest.raises(ValueError, match="face index"):
         EmuScene.decode(reseal(bytes(mb)))
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_fuzzed_files_are_refused_or_safe(seed):
+    """Random byte changes, insertions and cuts, with the checksum recomputed so that the
+    parser goes past it: every result is a refusal with a reason or a scene whose trees passed
+    the checks and that traces rays without a bounds error."""
+    rng = np.random.default_rng(seed)
+    wl = W.mixed_primitives(n_rays=64, n_spheres=40, n_cylinders=12, n_planes=6, seed=seed)
+    spec = W.SceneSpec()
+    spec.add_mesh(*W.icosphere(1))
+    for kind in wl.scene.order:
+        getattr(spec, "add_" + kind)(*getattr(wl.scene, kind).values())
+    body = EmuScene(spec, min_leaf=2).encode()[:-8]
+    refused = loaded = 0
+    for _ in range(150):
+        b = bytearray(body)
+        op = rng.integers(3)
+        if op == 0:
+            for _ in range(int(rng.integers(1, 4))):
+                b[int(rng.integers(len(b)))] = int(rng.integers(256))
+        elif op == 1:
+            at = int(rng.integers(len(b)))
+            b[at:at] = bytes(rng.integers(0, 256, int(rng.integers(1, 16)), dtype=np.uint8))
+        else:
+            del b[int(rng.integers(len(b))):]
+        try:
+            s = EmuScene.decode(reseal(bytes(b)))
+        except ValueError as e:
+            assert str(e)
+            refused += 1
+            continue
+        loaded += 1
+        R = wl.rays
+        out = s.intersect(R.origins, R.directions)
+        assert out["error_word"] == 0
+    assert refused > 0
