@@ -18,14 +18,17 @@ namespace {
 constexpr int kDistanceThreads = 256;
 constexpr uint32_t kNearestStack = 64;
 
+// One kind per instantiation, so that each kind's pass carries only its own code (registers,
+// occupancy): spheres and planes are a gather and a few flops per query.
+template <int KIND>
 __global__ void __launch_bounds__(kDistanceThreads)
-    distance_kernel(const SceneView S, const int kind, const DistanceIO io) {
+    distance_kernel(const SceneView S, const DistanceIO io) {
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < io.n; i += stride) {
     const D3 p = d3(io.points[3 * i], io.points[3 * i + 1], io.points[3 * i + 2]);
     D3 c;
     bool bad = false;
-    io.distance[i] = distance_query(S, kind, io.ids[i], p, &c, &bad);
+    io.distance[i] = distance_query(S, KIND, io.ids[i], p, &c, &bad);
     if (io.closest) {
       io.closest[3 * i] = c.x;
       io.closest[3 * i + 1] = c.y;
@@ -135,10 +138,21 @@ int grid_of(uint64_t n, int sms, int per_sm) {
 cudaError_t launch_distance(const SceneView &S, int kind, const DistanceIO &io, int sms,
                             cudaStream_t stream) {
   if (io.n == 0) return cudaSuccess;
-  if (kind == kCylinders)
-    cylinder_distance_kernel<<<grid_of(io.n, sms, 8), kDistanceThreads, 0, stream>>>(S, io);
-  else
-    distance_kernel<<<grid_of(io.n, sms, 8), kDistanceThreads, 0, stream>>>(S, kind, io);
+  const int grid = grid_of(io.n, sms, 8);
+  switch (kind) {
+    case kMesh:
+      distance_kernel<kMesh><<<grid, kDistanceThreads, 0, stream>>>(S, io);
+      break;
+    case kSpheres:
+      distance_kernel<kSpheres><<<grid, kDistanceThreads, 0, stream>>>(S, io);
+      break;
+    case kPlanes:
+      distance_kernel<kPlanes><<<grid, kDistanceThreads, 0, stream>>>(S, io);
+      break;
+    default:
+      cylinder_distance_kernel<<<grid, kDistanceThreads, 0, stream>>>(S, io);
+      break;
+  }
   return cudaGetLastError();
 }
 
