@@ -4,7 +4,8 @@
 //
 // Types mirror the reference's aliases (blazert/datatypes.h:31-59) with standard containers:
 // Vec3r<T> = std::array<T, 3>, Vec3rList<T> = std::vector<Vec3r<T>>, Mat3r<T> a row-major 3x3
-// with nested-brace construction.  Only T = double is supported (the GPU path is FP64).
+// with nested-brace construction.  T = double is the reference's double path bit for bit;
+// T = float widens to it (see Scene).
 #pragma once
 
 #include <array>
@@ -98,10 +99,14 @@ inline void check(int rc) {
   if (rc != BZR_OK) throw Error(rc, bzr_last_error_string());
 }
 
-// blazert/scene.h:38-115
+// blazert/scene.h:38-115.  Scene<double> is the reference's double path, bit for bit.
+// Scene<float> accepts the reference's float call sites and answers with the double-precision
+// query of the widened geometry and rays, rounded to float (not the reference's float BVH and
+// traversal, which this build does not reproduce).
 template <typename T>
 class Scene {
-  static_assert(std::is_same<T, double>::value, "blazert_b200 scenes are double precision");
+  static_assert(std::is_same<T, double>::value || std::is_same<T, float>::value,
+                "Scene<double> or Scene<float>");
 
  public:
   BVHBuildOptions<T> build_options;
@@ -113,21 +118,28 @@ class Scene {
 
   // Each returns the geom id, or static_cast<unsigned>(-1) for a second add of a kind or an
   // add after commit (as the reference does); other errors throw blazert_b200::Error.
-  unsigned int add_mesh(const Vec3rList<T> &vertices, const Vec3iList &triangles) {
+  unsigned int add_mesh(const Vec3rList<T> &vertices_in, const Vec3iList &triangles) {
+    const auto &vertices = wide(vertices_in);
     uint32_t id = 0;
     const int rc = bzr_add_mesh(s_, flat(vertices), vertices.size(),
                                 reinterpret_cast<const uint32_t *>(triangles.data()),
                                 triangles.size(), &id);
     return added(rc, id);
   }
-  unsigned int add_spheres(const Vec3rList<T> &centers, const std::vector<T> &radii) {
+  unsigned int add_spheres(const Vec3rList<T> &centers_in, const std::vector<T> &radii_in) {
+    const auto &centers = wide(centers_in);
+    const auto &radii = wide(radii_in);
     uint32_t id = 0;
     if (centers.size() != radii.size()) throw Error(BZR_EINVAL, "centers and radii differ");
     const int rc = bzr_add_spheres(s_, flat(centers), radii.data(), radii.size(), &id);
     return added(rc, id);
   }
-  unsigned int add_planes(const Vec3rList<T> &centers, const std::vector<T> &dxs,
-                          const std::vector<T> &dys, const Mat3rList<T> &rotations) {
+  unsigned int add_planes(const Vec3rList<T> &centers_in, const std::vector<T> &dxs_in,
+                          const std::vector<T> &dys_in, const Mat3rList<T> &rotations_in) {
+    const auto &centers = wide(centers_in);
+    const auto &dxs = wide(dxs_in);
+    const auto &dys = wide(dys_in);
+    const auto &rotations = wide(rotations_in);
     uint32_t id = 0;
     const size_t n = centers.size();
     if (dxs.size() != n || dys.size() != n || rotations.size() != n)
@@ -136,9 +148,14 @@ class Scene {
         bzr_add_planes(s_, flat(centers), dxs.data(), dys.data(), flat(rotations), n, &id);
     return added(rc, id);
   }
-  unsigned int add_cylinders(const Vec3rList<T> &centers, const std::vector<T> &semi_axes_a,
-                             const std::vector<T> &semi_axes_b, const std::vector<T> &heights,
-                             const Mat3rList<T> &rotations) {
+  unsigned int add_cylinders(const Vec3rList<T> &centers_in, const std::vector<T> &a_in,
+                             const std::vector<T> &b_in, const std::vector<T> &heights_in,
+                             const Mat3rList<T> &rotations_in) {
+    const auto &centers = wide(centers_in);
+    const auto &semi_axes_a = wide(a_in);
+    const auto &semi_axes_b = wide(b_in);
+    const auto &heights = wide(heights_in);
+    const auto &rotations = wide(rotations_in);
     uint32_t id = 0;
     const size_t n = centers.size();
     if (semi_axes_a.size() != n || semi_axes_b.size() != n || heights.size() != n ||
@@ -156,24 +173,26 @@ class Scene {
     return true;
   }
 
-  // Batched query, structure of arrays (see bzr_intersectN_ex); returns nothing, fills
-  // outputs.  ray_flags: 0 or BZR_RAY_ANY_HIT for every ray.
-  void intersectN(size_t n, const T *origins, const T *directions, const T *tmin,
-                  const T *tmax, T *hit_distance, T *uv, T *normal, uint32_t *prim_id,
-                  uint32_t *geom_id, uint8_t *hit, int mode = BZR_MODE_FP64,
-                  void *stream = nullptr, uint32_t ray_flags = 0) const {
+  // Batched query, structure of arrays of doubles (see bzr_intersectN_ex); returns nothing,
+  // fills outputs.  ray_flags: 0 or BZR_RAY_ANY_HIT for every ray.
+  void intersectN(size_t n, const double *origins, const double *directions,
+                  const double *tmin, const double *tmax, double *hit_distance, double *uv,
+                  double *normal, uint32_t *prim_id, uint32_t *geom_id, uint8_t *hit,
+                  int mode = BZR_MODE_FP64, void *stream = nullptr,
+                  uint32_t ray_flags = 0) const {
     check(bzr_intersectN_ex(s_, n, origins, directions, tmin, tmax, hit_distance, uv, normal,
                             prim_id, geom_id, hit, mode, ray_flags, stream));
   }
 
   // Distances (bzr_distance_to_surface): kind 0 triangles, 1 spheres, 2 planes, 3 cylinders;
   // closest (triangles only) may be null.
-  void distance_to_surface(int kind, size_t n, const uint32_t *prim_ids, const T *points,
-                           T *distance, T *closest = nullptr, void *stream = nullptr) const {
+  void distance_to_surface(int kind, size_t n, const uint32_t *prim_ids, const double *points,
+                           double *distance, double *closest = nullptr,
+                           void *stream = nullptr) const {
     check(bzr_distance_to_surface(s_, kind, n, prim_ids, points, distance, closest, stream));
   }
   // Nearest surface of the scene per point (bzr_closest_surface).
-  void closest_surface(size_t n, const T *points, T *distance, uint32_t *prim_id,
+  void closest_surface(size_t n, const double *points, double *distance, uint32_t *prim_id,
                        uint32_t *geom_id, void *stream = nullptr) const {
     check(bzr_closest_surface(s_, n, points, distance, prim_id, geom_id, stream));
   }
@@ -192,9 +211,28 @@ class Scene {
  private:
   explicit Scene(bzr_scene *h) : s_(h) {}
   template <typename V>
-  static const T *flat(const std::vector<V> &v) {
-    static_assert(sizeof(V) % sizeof(T) == 0, "contiguous scalar storage");
-    return reinterpret_cast<const T *>(v.data());
+  static const double *flat(const std::vector<V> &v) {
+    static_assert(sizeof(V) % sizeof(double) == 0, "contiguous double storage");
+    return reinterpret_cast<const double *>(v.data());
+  }
+  // double inputs pass through; float inputs are widened
+  static const Vec3rList<double> &wide(const Vec3rList<double> &v) { return v; }
+  static const std::vector<double> &wide(const std::vector<double> &v) { return v; }
+  static const Mat3rList<double> &wide(const Mat3rList<double> &v) { return v; }
+  static Vec3rList<double> wide(const Vec3rList<float> &v) {
+    Vec3rList<double> r(v.size());
+    for (size_t i = 0; i < v.size(); ++i) r[i] = {v[i][0], v[i][1], v[i][2]};
+    return r;
+  }
+  static std::vector<double> wide(const std::vector<float> &v) {
+    return std::vector<double>(v.begin(), v.end());
+  }
+  static Mat3rList<double> wide(const Mat3rList<float> &v) {
+    Mat3rList<double> r(v.size());
+    for (size_t i = 0; i < v.size(); ++i)
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) r[i](a, b) = v[i](a, b);
+    return r;
   }
   static unsigned int added(int rc, uint32_t id) {
     if (rc == BZR_ESTATE) return static_cast<unsigned int>(-1);
@@ -212,12 +250,14 @@ inline bool intersect1(const Scene<T> &scene, const Ray<T> &ray, RayHit<T> &rayh
   bzr_rayhit rh;
   int hit = 0;
   const uint32_t flags = ray.any_hit == Ray<T>::AnyHit::yes ? BZR_RAY_ANY_HIT : 0u;
-  check(bzr_intersect1_ex(scene.handle(), ray.origin.data(), ray.direction.data(),
-                          ray.min_hit_distance, ray.max_hit_distance, flags, &rh, &hit));
+  const double o[3] = {ray.origin[0], ray.origin[1], ray.origin[2]};
+  const double d[3] = {ray.direction[0], ray.direction[1], ray.direction[2]};
+  check(bzr_intersect1_ex(scene.handle(), o, d, ray.min_hit_distance, ray.max_hit_distance,
+                          flags, &rh, &hit));
   if (hit) {
-    rayhit.normal = {rh.normal[0], rh.normal[1], rh.normal[2]};
-    rayhit.uv = {rh.uv[0], rh.uv[1]};
-    rayhit.hit_distance = rh.hit_distance;
+    rayhit.normal = {T(rh.normal[0]), T(rh.normal[1]), T(rh.normal[2])};
+    rayhit.uv = {T(rh.uv[0]), T(rh.uv[1])};
+    rayhit.hit_distance = T(rh.hit_distance);
     rayhit.prim_id = rh.prim_id;
     rayhit.geom_id = rh.geom_id;
   }

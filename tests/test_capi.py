@@ -113,6 +113,8 @@ int main(int argc, char **argv) {
   const unsigned a = fs.add_spheres(Vec3rList<float>{{0.f, 0.f, 0.f}, {3.f, 0.f, 0.f}}, {1.f, 0.5f});
   const unsigned b = ds.add_spheres(Vec3rList<double>{{0.0, 0.0, 0.0}, {3.0, 0.0, 0.0}}, {1.0, 0.5});
   if (a != 0 || b != 0) return 1;
+  Scene<float> sf;  // the reference's float call sites (blazert::Scene<float>)
+  if (sf.add_spheres(Vec3rList<float>{{0.f, 0.f, 0.f}}, {1.f}) != 0) return 1;
   if (argc > 1) {  // needs a GPU; argv[1]: a scene file to write
     fs.commit();
     ds.commit();
@@ -130,8 +132,12 @@ int main(int argc, char **argv) {
     auto loaded = Scene<double>::load(argv[1]);
     RayHit<double> h3;
     const bool h3hit = intersect1(*loaded, rd, h3);
-    std::printf("%d %u %.9g %d %u %.17g %.17g %.17g %d %.17g\n", h1, hf.prim_id, hf.hit_distance,
-                h2, hd.prim_id, hd.hit_distance, dist[0], dist[1], h3hit, h3.hit_distance);
+    sf.commit();
+    RayHit<float> hs;
+    const bool h4 = intersect1(sf, Ray<float>{{0.f, 0.f, 5.f}, {0.f, 0.f, -1.f}}, hs);
+    std::printf("%d %u %.9g %d %u %.17g %.17g %.17g %d %.17g %d %.9g\n", h1, hf.prim_id,
+                hf.hit_distance, h2, hd.prim_id, hd.hit_distance, dist[0], dist[1], h3hit,
+                h3.hit_distance, h4, hs.hit_distance);
   }
   return 0;
 }

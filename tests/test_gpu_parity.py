@@ -150,6 +150,7 @@ def test_embree_facade_runs_on_gpu(tmp_path):
     assert f[3] == "1" and f[4] == "1" and float(f[5]) == 4.5
     assert float(f[6]) == 2.0 and float(f[7]) == 2.5
     assert f[8] == "1" and float(f[9]) == 4.5
+    assert f[10] == "1" and float(f[11]) == 4.0  # Scene<float>: unit sphere from z = 5
 
 
 def test_intersect1_matches_batch():
