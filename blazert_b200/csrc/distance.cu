@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kDistanceThreads, 4)
 __global__ void __launch_bounds__(kDistanceThreads)
     nearest_kernel(const SceneView S, const DistanceIO io) {
   uint32_t stack_ref[kNearestStack];
-  double stack_key[kNearestStack];
+  float stack_key[kNearestStack];
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
   for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < io.n; j += stride) {
     const uint64_t i = io.perm ? io.perm[j] : j;

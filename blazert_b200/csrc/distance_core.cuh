@@ -18,6 +18,8 @@
 //             (trimesh.h:183-192) cannot be instantiated: it returns a vector as a scalar and
 //             rebuilds v1, v2 from the stored edges with the wrong signs.
 #pragma once
+#include <limits>
+
 #include "trace_core.cuh"
 
 namespace bzr {
@@ -365,6 +367,18 @@ struct NearestState {
 
 BZR_HD double distance_margin(double scale, double best) { return 1e-12 * (scale + best); }
 
+// The float at or below x (the stack keeps box distances as floats: a key that is not larger
+// than the distance only lets the search visit more, never less).
+BZR_HD float float_below(double x) {
+#if defined(__CUDA_ARCH__)
+  return __double2float_rd(x);
+#else
+  float f = static_cast<float>(x);
+  if (static_cast<double>(f) > x) f = std::nextafter(f, -std::numeric_limits<float>::infinity());
+  return f;
+#endif
+}
+
 // The smallest (distance, kind, id) wins, so the order in which kinds and primitives are
 // searched does not change the result.
 BZR_HD void nearest_offer(NearestState &st, int kind, uint32_t geom, uint32_t id, double d) {
@@ -418,7 +432,7 @@ BZR_HD void nearest_all(const SceneView &S, int kind, D3 p, double scale, Neares
 // Nearest-first walk of one kind's BVH (triangles, spheres).  stack holds cap entries; a tree
 // that would need more is evaluated exhaustively instead (only trees deeper than the stack).
 BZR_HD void nearest_bvh(const SceneView &S, int kind, D3 p, double scale, NearestState &st,
-                        uint32_t *stack_ref, double *stack_key, uint32_t cap) {
+                        uint32_t *stack_ref, float *stack_key, uint32_t cap) {
   const KindView &K = S.k[kind];
   if (S.stack_cap > cap) {
     nearest_all(S, kind, p, scale, st);
@@ -443,7 +457,7 @@ BZR_HD void nearest_bvh(const SceneView &S, int kind, D3 p, double scale, Neares
       if (t0 && t1) {
         const bool first1 = d1 < d0;
         stack_ref[sp] = first1 ? meta[0] : meta[1];
-        stack_key[sp] = first1 ? d0 : d1;
+        stack_key[sp] = float_below(first1 ? d0 : d1);
         ++sp;
         ref = first1 ? meta[1] : meta[0];
         continue;
@@ -469,7 +483,7 @@ BZR_HD void nearest_bvh(const SceneView &S, int kind, D3 p, double scale, Neares
 // Search order: the smaller of the two BVH kinds first (a cheap early bound prunes the larger
 // one), then the other, then cylinders (whose skip test uses the bound) and planes.
 BZR_HD NearestState nearest_surface(const SceneView &S, D3 p, uint32_t *stack_ref,
-                                    double *stack_key, uint32_t cap) {
+                                    float *stack_key, uint32_t cap) {
   NearestState st;
   st.best = BZR_INF;
   const double ps = fmax(fmax(fabs(p.x), fabs(p.y)), fabs(p.z));

@@ -256,7 +256,7 @@ void emu_closest_surface(void *h, long n, const double *points, double *distance
                          uint32_t *geom) {
   const Emu *e = static_cast<Emu *>(h);
   uint32_t stack_ref[64];
-  double stack_key[64];
+  float stack_key[64];
   for (long i = 0; i < n; ++i) {
     const bzr::D3 p = bzr::d3(points[3 * i], points[3 * i + 1], points[3 * i + 2]);
     const bzr::NearestState st = bzr::nearest_surface(e->view, p, stack_ref, stack_key, 64);
