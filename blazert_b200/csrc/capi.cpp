@@ -427,6 +427,26 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
 
 static bool is_device_ptr(const void *p) { return bzr::is_device_pointer(p); }
 
+// The host-array pipeline's streams and events, made on the first host-array call (scenes
+// only queried with device arrays, or through a batch, never need them).  The caller holds
+// stage_mu.
+static cudaError_t make_pipeline(bzr_scene *s) {
+  if (s->copy_out) return cudaSuccess;
+  cudaError_t ce = cudaSuccess;
+  for (cudaStream_t &st : s->streams)
+    if (ce == cudaSuccess && !st) ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  for (size_t c = 0; c < kMaxChunks && ce == cudaSuccess; ++c) {
+    if (!s->ev_in[c]) ce = cudaEventCreateWithFlags(&s->ev_in[c], cudaEventDisableTiming);
+    if (ce == cudaSuccess && !s->ev_done[c])
+      ce = cudaEventCreateWithFlags(&s->ev_done[c], cudaEventDisableTiming);
+  }
+  if (ce == cudaSuccess && !s->copy_in)
+    ce = cudaStreamCreateWithFlags(&s->copy_in, cudaStreamNonBlocking);
+  // copy_out last: its presence marks the whole set as made
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&s->copy_out, cudaStreamNonBlocking);
+  return ce;
+}
+
 // Waits for a stream: spins on cudaStreamQuery for up to spin_us (a small batch finishes in
 // tens of microseconds, well inside a sleeping wait's granularity), then waits as usual.
 static int wait_stream_spin(cudaStream_t st, int spin_us) {
@@ -579,23 +599,7 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
 
   // Host arrays: stage through device buffers on the scene's stream.
   std::lock_guard<std::mutex> lock(s->stage_mu);
-  // the pipeline's streams and events are made on the first host-array call: scenes that are
-  // only queried with device arrays (or through a batch) never need them
-  if (!s->copy_out) {
-    cudaError_t ce = cudaSuccess;
-    for (cudaStream_t &st : s->streams)
-      if (ce == cudaSuccess && !st) ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    for (size_t c = 0; c < kMaxChunks && ce == cudaSuccess; ++c) {
-      if (!s->ev_in[c]) ce = cudaEventCreateWithFlags(&s->ev_in[c], cudaEventDisableTiming);
-      if (ce == cudaSuccess && !s->ev_done[c])
-        ce = cudaEventCreateWithFlags(&s->ev_done[c], cudaEventDisableTiming);
-    }
-    if (ce == cudaSuccess && !s->copy_in)
-      ce = cudaStreamCreateWithFlags(&s->copy_in, cudaStreamNonBlocking);
-    // copy_out last: its presence marks the whole set as made
-    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&s->copy_out, cudaStreamNonBlocking);
-    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamCreate");
-  }
+  if (const cudaError_t ce = make_pipeline(s)) return cuda_fail(ce, "cudaStreamCreate");
   if (n <= kSmallBatch)
     return run_small(s, n, org, dir, tmin, tmax, t, uv, normal, prim, geom, hit, mode, io,
                      counters, totals);
@@ -875,39 +879,73 @@ static int run_distance(const bzr_scene *cs, int kind, size_t n, const uint32_t 
     const cudaError_t e = launch();
     return e == cudaSuccess ? BZR_OK : cuda_fail(e, "distance launch");
   }
-  if (kind >= 0) {
-    const size_t count = s->host.kind[kind].n;
-    for (size_t i = 0; i < n; ++i)
-      if (ids[i] >= count) return fail(BZR_EINVAL, "primitive id outside the kind");
-  }
-  const size_t piece[6] = {kind >= 0 ? 4 * n : 0, 24 * n, 8 * n, closest ? 24 * n : 0,
-                           prim ? 4 * n : 0, geom ? 4 * n : 0};
-  size_t total = 0;
-  for (size_t b : piece) total += align_up(b, 256);
+  // Host arrays: the ray path's three-stage pipeline over chunks -- copies in on copy_in,
+  // each chunk's kernel on one of the scene's streams once its copies are in, copies out on
+  // copy_out once its kernel is done -- with stream-ordered staging from the scene's pool.
+  std::lock_guard<std::mutex> lock(s->stage_mu);
+  if (const cudaError_t ce = make_pipeline(s)) return cuda_fail(ce, "cudaStreamCreate");
+  // bytes per query of each staged array: ids, points | distance, closest, prim, geom
+  const size_t per[6] = {kind >= 0 ? 4u : 0u, 24, 8, closest ? 24u : 0u, prim ? 4u : 0u,
+                         geom ? 4u : 0u};
+  size_t total = 256;  // the call's own error word first (ids outside the kind)
+  for (size_t b : per) total += align_up(b * n, 256);
   char *dev = nullptr;
-  cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&dev), total, s->plan.pool, st);
+  cudaError_t e =
+      cudaMallocFromPoolAsync(reinterpret_cast<void **>(&dev), total, s->plan.pool, s->copy_in);
   if (e != cudaSuccess) return fail(BZR_ENOMEM, "distance staging allocation failed");
+  uint32_t *err = reinterpret_cast<uint32_t *>(dev);
+  e = cudaMemsetAsync(err, 0, sizeof(uint32_t), s->copy_in);
+  io.error_word = err;
+  dev += 256;
   char *at[6];
   for (size_t j = 0, off = 0; j < 6; ++j) {
-    at[j] = piece[j] ? dev + off : nullptr;
-    off += align_up(piece[j], 256);
+    at[j] = per[j] ? dev + off : nullptr;
+    off += align_up(per[j] * n, 256);
   }
-  io.ids = reinterpret_cast<const uint32_t *>(at[0]);
-  io.points = reinterpret_cast<const double *>(at[1]);
-  io.distance = reinterpret_cast<double *>(at[2]);
-  io.closest = reinterpret_cast<double *>(at[3]);
-  io.prim = reinterpret_cast<uint32_t *>(at[4]);
-  io.geom = reinterpret_cast<uint32_t *>(at[5]);
-  if (kind >= 0) e = cudaMemcpyAsync(at[0], ids, piece[0], cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(at[1], points, piece[1], cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = launch();
+  const void *ins[2] = {ids, points};
   void *outs[4] = {distance, closest, prim, geom};
-  for (int j = 0; j < 4 && e == cudaSuccess; ++j)
-    if (outs[j])
-      e = cudaMemcpyAsync(outs[j], at[2 + j], piece[2 + j], cudaMemcpyDeviceToHost, st);
-  cudaFreeAsync(dev, st);
+  const size_t chunk = std::max<size_t>(size_t(1) << 18, (n + kHostChunks - 1) / kHostChunks);
+  const size_t nchunks = (n + chunk - 1) / chunk;
+  for (size_t c = 0; c < nchunks && e == cudaSuccess; ++c) {
+    const size_t a = c * chunk, m = std::min(n, a + chunk) - a;
+    for (int j = 0; j < 2 && e == cudaSuccess; ++j)
+      if (at[j])
+        e = cudaMemcpyAsync(at[j] + per[j] * a, static_cast<const char *>(ins[j]) + per[j] * a,
+                            per[j] * m, cudaMemcpyHostToDevice, s->copy_in);
+    cudaStream_t ks = s->streams[c % kStreams];
+    if (e == cudaSuccess) e = cudaEventRecord(s->ev_in[c], s->copy_in);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ks, s->ev_in[c], 0);
+    bzr::DistanceIO ci = io;
+    ci.n = m;
+    ci.ids = at[0] ? reinterpret_cast<const uint32_t *>(at[0]) + a : nullptr;
+    ci.points = reinterpret_cast<const double *>(at[1]) + 3 * a;
+    ci.distance = reinterpret_cast<double *>(at[2]) + a;
+    ci.closest = at[3] ? reinterpret_cast<double *>(at[3]) + 3 * a : nullptr;
+    ci.prim = at[4] ? reinterpret_cast<uint32_t *>(at[4]) + a : nullptr;
+    ci.geom = at[5] ? reinterpret_cast<uint32_t *>(at[5]) + a : nullptr;
+    if (e == cudaSuccess)
+      e = kind >= 0 ? bzr::launch_distance(s->view, kind, ci, s->plan.sms, ks)
+                    : bzr::launch_nearest(s->view, ci, s->plan.sms, s->plan.pool, ks);
+    if (e == cudaSuccess) e = cudaEventRecord(s->ev_done[c], ks);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s->copy_out, s->ev_done[c], 0);
+    for (int j = 0; j < 4 && e == cudaSuccess; ++j)
+      if (outs[j])
+        e = cudaMemcpyAsync(static_cast<char *>(outs[j]) + per[2 + j] * a,
+                            at[2 + j] + per[2 + j] * a, per[2 + j] * m, cudaMemcpyDeviceToHost,
+                            s->copy_out);
+  }
+  // copy_out is ordered after every chunk's kernel, and each kernel after its copies in
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s->pinned_err, err, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                        s->copy_out);
+  cudaFreeAsync(dev - 256, s->copy_out);
   if (e != cudaSuccess) return cuda_fail(e, "distance staging");
-  return wait_stream(st, default_timeout_ms());
+  (void)st;
+  const int rc = wait_stream_spin(s->copy_out, 200);
+  if (rc) return rc;
+  if (s->pinned_err[0] & bzr::kErrPrimIndex)
+    return fail(BZR_EINVAL, "primitive id outside the kind (its distance is NaN)");
+  return BZR_OK;
 }
 
 int bzr_distance_to_surface(const bzr_scene *s, int kind, size_t n, const uint32_t *prim_ids,

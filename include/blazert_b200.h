@@ -269,8 +269,9 @@ long bzr_scene_tree(const bzr_scene *scene, int kind, double *bmin, double *bmax
  * and for triangles closest_point_on_triangle (blazert/primitives/trimesh_distance.h:177-218)
  * on the face's vertices with distance norm(closest - p); closest (n x 3, triangles only, may
  * be NULL) receives those points.  All arrays host memory (the call returns when the results
- * are written; an id outside the kind is BZR_EINVAL) or all device memory (queued on stream;
- * an id outside the kind gives NaN and sets the error word bzr_scene_check reads). */
+ * are written; an id outside the kind gives NaN there and the call returns BZR_EINVAL) or all
+ * device memory (queued on stream; an id outside the kind gives NaN and sets the error word
+ * bzr_scene_check reads). */
 int bzr_distance_to_surface(const bzr_scene *scene, int kind, size_t n, const uint32_t *prim_ids,
                             const double *points, double *distance, double *closest,
                             void *stream);

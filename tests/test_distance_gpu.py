@@ -138,3 +138,23 @@ def test_degenerate_primitives_and_points_on_the_gpu():
     got = s.closest_surface(pts)
     assert same_or_both_nan(got["distance"], want["distance"])
     assert np.array_equal(got["prim"], want["prim"]) and np.array_equal(got["geom"], want["geom"])
+
+
+def test_large_host_batches_are_pipelined_and_exact():
+    """Host-array batches above 262,144 queries run as a pipeline of chunks (copies in, kernels
+    and copies out overlapping): every chunk's results land at their own indices."""
+    from tests.emu.emu import EmuScene
+
+    wl = W.mixed_primitives(n_rays=16, seed=4)
+    s, ora = product_scene(wl.scene), Oracle(wl.scene)
+    rng = np.random.default_rng(31)
+    for kind in ("spheres", "planes"):
+        ids, pts = distance_queries(wl.scene, kind, rng, 700_000)
+        assert bits_equal(s.distance_to_surface(kind, ids, pts),
+                          ora.distance_to_surface(kind, ids, pts)[0]), kind
+    near = W.closest_surface_points(n_points=600_000)
+    s2 = product_scene(near.scene)
+    got = s2.closest_surface(near.meta["points"])
+    want = EmuScene(near.scene).closest_surface(near.meta["points"])
+    assert bits_equal(got["distance"], want["distance"])
+    assert np.array_equal(got["prim"], want["prim"]) and np.array_equal(got["geom"], want["geom"])
