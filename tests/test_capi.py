@@ -179,3 +179,50 @@ def test_cpp_facade_compiles_links_and_keeps_add_rules(tmp_path):
     subprocess.run([cxx, "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), str(src),
                     "-L", lib, "-lblazert_b200", f"-Wl,-rpath,{lib}", "-o", str(exe)], check=True)
     subprocess.run([str(exe)], check=True)
+
+
+C_APP = r"""
+#include "blazert_b200.h"
+#include <stdio.h>
+
+int main(void) {
+  bzr_scene *s = NULL;
+  uint32_t gid = 0;
+  const double c[3] = {0.0, 0.0, 0.0}, r[1] = {1.0};
+  if (bzr_scene_create(&s) != BZR_OK) return 1;
+  if (bzr_add_spheres(s, c, r, 1, &gid) != BZR_OK || gid != 0) return 2;
+  if (bzr_add_spheres(s, c, r, 1, &gid) != BZR_ESTATE || gid != BZR_INVALID_ID) return 3;
+  /* queries before commit are refused with a reason */
+  double d = 0.0;
+  const uint32_t id = 0;
+  if (bzr_distance_to_surface(s, 1, 1, &id, c, &d, NULL, NULL) != BZR_ESTATE) return 4;
+  if (bzr_scene_serialize(s, NULL, 0) != BZR_ESTATE) return 5;
+  if (bzr_last_error_string()[0] == 0) return 6;
+  bzr_scene_destroy(s);
+  return 0;
+}
+"""
+
+
+def test_c_header_compiles_as_c_and_headers_are_warning_free(tmp_path):
+    """include/blazert_b200.h is plain C (C99, -Wall -Wextra -Werror) and the C++ facade
+    headers compile without warnings; the C program runs the add and state rules without a
+    GPU."""
+    import subprocess
+
+    lib = os.path.join(ROOT, "blazert_b200", "_lib")
+    inc = os.path.join(ROOT, "include")
+    src = tmp_path / "app.c"
+    src.write_text(C_APP)
+    exe = tmp_path / "app_c"
+    subprocess.run([os.environ.get("BZR_CC", "gcc"), "-std=c99", "-Wall", "-Wextra", "-Werror",
+                    "-pedantic", "-I", inc,
+                    str(src), "-L", lib, "-lblazert_b200", f"-Wl,-rpath,{lib}", "-o", str(exe)],
+                   check=True)
+    subprocess.run([str(exe)], check=True)
+    cpp = tmp_path / "headers.cpp"
+    cpp.write_text("#include <blazert_b200/scene.hpp>\n#include <blazert_b200/embree_scene.hpp>\n"
+                   "int main() { blazert_b200::Scene<double> a; blazert_b200::Scene<float> b;"
+                   " blazert_b200::EmbreeScene<float> c; (void)a; (void)b; (void)c; return 0; }\n")
+    subprocess.run([os.environ.get("BZR_CXX", "g++"), "-std=c++17", "-Wall", "-Wextra", "-Werror",
+                    "-fsyntax-only", "-I", inc, str(cpp)], check=True)
