@@ -938,8 +938,15 @@ static int run_distance(const bzr_scene *cs, int kind, size_t n, const uint32_t 
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s->pinned_err, err, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                         s->copy_out);
+  if (e != cudaSuccess) {
+    // a chunk may have been left half submitted: nothing may still use the staging when it
+    // goes back to the pool
+    for (cudaStream_t q : {s->copy_in, s->streams[0], s->streams[1], s->streams[2], s->copy_out})
+      wait_stream(q, default_timeout_ms());
+    cudaFreeAsync(dev - 256, s->copy_out);
+    return cuda_fail(e, "distance staging");
+  }
   cudaFreeAsync(dev - 256, s->copy_out);
-  if (e != cudaSuccess) return cuda_fail(e, "distance staging");
   (void)st;
   const int rc = wait_stream_spin(s->copy_out, 200);
   if (rc) return rc;
