@@ -266,4 +266,25 @@ void emu_closest_surface(void *h, long n, const double *points, double *distance
   }
 }
 
+// The product's OBJ reader (obj.cpp), for the sanitizer run: vertices and faces into the
+// caller's arrays (when large enough); returns 0, or 1 with the reason in `why`.
+int emu_obj_load(const char *path, double *v, long vcap, uint32_t *f, long fcap, long *nv,
+                 long *nf, char *why, long why_cap) {
+  std::vector<double> vv;
+  std::vector<uint32_t> ff;
+  const std::string err = bzr::load_obj(path, &vv, &ff);
+  if (!err.empty()) {
+    if (why && why_cap > 0) {
+      std::strncpy(why, err.c_str(), static_cast<size_t>(why_cap) - 1);
+      why[why_cap - 1] = 0;
+    }
+    return 1;
+  }
+  *nv = static_cast<long>(vv.size() / 3);
+  *nf = static_cast<long>(ff.size() / 3);
+  if (v && vcap >= static_cast<long>(vv.size())) std::memcpy(v, vv.data(), vv.size() * 8);
+  if (f && fcap >= static_cast<long>(ff.size())) std::memcpy(f, ff.data(), ff.size() * 4);
+  return 0;
+}
+
 }  // extern "C"

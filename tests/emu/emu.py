@@ -17,11 +17,19 @@ KINDS = ("mesh", "spheres", "planes", "cylinders")
 _lib = None
 
 
-def build(force=False):
-    """Compiles the emulator with the host compiler (no GPU or nvcc needed)."""
+def build(force=False, out=None, flags=()):
+    """Compiles the emulator with the host compiler (no GPU or nvcc needed); `out` and `flags`
+    build a variant elsewhere (the sanitizer run)."""
     root = os.path.dirname(os.path.dirname(HERE))
     srcs = [os.path.join(HERE, "emu.cpp"), os.path.join(root, "blazert_b200", "csrc", "scene.cpp"),
-            os.path.join(root, "blazert_b200", "csrc", "scene_io.cpp")]
+            os.path.join(root, "blazert_b200", "csrc", "scene_io.cpp"),
+            os.path.join(root, "blazert_b200", "csrc", "obj.cpp")]
+    if out is not None:
+        cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+        subprocess.run([os.environ.get("BZR_CXX", "g++"), "-std=c++17", "-O1", "-g",
+                        "-ffp-contract=off", "-fPIC", "-fopenmp", "-shared", "-I", cuda_inc,
+                        *flags] + srcs + ["-o", out], check=True)
+        return out
     deps = srcs + [os.path.join(root, "blazert_b200", "csrc", f)
                    for f in ("layout.h", "scene.h", "trace_core.cuh", "distance_core.cuh")]
     if not force and os.path.exists(LIB) and all(os.path.getmtime(d) <= os.path.getmtime(LIB) for d in deps):
