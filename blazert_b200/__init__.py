@@ -108,6 +108,7 @@ def library():
                                      C.POINTER(C.c_size_t), C.POINTER(C.POINTER(C.c_uint32)),
                                      C.POINTER(C.c_size_t)]
         lib.bzr_obj_free.argtypes = [P]
+        lib.bzr_scene_build_statistics.argtypes = [P, C.c_int, P]
         lib.bzr_last_error_string.restype = C.c_char_p
         _lib = lib
     return _lib
@@ -491,6 +492,21 @@ class Scene:
             _check(self._lib.bzr_scene_tune(self._h, 4, int(bool(shared_stack))))
         if chunk is not None:
             _check(self._lib.bzr_scene_tune(self._h, 5, int(chunk)))
+
+    def build_statistics(self, kind):
+        """The reference's BVHBuildStatistics of one kind's BVH as built at commit
+        (bzr_scene_build_statistics): max_tree_depth, leaf_nodes, max_num_prims_per_leaf,
+        min_num_prims_per_leaf, branch_nodes, bad_splits, build_seconds."""
+
+        class _Stats(C.Structure):
+            _fields_ = [(n, C.c_uint32) for n in ("max_tree_depth", "leaf_nodes",
+                                                   "max_num_prims_per_leaf",
+                                                   "min_num_prims_per_leaf", "branch_nodes",
+                                                   "bad_splits")] + [("build_seconds", C.c_double)]
+
+        st = _Stats()
+        _check(self._lib.bzr_scene_build_statistics(self._h, KIND_NAMES.index(kind), C.byref(st)))
+        return {n: getattr(st, n) for n, _ in _Stats._fields_}
 
     def work_counts(self, origins, directions, tmin=None, tmax=None, stream=None):
         """Box tests and primitive tests per kind for a batch (counting kernel; see

@@ -1203,6 +1203,23 @@ long bzr_scene_tree(const bzr_scene *s, int kind, double *bmin, double *bmax, ui
   return n;
 }
 
+int bzr_scene_build_statistics(const bzr_scene *s, int kind, bzr_build_statistics *out) {
+  if (!s || !out) return fail(BZR_EINVAL, "null argument");
+  if (kind < 0 || kind >= bzr::kNumKinds) return fail(BZR_EINVAL, "bad primitive kind");
+  if (!s->host.committed) return fail(BZR_ESTATE, "scene is not committed");
+  const bzr::Collection &c = s->host.kind[kind];
+  if (!c.present) return fail(BZR_EINVAL, "the scene has no primitives of this kind");
+  const bzr::BuildStatistics st = bzr::tree_statistics(c.tree);
+  out->max_tree_depth = st.max_tree_depth;
+  out->leaf_nodes = st.leaf_nodes;
+  out->max_num_prims_per_leaf = st.max_num_prims_per_leaf;
+  out->min_num_prims_per_leaf = st.min_num_prims_per_leaf;
+  out->branch_nodes = st.branch_nodes;
+  out->bad_splits = st.bad_splits;
+  out->build_seconds = c.tree.build_seconds;
+  return BZR_OK;
+}
+
 int bzr_scene_stats(const bzr_scene *s, int kind, uint64_t *n_nodes, uint32_t *max_depth,
                     double *build_seconds) {
   if (!s || kind < 0 || kind >= bzr::kNumKinds) return fail(BZR_EINVAL, "bad argument");

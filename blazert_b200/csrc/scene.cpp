@@ -385,6 +385,22 @@ void add_cylinders(HostScene &s, const double *ctr, const double *a, const doubl
   }
 }
 
+BuildStatistics tree_statistics(const Tree &t) {
+  BuildStatistics st;
+  st.max_tree_depth = t.max_depth;
+  st.bad_splits = t.bad_splits;
+  for (const TreeNode &nd : t.nodes) {
+    if (nd.leaf == 1) {
+      ++st.leaf_nodes;
+      st.max_num_prims_per_leaf = std::max(st.max_num_prims_per_leaf, nd.prim_cnt);
+      st.min_num_prims_per_leaf = std::min(st.min_num_prims_per_leaf, nd.prim_cnt);
+    } else {
+      ++st.branch_nodes;
+    }
+  }
+  return st;
+}
+
 KindImage flatten(const HostScene &s, int kind) {
   const Collection &c = s.kind[kind];
   const Tree &t = c.tree;

@@ -42,6 +42,15 @@ struct Tree {
 
 Tree build_tree(const PrimBoxes &boxes, const BuildOptions &opt);
 
+// The reference's BVHBuildStatistics (blazert/bvh/statistics.h:11-38, filled by
+// bvh/builder.h:84-226) of a built tree: deepest node, leaf and branch counts, fewest and most
+// primitives in a leaf (UINT32_MAX / 0 without leaves), failed partition attempts.
+struct BuildStatistics {
+  uint32_t max_tree_depth = 0, leaf_nodes = 0, max_num_prims_per_leaf = 0;
+  uint32_t min_num_prims_per_leaf = 0xFFFFFFFFu, branch_nodes = 0, bad_splits = 0;
+};
+BuildStatistics tree_statistics(const Tree &t);
+
 // The same tree built on the current CUDA device (gbuild.cu): level by level, one CTA per
 // node.  Possible for finite boxes and centres, at least one primitive, min_leaf >= 1 and at
 // most 256 bins;

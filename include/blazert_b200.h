@@ -249,6 +249,22 @@ int bzr_scene_tune(bzr_scene *scene, int option, int64_t value);
 int bzr_scene_stats(const bzr_scene *scene, int kind, uint64_t *n_nodes, uint32_t *max_depth,
                     double *build_seconds);
 
+/* The reference's BVHBuildStatistics (blazert/bvh/statistics.h:11-38) of one kind's BVH
+ * (0 triangles, 1 spheres, 2 planes, 3 cylinders) as built at commit: deepest node, leaf and
+ * branch node counts, fewest and most primitives in a leaf, failed partition attempts (the
+ * reference's bad_splits, builder.h:217-221) and the build time.  The reference's
+ * Scene::commit drops these; here they are kept per kind. */
+typedef struct bzr_build_statistics {
+  uint32_t max_tree_depth;
+  uint32_t leaf_nodes;
+  uint32_t max_num_prims_per_leaf;
+  uint32_t min_num_prims_per_leaf;
+  uint32_t branch_nodes;
+  uint32_t bad_splits;
+  double build_seconds;
+} bzr_build_statistics;
+int bzr_scene_build_statistics(const bzr_scene *scene, int kind, bzr_build_statistics *out);
+
 /* Node arrays of a committed scene's BVH of one kind (0 triangles, 1 spheres, 2 planes,
  * 3 cylinders) in the reference's DFS node order (blazert/bvh/node.h:15-41): per node its box
  * (3 + 3 doubles), leaf flag, split axis, two child indices and, for leaves, its primitive

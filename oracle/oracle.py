@@ -135,6 +135,8 @@ class _Base:
 
 
 _DIST_ARGS = [C.c_void_p, C.c_int, C.c_long, _u32p, _dp, _dp, _dp]
+STAT_KEYS = ("max_tree_depth", "leaf_nodes", "max_num_prims_per_leaf", "min_num_prims_per_leaf",
+             "branch_nodes", "bad_splits")
 _NEAREST_ARGS = [C.c_void_p, C.c_long, _dp, _dp, _u32p, _u32p]
 
 
@@ -304,9 +306,18 @@ class RefScene(_Base):
                                                     _u32p, _u8p, C.c_int]
             if hasattr(lib, "ref_distance_to_surface"):
                 lib.ref_distance_to_surface.argtypes = _DIST_ARGS
+            if hasattr(lib, "ref_build_statistics"):
+                lib.ref_build_statistics.argtypes = [C.c_void_p, C.c_int, _u32p]
             RefScene._libs[flavour] = lib
         self._lib = RefScene._libs[flavour]
         super().__init__(spec, **kw)
+
+    def build_statistics(self, kind):
+        """The reference's BVHBuildStatistics of one kind (SAHBinnedBuilder::build's return)."""
+        out = np.zeros(6, np.uint32)
+        if self._lib.ref_build_statistics(self._h, KINDS.index(kind), _ptr(out, _u32p)) != 0:
+            return None
+        return dict(zip(STAT_KEYS, (int(x) for x in out)))
 
     def distance_to_surface(self, kind, ids, points):
         """The reference's own distance_to_surface (closest_point_on_triangle for meshes)."""

@@ -102,6 +102,23 @@ long dump_tree(const RefScene *s, double *bmin, double *bmax, uint32_t *leaf, ui
   return n;
 }
 
+// The reference's own BVHBuildStatistics (blazert/bvh/statistics.h:11-38) of one kind: a fresh
+// BVH over the scene's collection built by SAHBinnedBuilder with the scene's options (the
+// statistics Scene::commit drops).  out: max_tree_depth, leaf_nodes, max_num_prims_per_leaf,
+// min_num_prims_per_leaf, branch_nodes, bad_splits.  Returns -1 for an absent kind.
+template <template <typename> class C>
+int build_statistics(const RefScene *s, uint32_t *out) {
+  const BVH<double, C> *have = bvh_of<C>(s);
+  if (!have) return -1;
+  BVH<double, C> bvh(have->collection);
+  SAHBinnedBuilder builder;
+  const auto st = builder.build(bvh, s->scene->build_options);
+  const uint32_t v[6] = {st.max_tree_depth, st.leaf_nodes, st.max_num_prims_per_leaf,
+                         st.min_num_prims_per_leaf, st.branch_nodes, st.bad_splits};
+  std::memcpy(out, v, sizeof v);
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -344,6 +361,17 @@ double ref_closest_surface_timed(void *h, long n, const double *points, double *
     if (geom) geom[i] = bg;
   }
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+int ref_build_statistics(void *h, int kind, uint32_t *out) {
+  const RefScene *s = static_cast<RefScene *>(h);
+  switch (kind) {
+    case 0: return build_statistics<TriangleMesh>(s, out);
+    case 1: return build_statistics<SphereCollection>(s, out);
+    case 2: return build_statistics<PlaneCollection>(s, out);
+    case 3: return build_statistics<CylinderCollection>(s, out);
+  }
+  return -1;
 }
 
 // Traversal of ONE per-type BVH (blazert/bvh/accel.h:60-120) for n rays, as the reference's

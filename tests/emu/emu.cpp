@@ -287,4 +287,16 @@ int emu_obj_load(const char *path, double *v, long vcap, uint32_t *f, long fcap,
   return 0;
 }
 
+// The build statistics of one kind's tree (host builder): max depth, leaf nodes, max and
+// min primitives per leaf, branch nodes, bad splits.  Returns -1 for an absent kind.
+int emu_build_statistics(void *h, int kind, uint32_t *out) {
+  const bzr::Collection &c = static_cast<Emu *>(h)->host.kind[kind];
+  if (!c.present) return -1;
+  const bzr::BuildStatistics st = bzr::tree_statistics(c.tree);
+  const uint32_t v[6] = {st.max_tree_depth, st.leaf_nodes, st.max_num_prims_per_leaf,
+                         st.min_num_prims_per_leaf, st.branch_nodes, st.bad_splits};
+  std::memcpy(out, v, sizeof v);
+  return 0;
+}
+
 }  // extern "C"

@@ -54,6 +54,7 @@ def load():
                                             _dp, _u32p, _u32p, _u8p, C.c_uint32, C.c_int]
         lib.emu_prim_box.argtypes = [C.c_void_p, C.c_int, C.c_uint32, _dp, _dp, _dp]
         lib.emu_box_accept.argtypes = [_dp, _dp, _dp, _dp, C.c_double, C.c_double]
+        lib.emu_build_statistics.argtypes = [C.c_void_p, C.c_int, _u32p]
         lib.emu_scene_encode.restype = C.c_long
         lib.emu_scene_encode.argtypes = [C.c_void_p, C.c_void_p, C.c_long]
         lib.emu_scene_decode.restype = C.c_void_p
@@ -85,6 +86,16 @@ class EmuScene(_Base):
                                     _ptr(mx, _dp), _ptr(c, _dp))
         assert rc == 0
         return mn, mx, c
+
+    def build_statistics(self, kind):
+        """The host builder's statistics of one kind (tree_statistics in scene.cpp)."""
+        import numpy as np
+        from oracle.oracle import STAT_KEYS
+
+        out = np.zeros(6, np.uint32)
+        if self._lib.emu_build_statistics(self._h, KINDS.index(kind), _ptr(out, _u32p)) != 0:
+            return None
+        return dict(zip(STAT_KEYS, (int(x) for x in out)))
 
     def encode(self) -> bytes:
         """The scene in the persistent format (scene_io.cpp)."""

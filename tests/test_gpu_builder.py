@@ -105,3 +105,18 @@ def test_gpu_build_on_a_large_mesh():
     print(f"build seconds: gpu {tg:.3f} host {th:.3f}")
     # the device build ran and was kept (a rejected device tree would add the host's time)
     assert tg < th
+
+
+def test_build_statistics_through_the_c_abi():
+    """bzr_scene_build_statistics of the device-built and host-built trees equal the reference's
+    own BVHBuildStatistics (bad splits included: icosphere meshes)."""
+    for wl in (W.icosphere_pinhole(), W.batched_icospheres(n_scenes=1, seed=4, scale=0.02)[0],
+               W.mixed_primitives(n_rays=16)):
+        ref = RefScene(wl.scene)
+        for gpu in (True, False):
+            s = gpu_scene(wl.scene, gpu=gpu)
+            for kind in wl.scene.order:
+                got = s.build_statistics(kind)
+                want = ref.build_statistics(kind)
+                assert {k: got[k] for k in want} == want, (kind, gpu)
+                assert got["build_seconds"] >= 0.0

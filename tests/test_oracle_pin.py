@@ -113,3 +113,28 @@ def test_reference_stack_depth_note():
     wl = W.mixed_primitives(n_rays=50_000)
     out = Oracle(wl.scene).intersect(wl.rays.origins, wl.rays.directions, counters=True)
     assert out["stack_peak"].max() < 28
+
+
+def test_build_statistics_match_the_reference():
+    """The host builder's BVHBuildStatistics (tree_statistics over the tree bzr_commit keeps) equal
+    the reference's own SAHBinnedBuilder::build statistics on every workload scene and edge
+    case, with the default and two other option sets: depth, leaf and branch counts, primitives
+    per leaf, and bad splits (one per failed partition attempt)."""
+    from blazert_b200 import workloads as W
+    from oracle.oracle import RefScene
+    from tests.emu.emu import EmuScene
+    from tests.scenes import edge_case_scenes
+
+    specs = [W.mixed_primitives(n_rays=16, n_spheres=3000, n_cylinders=300, n_planes=30).scene,
+             W.icosphere_pinhole().scene, W.adjoint_scene(n_rays=16).scene,
+             W.batched_icospheres(n_scenes=2, seed=4, scale=0.01)[1].scene]
+    specs += [spec for _, spec, _ in edge_case_scenes()]
+    saw_bad = False
+    for spec in specs:
+        for kw in (dict(), dict(min_leaf=1, max_depth=40, bins=3), dict(min_leaf=8, max_depth=6, bins=16)):
+            ref, emu = RefScene(spec, **kw), EmuScene(spec, **kw)
+            for kind in spec.order:
+                want, got = ref.build_statistics(kind), emu.build_statistics(kind)
+                assert got == want, (kind, kw, got, want)
+                saw_bad = saw_bad or want["bad_splits"] > 0
+    assert saw_bad  # the icosphere meshes exercise the bad-split fallback
