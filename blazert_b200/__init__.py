@@ -131,8 +131,17 @@ def _check(rc):
 
 
 def _f64(a, cols=None):
+    """float64, C-contiguous; with cols, n x cols.  Accepts flat arrays (a multiple of cols
+    values) and arrays whose rows hold cols values (n x 3 points; n x 3 x 3 or n x 9 rotations,
+    or one 3 x 3 rotation); anything else is refused rather than silently reshaped."""
     a = np.ascontiguousarray(a, dtype=np.float64)
-    return a.reshape(-1, cols) if cols else a.reshape(-1)
+    if not cols:
+        return a.reshape(-1)
+    if a.ndim >= 2 and int(np.prod(a.shape[1:])) != cols and not (cols == 9 and a.shape == (3, 3)):
+        raise ValueError(f"expected rows of {cols} values, got an array of shape {a.shape}")
+    if a.ndim <= 1 and a.size % cols:
+        raise ValueError(f"expected a multiple of {cols} values, got {a.size}")
+    return a.reshape(-1, cols)
 
 
 @dataclass

@@ -226,3 +226,26 @@ def test_c_header_compiles_as_c_and_headers_are_warning_free(tmp_path):
                    " blazert_b200::EmbreeScene<float> c; (void)a; (void)b; (void)c; return 0; }\n")
     subprocess.run([os.environ.get("BZR_CXX", "g++"), "-std=c++17", "-Wall", "-Wextra", "-Werror",
                     "-fsyntax-only", "-I", inc, str(cpp)], check=True)
+
+
+def test_python_inputs_are_checked_not_reshaped():
+    """Arrays whose rows do not hold 3 values (9 for rotations) are refused instead of being
+    silently reshaped; flat arrays and one 3 x 3 rotation are accepted; shape mismatches between
+    arrays and out-of-range faces are reported."""
+    import numpy as np
+
+    import blazert_b200 as B
+
+    with pytest.raises(ValueError):
+        B.Scene().add_spheres(np.zeros((6, 2)), np.ones(4))  # would reshape to 4 x 3
+    with pytest.raises(ValueError):
+        B.Scene().add_planes(np.zeros((2, 3)), np.ones(2), np.ones(2), np.zeros((2, 3, 2)))
+    with pytest.raises(ValueError):
+        B.Scene().add_mesh(np.zeros(7), np.zeros((1, 3), np.uint32))
+    with pytest.raises(B.BlazertError):
+        B.Scene().add_spheres(np.zeros((3, 3)), np.ones(2))
+    with pytest.raises(B.BlazertError):
+        B.Scene().add_mesh(np.zeros((4, 3)), np.array([[0, 1, 9]], np.uint32))
+    assert B.Scene().add_spheres(np.zeros(6), np.ones(2)) == 0  # flat centres
+    assert B.Scene().add_cylinders(np.zeros((1, 3)), [1.0], [1.0], [2.0], np.eye(3)) == 0
+    assert B.Scene().add_planes(np.zeros((2, 3)), [1.0, 1.0], [1.0, 1.0], np.zeros((2, 9))) == 0
