@@ -9,11 +9,13 @@
 #pragma once
 
 #include <array>
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
 #include <initializer_list>
 #include <limits>
 #include <memory>
+#include <ostream>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -80,6 +82,49 @@ struct RayHit {
   unsigned int prim_id = static_cast<unsigned int>(-1);
   unsigned int geom_id = static_cast<unsigned int>(-1);
 };
+
+// blazert/ray.h:86-120: the same field dump.  The reference's Ray keeps the normalised
+// direction, its inverse and signs from its constructor (ray.h:56-65); this Ray keeps the raw
+// direction, so they are formed here the same way for the dump.
+template <typename T>
+std::ostream &operator<<(std::ostream &stream, const Ray<T> &ray) {
+  const T len = std::sqrt((ray.direction[0] * ray.direction[0] +
+                           ray.direction[1] * ray.direction[1]) +
+                          ray.direction[2] * ray.direction[2]);
+  const T inv_len = T(1) / len;
+  stream << "{\n";
+  stream << "  Ray: " << &ray << ",\n";
+  stream << "  origin: [" << ray.origin[0] << "," << ray.origin[1] << "," << ray.origin[2]
+         << "],\n";
+  stream << "  direction: [" << ray.direction[0] * inv_len << "," << ray.direction[1] * inv_len
+         << "," << ray.direction[2] * inv_len << "],\n";
+  stream << "  direction_inv: [" << T(1) / ray.direction[0] << "," << T(1) / ray.direction[1]
+         << "," << T(1) / ray.direction[2] << "],\n";
+  stream << "  direction_sign: [" << (ray.direction[0] < T(0)) << "," << (ray.direction[1] < T(0))
+         << "," << (ray.direction[2] < T(0)) << "],\n";
+  stream << "  min_hit_distance: " << ray.min_hit_distance << ",\n";
+  stream << "  max_hit_distance " << ray.max_hit_distance << ",\n";
+  stream << "  cull_back_face "
+         << (ray.cull_back_face == Ray<T>::CullBackFace::no ? "no" : "yes") << ",\n";
+  stream << "  any_hit: " << (ray.any_hit == Ray<T>::AnyHit::no ? "no" : "yes") << "\n";
+  stream << "}\n";
+  return stream;
+}
+
+// blazert/ray.h:105-118
+template <typename T>
+std::ostream &operator<<(std::ostream &stream, const RayHit<T> &rayhit) {
+  stream << "{\n";
+  stream << "  Ray: " << &rayhit << ",\n";
+  stream << "  normal: [" << rayhit.normal[0] << "," << rayhit.normal[1] << ","
+         << rayhit.normal[2] << "],\n";
+  stream << "  uv: [" << rayhit.uv[0] << "," << rayhit.uv[1] << "],\n";
+  stream << "  hit_distance: " << rayhit.hit_distance << ",\n";
+  stream << "  prim_id: " << rayhit.prim_id << ",\n";
+  stream << "  geom_id: " << rayhit.geom_id << ",\n";
+  stream << "}\n";
+  return stream;
+}
 
 // blazert/bvh/options.h:15-29
 template <typename T>

@@ -222,8 +222,11 @@ def test_c_header_compiles_as_c_and_headers_are_warning_free(tmp_path):
     subprocess.run([str(exe)], check=True)
     cpp = tmp_path / "headers.cpp"
     cpp.write_text("#include <blazert_b200/scene.hpp>\n#include <blazert_b200/embree_scene.hpp>\n"
+                   "#include <sstream>\n"
                    "int main() { blazert_b200::Scene<double> a; blazert_b200::Scene<float> b;"
-                   " blazert_b200::EmbreeScene<float> c; (void)a; (void)b; (void)c; return 0; }\n")
+                   " blazert_b200::EmbreeScene<float> c; (void)a; (void)b; (void)c;"
+                   " std::ostringstream o; o << blazert_b200::Ray<double>{{0, 0, 0}, {1, 2, -2}}"
+                   " << blazert_b200::RayHit<float>{}; return o.str().empty(); }\n")
     subprocess.run([os.environ.get("BZR_CXX", "g++"), "-std=c++17", "-Wall", "-Wextra", "-Werror",
                     "-fsyntax-only", "-I", inc, str(cpp)], check=True)
 
