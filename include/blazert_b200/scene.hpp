@@ -9,6 +9,7 @@
 #pragma once
 
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
@@ -134,6 +135,19 @@ struct BVHBuildOptions {
   unsigned int bin_size = 64;
 };
 
+// blazert/bvh/statistics.h:11-38, member for member (the reference's builder returns it;
+// Scene::build_statistics gives it per kind after commit).
+template <typename T>
+struct BVHBuildStatistics {
+  unsigned int max_tree_depth = 0;
+  unsigned int leaf_nodes = 0;
+  unsigned int max_num_prims_per_leaf = 0;
+  unsigned int min_num_prims_per_leaf = static_cast<unsigned int>(-1);
+  unsigned int branch_nodes = 0;
+  unsigned int bad_splits = 0;
+  std::chrono::duration<T> build_time{T(0)};
+};
+
 class Error : public std::runtime_error {
  public:
   Error(int code, const std::string &what) : std::runtime_error(what), code(code) {}
@@ -249,6 +263,21 @@ class Scene {
     bzr_scene *h = nullptr;
     check(bzr_scene_load(&h, path.c_str()));
     return std::unique_ptr<Scene>(new Scene(h));
+  }
+
+  // Build statistics of one kind's BVH (0 triangles, 1 spheres, 2 planes, 3 cylinders).
+  BVHBuildStatistics<T> build_statistics(int kind) const {
+    bzr_build_statistics b;
+    check(bzr_scene_build_statistics(s_, kind, &b));
+    BVHBuildStatistics<T> st;
+    st.max_tree_depth = b.max_tree_depth;
+    st.leaf_nodes = b.leaf_nodes;
+    st.max_num_prims_per_leaf = b.max_num_prims_per_leaf;
+    st.min_num_prims_per_leaf = b.min_num_prims_per_leaf;
+    st.branch_nodes = b.branch_nodes;
+    st.bad_splits = b.bad_splits;
+    st.build_time = std::chrono::duration<T>(static_cast<T>(b.build_seconds));
+    return st;
   }
 
   const bzr_scene *handle() const { return s_; }

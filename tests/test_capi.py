@@ -226,7 +226,10 @@ def test_c_header_compiles_as_c_and_headers_are_warning_free(tmp_path):
                    "int main() { blazert_b200::Scene<double> a; blazert_b200::Scene<float> b;"
                    " blazert_b200::EmbreeScene<float> c; (void)a; (void)b; (void)c;"
                    " std::ostringstream o; o << blazert_b200::Ray<double>{{0, 0, 0}, {1, 2, -2}}"
-                   " << blazert_b200::RayHit<float>{}; return o.str().empty(); }\n")
+                   " << blazert_b200::RayHit<float>{};"
+                   " blazert_b200::BVHBuildStatistics<double> st = a.handle() ? a.build_statistics(1)"
+                   " : blazert_b200::BVHBuildStatistics<double>{}; (void)st;"
+                   " return o.str().empty(); }\n")
     subprocess.run([os.environ.get("BZR_CXX", "g++"), "-std=c++17", "-Wall", "-Wextra", "-Werror",
                     "-fsyntax-only", "-I", inc, str(cpp)], check=True)
 
