@@ -14,8 +14,8 @@
 #include <cstring>
 #include <future>
 #include <limits>
+#include <memory>
 #include <numeric>
-#include <queue>
 #include <system_error>
 #include <thread>
 
@@ -274,6 +274,115 @@ inline float round_up(double d) {
   return f;
 }
 
+// Flattening splits long loops into contiguous ranges, one per worker thread, each range at
+// least this long.
+constexpr size_t kFlattenNodesPerThread = size_t(1) << 15;
+constexpr size_t kFlattenPrimsPerThread = size_t(1) << 16;
+
+size_t flatten_workers(size_t n, size_t min_per_thread, size_t cap) {
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  return std::max<size_t>(1, std::min({hw, cap, n / min_per_thread}));
+}
+
+// Runs body(begin, end, w) over [0, n) split into `workers` contiguous ranges.  Range 0 runs
+// on the calling thread, and so does any range whose thread cannot be started.
+template <class F>
+void run_ranges(size_t n, size_t workers, const F &body) {
+  auto lo = [&](size_t w) { return n * w / workers; };
+  std::vector<std::thread> th;
+  try {
+    for (size_t w = 1; w < workers; ++w) th.emplace_back([&, w] { body(lo(w), lo(w + 1), w); });
+  } catch (const std::system_error &) {
+  }
+  body(lo(0), lo(1), 0);
+  for (size_t w = th.size() + 1; w < workers; ++w) body(lo(w), lo(w + 1), w);
+  for (std::thread &x : th) x.join();
+}
+
+// Mesh part of the image: the vertices numbered in order of first use by the leaf-ordered
+// triangles (use u = 3 at + j for corner j of the triangle at position at), stored once each,
+// and per triangle {i0, i1, i2, id word}.  With several workers this takes four passes over
+// ranges of triangles: the first use of every vertex (an atomic minimum), the number of first
+// uses in each range, the vertex numbers from the prefix sums of those counts, and the
+// triangles' indices.  Both ways give the same numbering.
+void number_vertices(const HostScene &s, KindImage *img, size_t workers) {
+  const size_t np = img->prim_ids.size(), nv = s.vertices.size() / 3;
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  img->tri.resize(4 * np);
+  if (workers <= 1 || 3 * uint64_t(np) >= kNone) {
+    std::vector<uint32_t> remap(nv, kNone);
+    img->verts.reserve(kVertexDoubles * std::min(nv, 3 * np));
+    for (size_t at = 0; at < np; ++at) {
+      const uint32_t *F = &s.faces[3 * size_t(img->prim_ids[at] & kIdMask)];
+      for (int j = 0; j < 3; ++j) {
+        uint32_t &r = remap[F[j]];
+        if (r == kNone) {
+          r = static_cast<uint32_t>(img->verts.size() / kVertexDoubles);
+          const double *v = &s.vertices[3 * size_t(F[j])];
+          img->verts.insert(img->verts.end(), {v[0], v[1], v[2], 0.0});
+        }
+        img->tri[4 * at + j] = r;
+      }
+      img->tri[4 * at + 3] = img->prim_ids[at];
+    }
+    return;
+  }
+  auto corners = [&](size_t at) { return &s.faces[3 * size_t(img->prim_ids[at] & kIdMask)]; };
+  std::unique_ptr<std::atomic<uint32_t>[]> first(new std::atomic<uint32_t>[nv]);
+  run_ranges(nv, workers, [&](size_t v0, size_t v1, size_t) {
+    for (size_t v = v0; v < v1; ++v) first[v].store(kNone, std::memory_order_relaxed);
+  });
+  run_ranges(np, workers, [&](size_t a0, size_t a1, size_t) {
+    for (size_t at = a0; at < a1; ++at) {
+      const uint32_t *F = corners(at);
+      for (int j = 0; j < 3; ++j) {
+        const auto u = static_cast<uint32_t>(3 * at + j);
+        std::atomic<uint32_t> &slot = first[F[j]];
+        uint32_t cur = slot.load(std::memory_order_relaxed);
+        while (u < cur && !slot.compare_exchange_weak(cur, u, std::memory_order_relaxed)) {
+        }
+      }
+    }
+  });
+  std::vector<size_t> base(workers + 1, 0);
+  run_ranges(np, workers, [&](size_t a0, size_t a1, size_t w) {
+    size_t n = 0;
+    for (size_t at = a0; at < a1; ++at) {
+      const uint32_t *F = corners(at);
+      for (int j = 0; j < 3; ++j)
+        n += first[F[j]].load(std::memory_order_relaxed) == 3 * at + j;
+    }
+    base[w + 1] = n;
+  });
+  for (size_t w = 0; w < workers; ++w) base[w + 1] += base[w];
+  img->verts.resize(kVertexDoubles * base[workers]);
+  RawVector<uint32_t> number(nv);  // read only for the vertices numbered below
+  run_ranges(np, workers, [&](size_t a0, size_t a1, size_t w) {
+    auto r = static_cast<uint32_t>(base[w]);
+    for (size_t at = a0; at < a1; ++at) {
+      const uint32_t *F = corners(at);
+      for (int j = 0; j < 3; ++j) {
+        if (first[F[j]].load(std::memory_order_relaxed) != 3 * at + j) continue;
+        number[F[j]] = r;
+        const double *v = &s.vertices[3 * size_t(F[j])];
+        double *o = &img->verts[kVertexDoubles * size_t(r)];
+        o[0] = v[0];
+        o[1] = v[1];
+        o[2] = v[2];
+        o[3] = 0.0;
+        ++r;
+      }
+    }
+  });
+  run_ranges(np, workers, [&](size_t a0, size_t a1, size_t) {
+    for (size_t at = a0; at < a1; ++at) {
+      const uint32_t *F = corners(at);
+      for (int j = 0; j < 3; ++j) img->tri[4 * at + j] = number[F[j]];
+      img->tri[4 * at + 3] = img->prim_ids[at];
+    }
+  });
+}
+
 }  // namespace
 
 // blazert/bvh/builder.h:46-65
@@ -401,7 +510,7 @@ BuildStatistics tree_statistics(const Tree &t) {
   return st;
 }
 
-KindImage flatten(const HostScene &s, int kind) {
+KindImage flatten(const HostScene &s, int kind, size_t max_workers) {
   const Collection &c = s.kind[kind];
   const Tree &t = c.tree;
   KindImage img;
@@ -414,19 +523,17 @@ KindImage flatten(const HostScene &s, int kind) {
       leaf_pos[i] = pos;
       pos += t.nodes[i].prim_cnt;
     }
-  // Breadth-first numbering of the internal nodes.
+  // Breadth-first numbering of the internal nodes; the order array is its own FIFO queue.
   std::vector<uint32_t> order;
   if (nn && t.nodes[0].leaf != 1) {
-    std::queue<uint32_t> q;
-    q.push(0);
-    while (!q.empty()) {
-      const uint32_t i = q.front();
-      q.pop();
-      dev_index[i] = static_cast<uint32_t>(order.size());
-      order.push_back(i);
+    order.reserve(nn / 2 + 1);
+    order.push_back(0);
+    for (size_t head = 0; head < order.size(); ++head) {
+      const uint32_t i = order[head];
+      dev_index[i] = static_cast<uint32_t>(head);
       for (int j = 0; j < 2; ++j) {
         const uint32_t ch = t.nodes[i].child[j];
-        if (t.nodes[ch].leaf != 1) q.push(ch);
+        if (t.nodes[ch].leaf != 1) order.push_back(ch);
       }
     }
   }
@@ -439,26 +546,36 @@ KindImage flatten(const HostScene &s, int kind) {
     return true;
   };
   img.n_internal = static_cast<uint32_t>(order.size());
-  img.nodes64.assign(size_t(img.n_internal) * kNode64Doubles, 0.0);
-  img.nodes32.assign(size_t(img.n_internal) * kNode32Floats, 0.0f);
-  for (uint32_t g = 0; g < img.n_internal; ++g) {
-    const TreeNode &nd = t.nodes[order[g]];
-    double *d = &img.nodes64[size_t(g) * kNode64Doubles];
-    float *f = &img.nodes32[size_t(g) * kNode32Floats];
-    for (int j = 0; j < 2; ++j) {
-      const TreeNode &ch = t.nodes[nd.child[j]];
-      if (!finite_box(ch)) img.mixed_ok = false;
-      for (int k = 0; k < 3; ++k) {
-        d[6 * j + 2 * k] = ch.mn[k];
-        d[6 * j + 2 * k + 1] = ch.mx[k];
-        f[6 * j + 2 * k] = round_down(ch.mn[k]);
-        f[6 * j + 2 * k + 1] = round_up(ch.mx[k]);
+  img.nodes64.resize(size_t(img.n_internal) * kNode64Doubles);
+  img.nodes32.resize(size_t(img.n_internal) * kNode32Floats);
+  // Each node reads only the tree and writes only its own slots, so ranges of nodes can be
+  // filled on separate threads.
+  const size_t workers =
+      flatten_workers(img.n_internal, kFlattenNodesPerThread, max_workers);
+  std::vector<char> finite(workers, 1);
+  run_ranges(img.n_internal, workers, [&](size_t g0, size_t g1, size_t w) {
+    for (size_t g = g0; g < g1; ++g) {
+      const TreeNode &nd = t.nodes[order[g]];
+      double *d = &img.nodes64[g * kNode64Doubles];
+      float *f = &img.nodes32[g * kNode32Floats];
+      for (int j = 0; j < 2; ++j) {
+        const TreeNode &ch = t.nodes[nd.child[j]];
+        if (!finite_box(ch)) finite[w] = 0;
+        for (int k = 0; k < 3; ++k) {
+          d[6 * j + 2 * k] = ch.mn[k];
+          d[6 * j + 2 * k + 1] = ch.mx[k];
+          f[6 * j + 2 * k] = round_down(ch.mn[k]);
+          f[6 * j + 2 * k + 1] = round_up(ch.mx[k]);
+        }
       }
+      const uint32_t meta[4] = {ref_of(nd.child[0]), ref_of(nd.child[1]), nd.axis, 0u};
+      std::memcpy(d + 12, meta, sizeof meta);
+      std::memcpy(f + 12, meta, sizeof meta);
+      d[14] = d[15] = 0.0;
     }
-    const uint32_t meta[4] = {ref_of(nd.child[0]), ref_of(nd.child[1]), nd.axis, 0u};
-    std::memcpy(d + 12, meta, sizeof meta);
-    std::memcpy(f + 12, meta, sizeof meta);
-  }
+  });
+  for (const char ok : finite)
+    if (!ok) img.mixed_ok = false;
   if (nn) {
     const TreeNode &root = t.nodes[0];
     img.root_ref = ref_of(0);
@@ -471,61 +588,50 @@ KindImage flatten(const HostScene &s, int kind) {
     }
     img.coord_max = round_up(cmax);
   }
-  // Leaf-ordered primitives.
+  // Leaf-ordered primitives: leaves own disjoint position ranges and the ids are a
+  // permutation, so ranges of leaves can be written on separate threads.
   const size_t np = t.leaf_prims.size();
   const int stride = kPayloadDoubles[kind];
   img.prim_ids.resize(np);
   img.pos_of.assign(np, 0u);
   img.payload.assign(np * stride, 0.0);
-  std::vector<uint32_t> remap;
-  if (kind == kMesh) {
-    img.tri.resize(4 * np);
-    remap.assign(s.vertices.size() / 3, 0xFFFFFFFFu);
-  }
-  for (size_t i = 0; i < nn; ++i) {
-    const TreeNode &nd = t.nodes[i];
-    if (nd.leaf != 1) continue;
-    for (uint32_t q = 0; q < nd.prim_cnt; ++q) {
-      const uint32_t at = leaf_pos[i] + q;
-      const uint32_t id = t.leaf_prims[nd.prim_off + q];
-      img.prim_ids[at] = id | (q + 1 == nd.prim_cnt ? kLastBit : 0u);
-      img.pos_of[id] = at;
-      double *p = img.payload.data() + size_t(at) * stride;
-      switch (kind) {
-        case kMesh: {
-          const uint32_t *F = &s.faces[3 * id];
-          for (int j = 0; j < 3; ++j) {
-            uint32_t &r = remap[F[j]];
-            if (r == 0xFFFFFFFFu) {
-              r = static_cast<uint32_t>(img.verts.size() / kVertexDoubles);
-              const double *v = &s.vertices[3 * size_t(F[j])];
-              img.verts.insert(img.verts.end(), {v[0], v[1], v[2], 0.0});
-            }
-            img.tri[4 * size_t(at) + j] = r;
-          }
-          img.tri[4 * size_t(at) + 3] = img.prim_ids[at];
-          break;
+  run_ranges(nn, flatten_workers(nn, kFlattenNodesPerThread, max_workers),
+             [&](size_t i0, size_t i1, size_t) {
+    for (size_t i = i0; i < i1; ++i) {
+      const TreeNode &nd = t.nodes[i];
+      if (nd.leaf != 1) continue;
+      for (uint32_t q = 0; q < nd.prim_cnt; ++q) {
+        const uint32_t at = leaf_pos[i] + q;
+        const uint32_t id = t.leaf_prims[nd.prim_off + q];
+        img.prim_ids[at] = id | (q + 1 == nd.prim_cnt ? kLastBit : 0u);
+        img.pos_of[id] = at;
+        double *p = img.payload.data() + size_t(at) * stride;
+        switch (kind) {
+          case kSpheres:
+            for (int k = 0; k < 3; ++k) p[k] = c.a[3 * id + k];
+            p[3] = c.b[id];
+            break;
+          case kPlanes:
+            for (int k = 0; k < 3; ++k) p[k] = c.a[3 * id + k];
+            p[3] = c.b[id];
+            p[4] = c.c[id];
+            for (int k = 0; k < 9; ++k) p[5 + k] = c.d[9 * id + k];
+            break;
+          case kCylinders:
+            for (int k = 0; k < 3; ++k) p[k] = c.a[3 * id + k];
+            p[3] = c.b[id];
+            p[4] = c.c[id];
+            p[5] = c.d[id];
+            for (int k = 0; k < 9; ++k) p[6 + k] = c.e[9 * id + k];
+            break;
+          default:
+            break;
         }
-        case kSpheres:
-          for (int k = 0; k < 3; ++k) p[k] = c.a[3 * id + k];
-          p[3] = c.b[id];
-          break;
-        case kPlanes:
-          for (int k = 0; k < 3; ++k) p[k] = c.a[3 * id + k];
-          p[3] = c.b[id];
-          p[4] = c.c[id];
-          for (int k = 0; k < 9; ++k) p[5 + k] = c.d[9 * id + k];
-          break;
-        case kCylinders:
-          for (int k = 0; k < 3; ++k) p[k] = c.a[3 * id + k];
-          p[3] = c.b[id];
-          p[4] = c.c[id];
-          p[5] = c.d[id];
-          for (int k = 0; k < 9; ++k) p[6 + k] = c.e[9 * id + k];
-          break;
       }
     }
-  }
+  });
+  if (kind == kMesh)
+    number_vertices(s, &img, flatten_workers(np, kFlattenPrimsPerThread, max_workers));
   return img;
 }
 

@@ -6,7 +6,10 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "layout.h"
@@ -86,15 +89,40 @@ void add_planes(HostScene &s, const double *c, const double *dx, const double *d
 void add_cylinders(HostScene &s, const double *c, const double *a, const double *b,
                    const double *h, const double *rot, size_t n);
 
-// Device image of one kind, ready to upload.
+// Allocator whose value-less construct leaves an element default-initialised: resize() on a
+// vector of numbers then allocates without writing, for arrays that are written in full
+// right after (by several threads, which then also take the page faults in parallel).
+template <class T>
+struct UninitAllocator : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = UninitAllocator<U>;
+  };
+  UninitAllocator() = default;
+  template <class U>
+  UninitAllocator(const UninitAllocator<U> &) noexcept {}
+  template <class U>
+  void construct(U *p) {
+    ::new (static_cast<void *>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U *p, A &&...a) {
+    ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using RawVector = std::vector<T, UninitAllocator<T>>;
+
+// Device image of one kind, ready to upload.  flatten writes every element of the RawVector
+// arrays.
 struct KindImage {
-  std::vector<double> nodes64;
-  std::vector<float> nodes32;
+  RawVector<double> nodes64;
+  RawVector<float> nodes32;
   std::vector<double> payload;
-  std::vector<uint32_t> prim_ids;
+  RawVector<uint32_t> prim_ids;
   std::vector<uint32_t> pos_of;  // leaf-ordered position of each primitive id
-  std::vector<uint32_t> tri;     // triangles: {i0, i1, i2, id word} per leaf-ordered triangle
-  std::vector<double> verts;     // triangles: {x, y, z, 0} per vertex, in order of first use
+  RawVector<uint32_t> tri;       // triangles: {i0, i1, i2, id word} per leaf-ordered triangle
+  RawVector<double> verts;       // triangles: {x, y, z, 0} per vertex, in order of first use
   uint32_t n_internal = 0;
   uint32_t root_ref = 0;
   double root_box[6] = {0, 0, 0, 0, 0, 0};
@@ -102,7 +130,9 @@ struct KindImage {
   bool mixed_ok = true;
 };
 
-KindImage flatten(const HostScene &s, int kind);
+// Device image of one kind's tree and primitives.  Long loops run on up to max_workers threads;
+// the image does not depend on how many.
+KindImage flatten(const HostScene &s, int kind, size_t max_workers = 16);
 
 // Persistent scene format (scene_io.cpp): a committed scene's inputs, build options and trees
 // as bytes, and back.  decode_scene fills a fresh HostScene (primitives added, trees checked

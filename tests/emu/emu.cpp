@@ -299,4 +299,37 @@ int emu_build_statistics(void *h, int kind, uint32_t *out) {
   return 0;
 }
 
+// FNV-1a digest of every array and field of one kind's device image, flattened again with at
+// most `workers` threads.  Returns -1 for an absent kind.
+int emu_image_digest(void *h, int kind, long workers, uint64_t *digest) {
+  const bzr::HostScene &s = static_cast<Emu *>(h)->host;
+  if (!s.kind[kind].present) return -1;
+  const bzr::KindImage im = bzr::flatten(s, kind, static_cast<size_t>(workers));
+  uint64_t x = 1469598103934665603ull;
+  auto mix = [&](const void *p, size_t n) {
+    const auto *b = static_cast<const unsigned char *>(p);
+    for (size_t i = 0; i < n; ++i) x = (x ^ b[i]) * 1099511628211ull;
+  };
+  auto mix_array = [&](const auto &v) {
+    const uint64_t n = v.size();
+    mix(&n, sizeof n);
+    mix(v.data(), v.size() * sizeof v[0]);
+  };
+  mix_array(im.nodes64);
+  mix_array(im.nodes32);
+  mix_array(im.payload);
+  mix_array(im.prim_ids);
+  mix_array(im.pos_of);
+  mix_array(im.tri);
+  mix_array(im.verts);
+  const uint8_t ok = im.mixed_ok;
+  mix(&im.n_internal, sizeof im.n_internal);
+  mix(&im.root_ref, sizeof im.root_ref);
+  mix(im.root_box, sizeof im.root_box);
+  mix(&im.coord_max, sizeof im.coord_max);
+  mix(&ok, 1);
+  *digest = x;
+  return 0;
+}
+
 }  // extern "C"

@@ -55,6 +55,7 @@ def load():
         lib.emu_prim_box.argtypes = [C.c_void_p, C.c_int, C.c_uint32, _dp, _dp, _dp]
         lib.emu_box_accept.argtypes = [_dp, _dp, _dp, _dp, C.c_double, C.c_double]
         lib.emu_build_statistics.argtypes = [C.c_void_p, C.c_int, _u32p]
+        lib.emu_image_digest.argtypes = [C.c_void_p, C.c_int, C.c_long, C.c_void_p]
         lib.emu_scene_encode.restype = C.c_long
         lib.emu_scene_encode.argtypes = [C.c_void_p, C.c_void_p, C.c_long]
         lib.emu_scene_decode.restype = C.c_void_p
@@ -96,6 +97,13 @@ class EmuScene(_Base):
         if self._lib.emu_build_statistics(self._h, KINDS.index(kind), _ptr(out, _u32p)) != 0:
             return None
         return dict(zip(STAT_KEYS, (int(x) for x in out)))
+
+    def image_digest(self, kind, workers):
+        """Digest of one kind's device image flattened with at most `workers` threads."""
+        out = np.zeros(1, np.uint64)
+        if self._lib.emu_image_digest(self._h, KINDS.index(kind), workers, out.ctypes.data) != 0:
+            return None
+        return int(out[0])
 
     def encode(self) -> bytes:
         """The scene in the persistent format (scene_io.cpp)."""

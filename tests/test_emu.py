@@ -80,3 +80,18 @@ def test_stack_overflow_is_flagged_not_silent():
     R = wl.rays
     got = EmuScene(wl.scene).intersect(R.origins, R.directions, stack_cap=1)
     assert got["error_word"] & 1
+
+
+def test_flatten_image_does_not_depend_on_threads():
+    """The flattener runs its long loops (node fill, leaf-ordered primitives, vertex numbering
+    by first use) over ranges on several threads.  The device image must be the same bytes for
+    every thread count; the sizes make each loop split into several ranges."""
+    rng = np.random.default_rng(11)
+    n = 200_000
+    spec = W.SceneSpec().add_mesh(*W.icosphere(7)).add_spheres(
+        rng.uniform(-10.0, 10.0, (n, 3)), rng.uniform(0.01, 0.1, n))
+    emu = EmuScene(spec)
+    for kind in ("mesh", "spheres"):
+        one = emu.image_digest(kind, 1)
+        assert [emu.image_digest(kind, w) for w in (2, 3, 16)] == [one] * 3, kind
+    assert emu.image_digest("planes", 4) is None
