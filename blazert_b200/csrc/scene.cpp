@@ -62,9 +62,9 @@ inline void grow(double *mn, double *mx, const double *bmn, const double *bmx) {
 
 void alloc_boxes(PrimBoxes &b, size_t n) {
   b.n = n;
-  b.bmin.assign(3 * n, 0.0);
-  b.bmax.assign(3 * n, 0.0);
-  b.center.assign(3 * n, 0.0);
+  b.bmin.resize(3 * n);
+  b.bmax.resize(3 * n);
+  b.center.resize(3 * n);
 }
 
 // Box of six points, reduced with std::min / std::max over an initializer list as the
@@ -274,12 +274,14 @@ inline float round_up(double d) {
   return f;
 }
 
-// Flattening splits long loops into contiguous ranges, one per worker thread, each range at
-// least this long.
-constexpr size_t kFlattenNodesPerThread = size_t(1) << 15;
-constexpr size_t kFlattenPrimsPerThread = size_t(1) << 16;
+// Long host loops (adding a mesh, flattening) split into contiguous ranges, one per worker
+// thread, each range at least this long.
+constexpr size_t kNodesPerRange = size_t(1) << 15;
+constexpr size_t kPrimsPerRange = size_t(1) << 16;
+constexpr size_t kFacesPerRange = size_t(1) << 14;
+constexpr size_t kMaxRangeWorkers = 16;
 
-size_t flatten_workers(size_t n, size_t min_per_thread, size_t cap) {
+size_t range_workers(size_t n, size_t min_per_thread, size_t cap) {
   const size_t hw = std::max(1u, std::thread::hardware_concurrency());
   return std::max<size_t>(1, std::min({hw, cap, n / min_per_thread}));
 }
@@ -402,7 +404,9 @@ Tree build_tree(const PrimBoxes &boxes, const BuildOptions &opt) {
 }
 
 // blazert/primitives/trimesh.h:78-130: centre (v0+v1+v2)/3, box of the corners, unit face
-// normal of cross(v1-v0, v2-v0) accumulated /3 into each corner's vertex normal.
+// normal of cross(v1-v0, v2-v0) accumulated /3 into each corner's vertex normal.  The
+// per-face values are computed over ranges of faces on several threads; the accumulation
+// stays one pass in face order, so each vertex normal is the same sum in the same order.
 void add_mesh(HostScene &s, const double *v, size_t nv, const uint32_t *f, size_t nf) {
   Collection &c = s.kind[kMesh];
   s.vertices.assign(v, v + 3 * nv);
@@ -410,10 +414,10 @@ void add_mesh(HostScene &s, const double *v, size_t nv, const uint32_t *f, size_
   s.vert_n.assign(3 * nv, 0.0);
   c.n = nf;
   alloc_boxes(c.boxes, nf);
-  for (size_t i = 0; i < nf; ++i) {
+  auto face = [&](size_t i) {
     const uint32_t *F = &s.faces[3 * i];
-    const V3 a = load3(&s.vertices[3 * F[0]]), b = load3(&s.vertices[3 * F[1]]),
-             cc = load3(&s.vertices[3 * F[2]]);
+    const V3 a = load3(&s.vertices[3 * size_t(F[0])]), b = load3(&s.vertices[3 * size_t(F[1])]),
+             cc = load3(&s.vertices[3 * size_t(F[2])]);
     store3(&c.boxes.center[3 * i], ((a + b) + cc) / 3.0);
     double mn[3] = {a.x, a.y, a.z}, mx[3] = {a.x, a.y, a.z};
     const double pb[3] = {b.x, b.y, b.z}, pc[3] = {cc.x, cc.y, cc.z};
@@ -421,12 +425,24 @@ void add_mesh(HostScene &s, const double *v, size_t nv, const uint32_t *f, size_
     grow(mn, mx, pc, pc);
     std::memcpy(&c.boxes.bmin[3 * i], mn, sizeof mn);
     std::memcpy(&c.boxes.bmax[3 * i], mx, sizeof mx);
-    const V3 share = normalize(cross(b - a, cc - a)) / 3.0;
+    return normalize(cross(b - a, cc - a)) / 3.0;
+  };
+  auto accumulate = [&](size_t i, V3 share) {
     for (int j = 0; j < 3; ++j) {
-      double *vn = &s.vert_n[3 * F[j]];
+      double *vn = &s.vert_n[3 * size_t(s.faces[3 * i + j])];
       store3(vn, load3(vn) + share);
     }
+  };
+  const size_t workers = range_workers(nf, kFacesPerRange, kMaxRangeWorkers);
+  if (workers == 1) {
+    for (size_t i = 0; i < nf; ++i) accumulate(i, face(i));
+    return;
   }
+  RawVector<double> share(3 * nf);
+  run_ranges(nf, workers, [&](size_t i0, size_t i1, size_t) {
+    for (size_t i = i0; i < i1; ++i) store3(&share[3 * i], face(i));
+  });
+  for (size_t i = 0; i < nf; ++i) accumulate(i, load3(&share[3 * i]));
 }
 
 // blazert/primitives/sphere.h:93-100: box = centre -+ radius.
@@ -551,7 +567,7 @@ KindImage flatten(const HostScene &s, int kind, size_t max_workers) {
   // Each node reads only the tree and writes only its own slots, so ranges of nodes can be
   // filled on separate threads.
   const size_t workers =
-      flatten_workers(img.n_internal, kFlattenNodesPerThread, max_workers);
+      range_workers(img.n_internal, kNodesPerRange, max_workers);
   std::vector<char> finite(workers, 1);
   run_ranges(img.n_internal, workers, [&](size_t g0, size_t g1, size_t w) {
     for (size_t g = g0; g < g1; ++g) {
@@ -595,7 +611,7 @@ KindImage flatten(const HostScene &s, int kind, size_t max_workers) {
   img.prim_ids.resize(np);
   img.pos_of.assign(np, 0u);
   img.payload.assign(np * stride, 0.0);
-  run_ranges(nn, flatten_workers(nn, kFlattenNodesPerThread, max_workers),
+  run_ranges(nn, range_workers(nn, kNodesPerRange, max_workers),
              [&](size_t i0, size_t i1, size_t) {
     for (size_t i = i0; i < i1; ++i) {
       const TreeNode &nd = t.nodes[i];
@@ -631,7 +647,7 @@ KindImage flatten(const HostScene &s, int kind, size_t max_workers) {
     }
   });
   if (kind == kMesh)
-    number_vertices(s, &img, flatten_workers(np, kFlattenPrimsPerThread, max_workers));
+    number_vertices(s, &img, range_workers(np, kPrimsPerRange, max_workers));
   return img;
 }
 

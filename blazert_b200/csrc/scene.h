@@ -16,6 +16,30 @@
 
 namespace bzr {
 
+// Allocator whose value-less construct leaves an element default-initialised: resize() on a
+// vector of numbers then allocates without writing, for arrays that are written in full
+// right after (by several threads, which then also take the page faults in parallel).
+template <class T>
+struct UninitAllocator : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = UninitAllocator<U>;
+  };
+  UninitAllocator() = default;
+  template <class U>
+  UninitAllocator(const UninitAllocator<U> &) noexcept {}
+  template <class U>
+  void construct(U *p) {
+    ::new (static_cast<void *>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U *p, A &&...a) {
+    ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using RawVector = std::vector<T, UninitAllocator<T>>;
+
 struct BuildOptions {
   uint32_t min_leaf = 4;  // blazert/bvh/options.h:20-21 defaults
   uint32_t max_depth = 28;
@@ -25,7 +49,7 @@ struct BuildOptions {
 // Per-primitive boxes and centres of one collection, n x 3 each.
 struct PrimBoxes {
   size_t n = 0;
-  std::vector<double> bmin, bmax, center;
+  RawVector<double> bmin, bmax, center;  // every element written by the collection's adder
 };
 
 // The reference tree (blazert/bvh/node.h:15-41) in its DFS pre-order.
@@ -88,30 +112,6 @@ void add_planes(HostScene &s, const double *c, const double *dx, const double *d
                 const double *rot, size_t n);
 void add_cylinders(HostScene &s, const double *c, const double *a, const double *b,
                    const double *h, const double *rot, size_t n);
-
-// Allocator whose value-less construct leaves an element default-initialised: resize() on a
-// vector of numbers then allocates without writing, for arrays that are written in full
-// right after (by several threads, which then also take the page faults in parallel).
-template <class T>
-struct UninitAllocator : std::allocator<T> {
-  template <class U>
-  struct rebind {
-    using other = UninitAllocator<U>;
-  };
-  UninitAllocator() = default;
-  template <class U>
-  UninitAllocator(const UninitAllocator<U> &) noexcept {}
-  template <class U>
-  void construct(U *p) {
-    ::new (static_cast<void *>(p)) U;
-  }
-  template <class U, class... A>
-  void construct(U *p, A &&...a) {
-    ::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
-  }
-};
-template <class T>
-using RawVector = std::vector<T, UninitAllocator<T>>;
 
 // Device image of one kind, ready to upload.  flatten writes every element of the RawVector
 // arrays.
