@@ -292,9 +292,10 @@ template <class F>
 void run_ranges(size_t n, size_t workers, const F &body) {
   auto lo = [&](size_t w) { return n * w / workers; };
   std::vector<std::thread> th;
+  th.reserve(workers);  // no reallocation below: a failed start leaves every thread joinable
   try {
     for (size_t w = 1; w < workers; ++w) th.emplace_back([&, w] { body(lo(w), lo(w + 1), w); });
-  } catch (const std::system_error &) {
+  } catch (...) {  // no thread (or no memory for its state): the rest runs here
   }
   body(lo(0), lo(1), 0);
   for (size_t w = th.size() + 1; w < workers; ++w) body(lo(w), lo(w + 1), w);
