@@ -331,6 +331,16 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
   const bzr::Collection &sph = s->host.kind[bzr::kSpheres];
   const size_t off_sc = place(sph.a.data(), sph.a.size() * sizeof(double));
   const size_t off_sr = place(sph.b.data(), sph.b.size() * sizeof(double));
+  // A commit that failed after its first device allocation leaves the scene uncommitted with
+  // those allocations held: free them before this attempt allocates its own.
+  if (s->arena) cudaFree(s->arena);
+  if (s->slots) cudaFree(s->slots);
+  if (s->pinned_err) cudaFreeHost(s->pinned_err);
+  if (s->plan.pool) cudaMemPoolDestroy(s->plan.pool);
+  s->arena = nullptr;
+  s->slots = nullptr;
+  s->pinned_err = nullptr;
+  s->plan.pool = nullptr;
   cudaError_t e = cudaGetDevice(&s->device);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
   e = cudaMalloc(&s->arena, total);
