@@ -977,15 +977,22 @@ int bzr_closest_surface(const bzr_scene *s, size_t n, const double *points, doub
   return run_distance(s, -1, n, nullptr, points, distance, nullptr, prim, geom, stream);
 }
 
-long bzr_scene_serialize(const bzr_scene *s, uint8_t *buffer, size_t capacity) {
+// The committed scene's bytes in the persistent format, or a negative status.
+static int encode_committed(const bzr_scene *s, std::vector<uint8_t> *out) {
   if (!s) return fail(BZR_EINVAL, "scene is null");
   if (!s->host.committed) return fail(BZR_ESTATE, "scene is not committed");
-  std::vector<uint8_t> b;
   try {
-    b = bzr::encode_scene(s->host);
+    *out = bzr::encode_scene(s->host);
   } catch (const std::bad_alloc &) {
     return fail(BZR_ENOMEM, "host allocation failed while writing the scene");
   }
+  return BZR_OK;
+}
+
+long bzr_scene_serialize(const bzr_scene *s, uint8_t *buffer, size_t capacity) {
+  std::vector<uint8_t> b;
+  const int rc = encode_committed(s, &b);
+  if (rc != BZR_OK) return rc;
   if (buffer) {
     if (capacity < b.size()) return fail(BZR_EINVAL, "buffer too small for the scene");
     std::memcpy(buffer, b.data(), b.size());
@@ -1019,11 +1026,9 @@ int bzr_scene_deserialize(bzr_scene **out, const uint8_t *buffer, size_t size) {
 
 int bzr_scene_save(const bzr_scene *s, const char *path) {
   if (!path) return fail(BZR_EINVAL, "path is null");
-  const long n = bzr_scene_serialize(s, nullptr, 0);
-  if (n < 0) return static_cast<int>(n);
-  std::vector<uint8_t> b(static_cast<size_t>(n));
-  const long m = bzr_scene_serialize(s, b.data(), b.size());
-  if (m < 0) return static_cast<int>(m);
+  std::vector<uint8_t> b;
+  const int rc = encode_committed(s, &b);
+  if (rc != BZR_OK) return rc;
   std::FILE *f = std::fopen(path, "wb");
   if (!f) return fail(BZR_EINVAL, std::string("cannot open for writing: ") + path);
   const bool ok = std::fwrite(b.data(), 1, b.size(), f) == b.size();

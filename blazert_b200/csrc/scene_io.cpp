@@ -28,6 +28,7 @@ namespace {
 
 constexpr char kMagic[8] = {'B', 'Z', 'R', 'S', 'C', 'E', 'N', 'E'};
 constexpr uint32_t kVersion = 1;
+constexpr size_t kNodeBytes = 6 * sizeof(double) + 6 * sizeof(uint32_t);  // one tree node
 
 uint64_t fnv1a(const uint8_t *p, size_t n) {
   uint64_t h = 1469598103934665603ull;
@@ -40,18 +41,19 @@ uint64_t fnv1a(const uint8_t *p, size_t n) {
 
 struct Writer {
   std::vector<uint8_t> out;
+  // appends `bytes` bytes and returns where they start
+  uint8_t *grow(size_t bytes) {
+    const size_t at = out.size();
+    out.resize(at + bytes);
+    return out.data() + at;
+  }
   template <class T>
   void put(const T &v) {
-    const size_t at = out.size();
-    out.resize(at + sizeof(T));
-    std::memcpy(out.data() + at, &v, sizeof(T));
+    std::memcpy(grow(sizeof(T)), &v, sizeof(T));
   }
   template <class T>
   void put_array(const T *p, size_t n) {
-    if (!n) return;
-    const size_t at = out.size();
-    out.resize(at + n * sizeof(T));
-    std::memcpy(out.data() + at, p, n * sizeof(T));
+    if (n) std::memcpy(grow(n * sizeof(T)), p, n * sizeof(T));
   }
 };
 
@@ -82,11 +84,13 @@ struct Reader {
 
 void put_tree(Writer &w, const Tree &t) {
   w.put<uint64_t>(t.nodes.size());
+  uint8_t *p = w.grow(t.nodes.size() * kNodeBytes);
   for (const TreeNode &nd : t.nodes) {
-    w.put_array(nd.mn, 3);
-    w.put_array(nd.mx, 3);
     const uint32_t u[6] = {nd.leaf, nd.axis, nd.child[0], nd.child[1], nd.prim_off, nd.prim_cnt};
-    w.put_array(u, 6);
+    std::memcpy(p, nd.mn, sizeof nd.mn);
+    std::memcpy(p + sizeof nd.mn, nd.mx, sizeof nd.mx);
+    std::memcpy(p + sizeof nd.mn + sizeof nd.mx, u, sizeof u);
+    p += kNodeBytes;
   }
   w.put<uint64_t>(t.leaf_prims.size());
   w.put_array(t.leaf_prims.data(), t.leaf_prims.size());
