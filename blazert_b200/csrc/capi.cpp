@@ -978,7 +978,7 @@ int bzr_closest_surface(const bzr_scene *s, size_t n, const double *points, doub
 }
 
 // The committed scene's bytes in the persistent format, or a negative status.
-static int encode_committed(const bzr_scene *s, std::vector<uint8_t> *out) {
+static int encode_committed(const bzr_scene *s, bzr::RawVector<uint8_t> *out) {
   if (!s) return fail(BZR_EINVAL, "scene is null");
   if (!s->host.committed) return fail(BZR_ESTATE, "scene is not committed");
   try {
@@ -990,7 +990,7 @@ static int encode_committed(const bzr_scene *s, std::vector<uint8_t> *out) {
 }
 
 long bzr_scene_serialize(const bzr_scene *s, uint8_t *buffer, size_t capacity) {
-  std::vector<uint8_t> b;
+  bzr::RawVector<uint8_t> b;
   const int rc = encode_committed(s, &b);
   if (rc != BZR_OK) return rc;
   if (buffer) {
@@ -1026,7 +1026,7 @@ int bzr_scene_deserialize(bzr_scene **out, const uint8_t *buffer, size_t size) {
 
 int bzr_scene_save(const bzr_scene *s, const char *path) {
   if (!path) return fail(BZR_EINVAL, "path is null");
-  std::vector<uint8_t> b;
+  bzr::RawVector<uint8_t> b;
   const int rc = encode_committed(s, &b);
   if (rc != BZR_OK) return rc;
   std::FILE *f = std::fopen(path, "wb");

@@ -281,27 +281,6 @@ constexpr size_t kPrimsPerRange = size_t(1) << 16;
 constexpr size_t kFacesPerRange = size_t(1) << 14;
 constexpr size_t kMaxRangeWorkers = 16;
 
-size_t range_workers(size_t n, size_t min_per_thread, size_t cap) {
-  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
-  return std::max<size_t>(1, std::min({hw, cap, n / min_per_thread}));
-}
-
-// Runs body(begin, end, w) over [0, n) split into `workers` contiguous ranges.  Range 0 runs
-// on the calling thread, and so does any range whose thread cannot be started.
-template <class F>
-void run_ranges(size_t n, size_t workers, const F &body) {
-  auto lo = [&](size_t w) { return n * w / workers; };
-  std::vector<std::thread> th;
-  th.reserve(workers);  // no reallocation below: a failed start leaves every thread joinable
-  try {
-    for (size_t w = 1; w < workers; ++w) th.emplace_back([&, w] { body(lo(w), lo(w + 1), w); });
-  } catch (...) {  // no thread (or no memory for its state): the rest runs here
-  }
-  body(lo(0), lo(1), 0);
-  for (size_t w = th.size() + 1; w < workers; ++w) body(lo(w), lo(w + 1), w);
-  for (std::thread &x : th) x.join();
-}
-
 // Mesh part of the image: the vertices numbered in order of first use by the leaf-ordered
 // triangles (use u = 3 at + j for corner j of the triangle at position at), stored once each,
 // and per triangle {i0, i1, i2, id word}.  With several workers this takes four passes over

@@ -4,11 +4,13 @@
 #pragma once
 #include <cuda_runtime_api.h>
 
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <memory>
 #include <new>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -40,6 +42,28 @@ struct UninitAllocator : std::allocator<T> {
 template <class T>
 using RawVector = std::vector<T, UninitAllocator<T>>;
 
+// Worker count for n items at min_per_thread items or more per worker, at most cap.
+inline size_t range_workers(size_t n, size_t min_per_thread, size_t cap) {
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  return std::max<size_t>(1, std::min({hw, cap, n / min_per_thread}));
+}
+
+// Runs body(begin, end, w) over [0, n) split into `workers` contiguous ranges.  Range 0 runs
+// on the calling thread, and so does any range whose thread cannot be started.
+template <class F>
+void run_ranges(size_t n, size_t workers, const F &body) {
+  auto lo = [&](size_t w) { return n * w / workers; };
+  std::vector<std::thread> th;
+  th.reserve(workers);  // no reallocation below: a failed start leaves every thread joinable
+  try {
+    for (size_t w = 1; w < workers; ++w) th.emplace_back([&, w] { body(lo(w), lo(w + 1), w); });
+  } catch (...) {  // no thread (or no memory for its state): the rest runs here
+  }
+  body(lo(0), lo(1), 0);
+  for (size_t w = th.size() + 1; w < workers; ++w) body(lo(w), lo(w + 1), w);
+  for (std::thread &x : th) x.join();
+}
+
 struct BuildOptions {
   uint32_t min_leaf = 4;  // blazert/bvh/options.h:20-21 defaults
   uint32_t max_depth = 28;
@@ -60,7 +84,7 @@ struct TreeNode {
 };
 
 struct Tree {
-  std::vector<TreeNode> nodes;
+  RawVector<TreeNode> nodes;  // every node written by the builder or reader that fills it
   std::vector<uint32_t> leaf_prims;  // primitive ids, leaves in node order
   uint32_t max_depth = 0;
   uint32_t bad_splits = 0;
@@ -137,7 +161,7 @@ KindImage flatten(const HostScene &s, int kind, size_t max_workers = 16);
 // Persistent scene format (scene_io.cpp): a committed scene's inputs, build options and trees
 // as bytes, and back.  decode_scene fills a fresh HostScene (primitives added, trees checked
 // and attached, not committed) or returns why the bytes were refused.
-std::vector<uint8_t> encode_scene(const HostScene &s);
+RawVector<uint8_t> encode_scene(const HostScene &s);
 std::string decode_scene(const uint8_t *data, size_t size, HostScene *out);
 
 // Wavefront OBJ mesh as the reference's examples build it (obj.cpp): vertices n x 3, faces

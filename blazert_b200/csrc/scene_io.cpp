@@ -10,7 +10,11 @@
 // Layout (little endian):
 //   "BZRSCENE" | u32 version (1) | u32 min_leaf, max_depth, bins | u32 n_kinds
 //   n_kinds x { u32 kind, u32 geom_id, u64 n, the kind's input arrays, the tree }
-//   u64 FNV-1a hash of every byte before it
+//   u64 hash of every byte before it
+// The hash of version 2 (written): the bytes before it cut into blocks of 2^20 bytes (the last
+// one shorter), each block hashed with 64-bit FNV-1a, then FNV-1a over the little-endian u64
+// block hashes in order; the blocks are hashed on several threads.  Version 1 (still read) is
+// FNV-1a over all those bytes at once and otherwise the same format.
 // Input arrays: mesh u64 n_vertices, f64 vertices[3 nv], u32 faces[3 n]; spheres centres[3n],
 // radii[n]; planes centres[3n], dxs[n], dys[n], rotations[9n]; cylinders centres[3n], a[n],
 // b[n], heights[n], rotations[9n].  Tree: u64 n_nodes, per node f64 min[3], max[3], u32 leaf,
@@ -27,7 +31,9 @@ namespace bzr {
 namespace {
 
 constexpr char kMagic[8] = {'B', 'Z', 'R', 'S', 'C', 'E', 'N', 'E'};
-constexpr uint32_t kVersion = 1;
+constexpr uint32_t kVersion = 2;       // written
+constexpr uint32_t kVersionWhole = 1;  // read: one FNV-1a over all the bytes
+constexpr size_t kHashBlock = size_t(1) << 20;
 constexpr size_t kNodeBytes = 6 * sizeof(double) + 6 * sizeof(uint32_t);  // one tree node
 
 uint64_t fnv1a(const uint8_t *p, size_t n) {
@@ -39,8 +45,21 @@ uint64_t fnv1a(const uint8_t *p, size_t n) {
   return h;
 }
 
+// The version-2 hash of n bytes (see the layout above).
+uint64_t block_hash(const uint8_t *p, size_t n) {
+  const size_t nb = (n + kHashBlock - 1) / kHashBlock;
+  std::vector<uint8_t> hashes(8 * nb);
+  run_ranges(nb, range_workers(nb, 4, 16), [&](size_t b0, size_t b1, size_t) {
+    for (size_t b = b0; b < b1; ++b) {
+      const uint64_t h = fnv1a(p + b * kHashBlock, std::min(kHashBlock, n - b * kHashBlock));
+      for (int i = 0; i < 8; ++i) hashes[8 * b + i] = static_cast<uint8_t>(h >> (8 * i));
+    }
+  });
+  return fnv1a(hashes.data(), hashes.size());
+}
+
 struct Writer {
-  std::vector<uint8_t> out;
+  RawVector<uint8_t> out;  // grow() writes every byte it appends
   // appends `bytes` bytes and returns where they start
   uint8_t *grow(size_t bytes) {
     const size_t at = out.size();
@@ -95,6 +114,31 @@ void put_tree(Writer &w, const Tree &t) {
   w.put<uint64_t>(t.leaf_prims.size());
   w.put_array(t.leaf_prims.data(), t.leaf_prims.size());
   w.put<uint32_t>(t.bad_splits);
+}
+
+// Bytes encode_scene writes for the kinds order[0..n_kinds), the hash included.
+size_t encoded_size(const HostScene &s, const uint32_t *order, int n_kinds) {
+  size_t bytes = 8 + 4 + 3 * 4 + 4 + 8;
+  for (int j = 0; j < n_kinds; ++j) {
+    const Collection &c = s.kind[order[j]];
+    bytes += 4 + 4 + 8;
+    switch (order[j]) {
+      case kMesh:
+        bytes += 8 + s.vertices.size() * sizeof(double) + s.faces.size() * sizeof(uint32_t);
+        break;
+      case kSpheres:
+        bytes += 4 * c.n * sizeof(double);
+        break;
+      case kPlanes:
+        bytes += 14 * c.n * sizeof(double);
+        break;
+      case kCylinders:
+        bytes += 15 * c.n * sizeof(double);
+        break;
+    }
+    bytes += 8 + c.tree.nodes.size() * kNodeBytes + 8 + c.tree.leaf_prims.size() * 4 + 4;
+  }
+  return bytes;
 }
 
 bool finite_boxes(const PrimBoxes &b) {
@@ -154,26 +198,29 @@ std::string check_tree(Tree &t, const PrimBoxes &boxes, const BuildOptions &opt)
   if (size[0] != nn) return "nodes outside the tree";
   if (max_depth > opt.max_depth) return "tree deeper than its build options allow";
   if (finite_boxes(boxes)) {
-    std::vector<double> lo(3 * nn), hi(3 * nn);
-    for (size_t i = nn; i-- > 0;) {
+    // A leaf's box against the union of its primitives' boxes, an internal node's against the
+    // union of its children's stored boxes: with every node checked, this holds exactly when
+    // every node box equals (by value) the union of the primitive boxes under it.
+    for (size_t i = 0; i < nn; ++i) {
       const TreeNode &nd = t.nodes[i];
-      double *l = &lo[3 * i], *h = &hi[3 * i];
+      double l[3], h[3];
       if (nd.leaf == 1) {
         for (int a = 0; a < 3; ++a) {
-          l[a] = boxes.bmin[3 * t.leaf_prims[nd.prim_off] + a];
-          h[a] = boxes.bmax[3 * t.leaf_prims[nd.prim_off] + a];
+          l[a] = boxes.bmin[3 * size_t(t.leaf_prims[nd.prim_off]) + a];
+          h[a] = boxes.bmax[3 * size_t(t.leaf_prims[nd.prim_off]) + a];
         }
         for (uint32_t q = 1; q < nd.prim_cnt; ++q) {
-          const uint32_t id = t.leaf_prims[nd.prim_off + q];
+          const size_t id = t.leaf_prims[nd.prim_off + q];
           for (int a = 0; a < 3; ++a) {
             l[a] = std::fmin(l[a], boxes.bmin[3 * id + a]);
             h[a] = std::fmax(h[a], boxes.bmax[3 * id + a]);
           }
         }
       } else {
+        const TreeNode &c0 = t.nodes[nd.child[0]], &c1 = t.nodes[nd.child[1]];
         for (int a = 0; a < 3; ++a) {
-          l[a] = std::fmin(lo[3 * nd.child[0] + a], lo[3 * nd.child[1] + a]);
-          h[a] = std::fmax(hi[3 * nd.child[0] + a], hi[3 * nd.child[1] + a]);
+          l[a] = std::fmin(c0.mn[a], c1.mn[a]);
+          h[a] = std::fmax(c0.mx[a], c1.mx[a]);
         }
       }
       for (int a = 0; a < 3; ++a)
@@ -186,7 +233,7 @@ std::string check_tree(Tree &t, const PrimBoxes &boxes, const BuildOptions &opt)
 
 }  // namespace
 
-std::vector<uint8_t> encode_scene(const HostScene &s) {
+RawVector<uint8_t> encode_scene(const HostScene &s) {
   // kinds in add order (their geom ids)
   uint32_t order[kNumKinds];
   int n_kinds = 0;
@@ -194,6 +241,7 @@ std::vector<uint8_t> encode_scene(const HostScene &s) {
     for (int k = 0; k < kNumKinds; ++k)
       if (s.kind[k].present && s.kind[k].geom_id == g) order[n_kinds++] = static_cast<uint32_t>(k);
   Writer w;
+  w.out.reserve(encoded_size(s, order, n_kinds));
   w.put_array(kMagic, 8);
   w.put<uint32_t>(kVersion);
   w.put<uint32_t>(s.opt.min_leaf);
@@ -232,7 +280,7 @@ std::vector<uint8_t> encode_scene(const HostScene &s) {
     }
     put_tree(w, c.tree);
   }
-  w.put<uint64_t>(fnv1a(w.out.data(), w.out.size()));
+  w.put<uint64_t>(block_hash(w.out.data(), w.out.size()));
   return std::move(w.out);
 }
 
@@ -241,10 +289,13 @@ std::string decode_scene(const uint8_t *data, size_t size, HostScene *out) {
   if (size < 8 + 4 + 8 || std::memcmp(data, kMagic, 8) != 0) return "not a scene file";
   uint64_t stored = 0;
   std::memcpy(&stored, data + size - 8, 8);
-  if (fnv1a(data, size - 8) != stored) return "checksum mismatch (damaged file)";
+  uint32_t version = 0;
+  std::memcpy(&version, data + 8, 4);
+  if (version != kVersion && version != kVersionWhole) return "unsupported scene file version";
+  const uint64_t hash = version == kVersion ? block_hash(data, size - 8) : fnv1a(data, size - 8);
+  if (hash != stored) return "checksum mismatch (damaged file)";
   Reader r{data, size - 8};
-  r.at = 8;
-  if (r.get<uint32_t>() != kVersion) return "unsupported scene file version";
+  r.at = 12;
   HostScene &s = *out;
   s = HostScene();
   s.opt.min_leaf = r.get<uint32_t>();
@@ -293,18 +344,24 @@ std::string decode_scene(const uint8_t *data, size_t size, HostScene *out) {
     col.geom_id = geom;
     const uint64_t nn = r.get<uint64_t>();
     if (!r.ok || nn > 2 * n + 1) return "bad node count";
+    if (nn > (r.n - r.at) / kNodeBytes) return "truncated tree";
     Tree t;
     t.nodes.resize(nn);
+    const uint8_t *q = r.p + r.at;
     for (TreeNode &nd : t.nodes) {
-      for (int a2 = 0; a2 < 3; ++a2) nd.mn[a2] = r.get<double>();
-      for (int a2 = 0; a2 < 3; ++a2) nd.mx[a2] = r.get<double>();
-      nd.leaf = r.get<uint32_t>();
-      nd.axis = r.get<uint32_t>();
-      nd.child[0] = r.get<uint32_t>();
-      nd.child[1] = r.get<uint32_t>();
-      nd.prim_off = r.get<uint32_t>();
-      nd.prim_cnt = r.get<uint32_t>();
+      uint32_t u[6];
+      std::memcpy(nd.mn, q, sizeof nd.mn);
+      std::memcpy(nd.mx, q + sizeof nd.mn, sizeof nd.mx);
+      std::memcpy(u, q + sizeof nd.mn + sizeof nd.mx, sizeof u);
+      nd.leaf = u[0];
+      nd.axis = u[1];
+      nd.child[0] = u[2];
+      nd.child[1] = u[3];
+      nd.prim_off = u[4];
+      nd.prim_cnt = u[5];
+      q += kNodeBytes;
     }
+    r.at += nn * kNodeBytes;
     const uint64_t nl = r.get<uint64_t>();
     if (!r.ok || nl != n || !r.get_array(t.leaf_prims, nl)) return "truncated tree";
     t.bad_splits = r.get<uint32_t>();

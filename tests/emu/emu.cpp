@@ -92,7 +92,7 @@ void *emu_scene_create(const int *order, int n_order, const double *verts, long 
 // The persistent scene format (scene_io.cpp) on the CPU: bytes of a scene, and a scene from
 // bytes (NULL and the reason in `why` when they are refused).
 long emu_scene_encode(void *h, uint8_t *out, long cap) {
-  const std::vector<uint8_t> b = bzr::encode_scene(static_cast<Emu *>(h)->host);
+  const auto b = bzr::encode_scene(static_cast<Emu *>(h)->host);
   if (out && cap >= static_cast<long>(b.size())) std::memcpy(out, b.data(), b.size());
   return static_cast<long>(b.size());
 }

@@ -38,6 +38,16 @@ def fnv1a(b):
     return h
 
 
+def reseal(body):
+    """body followed by the hash its version field names (1: FNV-1a over the whole body; else
+    FNV-1a over the FNV-1a hashes of its 2^20-byte blocks)."""
+    if len(body) >= 12 and struct.unpack_from("<I", body, 8)[0] == 1:
+        return body + struct.pack("<Q", fnv1a(body))
+    blocks = b"".join(struct.pack("<Q", fnv1a(body[i:i + (1 << 20)]))
+                      for i in range(0, len(body), 1 << 20))
+    return body + struct.pack("<Q", fnv1a(blocks))
+
+
 rng = np.random.default_rng(0)
 scenes = [W.mixed_primitives(n_rays=2000, n_spheres=300, n_cylinders=60, n_planes=20, seed=3),
           W.icosphere_pinhole(n_rays=2000)]
@@ -69,7 +79,7 @@ for wl in scenes:
             else:
                 del b[int(rng.integers(len(b))):]
             try:
-                t = EmuScene.decode(bytes(b) + struct.pack("<Q", fnv1a(bytes(b))))
+                t = EmuScene.decode(reseal(bytes(b)))
                 t.intersect(R.origins[:64], R.directions[:64])
             except ValueError:
                 pass

@@ -23,9 +23,18 @@ def fnv1a(b: bytes) -> int:
     return h
 
 
+def block_hash(b: bytes, block=1 << 20) -> int:
+    """The version-2 hash: FNV-1a of each 2^20-byte block, then FNV-1a over the block hashes
+    as little-endian u64."""
+    return fnv1a(b"".join(struct.pack("<Q", fnv1a(b[i:i + block]))
+                          for i in range(0, len(b), block)))
+
+
 def reseal(body: bytes) -> bytes:
-    """body (without the hash) followed by its FNV-1a hash."""
-    return body + struct.pack("<Q", fnv1a(body))
+    """body (without the hash) followed by the hash its version field names: FNV-1a over the
+    whole body for version 1, the block hash otherwise."""
+    version = struct.unpack_from("<I", body, 8)[0] if len(body) >= 12 else 0
+    return body + struct.pack("<Q", fnv1a(body) if version == 1 else block_hash(body))
 
 
 def _scenes():
@@ -94,7 +103,26 @@ def test_damaged_data_is_refused():
     with pytest.raises(ValueError):
         EmuScene.decode(b"")
     with pytest.raises(ValueError, match="version"):
-        EmuScene.decode(reseal(data[:8] + struct.pack("<I", 2) + data[12:-8]))
+        EmuScene.decode(reseal(data[:8] + struct.pack("<I", 3) + data[12:-8]))
+
+
+def test_hash_is_the_block_hash_and_version_1_files_still_load():
+    """Files are written as version 2 with the block hash (blocks of 2^20 bytes, so a scene of
+    a few MB spans several); a version-1 file, the same bytes hashed with one FNV-1a over the
+    whole body, loads to the same scene, which is written back as version 2."""
+    spec = W.adjoint_scene(n_rays=16).scene
+    a = EmuScene(spec)
+    data = a.encode()
+    body = data[:-8]
+    assert len(body) > 3 << 20
+    assert struct.unpack_from("<I", body, 8)[0] == 2
+    assert struct.unpack("<Q", data[-8:])[0] == block_hash(body)
+    v1 = reseal(body[:8] + struct.pack("<I", 1) + body[12:])
+    b = EmuScene.decode(v1)
+    assert same_trees(a, b, spec) is None
+    assert b.encode() == data
+    with pytest.raises(ValueError, match="checksum"):
+        EmuScene.decode(v1[:-8] + data[-8:])  # version 1 with a version-2 hash
 
 
 def test_inconsistent_trees_are_refused():
