@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 #include <memory>
 #include <new>
 #include <string>
@@ -28,6 +29,13 @@ struct UninitAllocator : std::allocator<T> {
     using other = UninitAllocator<U>;
   };
   UninitAllocator() = default;
+#ifdef BZR_POISON_RAW  // test builds: new storage filled with 0xA5, so an unwritten element shows
+  T *allocate(size_t n) {
+    T *p = std::allocator<T>::allocate(n);
+    std::memset(static_cast<void *>(p), 0xA5, n * sizeof(T));
+    return p;
+  }
+#endif
   template <class U>
   UninitAllocator(const UninitAllocator<U> &) noexcept {}
   template <class U>

@@ -95,3 +95,56 @@ def test_flatten_image_does_not_depend_on_threads():
         one = emu.image_digest(kind, 1)
         assert [emu.image_digest(kind, w) for w in (2, 3, 16)] == [one] * 3, kind
     assert emu.image_digest("planes", 4) is None
+
+
+POISON_RUN = r'''
+import hashlib, json, os, sys
+import numpy as np
+sys.path.insert(0, os.environ["BZR_ROOT"])
+import tests.emu.emu as E
+E.build = lambda force=False, out=None, flags=(): os.environ["BZR_EMU_LIB"]
+from tests.test_emu import _raw_storage_results
+print(json.dumps(_raw_storage_results()))
+'''
+
+
+def _raw_storage_results():
+    """Image digests (every kind, 1 and 16 threads) and scene-file hashes of scenes that take
+    the threaded paths, small and edge-case scenes."""
+    rng = np.random.default_rng(12)
+    n = 150_000
+    specs = [W.SceneSpec().add_mesh(*W.icosphere(7)).add_spheres(
+                 rng.uniform(-10.0, 10.0, (n, 3)), rng.uniform(0.01, 0.1, n)),
+             W.mixed_primitives(n_rays=16).scene]
+    specs += [spec for _, spec, _ in edge_case_scenes()]
+    out = []
+    for spec in specs:
+        emu = EmuScene(spec)
+        out.append([emu.image_digest(k, w) for k in spec.order for w in (1, 16)])
+        data = emu.encode()
+        out.append(__import__("hashlib").sha256(data).hexdigest())
+        out.append(EmuScene.decode(data).encode() == data)
+    return out
+
+
+def test_raw_storage_is_written_in_full(tmp_path):
+    """The host arrays allocated without zero-fill (prim boxes, tree nodes, device images, the
+    scene-file buffer) must be written in full: an emulator built with BZR_POISON_RAW, which
+    fills that storage with 0xA5 bytes when it is allocated, gives the same images and files as
+    the normal build."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    from tests.emu import emu as E
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib = E.build(out=str(tmp_path / "libemu_poison.so"), flags=("-DBZR_POISON_RAW",))
+    script = tmp_path / "run.py"
+    script.write_text(POISON_RUN)
+    r = subprocess.run([sys.executable, str(script)], capture_output=True, text=True, timeout=900,
+                       env=dict(os.environ, BZR_EMU_LIB=lib, BZR_ROOT=root))
+    assert r.returncode == 0, r.stderr[-3000:]
+    poisoned = json.loads(r.stdout.strip().splitlines()[-1])
+    assert poisoned == json.loads(json.dumps(_raw_storage_results()))
