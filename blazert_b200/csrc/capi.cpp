@@ -1042,13 +1042,32 @@ int bzr_scene_load(bzr_scene **out, const char *path) {
   *out = nullptr;
   std::FILE *f = std::fopen(path, "rb");
   if (!f) return fail(BZR_EINVAL, std::string("cannot open: ") + path);
-  std::vector<uint8_t> b;
-  uint8_t chunk[1 << 16];
-  size_t got;
-  while ((got = std::fread(chunk, 1, sizeof chunk, f)) > 0) b.insert(b.end(), chunk, chunk + got);
-  const bool err = std::ferror(f) != 0;
+  bzr::RawVector<uint8_t> b;
+  bool err = false;
+  try {
+    // one read when the file's size is known; 64 KiB pieces otherwise (a pipe)
+    long size = -1;
+    if (std::fseek(f, 0, SEEK_END) == 0) {
+      size = std::ftell(f);
+      err = std::fseek(f, 0, SEEK_SET) != 0;
+    }
+    if (size >= 0 && !err) {
+      b.resize(static_cast<size_t>(size));
+      err = std::fread(b.data(), 1, b.size(), f) != b.size();
+    } else if (!err) {
+      uint8_t chunk[1 << 16];
+      size_t got;
+      while ((got = std::fread(chunk, 1, sizeof chunk, f)) > 0)
+        b.insert(b.end(), chunk, chunk + got);
+    }
+    err = err || std::ferror(f) != 0;
+  } catch (const std::bad_alloc &) {
+    std::fclose(f);
+    return fail(BZR_ENOMEM, std::string("host allocation failed while reading: ") + path);
+  }
   std::fclose(f);
   if (err) return fail(BZR_EINVAL, std::string("read failed: ") + path);
+  if (b.empty()) return fail(BZR_EINVAL, std::string("not a scene file (empty): ") + path);
   return bzr_scene_deserialize(out, b.data(), b.size());
 }
 

@@ -255,3 +255,42 @@ def test_python_inputs_are_checked_not_reshaped():
     assert B.Scene().add_spheres(np.zeros(6), np.ones(2)) == 0  # flat centres
     assert B.Scene().add_cylinders(np.zeros((1, 3)), [1.0], [1.0], [2.0], np.eye(3)) == 0
     assert B.Scene().add_planes(np.zeros((2, 3)), [1.0, 1.0], [1.0, 1.0], np.zeros((2, 9))) == 0
+
+
+def test_scene_file_reading_without_gpu(tmp_path):
+    """bzr_scene_load reads the whole file (in one read, or in pieces from a pipe) and checks it
+    before the commit, which is the step that needs a device: a valid file gets as far as
+    BZR_ENODEV here, a damaged, empty or missing one is refused with its reason."""
+    import threading
+
+    from blazert_b200 import workloads as W
+    from tests.emu.emu import EmuScene
+
+    lib = B.library()
+    lib.bzr_scene_load.argtypes = [C.POINTER(C.c_void_p), C.c_char_p]
+    lib.bzr_last_error_string.restype = C.c_char_p
+    data = EmuScene(W.mixed_primitives(n_rays=16).scene).encode()
+
+    def load(path):
+        out = C.c_void_p()
+        rc = lib.bzr_scene_load(C.byref(out), str(path).encode())
+        assert not out.value
+        return rc, lib.bzr_last_error_string().decode()
+
+    good = tmp_path / "good.bzrscene"
+    good.write_bytes(data)
+    assert load(good)[0] == B.ENODEV
+    bad = tmp_path / "bad.bzrscene"
+    bad.write_bytes(data[:100] + bytes([data[100] ^ 1]) + data[101:])
+    assert load(bad)[0] == B.EINVAL and "checksum" in load(bad)[1]
+    empty = tmp_path / "empty.bzrscene"
+    empty.write_bytes(b"")
+    assert load(empty)[0] == B.EINVAL and "empty" in load(empty)[1]
+    assert load(tmp_path / "missing.bzrscene")[0] == B.EINVAL
+    if hasattr(os, "mkfifo"):
+        fifo = tmp_path / "pipe.bzrscene"
+        os.mkfifo(fifo)
+        writer = threading.Thread(target=lambda: fifo.write_bytes(data))
+        writer.start()
+        assert load(fifo)[0] == B.ENODEV
+        writer.join(timeout=60)
