@@ -1,26 +1,33 @@
 #!/usr/bin/env python3
-"""Mrays/s of blazeRT closest-hit queries (intersect1 semantics) on B200.
+"""Mrays/s of blazeRT closest-hit queries (intersect1 semantics) on B200: FP64 vs mixed.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload mixed_primitives] [--mode fp64|mixed]
+                    [--workload heightfield] [--mode both|fp64|mixed]
 
-Workload (default): the mixed-primitive scene -- 10,000 spheres, 1,000 cylinders and 100
-finite planes in [-100, 100]^3 -- with 1,048,576 incoherent rays (origins in [-120, 120]^3,
-isotropic directions), float64, seeded.  A step is one intersectN over the whole batch.
+Workload (default): the 2,093,058-triangle heightfield -- a 1024 x 1024 vertex grid over
+[0, 1000]^2 with 6-octave value-noise fBm heights (amplitude 100) -- and 8,388,608 secondary
+rays leaving the surface (area-weighted points offset 1e-6 along the normal, cosine-weighted
+directions), float64, seeded.  A step is one intersectN over the whole batch.
 
-  value      Mrays/s over all ranks, rays resident in HBM, device time (CUDA events on the
-             launching stream), the L2 flushed (256 MiB written) between timed steps.
+  value      Mrays/s of the FP64 path over all ranks, rays resident in HBM, device time (CUDA
+             events on the launching stream), the L2 flushed (256 MiB written) between timed
+             steps.
+  precision  the mixed FP32/FP64 path timed the same way on the same rays (--mode both, the
+             default): its Mrays/s, its ratio to the FP64 path, hit mismatches and distance
+             errors against the FP64 path's results, and its own e2e.
   e2e        the same metric through the public host API (Scene.intersectN with pinned host
              arrays): host->device copy of the rays, the kernel, device->host copy of all
              results, every step.
-  roofline   algorithmic bytes of the traversal kernel / its event time, against the measured
-             HBM copy bandwidth (MEASURED_PEAKS.json).  Bytes per ray: ray I/O (121 B) +
-             64 B per box test (half of a 128-byte two-child FP64 node) + the leaf-ordered
-             primitive record per primitive test; counts come from the counting kernel.
+  roofline   the FP64 traversal kernel against two measured ceilings: algorithmic bytes (ray
+             I/O 121 B + 64 B per box test + the primitive record per primitive test; counts
+             from the counting kernel) against the L2 read bandwidth measured in the run
+             (bound "l2"), and the compulsory bytes (ray I/O + the scene's device image once)
+             against the HBM copy bandwidth (MEASURED_PEAKS.json).
   cpu_baseline  the reference's own intersect1 loop (its headers, release flags, OpenMP over
-             all host cores) on the same rays, rank 0 at N = 1.
+             all host cores) on a bounded sample of the same rays, rank 0 at N = 1; also on
+             one core, with the host's CPU model.
 
-Other forms: --workload heightfield | icosphere_pinhole (same line), batched_icospheres
+Other forms: --workload mixed_primitives | icosphere_pinhole (same line), batched_icospheres
 (batching), adjoint_scene (differentiation), distance_queries (the reference's per-primitive
 distance_to_surface over 4M (primitive, point) pairs per kind, Mqueries/s) and closest_surface
 (nearest surface over the scene for 1M points, Mqueries/s).
@@ -56,8 +63,10 @@ def parse(argv=None):
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mixed_primitives")
-    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="heightfield")
+    ap.add_argument("--mode", default="both", choices=["both", "fp64", "mixed"],
+                    help="both: value = the FP64 path, precision = the mixed path on the same "
+                         "rays")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -142,22 +151,40 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# Rays of the bounded CPU samples (all host cores; one core), per workload: about 10 s and 5 s
+# of the reference's ray loop.
+CPU_SAMPLE_RAYS = {"heightfield": 1 << 20}
+CPU_ONE_CORE_RAYS = {"heightfield": 1 << 16, "mixed_primitives": 1 << 16,
+                     "icosphere_pinhole": 1 << 18, "adjoint_scene": 1 << 16}
+
+
 def cpu_baseline(workload, seconds, max_rays=0):
-    cmd = [sys.executable, "-m", "oracle.cpu_baseline", "--workload", workload,
-           "--seconds", str(seconds)]
-    if max_rays:
-        cmd += ["--max-rays", str(max_rays)]
-    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900)
-    if r.returncode != 0:
-        return {"error": r.stderr.strip()[-400:]}
-    return json.loads(r.stdout.strip().splitlines()[-1])
+    """The reference's intersect1 loop on this host: all cores (the reported baseline) and one
+    core (comparable with the reference's own single-thread plots), with the CPU model."""
+    def run(threads, secs, rays):
+        cmd = [sys.executable, "-m", "oracle.cpu_baseline", "--workload", workload,
+               "--seconds", str(secs), "--threads", str(threads)]
+        if rays:
+            cmd += ["--max-rays", str(rays)]
+        r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900)
+        if r.returncode != 0:
+            return {"error": r.stderr.strip()[-400:]}
+        return json.loads(r.stdout.strip().splitlines()[-1])
+
+    out = run(0, seconds, max_rays)
+    if "error" not in out:
+        one = run(1, seconds / 2, CPU_ONE_CORE_RAYS.get(workload, 1 << 16))
+        out["one_core"] = {k: one.get(k) for k in ("value", "unit", "sample", "error") if k in one}
+    return out
 
 
-def config_of(args, wl, world):
+def config_of(args, wl, world, mode="fp64"):
     m = wl.meta
     return {"workload": args.workload, "rays_per_gpu": wl.rays.n,
             "scene": {k: v for k, v in m.items() if k != "seed"},
-            "seed": m.get("seed"), "mode": args.mode, "parallelism": f"replicated-scene x{world}",
+            "seed": m.get("seed"), "mode": mode,
+            "modes_timed": ["fp64", "mixed"] if args.mode == "both" else [args.mode],
+            "parallelism": f"replicated-scene x{world}",
             "rays": "any-hit (shadow)" if getattr(args, "any_hit", False) else "closest-hit",
             "l2": "flushed between timed steps (256 MiB write)"}
 
@@ -167,6 +194,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     from blazert_b200 import workloads as W
+    from oracle.cpu_baseline import host_cpu
     from oracle.oracle import Oracle, RefScene
     threads = os.cpu_count() or 1
     if args.workload in W.DISTANCE_WORKLOADS:
@@ -211,7 +239,8 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)", "config": config_of(args, wl, 1), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": kind,
-                             "sample": f"{args.workload}: full batch of {R.n} rays per step"},
+                             "sample": f"{args.workload}: full batch of {R.n} rays per step",
+                             **host_cpu()},
             "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -304,6 +333,72 @@ def run_batched(args):
     return 0
 
 
+def l2_read_peak():
+    """Measured L2 -> SM read bandwidth of the current GPU (GB/s): the probe library's
+    ld.global.cg read of buffers that fit in L2, best over a few sizes (per-size figures too)."""
+    import ctypes as C
+    path = os.path.join(ROOT, "blazert_b200", "_lib", "libbzr_probe.so")
+    if not os.path.exists(path):
+        return None, {}
+    lib = C.CDLL(path)
+    lib.bzr_probe_read_gbs.argtypes = [C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    lib.bzr_probe_read_gbs.restype = C.c_int
+    per = {}
+    for mb in (8, 16, 32, 48):
+        g = C.c_double(0.0)
+        if lib.bzr_probe_read_gbs(mb << 20, 40, 1, C.byref(g)) == 0:
+            per[f"{mb}MiB"] = g.value
+    return (max(per.values()) if per else None), per
+
+
+def scene_bytes(scene, wl):
+    """Bytes of the FP64 device image a launch needs at least once (S of the compulsory HBM
+    ceiling): per kind 128 B per internal node plus the leaf-ordered primitive data (mesh:
+    16 B per triangle and 32 B per vertex)."""
+    total = 0
+    rec = {"spheres": 32 + 4, "planes": 112 + 4, "cylinders": 128 + 4}
+    for kind in wl.scene.order:
+        st = scene.build_statistics(kind)
+        total += 128 * st["branch_nodes"]
+        if kind == "mesh":
+            total += 16 * len(wl.scene.mesh["faces"]) + 32 * len(wl.scene.mesh["vertices"])
+        else:
+            total += rec[kind] * len(next(iter(getattr(wl.scene, kind).values())))
+    return total
+
+
+def time_steps(step, stream, flush, steps, warmup, dev, pg):
+    """W untimed steps, then K steps each bracketed by CUDA events on `stream`, the L2 flushed
+    (256 MiB written) before every step; barrier + synchronize on both sides of the timed
+    region.  Returns the per-step times and their total, the max over ranks."""
+    import torch
+
+    from blazert_b200 import multi
+    for i in range(warmup):
+        flush.fill_(i & 0xFF)
+        step()
+    torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    for i in range(steps):
+        flush.fill_((i + 1) & 0xFF)  # untimed: evicts the previous step's rays from L2
+        evs[i][0].record(stream)
+        step()
+        evs[i][1].record(stream)
+    torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    if pg:
+        total_ms = multi.max_over_ranks(total_ms)
+    return step_ms, total_ms
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -319,10 +414,10 @@ def run_ours(args):
                                 device_id=dev)
         pg = dist
     import blazert_b200 as B
+    from blazert_b200 import multi
     from blazert_b200 import workloads as W
 
-    from blazert_b200 import multi
-
+    modes = ["fp64", "mixed"] if args.mode == "both" else [args.mode]
     wl = W.WORKLOADS[args.workload](**({"n_rays": args.rays} if args.rays else {}))
     R = wl.rays
     if rank > 0:  # weak scaling: each rank traces its own full-size batch
@@ -340,93 +435,119 @@ def run_ours(args):
     tmn = torch.from_numpy(R.tmin).to(dev)
     tmx = torch.from_numpy(R.tmax).to(dev)
     f64 = torch.float64
-    out = dict(t=torch.empty(n, dtype=f64, device=dev), uv=torch.empty((n, 2), dtype=f64, device=dev),
-               normal=torch.empty((n, 3), dtype=f64, device=dev),
-               prim=torch.empty(n, dtype=torch.int32, device=dev),
-               geom=torch.empty(n, dtype=torch.int32, device=dev),
-               hit=torch.empty(n, dtype=torch.uint8, device=dev))
+
+    def outputs():
+        return dict(t=torch.empty(n, dtype=f64, device=dev),
+                    uv=torch.empty((n, 2), dtype=f64, device=dev),
+                    normal=torch.empty((n, 3), dtype=f64, device=dev),
+                    prim=torch.empty(n, dtype=torch.int32, device=dev),
+                    geom=torch.empty(n, dtype=torch.int32, device=dev),
+                    hit=torch.empty(n, dtype=torch.uint8, device=dev))
+
+    outs = {m: outputs() for m in modes}
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
+    l2_peak, l2_sizes = l2_read_peak()
+    hbm_peak, peak_src = load_peaks()
 
-    tuning = None
-    if args.sort == "auto":
-        from blazert_b200.autotune import autotune
-        tuning = autotune(scene, o, d, tmn, tmx, mode=args.mode, stream=stream)
-    else:
-        scene.tune(sort=args.sort == "on")
-
-    def step():
-        scene.intersectN(o, d, tmn, tmx, mode=args.mode, out=out, stream=stream,
-                         any_hit=args.any_hit)
-
-    for i in range(args.warmup):
-        flush.fill_(i & 0xFF)
-        step()
-    torch.cuda.synchronize(dev)
-    scene.check()
-    if pg:
-        pg.barrier()
-    torch.cuda.synchronize(dev)
     sampler = ClockSampler(local) if rank == 0 else None
     if sampler:
         sampler.start()
         time.sleep(0.3)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
+    res = {}
     wall0 = time.perf_counter()
-    for i in range(args.steps):
-        flush.fill_((i + 1) & 0xFF)  # untimed: evicts the previous step's rays from L2
-        evs[i][0].record(stream)
-        step()
-        evs[i][1].record(stream)
-    torch.cuda.synchronize(dev)
-    if pg:
-        pg.barrier()
-    torch.cuda.synchronize(dev)
+    for m in modes:
+        tuning = None
+        if args.sort == "auto":
+            from blazert_b200.autotune import autotune
+            tuning = autotune(scene, o, d, tmn, tmx, mode=m, stream=stream)
+        else:
+            scene.tune(sort=args.sort == "on")
+
+        def step(m=m):
+            scene.intersectN(o, d, tmn, tmx, mode=m, out=outs[m], stream=stream,
+                             any_hit=args.any_hit)
+
+        step_ms, total_ms = time_steps(step, stream, flush, args.steps, args.warmup, dev, pg)
+        scene.check()
+        res[m] = dict(step_ms=step_ms, total_ms=total_ms, tuning=tuning,
+                      value=world * n * args.steps / (total_ms / 1e3) / 1e6)
     wall = time.perf_counter() - wall0
     clocks = sampler.stop() if sampler else None
-    scene.check()
-    step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = sum(step_ms)
-    if pg:
-        total_ms = multi.max_over_ranks(total_ms)
-    value = world * n * args.steps / (total_ms / 1e3) / 1e6
+    primary = modes[0]
+    value, total_ms, step_ms = res[primary]["value"], res[primary]["total_ms"], res[primary]["step_ms"]
+    out = outs[primary]
     hits = float(out["hit"].float().mean().item())
+
     precision = None
-    if args.mode == "mixed":  # the precision form's report: its results against the FP64 path's
-        ref = scene.intersectN(o, d, tmn, tmx, mode="fp64", stream=stream, any_hit=args.any_hit)
+    if "mixed" in modes:  # the precision form's report: its results against the FP64 path's
+        got = outs["mixed"]
+        ref = outs["fp64"] if "fp64" in outs else scene.intersectN(
+            o, d, tmn, tmx, mode="fp64", stream=stream, any_hit=args.any_hit)
         torch.cuda.synchronize(dev)
-        hm = out["hit"] == ref["hit"]
-        same = hm & (out["prim"] == ref["prim"]) & (out["geom"] == ref["geom"])
-        both = (out["hit"] == 1) & (ref["hit"] == 1)
-        rel = ((out["t"] - ref["t"]).abs() / ref["t"].abs().clamp_min(1e-300))[both]
-        precision = {"vs": "FP64 GPU path (bit-identical to the oracle in the parity tests)",
-                     "hit_mismatches": int((~same).sum().item()),
-                     "t_max_rel_err": float(rel.max().item()) if rel.numel() else 0.0,
-                     "t_mean_rel_err": float(rel.mean().item()) if rel.numel() else 0.0,
-                     "bit_identical": bool(torch.equal(out["t"].view(torch.int64),
-                                                       ref["t"].view(torch.int64))
-                                           and torch.equal(out["normal"].view(torch.int64),
-                                                           ref["normal"].view(torch.int64))
-                                           and torch.equal(out["uv"].view(torch.int64),
-                                                           ref["uv"].view(torch.int64)))}
+        same = (got["hit"] == ref["hit"]) & (got["prim"] == ref["prim"]) & \
+            (got["geom"] == ref["geom"])
+        both = (got["hit"] == 1) & (ref["hit"] == 1)
+        rel = ((got["t"] - ref["t"]).abs() / ref["t"].abs().clamp_min(1e-300))[both]
+        eq = lambda k: torch.equal(got[k].view(torch.int64), ref[k].view(torch.int64))
+        precision = {
+            "mode": "mixed", "value": res["mixed"]["value"], "unit": "Mrays/s",
+            "ms_per_step": res["mixed"]["total_ms"] / args.steps,
+            "vs_fp64": (res["mixed"]["value"] / res["fp64"]["value"]) if "fp64" in res else None,
+            "against": "FP64 GPU path of the same run (bit-identical to the oracle in the "
+                       "parity tests)",
+            "hit_mismatches": int((~same).sum().item()),
+            "t_max_rel_err": float(rel.max().item()) if rel.numel() else 0.0,
+            "t_mean_rel_err": float(rel.mean().item()) if rel.numel() else 0.0,
+            "t_uv_normal_bit_identical": bool(eq("t") and eq("uv") and eq("normal")),
+            "tuning": res["mixed"]["tuning"],
+            "step_ms_min_max": [min(res["mixed"]["step_ms"]), max(res["mixed"]["step_ms"])]}
     # one traversal kernel per primitive kind present, per step
     n_passes = sum(1 for k in wl.scene.order if len(next(iter(getattr(wl.scene, k).values()))))
 
-    # roofline: algorithmic bytes from the kernel's own work counts (untimed counting run)
+    # roofline of the primary path's traversal kernel.  Algorithmic bytes from the kernel's own
+    # work counts (untimed counting run): ray I/O + 64 B per box test (half a 128-byte two-child
+    # node) + the primitive record per primitive test.
     counts = scene.work_counts(o, d, tmn, tmx, stream=stream)
     alg_bytes = n * RAY_IO_BYTES + BOX_TEST_BYTES * sum(counts["box"]) + \
         sum(PRIM_RECORD_BYTES[k] * counts["prim"][k] for k in range(4))
     mean_ms = statistics.mean(step_ms)
     achieved = alg_bytes / (mean_ms / 1e3) / 1e9
-    peak, peak_src = load_peaks()
-    traffic = None
+    s_bytes = scene_bytes(scene, wl)
+    hbm_need = n * RAY_IO_BYTES + s_bytes
+    hbm_achieved = hbm_need / (mean_ms / 1e3) / 1e9
+    traffic, traffic_src = None, None
     tf = os.path.join(ROOT, "profiles", f"trace_fp64_{args.workload}.json")
-    if os.path.exists(tf) and not args.any_hit:
+    if os.path.exists(tf) and not args.any_hit and primary == "fp64":
         with open(tf) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+            tj = json.load(f)
+        traffic = tj.get("dram_bytes_per_launch")
+        traffic_src = tj.get("source")
+    frac_l2 = achieved / l2_peak if l2_peak else None
+    roofline = {
+        "bound": "l2", "achieved": achieved, "peak": l2_peak, "unit": "GB/s", "frac": frac_l2,
+        "traffic": traffic, "traffic_source": traffic_src,
+        "peak_source": "measured in this run (L2-resident ld.global.cg read, best of "
+                       + ", ".join(f"{k}: {v:.0f}" for k, v in l2_sizes.items()) + " GB/s)",
+        "alg_bytes_per_ray": alg_bytes / n,
+        "box_tests_per_ray": [c / n for c in counts["box"]],
+        "prim_tests_per_ray": [c / n for c in counts["prim"]],
+        "ceilings": {
+            "l2": {"achieved": achieved, "peak": l2_peak, "frac": frac_l2,
+                   "what": "algorithmic traversal bytes (ray I/O + box tests + primitive "
+                           "records) / kernel time, against the measured L2 read bandwidth"},
+            "hbm_compulsory": {"achieved": hbm_achieved, "peak": hbm_peak, "frac":
+                               hbm_achieved / hbm_peak, "peak_source": peak_src,
+                               "bytes_per_ray": RAY_IO_BYTES + s_bytes / n,
+                               "what": "(ray I/O 120 B + scene bytes S / rays R) per ray, "
+                                       "against the measured HBM copy bandwidth"}},
+        "binding": ("latency and SIMD divergence: neither byte ceiling is reached (see the "
+                    "ncu summaries: long-scoreboard stalls, active lanes per warp)"
+                    if (frac_l2 or 0) < 0.6 and hbm_achieved / hbm_peak < 0.6 else "bandwidth"),
+        "note": ("work counts are the closest-hit traversal's; any-hit rays do less, so "
+                 "achieved is an upper bound") if args.any_hit else None}
 
-    e2e = None
+    e2e, e2e_mixed = None, None
     if not args.no_e2e:
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
         ho, hd, htmn, htmx = pin(R.origins), pin(R.directions), pin(R.tmin), pin(R.tmax)
@@ -439,47 +560,52 @@ def run_ours(args):
         host_tuning = None
         if args.sort == "auto" and not args.any_hit:
             from blazert_b200.autotune import autotune_host
-            host_tuning = autotune_host(scene, ho, hd, htmn, htmx, out=hout, mode=args.mode)
+            host_tuning = autotune_host(scene, ho, hd, htmn, htmx, out=hout, mode=primary)
             host_tuning = {"choice": host_tuning["choice"], "best_ms": host_tuning["best_ms"]}
-        for _ in range(max(1, args.warmup)):
-            scene.intersectN(ho, hd, htmn, htmx, mode=args.mode, out=hout, any_hit=args.any_hit)
-        if pg:
-            pg.barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            scene.intersectN(ho, hd, htmn, htmx, mode=args.mode, out=hout, any_hit=args.any_hit)
-        el = time.perf_counter() - t0
-        if pg:
-            el = multi.max_over_ranks(el)
-        e2e = {"value": world * n * args.steps / el / 1e6, "unit": "Mrays/s",
-               "h2d_bytes_per_step": n * (24 + 24 + 8 + 8),
-               "d2h_bytes_per_step": n * (8 + 16 + 24 + 4 + 4 + 1), "host_tuning": host_tuning}
-        ok = np.array_equal(hout["prim"], out["prim"].cpu().numpy().view(np.uint32))
-        if not ok:
-            e2e["warning"] = "host-path results differ from the device path"
+
+        def e2e_of(m):
+            if res[m]["tuning"]:  # the device knobs this mode was timed with
+                c = res[m]["tuning"]["choice"]
+                scene.tune(sort=c["sort"], sort_min_rays=0 if c["sort"] else 1 << 16,
+                           threads=c["threads"], shared_stack=c["shared_stack"], chunk=c["chunk"])
+            for _ in range(max(1, args.warmup)):
+                scene.intersectN(ho, hd, htmn, htmx, mode=m, out=hout, any_hit=args.any_hit)
+            if pg:
+                pg.barrier()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                scene.intersectN(ho, hd, htmn, htmx, mode=m, out=hout, any_hit=args.any_hit)
+            el = time.perf_counter() - t0
+            if pg:
+                el = multi.max_over_ranks(el)
+            r = {"value": world * n * args.steps / el / 1e6, "unit": "Mrays/s",
+                 "h2d_bytes_per_step": n * (24 + 24 + 8 + 8),
+                 "d2h_bytes_per_step": n * (8 + 16 + 24 + 4 + 4 + 1), "mode": m}
+            if not np.array_equal(hout["prim"], outs[m]["prim"].cpu().numpy().view(np.uint32)):
+                r["warning"] = "host-path results differ from the device path"
+            return r
+
+        e2e = e2e_of(primary)
+        e2e["host_tuning"] = host_tuning
+        if precision is not None and primary != "mixed":
+            e2e_mixed = e2e_of("mixed")
+            precision["e2e"] = e2e_mixed
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.workload, args.cpu_seconds)
+        cpu = cpu_baseline(args.workload, args.cpu_seconds,
+                           max_rays=CPU_SAMPLE_RAYS.get(args.workload, 0))
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)", "config": config_of(args, wl, world),
-            "e2e": e2e, "gpu_launches": args.steps * n_passes,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": peak_src,
-                         "alg_bytes_per_ray": alg_bytes / n,
-                         "box_tests_per_ray": [c / n for c in counts["box"]],
-                         "prim_tests_per_ray": [c / n for c in counts["prim"]],
-                         "note": ("work counts are the closest-hit traversal's; any-hit rays do "
-                                  "less, so achieved is an upper bound") if args.any_hit else None},
-            "cpu_baseline": cpu, "clocks": clocks, "hit_fraction": hits, "precision": precision,
-            "commit_seconds": commit_s, "wall_seconds_timed": wall, "tuning": tuning,
-            "step_ms_min_max": [min(step_ms), max(step_ms)],
+            "data": "synthetic (seeded)", "config": config_of(args, wl, world, primary),
+            "e2e": e2e, "gpu_launches": args.steps * n_passes * len(modes),
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "hit_fraction": hits,
+            "precision": precision, "commit_seconds": commit_s, "wall_seconds_timed": wall,
+            "tuning": res[primary]["tuning"], "step_ms_min_max": [min(step_ms), max(step_ms)],
         }
         print(json.dumps(line), flush=True)
     scene.close()
@@ -811,6 +937,8 @@ def main(argv=None):
     args = parse(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload in ("batched_icospheres", "adjoint_scene") and args.mode == "both":
+        args.mode = "fp64"  # these forms time one path per run
     if args.workload == "batched_icospheres":
         return run_batched(args)
     if args.workload == "adjoint_scene":

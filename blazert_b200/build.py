@@ -20,6 +20,8 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libblazert_b200.so")
+# measurement-only read-bandwidth probe (the roofline's L2 ceiling), kept out of the product
+PROBE = os.path.join(LIBDIR, "libbzr_probe.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXX = os.environ.get("BZR_CXX", "g++")
@@ -73,6 +75,12 @@ def build(force=False, verbose=False, ptxas_verbose=False):
         subprocess.run(cmd, check=True)
     if force or _stale(LIB, objs):
         cmd = [nvcc] + ARCH + ["-shared", "-ccbin", CXX, "-o", LIB] + objs
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    probe_src = os.path.join(CSRC, "probe.cu")
+    if force or _stale(PROBE, [probe_src]):
+        cmd = [nvcc] + CU_FLAGS + ["-shared", "-o", PROBE, probe_src]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

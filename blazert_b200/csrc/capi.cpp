@@ -101,6 +101,9 @@ struct bzr_scene {
   size_t host_chunks = kHostChunks, host_min_chunk = kMinChunk;  // bzr_scene_tune
   size_t host_edge = 0;  // rays of the first and last chunk (0: all chunks the same size)
   int host_grid_div = 1;  // host-array chunks launch 1/host_grid_div of each kind's grid
+  // a host-array call returned BZR_ETIMEOUT while its copies and kernels were still queued on
+  // the pipeline streams, using the staging blocks (see settle_staging)
+  bool stage_pending = false;
 
   ~bzr_scene() {
     if (device >= 0) {
@@ -469,6 +472,27 @@ static int wait_stream_spin(cudaStream_t st, int spin_us) {
   return wait_stream(st, default_timeout_ms());
 }
 
+// A host-array call that timed out left its copies and kernels queued on the pipeline streams,
+// still reading and writing the staging blocks.  Before a later call reuses them, every
+// pipeline stream must have finished; if one is still busy after the bounded wait, that call
+// times out too and the staging stays reserved.  The caller holds stage_mu.
+static int settle_staging(bzr_scene *s) {
+  if (!s->stage_pending) return BZR_OK;
+  for (cudaStream_t q : {s->copy_in, s->streams[0], s->streams[1], s->streams[2], s->copy_out}) {
+    if (!q) continue;
+    const int rc = wait_stream(q, default_timeout_ms());
+    if (rc) return rc;
+  }
+  s->stage_pending = false;
+  return BZR_OK;
+}
+
+// Return code of a wait on queued host-array work; a timeout marks the staging as still in use.
+static int staged_wait_result(bzr_scene *s, int rc) {
+  if (rc == BZR_ETIMEOUT) s->stage_pending = true;
+  return rc;
+}
+
 // The latency path of small host-array batches (the caller holds stage_mu).  One pinned block
 // mirrors one device block: inputs org, dir, [tmin], [tmax]; then the error word; then the
 // outputs t, [uv], [normal], [prim], [geom], [hit]; each piece 256-byte aligned.  One copy in,
@@ -540,7 +564,7 @@ static int run_small(bzr_scene *s, size_t n, const double *org, const double *di
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(h + p_err.off, d + p_err.off, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
   if (e != cudaSuccess) return cuda_fail(e, "small batch submission");
-  const int rc = wait_stream_spin(st, 2000);
+  const int rc = staged_wait_result(s, wait_stream_spin(st, 2000));
   if (rc) return rc;
   if (t) std::memcpy(t, h + p_t.off, p_t.bytes);
   if (uv) std::memcpy(uv, h + p_uv.off, p_uv.bytes);
@@ -610,6 +634,7 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
   // Host arrays: stage through device buffers on the scene's stream.
   std::lock_guard<std::mutex> lock(s->stage_mu);
   if (const cudaError_t ce = make_pipeline(s)) return cuda_fail(ce, "cudaStreamCreate");
+  if (const int rc = settle_staging(s)) return rc;
   if (n <= kSmallBatch)
     return run_small(s, n, org, dir, tmin, tmax, t, uv, normal, prim, geom, hit, mode, io,
                      counters, totals);
@@ -720,7 +745,7 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
   }
   if (e != cudaSuccess) return cuda_fail(e, "batch submission");
   for (cudaStream_t q : {s->copy_in, s->streams[0], s->streams[1], s->streams[2], s->copy_out}) {
-    const int rc = wait_stream(q, default_timeout_ms());
+    const int rc = staged_wait_result(s, wait_stream(q, default_timeout_ms()));
     if (rc) return rc;
   }
   uint32_t bits = 0;
@@ -894,6 +919,7 @@ static int run_distance(const bzr_scene *cs, int kind, size_t n, const uint32_t 
   // copy_out once its kernel is done -- with stream-ordered staging from the scene's pool.
   std::lock_guard<std::mutex> lock(s->stage_mu);
   if (const cudaError_t ce = make_pipeline(s)) return cuda_fail(ce, "cudaStreamCreate");
+  if (const int rc = settle_staging(s)) return rc;
   // bytes per query of each staged array: ids, points | distance, closest, prim, geom
   const size_t per[6] = {kind >= 0 ? 4u : 0u, 24, 8, closest ? 24u : 0u, prim ? 4u : 0u,
                          geom ? 4u : 0u};
@@ -958,7 +984,7 @@ static int run_distance(const bzr_scene *cs, int kind, size_t n, const uint32_t 
   }
   cudaFreeAsync(dev - 256, s->copy_out);
   (void)st;
-  const int rc = wait_stream_spin(s->copy_out, 200);
+  const int rc = staged_wait_result(s, wait_stream_spin(s->copy_out, 200));
   if (rc) return rc;
   if (s->pinned_err[0] & bzr::kErrPrimIndex)
     return fail(BZR_EINVAL, "primitive id outside the kind (its distance is NaN)");
@@ -1045,16 +1071,20 @@ int bzr_scene_load(bzr_scene **out, const char *path) {
   bzr::RawVector<uint8_t> b;
   bool err = false;
   try {
-    // one read when the file's size is known; 64 KiB pieces otherwise (a pipe)
+    // One read of the size the file reports, then 64 KiB pieces up to the end of the file:
+    // a pipe reports no size, procfs-like files report 0 for content they have, and a file
+    // that grew after the size was taken is read to its end.
     long size = -1;
     if (std::fseek(f, 0, SEEK_END) == 0) {
       size = std::ftell(f);
       err = std::fseek(f, 0, SEEK_SET) != 0;
     }
-    if (size >= 0 && !err) {
+    if (size > 0 && !err) {
       b.resize(static_cast<size_t>(size));
-      err = std::fread(b.data(), 1, b.size(), f) != b.size();
-    } else if (!err) {
+      const size_t got = std::fread(b.data(), 1, b.size(), f);
+      b.resize(got);  // a file that shrank meanwhile: keep what was read
+    }
+    if (!err && !std::ferror(f)) {
       uint8_t chunk[1 << 16];
       size_t got;
       while ((got = std::fread(chunk, 1, sizeof chunk, f)) > 0)

@@ -21,7 +21,10 @@
 //    GPU work overlaps (for example on two streams) race on the array and give wrong results --
 //    order them on one stream or with events;
 //  * the first call on each device looks up the array's device address (cudaGetSymbolAddress,
-//    with that device current) and caches it; make that first call before any stream capture.
+//    with that device current) and caches it; make that first call before any stream capture;
+//  * a device reset (cudaDeviceReset) ends the context the cached address belongs to, as it
+//    frees every scene of that device: do not use this entry point on a device after
+//    resetting it in the same process.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -82,10 +85,12 @@ extern "C" int bzr_intersectN_noalloc(const bzr_scene *scene, size_t n, const do
       return bzr::set_error(BZR_EINVAL, "bzr_intersectN_noalloc takes device arrays only");
   if (h.device < 0 || h.device >= kMaxDevices) return bzr::set_error(BZR_EINVAL, "device index");
   int cur = 0;
-  cudaGetDevice(&cur);
-  if (cur != h.device) cudaSetDevice(h.device);
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e != cudaSuccess) return bzr::set_error(BZR_ECUDA, cudaGetErrorString(e));
+  if (cur != h.device && (e = cudaSetDevice(h.device)) != cudaSuccess)
+    return bzr::set_error(BZR_ECUDA, cudaGetErrorString(e));
   unsigned char *scratch = nullptr;
-  cudaError_t e = scratch_address(h.device, &scratch);
+  e = scratch_address(h.device, &scratch);
   if (e == cudaSuccess) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     bzr::RayIO io;
@@ -106,7 +111,10 @@ extern "C" int bzr_intersectN_noalloc(const bzr_scene *scene, size_t n, const do
     // launch_trace clears the counters on `st` before the kernels run
     e = bzr::launch_trace(*h.view, io, mode, plan, st, reinterpret_cast<uint32_t *>(scratch));
   }
-  if (cur != h.device) cudaSetDevice(cur);
+  if (cur != h.device) {
+    const cudaError_t back = cudaSetDevice(cur);  // the caller's device, as it was
+    if (e == cudaSuccess) e = back;
+  }
   if (e != cudaSuccess) return bzr::set_error(BZR_ECUDA, cudaGetErrorString(e));
   return BZR_OK;
 }

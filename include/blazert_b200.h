@@ -158,7 +158,8 @@ int bzr_intersectN_ex(const bzr_scene *scene, size_t n, const double *origins,
  * BZR_EINVAL), and no coherence sort.  The call allocates nothing: its scratch is one 8 MiB
  * static device array per GPU, held until the process exits.  All calls on a device share that
  * array; calls whose GPU work overlaps race -- order them on one stream.  The first call on each
- * device looks up the array's address; make it before any stream capture. */
+ * device looks up the array's address and keeps it; make it before any stream capture, and do
+ * not use this entry point on a device after a cudaDeviceReset of it in the same process. */
 int bzr_intersectN_noalloc(const bzr_scene *scene, size_t n, const double *origins,
                            const double *directions, const double *tmin, const double *tmax,
                            double *hit_distance, double *uv, double *normal, uint32_t *prim_id,

@@ -24,6 +24,20 @@ from blazert_b200 import workloads as W  # noqa: E402
 from oracle.oracle import Oracle, RefScene  # noqa: E402
 
 
+def host_cpu():
+    """CPU model (from /proc/cpuinfo where it exists) and the count of logical CPUs."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count()}
+
+
 def measure(workload="mixed_primitives", seconds=10.0, threads=0, max_rays=0, min_reps=3,
             flavour="bench"):
     wl = W.WORKLOADS[workload]()
@@ -52,7 +66,7 @@ def measure(workload="mixed_primitives", seconds=10.0, threads=0, max_rays=0, mi
     return dict(value=rays.n / med / 1e6, unit="Mrays/s", cores=threads, kind=kind,
                 sample=f"{workload}: {rays.n} rays x {len(times)} repetitions "
                        f"({sum(times):.1f} s of CPU ray loop), median",
-                seconds_per_batch=med, rays=rays.n, repetitions=len(times))
+                seconds_per_batch=med, rays=rays.n, repetitions=len(times), **host_cpu())
 
 
 def measure_distance(workload="distance_queries", seconds=10.0, threads=0, max_queries=0,

@@ -2,7 +2,9 @@
 """Regenerates the golden fixtures in tests/golden/ from the reference (run where the reference
 sources are; the fixtures are committed so the tests do not need them).
 
-    make -C oracle all && python tests/golden/make_golden.py [--reference /root/reference]
+    make -C oracle all && python tests/golden/make_golden.py [--reference DIR]
+
+DIR defaults to the directory "reference" beside this repository.
 
 kats.json
     Every known-answer vector the reference's own test files assert for the double-precision
@@ -161,7 +163,8 @@ def make_image_classes(ref_root):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference",
+                    default=os.path.normpath(os.path.join(HERE, "..", "..", "..", "reference")))
     a = ap.parse_args(argv)
     kats = make_kats(a.reference)
     with open(os.path.join(HERE, "kats.json"), "w") as f:
