@@ -315,11 +315,14 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
     total = align_up(total + std::max<size_t>(bytes, 1), 256);
     return off;
   };
-  size_t off_nodes64[4], off_nodes32[4], off_payload[4], off_ids[4], off_tri[4], off_tv[4],
-      off_pos[4];
+  size_t off_nodes64[4], off_wide[4], off_leaves[4], off_payload[4], off_ids[4], off_tri[4],
+      off_tv[4], off_pos[4];
+  uint32_t wide_stack = 0;
   for (int k = 0; k < bzr::kNumKinds; ++k) {
     off_nodes64[k] = place(img[k].nodes64.data(), img[k].nodes64.size() * sizeof(double));
-    off_nodes32[k] = place(img[k].nodes32.data(), img[k].nodes32.size() * sizeof(float));
+    off_wide[k] = place(img[k].wide.data(), img[k].wide.size());
+    off_leaves[k] = place(img[k].leaves.data(), img[k].leaves.size() * sizeof(double));
+    if (img[k].mixed_ok) wide_stack = std::max(wide_stack, img[k].wide_stack);
     off_payload[k] = place(img[k].payload.data(), img[k].payload.size() * sizeof(double));
     off_ids[k] = place(img[k].prim_ids.data(), img[k].prim_ids.size() * sizeof(uint32_t));
     off_pos[k] = place(img[k].pos_of.data(), img[k].pos_of.size() * sizeof(uint32_t));
@@ -361,7 +364,12 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
     v.geom_id = c.geom_id;
     if (!c.present) continue;
     v.nodes64 = reinterpret_cast<const double *>(base + off_nodes64[k]);
-    v.nodes32 = reinterpret_cast<const float *>(base + off_nodes32[k]);
+    v.wide = reinterpret_cast<const unsigned char *>(base + off_wide[k]);
+    v.leaves = reinterpret_cast<const double *>(base + off_leaves[k]);
+    v.n_wide = img[k].n_wide;
+    v.n_leaf16 = img[k].n_leaf16;
+    v.wide_root_ref = img[k].wide_root_ref;
+    v.wide_coord_max = img[k].wide_coord_max;
     v.payload = reinterpret_cast<const double *>(base + off_payload[k]);
     v.prim_ids = reinterpret_cast<const uint32_t *>(base + off_ids[k]);
     v.pos_of = reinterpret_cast<const uint32_t *>(base + off_pos[k]);
@@ -389,7 +397,7 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
     s->adj.radii = reinterpret_cast<const double *>(base + off_sr);
     s->adj.sphere_geom = sph.geom_id;
   }
-  s->view.stack_cap = std::max<uint32_t>(8, depth + 2);
+  s->view.stack_cap = std::max<uint32_t>({8, depth + 2, wide_stack});
   e = cudaMalloc(&s->slots, (kStickyWord + 1) * sizeof(uint32_t));
   if (e != cudaSuccess) return fail(BZR_ENOMEM, "slot allocation failed");
   e = cudaMemset(s->slots, 0, (kStickyWord + 1) * sizeof(uint32_t));

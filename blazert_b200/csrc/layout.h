@@ -30,10 +30,6 @@ enum Kind : int { kMesh = 0, kSpheres = 1, kPlanes = 2, kCylinders = 3, kNumKind
 //   d[12..13] uint32 {ref0, ref1, axis, 0}
 //   d[14..15] unused
 constexpr int kNode64Doubles = 16;
-// FP32 node for the mixed path, 16 floats = 64 bytes (4 x 16-byte loads); lo rounded toward
-// -inf, hi toward +inf, same slot order as the FP64 node:
-//   f[0..5]   child 0 pairs, f[6..11] child 1 pairs, f[12..15] uint32 {ref0, ref1, axis, 0}
-constexpr int kNode32Floats = 16;
 
 // Leaf-ordered primitive payload, doubles per primitive:
 //   spheres     4: center(3), radius
@@ -50,9 +46,38 @@ constexpr int kNode32Floats = 16;
 constexpr int kPayloadDoubles[kNumKinds] = {0, 4, 14, 16};
 constexpr int kVertexDoubles = 4;
 
+// Mixed-precision image (triangles, spheres, planes; BZR_MODE_MIXED).  The reference's binary
+// tree is cut into treelets of up to kWideMax children -- from an internal node, the internal
+// child of largest box surface is replaced by its two children until the treelet has
+// kWideMax children or only leaves -- and each treelet becomes one 128-byte wide node whose
+// children's boxes are stored as 8-bit integers on a per-axis grid of spacing 2^e, rounded
+// outward, so every stored box contains the child's exact box:
+//   bytes  0..11  float origin[3]: k_a * 2^e_a, exactly representable (|k_a| < 2^24)
+//   bytes 12..15  u32 e_x + 127 | (e_y + 127) << 8 | (e_z + 127) << 16 | children << 24
+//   bytes 16..63  u8: for axis a, lo[8] at 16 + 16a and hi[8] at 24 + 16a; child c's box on
+//                 axis a is [origin + lo[c] * 2^e, origin + hi[c] * 2^e]; an unused slot has
+//                 lo = 255, hi = 0 (an empty box)
+//   bytes 64..95  u32 ref[8]: a wide node index, or kLeafBit | a leaf record's offset in
+//                 16-byte units
+//   bytes 96..127 u32 perm[8]: for a ray of direction-sign octant s = sx | sy << 1 | sz << 2,
+//                 nibble j of perm[s] is the slot of the j-th child in the reference's visit
+//                 order (the reference visits children[direction_sign[axis]] first at every
+//                 binary node, blazert/bvh/accel.h:100-104, so a treelet's order depends on s
+//                 only).
+// Leaf records (16-byte aligned): the leaf's exact FP64 box (lo.x, hi.x, lo.y, hi.y, lo.z,
+// hi.z; 48 B), u32 first leaf-ordered position, u32 count, 8 B zero; then the leaf's
+// primitives: triangles {i0, i1, i2, 0} (16 B, indices into the vertex array), spheres and
+// planes their payload records (32 B, 112 B).
+constexpr int kWideMax = 8;
+// Entries of the thread-local traversal stack; trees whose stack needs more (depth > 62,
+// reachable only with max_tree_depth above 62) trace with the stack in shared memory in FP64,
+// and a kind whose wide traversal could need more has no mixed-precision image.
+constexpr uint32_t kLocalStack = 64;
+constexpr int kWideBytes = 128;
+constexpr int kLeafHeaderBytes = 64;
+
 struct KindView {
   const double *nodes64 = nullptr;  // n_internal * kNode64Doubles
-  const float *nodes32 = nullptr;   // n_internal * kNode32Floats
   const double *payload = nullptr;  // n_prims * kPayloadDoubles[kind] (spheres, planes, cylinders)
   const uint32_t *tri = nullptr;    // triangles: n_prims * 4 {i0, i1, i2, id word}
   const double *verts = nullptr;    // triangles: kVertexDoubles per vertex {x, y, z, 0}
@@ -64,9 +89,16 @@ struct KindView {
   uint32_t root_ref = 0;
   uint32_t geom_id = 0xFFFFFFFFu;
   int present = 0;
-  int mixed_ok = 0;                 // all boxes finite: the FP32 path may be used
+  int mixed_ok = 0;                 // wide image present: the FP32 path may be used
   double root_box[6] = {0, 0, 0, 0, 0, 0};  // (lo.x, hi.x, lo.y, hi.y, lo.z, hi.z)
-  float coord_max = 0.0f;           // largest |coordinate| of any box (mixed-mode error bound)
+  // mixed-precision image (see kWideBytes); the root's wide node is index 0
+  const unsigned char *wide = nullptr;   // n_wide * kWideBytes
+  const double *leaves = nullptr;        // leaf records, n_leaf16 16-byte units
+  uint32_t n_wide = 0;
+  uint32_t n_leaf16 = 0;
+  uint32_t wide_root_ref = 0;            // 0 (wide root) or kLeafBit | offset of a leaf root
+  float wide_coord_max = 0.0f;  // largest |quantised bound| of the wide nodes, rounded up
+  float coord_max = 0.0f;       // largest |coordinate| of the root box, rounded up
 };
 
 struct SceneView {

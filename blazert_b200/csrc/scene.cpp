@@ -506,6 +506,188 @@ BuildStatistics tree_statistics(const Tree &t) {
   return st;
 }
 
+namespace {
+
+double box_area(const TreeNode &nd) {
+  const double x = nd.mx[0] - nd.mn[0], y = nd.mx[1] - nd.mn[1], z = nd.mx[2] - nd.mn[2];
+  return 2.0 * ((x * y + y * z) + z * x);
+}
+
+// Grid of one axis of a wide node: the smallest exponent e with the node's [lo, hi] covered
+// by 255 cells of 2^e from k * 2^e (k = floor(lo / 2^e)) and |k|, |k + 255| below 2^24, so
+// that every stored bound k' * 2^e is exact in float.  Returns false if none in [-100, 100].
+bool axis_grid(double lo, double hi, int *e_out, int64_t *k_out) {
+  const double m = std::max(std::abs(lo), std::abs(hi));
+  int e = m > 0.0 ? std::ilogb(m) - 22 : -100;
+  const double ext = hi - lo;
+  if (ext > 0.0) e = std::max(e, std::ilogb(ext / 255.0) - 1);
+  e = std::max(e, -100);
+  for (; e <= 100; ++e) {
+    const double k = std::floor(std::ldexp(lo, -e)), top = std::ceil(std::ldexp(hi, -e));
+    if (top - k <= 255.0 && std::abs(k) < 16777216.0 - 256.0) {
+      *e_out = e;
+      *k_out = static_cast<int64_t>(k);
+      return true;
+    }
+  }
+  return false;
+}
+
+}  // namespace
+
+// The mixed-precision image of one kind (layout.h, kWideBytes): leaf records in tree order,
+// then the wide nodes breadth-first from the root's treelet.  Leaves the image's mixed_ok
+// false when a box cannot be quantised or the traversal stack could exceed kLocalStack.
+void build_wide(const Tree &t, int kind, const std::vector<uint32_t> &leaf_pos, KindImage *img) {
+  const size_t nn = t.nodes.size();
+  const uint32_t units = kind == kMesh ? 1u : uint32_t(kPayloadDoubles[kind] * 8 / 16);
+  // leaf records: 4 units of header, then `units` per primitive
+  std::vector<uint32_t> leaf_off(nn, 0);
+  uint64_t total = 0;
+  for (size_t i = 0; i < nn; ++i)
+    if (t.nodes[i].leaf == 1) {
+      leaf_off[i] = static_cast<uint32_t>(total);
+      total += kLeafHeaderBytes / 16 + uint64_t(units) * t.nodes[i].prim_cnt;
+    }
+  if (total >= kIdMask) {
+    img->mixed_ok = false;
+    return;
+  }
+  img->leaves.resize(size_t(total) * 2);
+  for (size_t i = 0; i < nn; ++i) {
+    const TreeNode &nd = t.nodes[i];
+    if (nd.leaf != 1) continue;
+    double *L = &img->leaves[size_t(leaf_off[i]) * 2];
+    for (int a = 0; a < 3; ++a) {
+      L[2 * a] = nd.mn[a];
+      L[2 * a + 1] = nd.mx[a];
+    }
+    const uint32_t head[4] = {leaf_pos[i], nd.prim_cnt, 0u, 0u};
+    std::memcpy(L + 6, head, sizeof head);
+    for (uint32_t q = 0; q < nd.prim_cnt; ++q) {
+      const size_t at = size_t(leaf_pos[i]) + q;
+      double *R = L + kLeafHeaderBytes / 8 + size_t(q) * units * 2;
+      if (kind == kMesh) {
+        const uint32_t rec[4] = {img->tri[4 * at], img->tri[4 * at + 1], img->tri[4 * at + 2], 0u};
+        std::memcpy(R, rec, sizeof rec);
+      } else {
+        std::memcpy(R, &img->payload[at * kPayloadDoubles[kind]],
+                    sizeof(double) * kPayloadDoubles[kind]);
+      }
+    }
+  }
+  img->n_leaf16 = static_cast<uint32_t>(total);
+  img->n_wide = 0;
+  img->wide_stack = 1;
+  if (t.nodes[0].leaf == 1) {
+    img->wide_root_ref = kLeafBit | leaf_off[0];
+    return;
+  }
+  img->wide_root_ref = 0;
+  // treelets, breadth-first; queue[w] is the tree node at the root of wide node w
+  std::vector<uint32_t> queue{0}, depth_sum{0};
+  std::vector<unsigned char> out;
+  double cmax = 0.0;
+  for (size_t head = 0; head < queue.size(); ++head) {
+    const TreeNode &root = t.nodes[queue[head]];
+    std::vector<uint32_t> ch{root.child[0], root.child[1]};
+    std::vector<uint32_t> expanded{queue[head]};
+    for (;;) {
+      if (ch.size() >= size_t(kWideMax)) break;
+      int pick = -1;
+      double best = -1.0;
+      for (size_t j = 0; j < ch.size(); ++j) {
+        const TreeNode &c = t.nodes[ch[j]];
+        if (c.leaf == 1) continue;
+        const double a = box_area(c);
+        if (a > best) {
+          best = a;
+          pick = static_cast<int>(j);
+        }
+      }
+      if (pick < 0) break;
+      const uint32_t x = ch[pick];
+      expanded.push_back(x);
+      ch[pick] = t.nodes[x].child[0];
+      ch.insert(ch.begin() + pick + 1, t.nodes[x].child[1]);
+    }
+    unsigned char node[kWideBytes] = {};
+    float origin[3];
+    uint32_t ex = 0;
+    for (int a = 0; a < 3; ++a) {
+      int e = 0;
+      int64_t k = 0;
+      if (!axis_grid(root.mn[a], root.mx[a], &e, &k)) {
+        img->mixed_ok = false;
+        return;
+      }
+      origin[a] = static_cast<float>(std::ldexp(static_cast<double>(k), e));
+      cmax = std::max({cmax, std::abs(std::ldexp(static_cast<double>(k), e)),
+                       std::abs(std::ldexp(static_cast<double>(k + 255), e))});
+      ex |= uint32_t(e + 127) << (8 * a);
+      for (size_t j = 0; j < size_t(kWideMax); ++j) {
+        unsigned char lo = 255, hi = 0;
+        if (j < ch.size()) {
+          const TreeNode &c = t.nodes[ch[j]];
+          const double ql = std::floor(std::ldexp(c.mn[a], -e)) - static_cast<double>(k);
+          const double qh = std::ceil(std::ldexp(c.mx[a], -e)) - static_cast<double>(k);
+          if (!(ql >= 0.0 && qh <= 255.0 && ql <= qh)) {
+            img->mixed_ok = false;
+            return;
+          }
+          lo = static_cast<unsigned char>(ql);
+          hi = static_cast<unsigned char>(qh);
+        }
+        node[16 + 16 * a + j] = lo;
+        node[24 + 16 * a + j] = hi;
+      }
+    }
+    ex |= uint32_t(ch.size()) << 24;
+    std::memcpy(node, origin, sizeof origin);
+    std::memcpy(node + 12, &ex, sizeof ex);
+    uint32_t ref[kWideMax] = {}, perm[8] = {};
+    for (size_t j = 0; j < ch.size(); ++j) {
+      const TreeNode &c = t.nodes[ch[j]];
+      if (c.leaf == 1) {
+        ref[j] = kLeafBit | leaf_off[ch[j]];
+      } else {
+        ref[j] = static_cast<uint32_t>(queue.size());
+        queue.push_back(ch[j]);
+        depth_sum.push_back(depth_sum[head] + uint32_t(ch.size()) - 1);
+      }
+    }
+    // visit order per octant: at every expanded node the child on the ray's sign side first
+    for (uint32_t oct = 0; oct < 8; ++oct) {
+      uint32_t pos = 0;
+      std::vector<uint32_t> todo{queue[head]};
+      while (!todo.empty()) {
+        const uint32_t x = todo.back();
+        todo.pop_back();
+        const auto it = std::find(ch.begin(), ch.end(), x);
+        if (it != ch.end() && x != queue[head]) {
+          perm[oct] |= uint32_t(it - ch.begin()) << (4 * pos++);
+          continue;
+        }
+        const TreeNode &nx = t.nodes[x];
+        const uint32_t first = (oct >> nx.axis) & 1u;
+        todo.push_back(nx.child[1 - first]);
+        todo.push_back(nx.child[first]);
+      }
+    }
+    std::memcpy(node + 64, ref, sizeof ref);
+    std::memcpy(node + 96, perm, sizeof perm);
+    out.insert(out.end(), node, node + kWideBytes);
+    img->wide_stack = std::max(img->wide_stack, depth_sum[head] + uint32_t(ch.size()) - 1);
+  }
+  if (img->wide_stack > kLocalStack || !(cmax <= 1e18)) {
+    img->mixed_ok = false;
+    return;
+  }
+  img->n_wide = static_cast<uint32_t>(queue.size());
+  img->wide.assign(out.begin(), out.end());
+  img->wide_coord_max = round_up(cmax);
+}
+
 KindImage flatten(const HostScene &s, int kind, size_t max_workers) {
   const Collection &c = s.kind[kind];
   const Tree &t = c.tree;
@@ -543,7 +725,6 @@ KindImage flatten(const HostScene &s, int kind, size_t max_workers) {
   };
   img.n_internal = static_cast<uint32_t>(order.size());
   img.nodes64.resize(size_t(img.n_internal) * kNode64Doubles);
-  img.nodes32.resize(size_t(img.n_internal) * kNode32Floats);
   // Each node reads only the tree and writes only its own slots, so ranges of nodes can be
   // filled on separate threads.
   const size_t workers =
@@ -553,20 +734,16 @@ KindImage flatten(const HostScene &s, int kind, size_t max_workers) {
     for (size_t g = g0; g < g1; ++g) {
       const TreeNode &nd = t.nodes[order[g]];
       double *d = &img.nodes64[g * kNode64Doubles];
-      float *f = &img.nodes32[g * kNode32Floats];
       for (int j = 0; j < 2; ++j) {
         const TreeNode &ch = t.nodes[nd.child[j]];
         if (!finite_box(ch)) finite[w] = 0;
         for (int k = 0; k < 3; ++k) {
           d[6 * j + 2 * k] = ch.mn[k];
           d[6 * j + 2 * k + 1] = ch.mx[k];
-          f[6 * j + 2 * k] = round_down(ch.mn[k]);
-          f[6 * j + 2 * k + 1] = round_up(ch.mx[k]);
         }
       }
       const uint32_t meta[4] = {ref_of(nd.child[0]), ref_of(nd.child[1]), nd.axis, 0u};
       std::memcpy(d + 12, meta, sizeof meta);
-      std::memcpy(f + 12, meta, sizeof meta);
       d[14] = d[15] = 0.0;
     }
   });
@@ -583,6 +760,7 @@ KindImage flatten(const HostScene &s, int kind, size_t max_workers) {
       cmax = std::max(cmax, std::max(std::abs(root.mn[k]), std::abs(root.mx[k])));
     }
     img.coord_max = round_up(cmax);
+    if (!(cmax <= 1e18)) img.mixed_ok = false;
   }
   // Leaf-ordered primitives: leaves own disjoint position ranges and the ids are a
   // permutation, so ranges of leaves can be written on separate threads.
@@ -628,6 +806,10 @@ KindImage flatten(const HostScene &s, int kind, size_t max_workers) {
   });
   if (kind == kMesh)
     number_vertices(s, &img, range_workers(np, kPrimsPerRange, max_workers));
+  // Cylinders may move the hit distance outward (blazert/primitives/cylinder.h:181-495), which
+  // the wide image's exactness argument excludes; their mixed mode runs the FP64 traversal.
+  if (img.mixed_ok && kind != kCylinders && nn) build_wide(t, kind, leaf_pos, &img);
+  else img.mixed_ok = false;
   return img;
 }
 

@@ -149,7 +149,6 @@ void add_cylinders(HostScene &s, const double *c, const double *a, const double 
 // arrays.
 struct KindImage {
   RawVector<double> nodes64;
-  RawVector<float> nodes32;
   std::vector<double> payload;
   RawVector<uint32_t> prim_ids;
   std::vector<uint32_t> pos_of;  // leaf-ordered position of each primitive id
@@ -158,9 +157,19 @@ struct KindImage {
   uint32_t n_internal = 0;
   uint32_t root_ref = 0;
   double root_box[6] = {0, 0, 0, 0, 0, 0};
-  float coord_max = 0.0f;  // largest |coordinate| of the root box, rounded up
-  bool mixed_ok = true;
+  // mixed-precision image (layout.h, kWideBytes): wide nodes and leaf records
+  std::vector<unsigned char> wide;
+  RawVector<double> leaves;     // every element written by build_wide
+  uint32_t n_wide = 0, n_leaf16 = 0;
+  uint32_t wide_root_ref = 0;
+  uint32_t wide_stack = 0;      // most stack entries the wide traversal can hold
+  float wide_coord_max = 0.0f;  // largest |quantised bound| of the wide nodes, rounded up
+  float coord_max = 0.0f;       // largest |coordinate| of the root box, rounded up
+  bool mixed_ok = true;         // the wide image was built
 };
+
+// Builds the mixed-precision image of a flattened kind (called by flatten).
+void build_wide(const Tree &t, int kind, const std::vector<uint32_t> &leaf_pos, KindImage *img);
 
 // Device image of one kind's tree and primitives.  Long loops run on up to max_workers threads;
 // the image does not depend on how many.

@@ -81,10 +81,13 @@ __device__ __forceinline__ void prefetch_l2(const void *base, size_t bytes) {
 
 template <int KIND, bool MIXED>
 __device__ __forceinline__ void prefetch_kind(const KindView &K) {
-  if (MIXED)
-    prefetch_l2(K.nodes32, size_t(K.n_internal) * kNode32Floats * sizeof(float));
-  else
-    prefetch_l2(K.nodes64, size_t(K.n_internal) * kNode64Doubles * sizeof(double));
+  if (MIXED && K.mixed_ok) {  // the wide image: nodes, then leaf records (and vertices)
+    prefetch_l2(K.wide, size_t(K.n_wide) * kWideBytes);
+    prefetch_l2(K.leaves, size_t(K.n_leaf16) * 16);
+    if (KIND == kMesh) prefetch_l2(K.verts, size_t(K.n_verts) * kVertexDoubles * sizeof(double));
+    return;
+  }
+  prefetch_l2(K.nodes64, size_t(K.n_internal) * kNode64Doubles * sizeof(double));
   if (KIND == kMesh) {
     prefetch_l2(K.tri, size_t(K.n_prims) * 4 * sizeof(uint32_t));
     prefetch_l2(K.verts, size_t(K.n_verts) * kVertexDoubles * sizeof(double));
@@ -96,12 +99,14 @@ __device__ __forceinline__ void prefetch_kind(const KindView &K) {
 }
 
 // One kind over the whole batch.  first: this pass writes the whole output record.
-// COUNT: also sums the work counters into totals[8] (box tests per kind, then primitive
-// tests per kind).
+// COUNT: also sums the work counters into totals[16] (per kind: box tests, primitive tests,
+// node fetches, leaf fetches; see Counts).  MIXED: rays the FP32 test covers walk the wide
+// image (cylinders always take the FP64 traversal).
 template <int KIND, bool COUNT, bool MIXED, bool LOCAL>
 __global__ void __launch_bounds__(kMaxTraceThreads)
     trace_kind_kernel(SceneView S, RayIO io, int first, uint32_t *work_counter,
                       unsigned long long *totals) {
+  constexpr bool kWide = MIXED && KIND != kCylinders;
   extern __shared__ __align__(16) unsigned char smem[];
   double lkey[LOCAL ? kLocalStack : 1];
   uint32_t lref[LOCAL ? kLocalStack : 1];
@@ -109,7 +114,7 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
   uint32_t tid;
   init_stack<LOCAL>(sk, tid, S.stack_cap, smem, lkey, lref);
   const KindView &K = S.k[KIND];
-  if (!COUNT) prefetch_kind<KIND, MIXED>(K);
+  if (!COUNT) prefetch_kind<KIND, kWide>(K);
   const unsigned lane = threadIdx.x & 31u;
   const unsigned below = (1u << lane) - 1u;
   uint32_t pool_next = 0, pool_end = 0;  // warp-uniform
@@ -117,7 +122,8 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
   bool active = false;
   uint32_t i = 0;
   Ray r;
-  RayF f;
+  RayW f;
+  float hl = 0.0f;
   bool use32 = false;
   KState st;
   Trav tv;
@@ -143,11 +149,14 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
           r = make_ray(io.org + 3 * size_t(i), io.dir + 3 * size_t(i), io.tmin ? io.tmin[i] : 0.0,
                        io.tmax ? io.tmax[i] : kDblMax);
           r.any_hit = io.any_hit != 0;
-          if (MIXED) {
-            f = make_ray_f(r, K.coord_max);
+          if constexpr (kWide) {
+            f = make_ray_w(r, K.wide_coord_max);
             use32 = K.mixed_ok && f.ok;
           }
-          trav_begin<KIND, COUNT>(K, r, st, tv, &cnt);
+          if (kWide && use32)
+            wtrav_begin<KIND, COUNT>(K, r, f, st, hl, tv, &cnt);
+          else
+            trav_begin<KIND, COUNT>(K, r, st, tv, &cnt);
         }
       }
       if (want > avail) {
@@ -160,9 +169,9 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
     }
     if (!__any_sync(kFull, active)) break;
     if (active) {
-      if (MIXED && use32) {
-        if (tv.live) trav_to_leaf32<KIND, COUNT>(K, r, f, st, tv, sk, tid, io.error_word, &cnt);
-        if (tv.live) trav_leaf32<KIND, COUNT>(K, r, f, st, tv, sk, tid, io.error_word, &cnt);
+      if (kWide && use32) {
+        if (tv.live) wtrav_to_leaf<KIND, COUNT>(K, r, f, hl, tv, sk, tid, io.error_word, &cnt);
+        if (tv.live) wtrav_leaf<KIND, COUNT>(K, r, f, st, hl, tv, sk, tid, io.error_word, &cnt);
       } else {
         if (tv.live) trav_to_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, io.error_word, &cnt);
         if (tv.live) trav_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, io.error_word, &cnt);
@@ -176,14 +185,10 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
   }
   if (COUNT) {
     for (int k = 0; k < kNumKinds; ++k) {
-      unsigned long long b = cnt.box[k], p = cnt.prim[k];
-      for (int off = 16; off > 0; off >>= 1) {
-        b += __shfl_down_sync(kFull, b, off);
-        p += __shfl_down_sync(kFull, p, off);
-      }
-      if (lane == 0) {
-        if (b) atomicAdd(totals + k, b);
-        if (p) atomicAdd(totals + kNumKinds + k, p);
+      unsigned long long v[4] = {cnt.box[k], cnt.prim[k], cnt.node[k], cnt.leaf[k]};
+      for (int j = 0; j < 4; ++j) {
+        for (int off = 16; off > 0; off >>= 1) v[j] += __shfl_down_sync(kFull, v[j], off);
+        if (lane == 0 && v[j]) atomicAdd(totals + j * kNumKinds + k, v[j]);
       }
     }
   }
@@ -196,6 +201,7 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
 template <int KIND, bool MIXED, bool LOCAL>
 __global__ void __launch_bounds__(kMaxTraceThreads)
     trace_batch_kernel(BatchView B, RayIO io, uint32_t *chunk_counter, uint32_t stack_cap) {
+  constexpr bool kWide = MIXED && KIND != kCylinders;
   extern __shared__ __align__(16) unsigned char smem[];
   double lkey[LOCAL ? kLocalStack : 1];
   uint32_t lref[LOCAL ? kLocalStack : 1];
@@ -210,7 +216,8 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
   uint32_t i = 0, sc = 0;
   const KindView *K = nullptr;
   Ray r;
-  RayF f;
+  RayW f;
+  float hl = 0.0f;
   bool use32 = false;
   KState st;
   Trav tv;
@@ -262,11 +269,14 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
           r = make_ray(io.org + 3 * size_t(i), io.dir + 3 * size_t(i), io.tmin ? io.tmin[i] : 0.0,
                        io.tmax ? io.tmax[i] : kDblMax);
           r.any_hit = io.any_hit != 0;
-          if (MIXED) {
-            f = make_ray_f(r, K->coord_max);
+          if constexpr (kWide) {
+            f = make_ray_w(r, K->wide_coord_max);
             use32 = K->mixed_ok && f.ok;
           }
-          trav_begin<KIND, false>(*K, r, st, tv, &cnt);
+          if (kWide && use32)
+            wtrav_begin<KIND, false>(*K, r, f, st, hl, tv, &cnt);
+          else
+            trav_begin<KIND, false>(*K, r, st, tv, &cnt);
         }
       }
       if (want > avail) {
@@ -284,9 +294,9 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
     }
     if (!__any_sync(kFull, active)) break;
     if (active) {
-      if (MIXED && use32) {
-        if (tv.live) trav_to_leaf32<KIND, false>(*K, r, f, st, tv, sk, tid, io.error_word, &cnt);
-        if (tv.live) trav_leaf32<KIND, false>(*K, r, f, st, tv, sk, tid, io.error_word, &cnt);
+      if (kWide && use32) {
+        if (tv.live) wtrav_to_leaf<KIND, false>(*K, r, f, hl, tv, sk, tid, io.error_word, &cnt);
+        if (tv.live) wtrav_leaf<KIND, false>(*K, r, f, st, hl, tv, sk, tid, io.error_word, &cnt);
       } else {
         if (tv.live) trav_to_leaf<KIND, false>(*K, r, st, tv, sk, tid, io.error_word, &cnt);
         if (tv.live) trav_leaf<KIND, false>(*K, r, st, tv, sk, tid, io.error_word, &cnt);
@@ -363,7 +373,7 @@ template <int KIND, bool COUNT>
 cudaError_t launch_kind(const SceneView &S, const RayIO &io, int mode, int first, int blocks,
                         const LaunchPlan &plan, cudaStream_t stream, uint32_t *counter,
                         unsigned long long *totals) {
-  const bool mixed = mode == kModeMixed;
+  const bool mixed = mode == kModeMixed && KIND != kCylinders;
   const int th = plan.threads;
   if (!COUNT && use_local(S, plan)) {
     if (mixed)
@@ -483,7 +493,7 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
   int first = 1;
   for (int k = 0; k < kNumKinds; ++k) {
     if (!S.k[k].present || S.k[k].n_prims == 0) continue;
-    const int b = mode == kModeMixed ? plan.blocks32[k] : plan.blocks[k];
+    const int b = mode == kModeMixed && k != kCylinders ? plan.blocks32[k] : plan.blocks[k];
     uint32_t *c = counters + k;
     switch (k) {
       case kMesh:
@@ -573,7 +583,7 @@ cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const Ba
   const size_t smem = local ? 0 : trace_smem_bytes(plan.stack_cap, th);
   for (int k = 0; k < kNumKinds; ++k) {
     if (!(plan.kinds_present & (1 << k))) continue;
-    const bool m = mode == kModeMixed;
+    const bool m = mode == kModeMixed && k != kCylinders;  // cylinders: FP64 traversal
     const int b = m ? plan.blocks32[k] : plan.blocks[k];
     uint32_t *c = counters + k;
 #define BZR_BATCH_LAUNCH(KK)                                                                 \

@@ -12,9 +12,6 @@ namespace bzr {
 constexpr int kTraceThreads = 128;     // default threads per block of the trace kernels
 constexpr int kMaxTraceThreads = 256;  // largest block the trace kernels are compiled for
 constexpr uint32_t kRayChunk = 32;     // default rays a warp takes from the global counter
-// Entries of the thread-local traversal stack; trees whose stack needs more (depth > 62,
-// reachable only with max_tree_depth above 62) trace with the stack in shared memory.
-constexpr uint32_t kLocalStack = 64;
 constexpr int kModeFp64 = 0;   // BZR_MODE_FP64
 constexpr int kModeMixed = 1;  // BZR_MODE_MIXED
 

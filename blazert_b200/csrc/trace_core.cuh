@@ -397,11 +397,16 @@ struct Stack {
   uint32_t cap, stride;
 };
 
-// Work counters of one ray (counting kernels only): per kind the box tests (the reference's
-// node pops: the root plus both children of every accepted internal node) and primitive tests.
+// Work counters of one ray (counting kernels only), per kind: box tests (FP64 path: the
+// reference's node pops, i.e. the root plus both children of every accepted internal node;
+// mixed path: the root plus every child slot tested), primitive tests, node fetches (internal
+// FP64 nodes, or wide nodes) and leaf fetches (FP64 path: leaves whose primitives run; mixed
+// path: leaf records read, each with its exact FP64 test).
 struct Counts {
   uint32_t box[kNumKinds];
   uint32_t prim[kNumKinds];
+  uint32_t node[kNumKinds];
+  uint32_t leaf[kNumKinds];
 };
 
 // Resumable traversal of one kind (blazert/bvh/accel.h:80-120).  trav_begin tests the root;
@@ -457,7 +462,10 @@ BZR_HD void trav_to_leaf(const KindView &K, const Ray &r, const KState &st, Trav
     const double2 b0 = ld2(nd + 6), b1 = ld2(nd + 8), b2 = ld2(nd + 10);
     const uint4 meta = ldg(reinterpret_cast<const uint4 *>(nd + 12));
     double k0, k1;
-    if (COUNT) cnt->box[KIND] += 2;
+    if (COUNT) {
+      cnt->box[KIND] += 2;
+      cnt->node[KIND] += 1;
+    }
     const bool p0 = box_test(a0, a1, a2, r, k0);
     const bool p1 = box_test(b0, b1, b2, r, k1);
     const unsigned near = meta.z == 0 ? r.sx : (meta.z == 1 ? r.sy : r.sz);
@@ -486,6 +494,7 @@ template <int KIND, bool COUNT>
 BZR_HD void trav_leaf(const KindView &K, const Ray &r, KState &st, Trav &tv, const Stack &sk,
                       uint32_t tid, uint32_t *err, Counts *cnt) {
   uint32_t pos = tv.cur & kIdMask;
+  if (COUNT) cnt->leaf[KIND] += 1;
   for (;;) {
     if (pos >= K.n_prims) {
       flag_error(err, kErrPrimIndex);
@@ -519,127 +528,100 @@ BZR_HD bool traverse(const KindView &K, const Ray &r, KState &st, const Stack &s
 }
 
 // ---------------------------------------------------------------------------------------------
-// Mixed precision (BZR_MODE_MIXED): slab tests in FP32 on the 64-byte nodes, with every
-// decision equal to the FP64 one.
+// Mixed precision (BZR_MODE_MIXED) for triangles, spheres and planes: the wide image (layout.h,
+// kWideBytes).
 //
-// For an eligible ray, every FP32 entry/exit distance a32 = (fl32(plane) - fl32(o)) * fl32(inv)
-// is within delta of the FP64 value of the reference's slab test:
-//   |a32 - a64| <= 2^-21 * max|inv| * (coord_max + max|o|)  (+ tiny absolute terms),
-// from the relative errors of the five FP32 roundings (<= 3 * 2^-23 in all) and the FP64 ones
-// (l1 = 1 + 2^-50 included).  A child is accepted or rejected in FP32 only when the FP32
-// comparison holds with that margin (sums rounded outward); otherwise its exact FP64 test
-// runs on the FP64 node.  The pop-time comparison of the entry distance with the hit distance
-// is decided the same way, re-testing the child in FP64 when it falls inside the margin.  So
-// the accepted nodes, and hence the leaves, primitive tests and results, are exactly the FP64
-// path's.  Rays that are not eligible (a zero, tiny or non-finite direction component, huge
-// coordinates, non-finite tmin, NaN tmax) and kinds with a non-finite box use the FP64 path.
-struct RayF {
+// Internal levels are walked on the wide nodes with FP32 slab tests of the children's
+// quantised boxes, which contain their exact boxes.  Each FP32 slab distance is within delta
+// (below) of the reference's FP64 distance for the exact box, on the side that can only keep
+// more: a child is kept when its FP32 entry distance is at most both its FP32 exit distance +
+// 2 delta and the current hit distance (rounded up) + delta, so every child the FP64 traversal
+// accepts is kept.  The kept children are visited in the reference's order (the node's rank
+// table for the ray's octant), and a stack entry is dropped at pop time only when its FP32
+// entry distance exceeds the hit distance + delta.  A leaf is processed when the reference's
+// exact FP64 test of the leaf's own box against the current hit distance passes
+// (blazert/bvh/intersect.h:33-51).
+//
+// Why the results are the FP64 path's: the walk reaches every node the FP64 traversal accepts,
+// in the same relative order (the wide tree is the binary tree with treelets contracted, and a
+// treelet's children are visited in the binary order).  The FP64 traversal processes a leaf
+// iff the leaf's own test passes at its pop time AND every ancestor passed its test at its own
+// pop time.  An ancestor's box contains the leaf's box, the rounded slab distances are
+// monotone in the box bounds, and the hit distance only decreases for triangles, spheres and
+// planes (cylinders, which may move it outward, keep the FP64 traversal); so when a leaf's own
+// test passes, no ancestor failed.  The same leaves are therefore processed in the same order
+// with the same hit distance, and every primitive test and result is identical.
+//
+// delta: the FP32 distance t = fma(q, 2^e * inv_f, (origin - o_f) * inv_f) of a stored bound
+// b = origin + q 2^e differs from (b - o) * inv by at most 5 * 2^-24 * |inv| * (|b| + |o|)
+// (o_f, inv_f, the difference, the product and the fma each round once), the reference's own
+// FP64 roundings and its l1 factor add 2^-49 relative, and fl32(tmin) 2^-24 |tmin|;
+// delta = 2^-20 * (max|inv| * (coord_max + max|o|) + |tmin|) + 1e-30 * (1 + max|inv|) covers
+// these and the roundings of the sums compared.  Rays with a zero, non-finite or huge (> 1e18)
+// inverse direction or origin component, or a non-finite or huge tmin or a NaN tmax, take the
+// FP64 traversal.
+struct RayW {
   float o[3], inv[3];
-  float tmin, delta;
+  float tmin, delta, delta2;  // delta2 = 2 delta, rounded up
+  uint32_t oct;               // sx | sy << 1 | sz << 2
   bool ok;
 };
 
-BZR_HD float fadd_up(float a, float b) {
+BZR_HD float f32_up(double x) {  // x rounded toward +inf
 #if defined(__CUDA_ARCH__)
-  return __fadd_ru(a, b);
+  return __double2float_ru(x);
 #else
-  return nextafterf(float(double(a) + double(b)), __builtin_inff());  // conservative
+  float f = static_cast<float>(x);
+  if (static_cast<double>(f) < x) f = nextafterf(f, __builtin_inff());
+  return f;
 #endif
 }
-BZR_HD float fadd_down(float a, float b) {
+BZR_HD float fbits(uint32_t u) {
 #if defined(__CUDA_ARCH__)
-  return __fadd_rd(a, b);
+  return __uint_as_float(u);
 #else
-  return nextafterf(float(double(a) + double(b)), -__builtin_inff());
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
 #endif
 }
-
-BZR_HD RayF make_ray_f(const Ray &r, float coord_max) {
-  RayF f;
+BZR_HD float fma32(float a, float b, float c) {
+#if defined(__CUDA_ARCH__)
+  return __fmaf_rn(a, b, c);
+#else
+  return fmaf(a, b, c);
+#endif
+}
+BZR_HD RayW make_ray_w(const Ray &r, float coord_max) {
+  RayW f;
   const double inv[3] = {r.inv.x, r.inv.y, r.inv.z}, o[3] = {r.o.x, r.o.y, r.o.z};
-  double imax = 0.0, imin = 1e300, omax = 0.0;
-  bool ok = isfinite(r.tmin) && !isnan(r.tmax) && isfinite(coord_max) &&
-            coord_max <= 1e18f;
+  double imax = 0.0, omax = 0.0;
+  bool ok = fabs(r.tmin) <= 1e18 && !isnan(r.tmax);
   for (int a = 0; a < 3; ++a) {
-    const double ai = fabs(inv[a]);
-    ok = ok && isfinite(inv[a]) && ai > 0.0 && isfinite(o[a]) && fabs(o[a]) <= 1e18;
+    const double ai = fabs(inv[a]), oa = fabs(o[a]);
+    ok = ok && ai > 0.0 && ai <= 1e18 && oa <= 1e18;  // false for NaN and infinities
     imax = ai > imax ? ai : imax;
-    imin = ai < imin ? ai : imin;
-    omax = fabs(o[a]) > omax ? fabs(o[a]) : omax;
-    f.o[a] = float(o[a]);
-    f.inv[a] = float(inv[a]);
+    omax = oa > omax ? oa : omax;
+    f.o[a] = static_cast<float>(o[a]);
+    f.inv[a] = static_cast<float>(inv[a]);
   }
-  ok = ok && imax <= 16384.0 * imin && imax <= 1e18;
-  const double d = 4.76837158203125e-07 /* 2^-21 */ * (imax * (double(coord_max) + omax) + fabs(r.tmin)) +
+  const double d = 9.5367431640625e-07 /* 2^-20 */ *
+                       (imax * (static_cast<double>(coord_max) + omax) + fabs(r.tmin)) +
                    1e-30 * (1.0 + imax);
-  f.tmin = float(r.tmin);
-  f.delta = ok ? nextafterf(float(d), __builtin_inff()) : 0.0f;
-  f.ok = ok && isfinite(f.delta);
+  f.tmin = static_cast<float>(r.tmin);
+  f.delta = f32_up(d);
+  f.delta2 = f32_up(2.0 * d);
+  f.oct = r.sx | (r.sy << 1) | (r.sz << 2);
+  f.ok = ok;
   return f;
 }
 
-// FP32 slab test of one box given as (lo, hi) pairs per axis: 1 accept for some hit distance,
-// 0 reject for every hit distance, 2 undecided in FP32.  mn receives the FP32 entry distance.
-BZR_HD int box_test32(float lx, float hx, float ly, float hy, float lz, float hz, const RayF &f,
-                      const Ray &r, float &mn) {
-  const float ax = ((r.sx ? hx : lx) - f.o[0]) * f.inv[0];
-  const float bx = ((r.sx ? lx : hx) - f.o[0]) * f.inv[0];
-  const float ay = ((r.sy ? hy : ly) - f.o[1]) * f.inv[1];
-  const float by = ((r.sy ? ly : hy) - f.o[1]) * f.inv[1];
-  const float az = ((r.sz ? hz : lz) - f.o[2]) * f.inv[2];
-  const float bz = ((r.sz ? lz : hz) - f.o[2]) * f.inv[2];
-  mn = fmaxf(fmaxf(f.tmin, ax), fmaxf(ay, az));
-  const float ex = fminf(fminf(bx, by), bz);
-  if (fadd_up(mn, f.delta) <= fadd_down(ex, -f.delta)) return 1;
-  if (fadd_down(mn, -f.delta) > fadd_up(ex, f.delta)) return 0;
-  return 2;
-}
-
-// Exact FP64 slab test of child `slot` of FP64 node `node`.
-BZR_HD bool child_test64(const KindView &K, uint32_t node, int slot, const Ray &r, double &key) {
-  const double *nd = K.nodes64 + size_t(node) * kNode64Doubles + 6 * slot;
-  return box_test(ld2(nd), ld2(nd + 2), ld2(nd + 4), r, key);
-}
-
-// Mixed stack entry: ref in sk.ref; the key slot holds {float key, uint32 aux} with
-// aux = parent << 2 | slot << 1 | exact.  exact: key is fl32 of the FP64 entry distance.
-BZR_HD void push32(const Stack &sk, uint32_t tid, uint32_t sp, uint32_t ref, float key,
-                   uint32_t aux) {
-  uint32_t *w = reinterpret_cast<uint32_t *>(sk.key + sp * sk.stride + tid);
-  float kk = key;
-  uint32_t kb;
-  std::memcpy(&kb, &kk, 4);
-  w[0] = kb;
-  w[1] = aux;
-  sk.ref[sp * sk.stride + tid] = ref;
-}
-
-// Pop-time decision !(key64 > h) from the FP32 key and its margin; -1 when undecided.
-BZR_HD int key_decide(float key, float margin, double h) {
-  if (double(fadd_up(key, margin)) <= h) return 1;
-  if (double(fadd_down(key, -margin)) > h) return 0;
-  return -1;
-}
-BZR_HD float exact_margin(float key) {
-  return nextafterf(fabsf(key) * 1.1920928955078125e-07f, __builtin_inff()) + 1.4e-45f;
-}
-
-template <int KIND>
-BZR_HD void trav_pop32(const KindView &K, const Ray &r, const RayF &f, Trav &tv, const KState &st,
-                       const Stack &sk, uint32_t tid) {
+// Pop-time test of the wide walk: drops entries whose FP32 entry distance exceeds hl.
+BZR_HD void wtrav_pop(Trav &tv, float hl, const Stack &sk, uint32_t tid) {
+  const float *skey = reinterpret_cast<const float *>(sk.key);
   while (tv.sp > 0) {
     --tv.sp;
-    const uint32_t *w = reinterpret_cast<const uint32_t *>(sk.key + tv.sp * sk.stride + tid);
-    const uint32_t kb = w[0], aux = w[1];
-    float key;
-    std::memcpy(&key, &kb, 4);
-    int d = key_decide(key, (aux & 1u) ? exact_margin(key) : f.delta, st.hit);
-    if (d < 0) {
-      double k64;
-      child_test64(K, aux >> 2, int((aux >> 1) & 1u), r, k64);
-      d = !(k64 > st.hit);
-    }
-    if (d) {
+    if (!(skey[tv.sp * sk.stride + tid] > hl)) {
       tv.cur = sk.ref[tv.sp * sk.stride + tid];
       return;
     }
@@ -647,109 +629,169 @@ BZR_HD void trav_pop32(const KindView &K, const Ray &r, const RayF &f, Trav &tv,
   tv.live = false;
 }
 
+// The exact root test (trav_begin), then the walk starts at the wide root.  hl is the hit
+// distance rounded up, plus delta.
 template <int KIND, bool COUNT>
-BZR_HD void trav_to_leaf32(const KindView &K, const Ray &r, const RayF &f, const KState &st,
-                           Trav &tv, const Stack &sk, uint32_t tid, uint32_t *err, Counts *cnt) {
+BZR_HD void wtrav_begin(const KindView &K, const Ray &r, const RayW &f, KState &st, float &hl,
+                        Trav &tv, Counts *cnt) {
+  trav_begin<KIND, COUNT>(K, r, st, tv, cnt);
+  tv.cur = K.wide_root_ref;
+  hl = f32_up(st.hit) + f.delta;
+}
+
+// Byte `slot` (0..7) of the 8-byte value (w0 low, w1 high) as a float (exact).
+BZR_HD float qslot(uint32_t w0, uint32_t w1, uint32_t slot) {
+#if defined(__CUDA_ARCH__)
+  return __uint_as_float(__byte_perm(__byte_perm(w0, w1, slot), 0x4B000000u, 0x7440u)) -
+         8388608.0f;
+#else
+  const uint64_t w = uint64_t(w0) | (uint64_t(w1) << 32);
+  return static_cast<float>((w >> (8 * slot)) & 0xFFu);
+#endif
+}
+
+// Walks wide nodes until the current reference is a leaf record (or the walk ends).  The
+// children are tested in the reverse of the ray's visit order (the node's permutation for the
+// ray's octant), so each kept child pushes the previously kept one, which lies later in the
+// order, and the last kept, first in the order, becomes current: the stack ends with the next
+// in order on top, as the reference's stack would.
+template <int KIND, bool COUNT>
+BZR_HD void wtrav_to_leaf(const KindView &K, const Ray &r, const RayW &f, float hl, Trav &tv,
+                          const Stack &sk, uint32_t tid, uint32_t *err, Counts *cnt) {
+  float *skey = reinterpret_cast<float *>(sk.key);
   while (tv.live && !(tv.cur & kLeafBit)) {
-    if (tv.cur >= K.n_internal) {
+    if (tv.cur >= K.n_wide) {
       flag_error(err, kErrNodeIndex);
       tv.live = false;
       return;
     }
-    const float *nf = K.nodes32 + size_t(tv.cur) * kNode32Floats;
-    const float4 q0 = ldg(reinterpret_cast<const float4 *>(nf));
-    const float4 q1 = ldg(reinterpret_cast<const float4 *>(nf + 4));
-    const float4 q2 = ldg(reinterpret_cast<const float4 *>(nf + 8));
-    const uint4 meta = ldg(reinterpret_cast<const uint4 *>(nf + 12));
-    if (COUNT) cnt->box[KIND] += 2;
-    float m0, m1;
-    int d0 = box_test32(q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, f, r, m0);
-    int d1 = box_test32(q1.z, q1.w, q2.x, q2.y, q2.z, q2.w, f, r, m1);
-    bool e0 = false, e1 = false;
-    double k0 = 0.0, k1 = 0.0;
-    if (d0 == 2) {
-      d0 = child_test64(K, tv.cur, 0, r, k0) ? 1 : 0;
-      e0 = true;
+    const unsigned char *base = K.wide + size_t(tv.cur) * kWideBytes;
+    const uint4 *nd = reinterpret_cast<const uint4 *>(base);
+    const uint32_t *words = reinterpret_cast<const uint32_t *>(base);
+    const uint4 hd = ldg(nd), qx = ldg(nd + 1), qy = ldg(nd + 2), qz = ldg(nd + 3);
+    const uint32_t perm = ldg(words + 24 + f.oct);
+    const uint32_t nch = hd.w >> 24;
+    // t(q) = fma(q, 2^e inv, (origin - o) inv) per axis
+    const float ax = fbits((hd.w & 0xFFu) << 23) * f.inv[0];
+    const float ay = fbits(((hd.w >> 8) & 0xFFu) << 23) * f.inv[1];
+    const float az = fbits(((hd.w >> 16) & 0xFFu) << 23) * f.inv[2];
+    const float bx = (fbits(hd.x) - f.o[0]) * f.inv[0];
+    const float by = (fbits(hd.y) - f.o[1]) * f.inv[1];
+    const float bz = (fbits(hd.z) - f.o[2]) * f.inv[2];
+    // near and far bound words per axis: the hi bounds are near for a negative direction
+    const uint32_t nx0 = r.sx ? qx.z : qx.x, nx1 = r.sx ? qx.w : qx.y;
+    const uint32_t fx0 = r.sx ? qx.x : qx.z, fx1 = r.sx ? qx.y : qx.w;
+    const uint32_t ny0 = r.sy ? qy.z : qy.x, ny1 = r.sy ? qy.w : qy.y;
+    const uint32_t fy0 = r.sy ? qy.x : qy.z, fy1 = r.sy ? qy.y : qy.w;
+    const uint32_t nz0 = r.sz ? qz.z : qz.x, nz1 = r.sz ? qz.w : qz.y;
+    const uint32_t fz0 = r.sz ? qz.x : qz.z, fz1 = r.sz ? qz.y : qz.w;
+    if (COUNT) {
+      cnt->node[KIND] += 1;
+      cnt->box[KIND] += nch;
     }
-    if (d1 == 2) {
-      d1 = child_test64(K, tv.cur, 1, r, k1) ? 1 : 0;
-      e1 = true;
-    }
-    const unsigned near = meta.z == 0 ? r.sx : (meta.z == 1 ? r.sy : r.sz);
-    const int dn = near ? d1 : d0, df = near ? d0 : d1;
-    const bool en = near ? e1 : e0, ef = near ? e0 : e1;
-    const double kn = near ? k1 : k0, kf = near ? k0 : k1;
-    const float mnn = near ? m1 : m0, mnf = near ? m0 : m1;
-    const uint32_t rn = near ? meta.y : meta.x, rf = near ? meta.x : meta.y;
-    if (df) {
-      if (tv.sp >= sk.cap) {
-        flag_error(err, kErrStack);
-        tv.live = false;
-        return;
-      }
-      push32(sk, tid, tv.sp, rf, ef ? float(kf) : mnf,
-             (tv.cur << 2) | ((near ? 0u : 1u) << 1) | (ef ? 1u : 0u));
-      ++tv.sp;
-    }
-    bool take_near = false;
-    if (dn) {
-      if (en) {
-        take_near = !(kn > st.hit);
-      } else {
-        const int d = key_decide(mnn, f.delta, st.hit);
-        if (d >= 0) {
-          take_near = d;
-        } else {
-          double k;
-          child_test64(K, tv.cur, int(near), r, k);
-          take_near = !(k > st.hit);
+    bool have = false;
+    uint32_t next = 0;
+    float next_key = 0.0f;
+#pragma unroll
+    for (int j = kWideMax - 1; j >= 0; --j) {
+      if (uint32_t(j) >= nch) continue;
+      const uint32_t slot = (perm >> (4 * j)) & 7u;
+      const float tnx = fma32(qslot(nx0, nx1, slot), ax, bx);
+      const float tny = fma32(qslot(ny0, ny1, slot), ay, by);
+      const float tnz = fma32(qslot(nz0, nz1, slot), az, bz);
+      const float tfx = fma32(qslot(fx0, fx1, slot), ax, bx);
+      const float tfy = fma32(qslot(fy0, fy1, slot), ay, by);
+      const float tfz = fma32(qslot(fz0, fz1, slot), az, bz);
+      const float entry = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, f.tmin));
+      const float exit = fminf(fminf(tfx, tfy), tfz) + f.delta2;
+      if (entry <= fminf(exit, hl)) {
+        if (have) {
+          if (tv.sp >= sk.cap) {
+            flag_error(err, kErrStack);
+            tv.live = false;
+            return;
+          }
+          skey[tv.sp * sk.stride + tid] = next_key;
+          sk.ref[tv.sp * sk.stride + tid] = next;
+          ++tv.sp;
         }
+        next = ldg(words + 16 + slot);
+        next_key = entry;
+        have = true;
       }
     }
-    if (take_near) {
-      tv.cur = rn;
-    } else {
-      trav_pop32<KIND>(K, r, f, tv, st, sk, tid);
-    }
+    if (have)
+      tv.cur = next;
+    else
+      wtrav_pop(tv, hl, sk, tid);
   }
 }
 
+// A leaf record: the exact FP64 test of the leaf's box, then its primitives in the reference's
+// stored order (blazert/bvh/intersect.h:67-78), then the next stack entry.
 template <int KIND, bool COUNT>
-BZR_HD void trav_leaf32(const KindView &K, const Ray &r, const RayF &f, KState &st, Trav &tv,
-                        const Stack &sk, uint32_t tid, uint32_t *err, Counts *cnt) {
-  uint32_t pos = tv.cur & kIdMask;
-  for (;;) {
-    if (pos >= K.n_prims) {
+BZR_HD void wtrav_leaf(const KindView &K, const Ray &r, const RayW &f, KState &st, float &hl,
+                       Trav &tv, const Stack &sk, uint32_t tid, uint32_t *err, Counts *cnt) {
+  constexpr uint32_t kUnits = KIND == kMesh ? 1u : uint32_t(kPayloadDoubles[KIND] / 2);
+  const uint32_t off = tv.cur & kIdMask;
+  if (uint64_t(off) + kLeafHeaderBytes / 16 > K.n_leaf16) {
+    flag_error(err, kErrPrimIndex);
+    tv.live = false;
+    return;
+  }
+  const double *L = K.leaves + 2 * size_t(off);
+  const double2 px = ld2(L), py = ld2(L + 2), pz = ld2(L + 4);
+  const uint4 hdr = ldg(reinterpret_cast<const uint4 *>(L + 6));
+  if (COUNT) cnt->leaf[KIND] += 1;
+  double key;
+  if (box_test(px, py, pz, r, key) && !(key > st.hit)) {
+    if (uint64_t(off) + kLeafHeaderBytes / 16 + uint64_t(kUnits) * hdr.y > K.n_leaf16 ||
+        uint64_t(hdr.x) + hdr.y > K.n_prims) {
       flag_error(err, kErrPrimIndex);
       tv.live = false;
       return;
     }
-    if (COUNT) cnt->prim[KIND] += 1;
-    bool h;
-    const uint32_t id = isect<KIND>(K, pos, r, st, h);
-    if (h && r.any_hit) {
-      tv.live = false;
-      return;
+    const double before = st.hit;
+    for (uint32_t j = 0; j < hdr.y; ++j) {
+      const uint32_t pos = hdr.x + j;
+      const double *P = L + kLeafHeaderBytes / 8 + size_t(j) * kUnits * 2;
+      if (COUNT) cnt->prim[KIND] += 1;
+      bool h;
+      if (KIND == kMesh)
+        h = isect_triangle(K.verts, ldg(reinterpret_cast<const uint4 *>(P)), pos, r, st);
+      else if (KIND == kSpheres)
+        h = isect_sphere(P, pos, r, st);
+      else
+        h = isect_plane(P, pos, r, st);
+      if (h && r.any_hit) {  // the first hit ends the leaf and the traversal
+        tv.live = false;
+        return;
+      }
     }
-    if (id & kLastBit) break;
-    ++pos;
+    if (st.hit != before) hl = f32_up(st.hit) + f.delta;
   }
-  trav_pop32<KIND>(K, r, f, tv, st, sk, tid);
+  wtrav_pop(tv, hl, sk, tid);
 }
 
-// Whole traversal of one kind in mixed precision (FP64 for rays or kinds not eligible).
+// Whole traversal of one kind in mixed precision (the FP64 traversal for cylinders, kinds
+// without a wide image and rays the FP32 test does not cover).
 template <int KIND, bool COUNT>
 BZR_HD bool traverse_mixed(const KindView &K, const Ray &r, KState &st, const Stack &sk,
                            uint32_t tid, uint32_t *err, Counts *cnt) {
-  const RayF f = make_ray_f(r, K.coord_max);
-  if (!(K.mixed_ok && f.ok)) return traverse<KIND, COUNT>(K, r, st, sk, tid, err, cnt);
-  Trav tv;
-  trav_begin<KIND, COUNT>(K, r, st, tv, cnt);
-  while (tv.live) {
-    trav_to_leaf32<KIND, COUNT>(K, r, f, st, tv, sk, tid, err, cnt);
-    if (tv.live) trav_leaf32<KIND, COUNT>(K, r, f, st, tv, sk, tid, err, cnt);
+  if constexpr (KIND == kCylinders) {
+    return traverse<KIND, COUNT>(K, r, st, sk, tid, err, cnt);
+  } else {
+    const RayW f = make_ray_w(r, K.wide_coord_max);
+    if (!(K.mixed_ok && f.ok)) return traverse<KIND, COUNT>(K, r, st, sk, tid, err, cnt);
+    Trav tv;
+    float hl;
+    wtrav_begin<KIND, COUNT>(K, r, f, st, hl, tv, cnt);
+    while (tv.live) {
+      wtrav_to_leaf<KIND, COUNT>(K, r, f, hl, tv, sk, tid, err, cnt);
+      if (tv.live) wtrav_leaf<KIND, COUNT>(K, r, f, st, hl, tv, sk, tid, err, cnt);
+    }
+    return st.hit < r.tmax;
   }
-  return st.hit < r.tmax;
 }
 
 struct Best {

@@ -36,7 +36,12 @@ static void commit(Emu *e, bool build) {
     e->img[k] = bzr::flatten(s, k);
     const bzr::KindImage &im = e->img[k];
     v.nodes64 = im.nodes64.data();
-    v.nodes32 = im.nodes32.data();
+    v.wide = im.wide.data();
+    v.leaves = im.leaves.data();
+    v.n_wide = im.n_wide;
+    v.n_leaf16 = im.n_leaf16;
+    v.wide_root_ref = im.wide_root_ref;
+    v.wide_coord_max = im.wide_coord_max;
     v.payload = im.payload.data();
     v.prim_ids = im.prim_ids.data();
     v.pos_of = im.pos_of.data();
@@ -52,7 +57,11 @@ static void commit(Emu *e, bool build) {
   }
   e->view.faces = s.faces.data();
   e->view.vert_n = s.vert_n.data();
-  e->view.stack_cap = (depth + 2) < 8 ? 8 : depth + 2;
+  uint32_t cap = (depth + 2) < 8 ? 8 : depth + 2;
+  for (int k = 0; k < 4; ++k)
+    if (s.kind[k].present && e->img[k].mixed_ok && e->img[k].wide_stack > cap)
+      cap = e->img[k].wide_stack;
+  e->view.stack_cap = cap;
   s.committed = true;
 }
 
@@ -146,6 +155,45 @@ long emu_scene_tree(void *h, int kind, double *bmin, double *bmax, uint32_t *lea
 // accumulated error word.
 }  // extern "C"
 
+// Work counters of one kind over a batch (the kernels' Counts, summed): totals[16] as
+// bzr_work_counts_ex lays them out (box, prim, node, leaf; each per kind).
+template <int KIND>
+static void emu_count_pass(const bzr::SceneView &view, long n, const double *org,
+                           const double *dir, const double *tmin, const double *tmax, int mode,
+                           uint64_t *totals) {
+  uint64_t box = 0, prim = 0, node = 0, leaf = 0;
+#pragma omp parallel reduction(+ : box, prim, node, leaf)
+  {
+    std::vector<double> key(view.stack_cap);
+    std::vector<uint32_t> ref(view.stack_cap);
+    bzr::Stack sk;
+    sk.key = key.data();
+    sk.ref = ref.data();
+    sk.cap = view.stack_cap;
+    sk.stride = 1;
+    uint32_t e = 0;
+#pragma omp for schedule(dynamic, 256)
+    for (long i = 0; i < n; ++i) {
+      bzr::Ray r = bzr::make_ray(org + 3 * i, dir + 3 * i, tmin ? tmin[i] : 0.0,
+                                 tmax ? tmax[i] : 1.7976931348623157e308);
+      bzr::KState st;
+      bzr::Counts c = {};
+      if (mode & 1)
+        bzr::traverse_mixed<KIND, true>(view.k[KIND], r, st, sk, 0, &e, &c);
+      else
+        bzr::traverse<KIND, true>(view.k[KIND], r, st, sk, 0, &e, &c);
+      box += c.box[KIND];
+      prim += c.prim[KIND];
+      node += c.node[KIND];
+      leaf += c.leaf[KIND];
+    }
+  }
+  totals[KIND] += box;
+  totals[4 + KIND] += prim;
+  totals[8 + KIND] += node;
+  totals[12 + KIND] += leaf;
+}
+
 template <int KIND>
 static void emu_pass(const bzr::SceneView &view, long n, const double *org, const double *dir,
                      const double *tmin, const double *tmax, bool first, double *t, double *uv,
@@ -178,6 +226,109 @@ static void emu_pass(const bzr::SceneView &view, long n, const double *org, cons
 }
 
 extern "C" {
+
+// Checks one kind's wide image against its tree: every leaf record is reached exactly once
+// from the wide root, every stored child box on the way contains the leaf's exact box (the
+// bounds origin + q 2^e evaluated exactly in double), and every leaf record's box and
+// primitive range are the tree leaf's.  Returns the number of violations, or -1 when the kind
+// has no wide image; *leaves receives the leaf records reached.
+long emu_wide_check(void *h, int kind, long *leaves) {
+  const Emu *e = static_cast<Emu *>(h);
+  const bzr::KindImage &im = e->img[kind];
+  *leaves = 0;
+  if (!e->host.kind[kind].present || !im.mixed_ok) return -1;
+  long bad = 0;
+  std::vector<long> seen(im.n_leaf16, 0);
+  struct Box {
+    double lo[3], hi[3];
+  };
+  struct Item {
+    uint32_t ref;
+    std::vector<Box> path;
+  };
+  std::vector<Item> todo{{im.wide_root_ref, {}}};
+  while (!todo.empty()) {
+    Item it = todo.back();
+    todo.pop_back();
+    if (it.ref & bzr::kLeafBit) {
+      const uint32_t off = it.ref & bzr::kIdMask;
+      if (off >= im.n_leaf16) {
+        ++bad;
+        continue;
+      }
+      ++seen[off];
+      ++*leaves;
+      const double *L = &im.leaves[2 * size_t(off)];
+      for (const Box &b : it.path)
+        for (int a = 0; a < 3; ++a)
+          if (!(b.lo[a] <= L[2 * a] && L[2 * a + 1] <= b.hi[a])) ++bad;
+      continue;
+    }
+    if (it.ref >= im.n_wide) {
+      ++bad;
+      continue;
+    }
+    const unsigned char *nd = &im.wide[size_t(it.ref) * bzr::kWideBytes];
+    float origin[3];
+    uint32_t ex, refs[8];
+    std::memcpy(origin, nd, 12);
+    std::memcpy(&ex, nd + 12, 4);
+    std::memcpy(refs, nd + 64, 32);
+    const uint32_t nch = ex >> 24;
+    if (nch < 2 || nch > 8) ++bad;
+    for (uint32_t c = 0; c < nch && c < 8; ++c) {
+      Item child{refs[c], it.path};
+      Box b;
+      for (int a = 0; a < 3; ++a) {
+        const int ea = int((ex >> (8 * a)) & 0xFFu) - 127;
+        b.lo[a] = double(origin[a]) + std::ldexp(double(nd[16 + 16 * a + c]), ea);
+        b.hi[a] = double(origin[a]) + std::ldexp(double(nd[24 + 16 * a + c]), ea);
+      }
+      child.path.push_back(b);
+      todo.push_back(child);
+    }
+  }
+  // every leaf of the tree has its record (records are in tree order), with its box and
+  // primitive range, reached once
+  const bzr::Tree &t = e->host.kind[kind].tree;
+  long n_leaves = 0;
+  for (const bzr::TreeNode &nd : t.nodes) n_leaves += nd.leaf == 1 ? 1 : 0;
+  if (n_leaves != *leaves) ++bad;
+  size_t off = 0;
+  uint32_t first = 0;
+  const uint32_t units = kind == 0 ? 1u : uint32_t(bzr::kPayloadDoubles[kind] / 2);
+  for (const bzr::TreeNode &nd : t.nodes) {
+    if (nd.leaf != 1) continue;
+    if (off + 4 > im.n_leaf16 || seen[off] != 1) {
+      ++bad;
+      break;
+    }
+    const double *L = &im.leaves[2 * off];
+    uint32_t head[2];
+    std::memcpy(head, L + 6, 8);
+    for (int a = 0; a < 3; ++a)
+      if (L[2 * a] != nd.mn[a] || L[2 * a + 1] != nd.mx[a]) ++bad;
+    if (head[0] != first || head[1] != nd.prim_cnt) ++bad;
+    first += nd.prim_cnt;
+    off += 4 + size_t(units) * nd.prim_cnt;
+  }
+  return bad;
+}
+
+void emu_work_counts(void *h, long n, const double *org, const double *dir, const double *tmin,
+                     const double *tmax, int mode, uint64_t *totals) {
+  const Emu *e = static_cast<Emu *>(h);
+  for (int k = 0; k < 16; ++k) totals[k] = 0;
+  for (int k = 0; k < 4; ++k) {
+    if (!e->view.k[k].present || e->view.k[k].n_prims == 0) continue;
+    switch (k) {
+      case 0: emu_count_pass<0>(e->view, n, org, dir, tmin, tmax, mode, totals); break;
+      case 1: emu_count_pass<1>(e->view, n, org, dir, tmin, tmax, mode, totals); break;
+      case 2: emu_count_pass<2>(e->view, n, org, dir, tmin, tmax, mode, totals); break;
+      default: emu_count_pass<3>(e->view, n, org, dir, tmin, tmax, mode, totals); break;
+    }
+  }
+}
 
 uint32_t emu_scene_intersect(void *h, long n, const double *org, const double *dir,
                              const double *tmin, const double *tmax, double *t, double *uv,
@@ -316,7 +467,8 @@ int emu_image_digest(void *h, int kind, long workers, uint64_t *digest) {
     mix(v.data(), v.size() * sizeof v[0]);
   };
   mix_array(im.nodes64);
-  mix_array(im.nodes32);
+  mix_array(im.wide);
+  mix_array(im.leaves);
   mix_array(im.payload);
   mix_array(im.prim_ids);
   mix_array(im.pos_of);
@@ -327,6 +479,11 @@ int emu_image_digest(void *h, int kind, long workers, uint64_t *digest) {
   mix(&im.root_ref, sizeof im.root_ref);
   mix(im.root_box, sizeof im.root_box);
   mix(&im.coord_max, sizeof im.coord_max);
+  mix(&im.n_wide, sizeof im.n_wide);
+  mix(&im.n_leaf16, sizeof im.n_leaf16);
+  mix(&im.wide_root_ref, sizeof im.wide_root_ref);
+  mix(&im.wide_stack, sizeof im.wide_stack);
+  mix(&im.wide_coord_max, sizeof im.wide_coord_max);
   mix(&ok, 1);
   *digest = x;
   return 0;

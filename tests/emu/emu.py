@@ -63,6 +63,10 @@ def load():
         lib.emu_distance_to_surface.restype = C.c_uint32
         lib.emu_distance_to_surface.argtypes = _DIST_ARGS
         lib.emu_closest_surface.argtypes = _NEAREST_ARGS
+        lib.emu_work_counts.argtypes = [C.c_void_p, C.c_long, _dp, _dp, _dp, _dp, C.c_int,
+                                        C.c_void_p]
+        lib.emu_wide_check.restype = C.c_long
+        lib.emu_wide_check.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_long)]
         _lib = lib
     return _lib
 
@@ -145,3 +149,18 @@ class EmuScene(_Base):
             _ptr(out["prim"], _u32p), _ptr(out["geom"], _u32p), _ptr(out["hit"], _u8p), stack_cap,
             (1 if mode == "mixed" else 0) | (2 if any_hit else 0)))
         return out
+
+    def work_counts(self, org, dirs, tmin=None, tmax=None, mode="fp64"):
+        """The kernels' work counters over a batch: dict of box, prim, node, leaf (4 per kind)."""
+        org, dirs, tmin, tmax, n = _rays(org, dirs, tmin, tmax)
+        tot = np.zeros(16, np.uint64)
+        self._lib.emu_work_counts(self._h, n, _ptr(org, _dp), _ptr(dirs, _dp), _ptr(tmin, _dp),
+                                  _ptr(tmax, _dp), 1 if mode == "mixed" else 0, tot.ctypes.data)
+        return {k: [int(x) for x in tot[4 * j:4 * j + 4]]
+                for j, k in enumerate(("box", "prim", "node", "leaf"))}
+
+    def wide_check(self, kind):
+        """(violations, leaf records reached) of the kind's wide image, or None without one."""
+        leaves = C.c_long(0)
+        bad = self._lib.emu_wide_check(self._h, KINDS.index(kind), C.byref(leaves))
+        return None if bad < 0 else (int(bad), int(leaves.value))

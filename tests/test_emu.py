@@ -148,3 +148,87 @@ def test_raw_storage_is_written_in_full(tmp_path):
     assert r.returncode == 0, r.stderr[-3000:]
     poisoned = json.loads(r.stdout.strip().splitlines()[-1])
     assert poisoned == json.loads(json.dumps(_raw_storage_results()))
+
+
+@pytest.mark.parametrize("name", ["icosphere_pinhole", "mixed_primitives", "heightfield"])
+def test_wide_image_contains_every_leaf(name):
+    """The mixed path's wide image: every leaf record is reached once from the wide root, each
+    quantised child box on the way contains the leaf's exact box, and the records hold the
+    tree leaves' exact boxes and primitive ranges.  Cylinders have no wide image (their hit
+    distance may grow, so their mixed mode runs the FP64 traversal)."""
+    kw = {"n_rays": 16}
+    if name == "heightfield":
+        kw["grid"] = 256
+    wl = W.WORKLOADS[name](**kw)
+    emu = EmuScene(wl.scene)
+    for kind in wl.scene.order:
+        got = emu.wide_check(kind)
+        if kind == "cylinders":
+            assert got is None
+            continue
+        bad, leaves = got
+        assert bad == 0 and leaves == emu.build_statistics(kind)["leaf_nodes"], (kind, got)
+
+
+def test_mixed_walk_uses_the_wide_image():
+    """The mixed path fetches far fewer nodes than the FP64 path on the same rays (wide nodes
+    of up to 8 children) and tests the same primitives."""
+    wl = W.heightfield(n_rays=20_000, grid=256)
+    R = wl.rays
+    emu = EmuScene(wl.scene)
+    a = emu.work_counts(R.origins, R.directions, R.tmin, R.tmax, mode="fp64")
+    b = emu.work_counts(R.origins, R.directions, R.tmin, R.tmax, mode="mixed")
+    assert a["prim"] == b["prim"]
+    assert b["node"][0] * 2 < a["node"][0]
+    assert b["leaf"][0] >= a["leaf"][0]
+
+
+def _grazing_rays(spec, n, rng):
+    """Rays aimed at box faces, edges and corners of the scene's primitives: origins on a face
+    plane or a corner, directions along an axis with tiny or zero other components, finite
+    tmax ending inside boxes, tmin > 0 starting inside them."""
+    emu = EmuScene(spec)
+    boxes = []
+    for kind in spec.order:
+        m = len(next(iter(getattr(spec, kind).values()))) if kind != "mesh" else \
+            len(spec.mesh["faces"])
+        for pid in rng.integers(0, m, min(m, 64)):
+            boxes.append(emu.prim_box(kind, int(pid))[:2])
+    org, dirs, tmin, tmax = [], [], [], []
+    for _ in range(n):
+        lo, hi = boxes[rng.integers(len(boxes))]
+        p = np.where(rng.random(3) < 0.5, lo, hi)
+        if rng.random() < 0.5:  # a point on a face instead of a corner
+            a = rng.integers(3)
+            p = p.copy()
+            p[a] = rng.uniform(lo[a], hi[a])
+        d = np.zeros(3)
+        a = rng.integers(3)
+        d[a] = rng.choice([-1.0, 1.0])
+        small = rng.choice([0.0, 1e-30, 1e-12, 1e-6, 1e-3])
+        d[(a + 1) % 3] = small * rng.choice([-1.0, 1.0])
+        d[(a + 2) % 3] = rng.choice([0.0, small, -small])
+        back = rng.uniform(0.0, 5.0)
+        org.append(p - back * d)
+        dirs.append(d * rng.choice([1.0, 3.0, 1e-3]))
+        tmin.append(rng.choice([0.0, 0.0, back * 0.5, back]))
+        tmax.append(rng.choice([np.inf, 1.7976931348623157e308, back + rng.uniform(0, 2)]))
+    return (np.array(org), np.array(dirs), np.array(tmin), np.array(tmax))
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_mixed_grazing_rays_match_the_oracle(seed):
+    """Rays that graze box faces, edges and corners, run parallel to slab planes or start and
+    end inside boxes: the mixed path's FP32 walk with the exact FP64 leaf test gives the
+    oracle's results bit for bit (rays with a zero direction component take the FP64 walk)."""
+    rng = np.random.default_rng(100 + seed)
+    specs = [W.icosphere_pinhole(level=3, width=8, height=8).scene,
+             W.mixed_primitives(n_rays=16, n_spheres=500, n_cylinders=50, n_planes=40,
+                                seed=seed).scene,
+             W.heightfield(n_rays=16, grid=64).scene]
+    for spec in specs:
+        o, d, tmn, tmx = _grazing_rays(spec, 4000, rng)
+        ref = Oracle(spec).intersect(o, d, tmn, tmx)
+        got = EmuScene(spec).intersect(o, d, tmn, tmx, mode="mixed")
+        assert got["error_word"] == 0
+        assert mismatches(got, ref) == []
