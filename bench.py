@@ -567,7 +567,8 @@ def run_ours(args):
             if res[m]["tuning"]:  # the device knobs this mode was timed with
                 c = res[m]["tuning"]["choice"]
                 scene.tune(sort=c["sort"], sort_min_rays=0 if c["sort"] else 1 << 16,
-                           threads=c["threads"], shared_stack=c["shared_stack"], chunk=c["chunk"])
+                           threads=c["threads"], shared_stack=c["shared_stack"], chunk=c["chunk"],
+                           top_nodes=c.get("top_nodes", 0))
             for _ in range(max(1, args.warmup)):
                 scene.intersectN(ho, hd, htmn, htmx, mode=m, out=hout, any_hit=args.any_hit)
             if pg:

@@ -476,13 +476,17 @@ class Scene:
         return out
 
     def tune(self, sort=None, sort_min_rays=None, threads=None, shared_stack=None, chunk=None,
-             host_chunks=None, host_min_chunk=None, host_edge=None, host_grid_div=None):
+             host_chunks=None, host_min_chunk=None, host_edge=None, host_grid_div=None,
+             top_nodes=None):
         """Speed knobs (bzr_scene_tune); results do not depend on them.  sort: coherence sort
         of each batch; threads: 64 / 128 / 256 per block; shared_stack: traversal stack in
         shared memory instead of thread-local; chunk: rays per warp fetch (32 / 64 / 128, or 0
         for exactly the idle lanes); host_chunks / host_min_chunk: the pipeline of host-array
         calls (at most this many chunks, 1 to 32, of at least this many rays) and host_edge,
-        the rays of an extra small first and last chunk (0: none)."""
+        the rays of an extra small first and last chunk (0: none); top_nodes: top-level nodes
+        each block stages in shared memory (0 to 256)."""
+        if top_nodes is not None:
+            _check(self._lib.bzr_scene_tune(self._h, 10, int(top_nodes)))
         if host_grid_div is not None:
             _check(self._lib.bzr_scene_tune(self._h, 9, int(host_grid_div)))
         if host_edge is not None:

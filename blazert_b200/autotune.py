@@ -8,6 +8,7 @@ shape, so tuning is safe to run on live data:
   shared_stack  traversal stack in shared memory (sized from the tree) or thread-local
   chunk         rays a warp takes from the work counter per fetch: 32, 64, 128, or 0 for
                 exactly the lanes that are idle
+  top_nodes     top-level nodes each block stages in shared memory: 0, 64, 256
 
 The search is coordinate-wise: starting from the defaults, each knob in turn is set to the
 value with the lowest time while the others stay at their current best; two sweeps.  Each
@@ -18,7 +19,7 @@ order, and so its tie-breaking, is defined on its binary tree.
 from __future__ import annotations
 
 KNOBS = {"sort": (False, True), "threads": (128, 64, 256), "shared_stack": (False, True),
-         "chunk": (32, 0, 64, 128)}
+         "chunk": (32, 0, 64, 128), "top_nodes": (0, 64, 256)}
 
 
 def autotune(scene, origins, directions, tmin=None, tmax=None, mode="fp64", reps=3,
@@ -39,7 +40,8 @@ def autotune(scene, origins, directions, tmin=None, tmax=None, mode="fp64", reps
 
     def apply(cfg):
         scene.tune(sort=cfg["sort"], sort_min_rays=0 if cfg["sort"] else 1 << 16,
-                   threads=cfg["threads"], shared_stack=cfg["shared_stack"], chunk=cfg["chunk"])
+                   threads=cfg["threads"], shared_stack=cfg["shared_stack"], chunk=cfg["chunk"],
+                   top_nodes=cfg.get("top_nodes", 0))
 
     def timed(cfg):
         nonlocal out

@@ -33,7 +33,7 @@ SOURCES = [("scene.cpp", "cxx"), ("capi.cpp", "cxx"), ("trace.cu", "cu"), ("adjo
            ("noalloc.cu", "cu"), ("batch.cpp", "cxx"), ("gbuild.cu", "cu"), ("distance.cu", "cu"),
            ("scene_io.cpp", "cxx"), ("obj.cpp", "cxx")]
 HEADERS = ["layout.h", "scene.h", "trace.h", "trace_core.cuh", "adjoint.h", "capi_internal.h",
-           "distance.h", "distance_core.cuh", "bucket_sort.cuh"]
+           "distance.h", "distance_core.cuh", "bucket_sort.cuh", "alloc.h"]
 
 
 def _cuda_home():

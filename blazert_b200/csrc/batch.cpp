@@ -9,6 +9,7 @@
 #include <new>
 #include <vector>
 
+#include "alloc.h"
 #include "../../include/blazert_b200.h"
 #include "capi_internal.h"
 #include "trace.h"
@@ -93,12 +94,12 @@ int bzr_batch_create(bzr_batch **out, const bzr_scene *const *scenes, size_t n_s
   cudaSetDevice(b->device);
   cudaError_t e = bzr::batch_prepare(cap, &b->plan);
   const size_t n = n_scenes;
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_views, n * sizeof(bzr::SceneView));
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_first, n);
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_last, n);
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_rays, n * sizeof(uint32_t));
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_left, n * sizeof(uint32_t));
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_words, 8 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = bzr::dev_malloc(&b->d_views, n * sizeof(bzr::SceneView));
+  if (e == cudaSuccess) e = bzr::dev_malloc(&b->d_first, n);
+  if (e == cudaSuccess) e = bzr::dev_malloc(&b->d_last, n);
+  if (e == cudaSuccess) e = bzr::dev_malloc(&b->d_rays, n * sizeof(uint32_t));
+  if (e == cudaSuccess) e = bzr::dev_malloc(&b->d_left, n * sizeof(uint32_t));
+  if (e == cudaSuccess) e = bzr::dev_malloc(&b->d_words, 8 * sizeof(uint32_t));
   if (e == cudaSuccess)
     e = cudaMemcpy(b->d_views, b->views.data(), n * sizeof(bzr::SceneView), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->d_first, b->first_kind.data(), n, cudaMemcpyHostToDevice);
@@ -162,7 +163,7 @@ int bzr_batch_intersect(bzr_batch *b, const uint64_t *ray_offsets, const double 
       cudaFree(b->d_chunks);
       b->d_chunks = nullptr;
       b->chunk_cap = 0;
-      e = cudaMalloc(&b->d_chunks, std::max<size_t>(1, chunks.size()) * sizeof(bzr::BatchChunk));
+      e = bzr::dev_malloc(&b->d_chunks, std::max<size_t>(1, chunks.size()) * sizeof(bzr::BatchChunk));
       if (e != cudaSuccess) {
         cudaSetDevice(cur);
         return fail(BZR_ENOMEM, "chunk table allocation failed");

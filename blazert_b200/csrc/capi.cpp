@@ -15,6 +15,7 @@
 #include <thread>
 #include <vector>
 
+#include "alloc.h"
 #include "../../include/blazert_b200.h"
 #include "layout.h"
 #include "scene.h"
@@ -32,8 +33,12 @@ int fail(int code, const std::string &msg) {
   return code;
 }
 int cuda_fail(cudaError_t e, const char *what) {
-  return fail(BZR_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return fail(e == cudaErrorMemoryAllocation ? BZR_ENOMEM : BZR_ECUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
 }
+
+// Allocations left before the injected failure (bzr_debug_fail_allocation); 0: none armed.
+std::atomic<int64_t> g_alloc_countdown{0};
 
 // Per-call device words: kSlots slots of kSlotWords = {work counter per kind pass (4), error
 // word, 3 spare}; one sticky error word for device-array calls follows the slots.
@@ -349,7 +354,7 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
   s->plan.pool = nullptr;
   cudaError_t e = cudaGetDevice(&s->device);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-  e = cudaMalloc(&s->arena, total);
+  e = bzr::dev_malloc(&s->arena, total);
   if (e != cudaSuccess) return fail(BZR_ENOMEM, "device arena allocation failed");
   for (const Piece &p : pieces) {
     if (!p.bytes) continue;
@@ -398,11 +403,11 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
     s->adj.sphere_geom = sph.geom_id;
   }
   s->view.stack_cap = std::max<uint32_t>({8, depth + 2, wide_stack});
-  e = cudaMalloc(&s->slots, (kStickyWord + 1) * sizeof(uint32_t));
+  e = bzr::dev_malloc(&s->slots, (kStickyWord + 1) * sizeof(uint32_t));
   if (e != cudaSuccess) return fail(BZR_ENOMEM, "slot allocation failed");
   e = cudaMemset(s->slots, 0, (kStickyWord + 1) * sizeof(uint32_t));
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemset");
-  e = cudaMallocHost(&s->pinned_err, kMaxChunks * sizeof(uint32_t));
+  e = bzr::host_malloc(&s->pinned_err, kMaxChunks * sizeof(uint32_t));
   if (e != cudaSuccess) return fail(BZR_ENOMEM, "pinned allocation failed");
   e = bzr::trace_prepare(s->view, &s->plan);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
@@ -527,7 +532,7 @@ static int run_small(bzr_scene *s, size_t n, const double *org, const double *di
   const size_t out_begin = p_t.off, out_bytes = total - out_begin;
   // the block for kSmallBatch rays with every piece bounds what any small batch needs
   const size_t cap = 8 * align_up(24 * kSmallBatch, 256) + 256;
-  if (!s->small_pin && cudaMallocHost(&s->small_pin, cap) != cudaSuccess) {
+  if (!s->small_pin && bzr::host_malloc(&s->small_pin, cap) != cudaSuccess) {
     s->small_pin = nullptr;
     return fail(BZR_ENOMEM, "pinned staging allocation failed");
   }
@@ -535,7 +540,7 @@ static int run_small(bzr_scene *s, size_t n, const double *org, const double *di
     cudaFree(s->stage_dev);
     s->stage_dev = nullptr;
     s->stage_bytes = 0;
-    if (cudaMalloc(&s->stage_dev, cap) != cudaSuccess)
+    if (bzr::dev_malloc(&s->stage_dev, cap) != cudaSuccess)
       return fail(BZR_ENOMEM, "staging allocation failed");
     s->stage_bytes = cap;
   }
@@ -630,7 +635,7 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
     io.error_word = s->slots + kStickyWord;  // sticky, read by bzr_scene_check
     cudaError_t e = cudaSuccess;
     if (!t) {  // the passes carry the closest distance in t: stream-ordered scratch
-      e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&io.t), 8 * n, s->plan.pool, st);
+      e = bzr::pool_malloc(&io.t, 8 * n, s->plan.pool, st);
       if (e != cudaSuccess) return fail(BZR_ENOMEM, "distance scratch allocation failed");
     }
     e = bzr::launch_trace(s->view, io, mode, s->plan, st, counters, totals);
@@ -657,7 +662,7 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
     cudaFree(s->stage_dev);
     s->stage_dev = nullptr;
     s->stage_bytes = 0;
-    if (cudaMalloc(&s->stage_dev, need) != cudaSuccess)
+    if (bzr::dev_malloc(&s->stage_dev, need) != cudaSuccess)
       return fail(BZR_ENOMEM, "staging allocation failed");
     s->stage_bytes = need;
   }
@@ -790,7 +795,7 @@ int bzr_work_counts(const bzr_scene *cs, size_t n, const double *org, const doub
   cudaGetDevice(&cur);
   cudaSetDevice(s->device);
   unsigned long long *dev = nullptr;
-  cudaError_t e = cudaMalloc(&dev, 8 * sizeof(unsigned long long));
+  cudaError_t e = bzr::dev_malloc(&dev, 8 * sizeof(unsigned long long));
   if (e != cudaSuccess) {
     cudaSetDevice(cur);
     return fail(BZR_ENOMEM, "counter allocation failed");
@@ -865,7 +870,7 @@ int bzr_adjoint_hit(const bzr_scene *cs, size_t n, const double *origins,
   if (e == cudaSuccess && grad_radii) e = cudaMemsetAsync(grad_radii, 0, 8 * ns, st);
   double *gvn = nullptr;
   if (e == cudaSuccess && grad_vertices && nv) {
-    e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&gvn), 24 * nv, s->plan.pool, st);
+    e = bzr::pool_malloc(&gvn, 24 * nv, s->plan.pool, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(gvn, 0, 24 * nv, st);
   }
   io.grad_vert_n = gvn;
@@ -935,7 +940,7 @@ static int run_distance(const bzr_scene *cs, int kind, size_t n, const uint32_t 
   for (size_t b : per) total += align_up(b * n, 256);
   char *dev = nullptr;
   cudaError_t e =
-      cudaMallocFromPoolAsync(reinterpret_cast<void **>(&dev), total, s->plan.pool, s->copy_in);
+      bzr::pool_malloc(&dev, total, s->plan.pool, s->copy_in);
   if (e != cudaSuccess) return fail(BZR_ENOMEM, "distance staging allocation failed");
   uint32_t *err = reinterpret_cast<uint32_t *>(dev);
   e = cudaMemsetAsync(err, 0, sizeof(uint32_t), s->copy_in);
@@ -1223,19 +1228,25 @@ int bzr_scene_tune(bzr_scene *s, int option, int64_t value) {
       s->plan.chunk = static_cast<uint32_t>(value);
       return BZR_OK;
     case BZR_TUNE_BLOCK:
-    case BZR_TUNE_STACK: {
+    case BZR_TUNE_STACK:
+    case BZR_TUNE_TOP_NODES: {
       bzr::LaunchPlan p = s->plan;
       if (option == BZR_TUNE_BLOCK) {
         if (value != 64 && value != 128 && value != 256)
           return fail(BZR_EINVAL, "threads per block must be 64, 128 or 256");
         p.threads = static_cast<int>(value);
+      } else if (option == BZR_TUNE_TOP_NODES) {
+        if (value < 0 || value > 256) return fail(BZR_EINVAL, "top nodes must be 0 to 256");
+        p.top_nodes = static_cast<uint32_t>(value);
       } else {
         if (value != 0 && value != 1) return fail(BZR_EINVAL, "stack storage must be 0 or 1");
         p.shared_stack = value == 1;
       }
-      if ((p.shared_stack || s->view.stack_cap > bzr::kLocalStack) &&
-          bzr::trace_smem_bytes(s->view.stack_cap, p.threads) > 227 * 1024)
-        return fail(BZR_EINVAL, "the traversal stack does not fit shared memory at this block size");
+      const bool local = !p.shared_stack && s->view.stack_cap <= bzr::kLocalStack;
+      if (bzr::trace_kind_smem(s->view.stack_cap, p.threads, local, p.top_nodes) > 227 * 1024)
+        return fail(BZR_EINVAL,
+                    "the traversal stack and staged nodes do not fit shared memory at this "
+                    "block size");
       int cur = 0;
       cudaGetDevice(&cur);
       cudaSetDevice(s->device);
@@ -1303,3 +1314,19 @@ int bzr_scene_stats(const bzr_scene *s, int kind, uint64_t *n_nodes, uint32_t *m
 }
 
 }  // extern "C"
+
+namespace bzr {
+bool injected_allocation_failure() {
+  int64_t left = g_alloc_countdown.load();
+  while (left > 0) {
+    if (g_alloc_countdown.compare_exchange_weak(left, left - 1)) return left == 1;
+  }
+  return false;
+}
+}  // namespace bzr
+
+int bzr_debug_fail_allocation(int64_t k) {
+  if (k < 0) return fail(BZR_EINVAL, "k must be >= 0");
+  g_alloc_countdown.store(k);
+  return BZR_OK;
+}

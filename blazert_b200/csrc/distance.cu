@@ -8,6 +8,7 @@
 // form walks the triangle and sphere BVHs nearest child first with a thread-local stack.
 #include <cmath>
 
+#include "alloc.h"
 #include "bucket_sort.cuh"
 #include "distance.h"
 #include "distance_core.cuh"
@@ -177,7 +178,7 @@ cudaError_t launch_nearest(const SceneView &S, const DistanceIO &io, int sms, cu
   if (any && pool && io.n >= kNearestSortMin && io.n < 0xFFFFFFFFull) {
     const uint32_t n = uint32_t(io.n);
     const size_t nb = size_t(1) << kSortBits;
-    e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&scratch),
+    e = bzr::pool_malloc(&scratch,
                                 (2 * size_t(n) + nb) * sizeof(uint32_t), pool, stream);
     if (e != cudaSuccess) return e;
     uint32_t *keys = scratch, *perm = scratch + n, *counts = scratch + 2 * size_t(n);

@@ -34,6 +34,7 @@
 #include <mutex>
 #include <vector>
 
+#include "alloc.h"
 #include "scene.h"
 
 namespace bzr {
@@ -628,7 +629,7 @@ cudaError_t gpu_build_tree(const PrimBoxes &boxes, const BuildOptions &opt, Tree
   if (ws.bytes < need) {
     if (ws.ptr) cudaFree(ws.ptr);
     ws = Workspace{};
-    e = cudaMalloc(&ws.ptr, need);
+    e = bzr::dev_malloc(&ws.ptr, need);
     if (e != cudaSuccess) {
       ws.ptr = nullptr;
       return e;

@@ -30,6 +30,7 @@
 
 #include <cstdint>
 
+#include "alloc.h"
 #include "layout.h"
 #include "bucket_sort.cuh"
 #include "trace.h"
@@ -39,6 +40,13 @@ namespace bzr {
 namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// Shared memory of the stack: none for a thread-local stack, else stack_cap entries of 12 bytes
+// per thread, rounded up to 16 bytes (the staged top-level nodes follow).
+template <bool LOCAL>
+__device__ __forceinline__ size_t stack_smem_bytes(uint32_t stack_cap) {
+  return LOCAL ? 0 : (size_t(stack_cap) * blockDim.x * 12 + 15) / 16 * 16;
+}
 
 // Traversal stack storage.  LOCAL: a thread-local array of kLocalStack entries (local memory,
 // cached in L1; the host picks it when the tree's stack fits, and it leaves the SM's shared
@@ -115,6 +123,23 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
   init_stack<LOCAL>(sk, tid, S.stack_cap, smem, lkey, lref);
   const KindView &K = S.k[KIND];
   if (!COUNT) prefetch_kind<KIND, kWide>(K);
+  // The first io.top_nodes nodes of the array this kernel walks (the top levels every ray
+  // visits) are staged in shared memory after the stack.  Rays of a mixed kernel that take
+  // the FP64 walk use the global FP64 nodes (sk64 has no staged nodes then).
+  const bool walk_wide = kWide && K.mixed_ok;
+  Stack sk64 = sk;
+  {
+    const uint32_t avail = walk_wide ? K.n_wide : K.n_internal;
+    const uint32_t n_top = io.top_nodes < avail ? io.top_nodes : avail;
+    uint4 *top = reinterpret_cast<uint4 *>(smem + stack_smem_bytes<LOCAL>(S.stack_cap));
+    const uint4 *src = walk_wide ? reinterpret_cast<const uint4 *>(K.wide)
+                                 : reinterpret_cast<const uint4 *>(K.nodes64);
+    for (uint32_t j = threadIdx.x; j < n_top * 8; j += blockDim.x) top[j] = ldg(src + j);
+    if (n_top) __syncthreads();
+    sk.top = top;
+    sk.n_top = n_top;
+    if (!walk_wide) sk64 = sk;
+  }
   const unsigned lane = threadIdx.x & 31u;
   const unsigned below = (1u << lane) - 1u;
   uint32_t pool_next = 0, pool_end = 0;  // warp-uniform
@@ -173,8 +198,8 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
         if (tv.live) wtrav_to_leaf<KIND, COUNT>(K, r, f, hl, tv, sk, tid, io.error_word, &cnt);
         if (tv.live) wtrav_leaf<KIND, COUNT>(K, r, f, st, hl, tv, sk, tid, io.error_word, &cnt);
       } else {
-        if (tv.live) trav_to_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, io.error_word, &cnt);
-        if (tv.live) trav_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, io.error_word, &cnt);
+        if (tv.live) trav_to_leaf<KIND, COUNT>(K, r, st, tv, sk64, tid, io.error_word, &cnt);
+        if (tv.live) trav_leaf<KIND, COUNT>(K, r, st, tv, sk64, tid, io.error_word, &cnt);
       }
       if (!tv.live) {
         finalize_kind<KIND>(S, r, st, i, first != 0, io.t, io.uv, io.normal, io.prim, io.geom,
@@ -376,14 +401,15 @@ cudaError_t launch_kind(const SceneView &S, const RayIO &io, int mode, int first
   const bool mixed = mode == kModeMixed && KIND != kCylinders;
   const int th = plan.threads;
   if (!COUNT && use_local(S, plan)) {
+    const size_t smem = trace_kind_smem(S.stack_cap, th, true, io.top_nodes);
     if (mixed)
-      trace_kind_kernel<KIND, false, true, true><<<blocks, th, 0, stream>>>(S, io, first, counter,
-                                                                           totals);
+      trace_kind_kernel<KIND, false, true, true><<<blocks, th, smem, stream>>>(S, io, first,
+                                                                              counter, totals);
     else
-      trace_kind_kernel<KIND, false, false, true><<<blocks, th, 0, stream>>>(S, io, first,
-                                                                            counter, totals);
+      trace_kind_kernel<KIND, false, false, true><<<blocks, th, smem, stream>>>(S, io, first,
+                                                                               counter, totals);
   } else {
-    const size_t smem = trace_smem_bytes(S.stack_cap, th);
+    const size_t smem = trace_kind_smem(S.stack_cap, th, false, io.top_nodes);
     if (mixed)
       trace_kind_kernel<KIND, COUNT, true, false><<<blocks, th, smem, stream>>>(S, io, first,
                                                                                counter, totals);
@@ -409,7 +435,8 @@ cudaError_t grid_for(const void *fn, int threads, size_t smem, int sms, int *blo
 template <int KIND>
 cudaError_t prepare_kind(const SceneView &S, LaunchPlan *plan) {
   const int th = plan->threads;
-  const size_t smem = trace_smem_bytes(S.stack_cap, th);
+  const size_t smem = trace_kind_smem(S.stack_cap, th, false, plan->top_nodes);
+  const size_t smem_local = trace_kind_smem(S.stack_cap, th, true, plan->top_nodes);
   const void *shared_fns[4] = {
       reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, false, false>),
       reinterpret_cast<const void *>(trace_kind_kernel<KIND, true, false, false>),
@@ -423,11 +450,11 @@ cudaError_t prepare_kind(const SceneView &S, LaunchPlan *plan) {
   int *blocks = &plan->blocks[KIND], *blocks32 = &plan->blocks32[KIND];
   if (use_local(S, *plan)) {
     const cudaError_t e = grid_for(
-        reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, false, true>), th, 0,
-        plan->sms, blocks);
+        reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, false, true>), th,
+        smem_local, plan->sms, blocks);
     if (e != cudaSuccess) return e;
     return grid_for(reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, true, true>), th,
-                    0, plan->sms, blocks32);
+                    smem_local, plan->sms, blocks32);
   }
   const cudaError_t e = grid_for(shared_fns[0], th, smem, plan->sms, blocks);
   if (e != cudaSuccess) return e;
@@ -446,6 +473,11 @@ cudaError_t launch_defaults(const RayIO &io, int sms, cudaStream_t stream) {
 
 size_t trace_smem_bytes(uint32_t stack_cap, int threads) {
   return size_t(stack_cap) * threads * (sizeof(double) + sizeof(uint32_t));
+}
+
+size_t trace_kind_smem(uint32_t stack_cap, int threads, bool local, uint32_t top_nodes) {
+  const size_t stack = local ? 0 : (trace_smem_bytes(stack_cap, threads) + 15) / 16 * 16;
+  return stack + size_t(top_nodes) * 128;
 }
 
 cudaError_t trace_prepare(const SceneView &S, LaunchPlan *plan) {
@@ -473,10 +505,11 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
   if (e != cudaSuccess) return e;
   RayIO sorted = io;
   sorted.chunk = plan.chunk;
+  sorted.top_nodes = plan.top_nodes;
   uint32_t *scratch = nullptr;
   if (plan.sort.enabled && io.n >= plan.sort_min_rays && trace_passes(S) > 0) {
     const size_t nb = size_t(1) << kSortBits;
-    e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&scratch),
+    e = bzr::pool_malloc(&scratch,
                                 (2 * size_t(io.n) + nb) * sizeof(uint32_t), plan.pool, stream);
     if (e != cudaSuccess) return e;
     uint32_t *keys = scratch, *perm = scratch + io.n, *counts = scratch + 2 * size_t(io.n);

@@ -34,6 +34,7 @@ struct RayIO {
   int any_hit = 0;                 // every ray is Ray::AnyHit::yes (blazert/ray.h:24-34)
   uint32_t chunk = kRayChunk;      // rays a warp takes per fetch: 32, 64, 128, or 0 for
                                    // exactly the lanes that are idle
+  uint32_t top_nodes = 0;          // top-level nodes each block stages in shared memory
 };
 
 // Coherence sort of a batch: rays are processed in the order of a 32-bit key -- the direction
@@ -53,6 +54,7 @@ struct LaunchPlan {
   int threads = kTraceThreads;     // threads per block: 64, 128 or 256
   bool shared_stack = false;       // traversal stack in shared memory even when it fits locally
   uint32_t chunk = kRayChunk;      // rays per warp fetch: 32, 64, 128 or 0 (exactly the idle lanes)
+  uint32_t top_nodes = 0;          // top-level nodes each block stages in shared memory (0..256)
   int blocks[kNumKinds] = {0, 0, 0, 0};    // FP64 kernels
   int blocks32[kNumKinds] = {0, 0, 0, 0};  // mixed-precision kernels
   RaySort sort;
@@ -99,6 +101,9 @@ cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const Ba
 cudaError_t launch_defaults(const RayIO &io, int sms, cudaStream_t stream);
 
 size_t trace_smem_bytes(uint32_t stack_cap, int threads);
+// Dynamic shared memory of a trace_kind_kernel launch: the stack unless thread-local, then
+// top_nodes staged 128-byte nodes.
+size_t trace_kind_smem(uint32_t stack_cap, int threads, bool local, uint32_t top_nodes);
 // Fills plan->sms and the per-kind grids for plan->threads and plan->shared_stack.
 cudaError_t trace_prepare(const SceneView &S, LaunchPlan *plan);
 // Number of per-kind passes a batch runs (kinds present with at least one primitive).

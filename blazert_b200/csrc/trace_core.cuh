@@ -390,12 +390,23 @@ BZR_HD uint32_t isect(const KindView &K, uint32_t pos, const Ray &r, KState &st,
   return id;
 }
 
-// Traversal stack in shared memory, entry j of thread t at [j * blockDim.x + t].
+// Traversal storage of a thread: the stack (entry j of thread t at [j * stride + t]; stride 1
+// for a thread-local array), and the first n_top nodes of the walked node array (FP64 nodes,
+// or wide nodes on the mixed path; the top levels, as nodes are numbered breadth-first)
+// staged in shared memory by the block, 8 x 16 bytes each.
 struct Stack {
   double *key;
   uint32_t *ref;
   uint32_t cap, stride;
+  const uint4 *top = nullptr;
+  uint32_t n_top = 0;
 };
+
+BZR_HD double2 as_d2(uint4 q) {
+  double2 d;
+  std::memcpy(&d, &q, sizeof d);
+  return d;
+}
 
 // Work counters of one ray (counting kernels only), per kind: box tests (FP64 path: the
 // reference's node pops, i.e. the root plus both children of every accepted internal node;
@@ -457,10 +468,19 @@ BZR_HD void trav_to_leaf(const KindView &K, const Ray &r, const KState &st, Trav
       tv.live = false;
       return;
     }
-    const double *nd = K.nodes64 + size_t(tv.cur) * kNode64Doubles;
-    const double2 a0 = ld2(nd), a1 = ld2(nd + 2), a2 = ld2(nd + 4);
-    const double2 b0 = ld2(nd + 6), b1 = ld2(nd + 8), b2 = ld2(nd + 10);
-    const uint4 meta = ldg(reinterpret_cast<const uint4 *>(nd + 12));
+    double2 a0, a1, a2, b0, b1, b2;
+    uint4 meta;
+    if (tv.cur < sk.n_top) {  // a top-level node staged in shared memory
+      const uint4 *q = sk.top + size_t(tv.cur) * 8;
+      a0 = as_d2(q[0]), a1 = as_d2(q[1]), a2 = as_d2(q[2]);
+      b0 = as_d2(q[3]), b1 = as_d2(q[4]), b2 = as_d2(q[5]);
+      meta = q[6];
+    } else {
+      const double *nd = K.nodes64 + size_t(tv.cur) * kNode64Doubles;
+      a0 = ld2(nd), a1 = ld2(nd + 2), a2 = ld2(nd + 4);
+      b0 = ld2(nd + 6), b1 = ld2(nd + 8), b2 = ld2(nd + 10);
+      meta = ldg(reinterpret_cast<const uint4 *>(nd + 12));
+    }
     double k0, k1;
     if (COUNT) {
       cnt->box[KIND] += 2;
@@ -665,11 +685,19 @@ BZR_HD void wtrav_to_leaf(const KindView &K, const Ray &r, const RayW &f, float 
       tv.live = false;
       return;
     }
-    const unsigned char *base = K.wide + size_t(tv.cur) * kWideBytes;
-    const uint4 *nd = reinterpret_cast<const uint4 *>(base);
-    const uint32_t *words = reinterpret_cast<const uint32_t *>(base);
-    const uint4 hd = ldg(nd), qx = ldg(nd + 1), qy = ldg(nd + 2), qz = ldg(nd + 3);
-    const uint32_t perm = ldg(words + 24 + f.oct);
+    const bool staged = tv.cur < sk.n_top;  // a top-level node staged in shared memory
+    const uint4 *nd = staged ? sk.top + size_t(tv.cur) * 8
+                             : reinterpret_cast<const uint4 *>(K.wide + size_t(tv.cur) * kWideBytes);
+    const uint32_t *words = reinterpret_cast<const uint32_t *>(nd);
+    uint4 hd, qx, qy, qz;
+    uint32_t perm;
+    if (staged) {
+      hd = nd[0], qx = nd[1], qy = nd[2], qz = nd[3];
+      perm = words[24 + f.oct];
+    } else {
+      hd = ldg(nd), qx = ldg(nd + 1), qy = ldg(nd + 2), qz = ldg(nd + 3);
+      perm = ldg(words + 24 + f.oct);
+    }
     const uint32_t nch = hd.w >> 24;
     // t(q) = fma(q, 2^e inv, (origin - o) inv) per axis
     const float ax = fbits((hd.w & 0xFFu) << 23) * f.inv[0];
@@ -715,7 +743,7 @@ BZR_HD void wtrav_to_leaf(const KindView &K, const Ray &r, const RayW &f, float 
           sk.ref[tv.sp * sk.stride + tid] = next;
           ++tv.sp;
         }
-        next = ldg(words + 16 + slot);
+        next = staged ? words[16 + slot] : ldg(words + 16 + slot);
         next_key = entry;
         have = true;
       }

@@ -243,6 +243,10 @@ int bzr_scene_check(const bzr_scene *scene, void *stream, int timeout_ms, uint32
 /* Host-array calls: each chunk's kernels use 1/value (1 to 8, default 1) of the grid, so that
  * chunks on the pipeline's three streams can run side by side. */
 #define BZR_TUNE_HOST_GRID_DIV 9
+/* Top-level nodes (0 to 256, default 0) each block of the traversal kernels copies into shared
+ * memory at launch and reads from there: the first nodes of the breadth-first node array the
+ * kernel walks (the FP64 nodes, or the wide nodes of the mixed path), which every ray visits. */
+#define BZR_TUNE_TOP_NODES 10
 int bzr_scene_tune(bzr_scene *scene, int option, int64_t value);
 
 /* Statistics of the last commit: per kind (0 mesh, 1 spheres, 2 planes, 3 cylinders) the
@@ -329,6 +333,12 @@ int bzr_obj_load(const char *path, double **vertices, size_t *n_vertices, uint32
 void bzr_obj_free(void *p);
 
 const char *bzr_last_error_string(void);
+
+/* Test hook (no counterpart in the reference): the k-th device or pinned-host allocation this
+ * library makes from now on fails as if the device were out of memory (k = 0 disarms; the
+ * hook disarms itself when it fires).  The entry point that meets the failure returns
+ * BZR_ENOMEM and releases what it had allocated; the scene stays usable. */
+int bzr_debug_fail_allocation(int64_t k);
 
 #ifdef __cplusplus
 }

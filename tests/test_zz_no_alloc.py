@@ -69,3 +69,76 @@ def test_noalloc_entry_matches_intersectN_twice():
     rc = _call(lib, scene, big, ob, ob, None, None, dict(hit=torch.zeros(big, dtype=torch.uint8, device=dev)), stream)
     assert rc == B.EINVAL
     assert "1,048,576" in lib.bzr_last_error_string().decode()
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["mixed_primitives", "heightfield"])
+def test_noalloc_modes_and_kinds_allocate_nothing(name, mode):
+    """Both modes, on a scene of several kinds and on a single-kind mesh scene: the results
+    equal bzr_intersectN's bit for bit on two calls in a row, no allocation of this library is
+    made (with the allocation-failure hook armed on the next allocation the calls still
+    succeed), and the device's free memory does not change."""
+    import torch
+
+    wl = W.mixed_primitives(n_rays=200_000, seed=22) if name == "mixed_primitives" else \
+        W.heightfield(n_rays=200_000, grid=256)
+    R = wl.rays
+    scene = product_scene(wl.scene)
+    dev = torch.device("cuda", 0)
+    o, d = torch.from_numpy(R.origins).to(dev), torch.from_numpy(R.directions).to(dev)
+    tmin, tmax = torch.from_numpy(R.tmin).to(dev), torch.from_numpy(R.tmax).to(dev)
+    ref = to_numpy(scene.intersectN(o, d, tmin, tmax, mode=("fp64", "mixed")[mode]))
+    for k in ("prim", "geom"):
+        ref[k] = ref[k].view(np.uint32)
+    lib = B.library()
+    lib.bzr_debug_fail_allocation.argtypes = [C.c_int64]
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    n = R.n
+    f64 = torch.float64
+    out = dict(t=torch.empty(n, dtype=f64, device=dev), uv=torch.empty((n, 2), dtype=f64, device=dev),
+               normal=torch.empty((n, 3), dtype=f64, device=dev),
+               prim=torch.empty(n, dtype=torch.int32, device=dev),
+               geom=torch.empty(n, dtype=torch.int32, device=dev),
+               hit=torch.empty(n, dtype=torch.uint8, device=dev))
+    lib.bzr_intersectN_noalloc.argtypes = [C.c_void_p, C.c_size_t] + [C.c_void_p] * 10 + \
+        [C.c_int, C.c_void_p]
+    ptr = lambda a: C.c_void_p(a.data_ptr())
+
+    def call():
+        return lib.bzr_intersectN_noalloc(scene._h, n, ptr(o), ptr(d), ptr(tmin), ptr(tmax),
+                                          ptr(out["t"]), ptr(out["uv"]), ptr(out["normal"]),
+                                          ptr(out["prim"]), ptr(out["geom"]), ptr(out["hit"]),
+                                          mode, C.c_void_p(stream))
+
+    assert call() == 0  # the first call on the device looks up the scratch's address
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    for _ in range(2):
+        for v in out.values():
+            v.fill_(7)
+        lib.bzr_debug_fail_allocation(1)
+        rc = call()
+        lib.bzr_debug_fail_allocation(0)
+        assert rc == 0, lib.bzr_last_error_string().decode()
+        torch.cuda.synchronize()
+        assert mismatches(out, ref) == []
+    assert torch.cuda.mem_get_info(dev)[0] == free0
+    assert scene.check() == 0
+    scene.close()
+
+
+def test_noalloc_rejects_host_arrays():
+    """Host arrays are refused with BZR_EINVAL (the entry point stages nothing)."""
+    wl = W.mixed_primitives(n_rays=1000, seed=23)
+    R = wl.rays
+    scene = product_scene(wl.scene)
+    lib = B.library()
+    lib.bzr_intersectN_noalloc.argtypes = [C.c_void_p, C.c_size_t] + [C.c_void_p] * 10 + \
+        [C.c_int, C.c_void_p]
+    t = np.empty(R.n)
+    hp = lambda a: C.c_void_p(a.ctypes.data)
+    rc = lib.bzr_intersectN_noalloc(scene._h, R.n, hp(R.origins), hp(R.directions), None, None,
+                                    hp(t), None, None, None, None, None, 0, None)
+    assert rc == B.EINVAL
+    assert "device arrays" in lib.bzr_last_error_string().decode()
+    scene.close()
