@@ -85,6 +85,8 @@ def library():
                                           C.c_uint32, P]
         lib.bzr_scene_check.argtypes = [P, P, C.c_int, _u32p]
         lib.bzr_work_counts.argtypes = [P, C.c_size_t, P, P, P, P, C.POINTER(C.c_uint64), P]
+        lib.bzr_work_counts_ex.argtypes = [P, C.c_size_t, P, P, P, P, C.c_int,
+                                           C.POINTER(C.c_uint64), P]
         lib.bzr_scene_tune.argtypes = [P, C.c_int, C.c_int64]
         lib.bzr_adjoint_hit.argtypes = [P, C.c_size_t] + [P] * 14 + [P]
         lib.bzr_batch_create.argtypes = [C.POINTER(P), C.POINTER(P), C.c_size_t]
@@ -521,10 +523,11 @@ class Scene:
         _check(self._lib.bzr_scene_build_statistics(self._h, KIND_NAMES.index(kind), C.byref(st)))
         return {n: getattr(st, n) for n, _ in _Stats._fields_}
 
-    def work_counts(self, origins, directions, tmin=None, tmax=None, stream=None):
-        """Box tests and primitive tests per kind for a batch (counting kernel; see
-        bzr_work_counts).  Returns dict(box=[4], prim=[4])."""
-        tot = (C.c_uint64 * 8)()
+    def work_counts(self, origins, directions, tmin=None, tmax=None, stream=None, mode="fp64"):
+        """Box tests, primitive tests, node fetches and leaf fetches per kind for a batch in
+        either mode (counting kernel; see bzr_work_counts_ex).  Returns dict(box=[4],
+        prim=[4], node=[4], leaf=[4])."""
+        tot = (C.c_uint64 * 16)()
         try:
             import torch
             dev = isinstance(origins, torch.Tensor) and origins.is_cuda
@@ -539,17 +542,18 @@ class Scene:
             tmx = None if tmax is None else torch.as_tensor(tmax, dtype=torch.float64, device=o.device).expand(n).contiguous()
             st = (stream or torch.cuda.current_stream(o.device)).cuda_stream
             ptr = lambda a: None if a is None else a.data_ptr()
-            _check(self._lib.bzr_work_counts(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
-                                             tot, C.c_void_p(st)))
+            _check(self._lib.bzr_work_counts_ex(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
+                                                MODES[mode], tot, C.c_void_p(st)))
         else:
             o, d = _f64(origins, 3), _f64(directions, 3)
             n = o.shape[0]
             tmn = None if tmin is None else np.ascontiguousarray(np.broadcast_to(tmin, (n,)), np.float64)
             tmx = None if tmax is None else np.ascontiguousarray(np.broadcast_to(tmax, (n,)), np.float64)
             ptr = lambda a: None if a is None else a.ctypes.data
-            _check(self._lib.bzr_work_counts(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
-                                             tot, None))
-        return dict(box=[int(x) for x in tot[:4]], prim=[int(x) for x in tot[4:]])
+            _check(self._lib.bzr_work_counts_ex(self._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx),
+                                                MODES[mode], tot, None))
+        return {k: [int(x) for x in tot[4 * j:4 * j + 4]]
+                for j, k in enumerate(("box", "prim", "node", "leaf"))}
 
     def adjoint(self, origins, directions, fwd, grad_t=None, grad_uv=None, grad_normal=None,
                 n_vertices=0, n_spheres=0, stream=None):

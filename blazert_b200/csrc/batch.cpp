@@ -52,7 +52,10 @@ struct bzr_batch {
 
 namespace {
 int fail(int code, const char *msg) { return bzr::set_error(code, msg); }
-int cuda_fail(cudaError_t e) { return bzr::set_error(BZR_ECUDA, cudaGetErrorString(e)); }
+int cuda_fail(cudaError_t e) {
+  return bzr::set_error(e == cudaErrorMemoryAllocation ? BZR_ENOMEM : BZR_ECUDA,
+                        cudaGetErrorString(e));
+}
 }  // namespace
 
 extern "C" {

@@ -786,39 +786,50 @@ int bzr_intersectN_ex(const bzr_scene *s, size_t n, const double *org, const dou
 
 int bzr_work_counts(const bzr_scene *cs, size_t n, const double *org, const double *dir,
                     const double *tmin, const double *tmax, uint64_t totals[8], void *stream) {
+  if (!totals) return fail(BZR_EINVAL, "null argument");
+  uint64_t all[16];
+  const int rc = bzr_work_counts_ex(cs, n, org, dir, tmin, tmax, BZR_MODE_FP64, all, stream);
+  for (int k = 0; k < 8; ++k) totals[k] = rc == BZR_OK ? all[k] : 0;
+  return rc;
+}
+
+int bzr_work_counts_ex(const bzr_scene *cs, size_t n, const double *org, const double *dir,
+                       const double *tmin, const double *tmax, int mode, uint64_t totals[16],
+                       void *stream) {
   bzr_scene *s = const_cast<bzr_scene *>(cs);
   if (!s || !totals) return fail(BZR_EINVAL, "null argument");
   if (!s->host.committed) return fail(BZR_ESTATE, "scene is not committed");
-  for (int k = 0; k < 8; ++k) totals[k] = 0;
+  if (mode != BZR_MODE_FP64 && mode != BZR_MODE_MIXED) return fail(BZR_EINVAL, "bad mode");
+  for (int k = 0; k < 16; ++k) totals[k] = 0;
   if (n == 0) return BZR_OK;
   int cur = 0;
   cudaGetDevice(&cur);
   cudaSetDevice(s->device);
   unsigned long long *dev = nullptr;
-  cudaError_t e = bzr::dev_malloc(&dev, 8 * sizeof(unsigned long long));
+  cudaError_t e = bzr::dev_malloc(&dev, 16 * sizeof(unsigned long long));
   if (e != cudaSuccess) {
     cudaSetDevice(cur);
     return fail(BZR_ENOMEM, "counter allocation failed");
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  e = cudaMemsetAsync(dev, 0, 8 * sizeof(unsigned long long), st);
+  e = cudaMemsetAsync(dev, 0, 16 * sizeof(unsigned long long), st);
   int rc = e == cudaSuccess ? BZR_OK : cuda_fail(e, "cudaMemsetAsync");
   cudaSetDevice(cur);
   if (rc == BZR_OK)
     rc = run_batch(s, n, org, dir, tmin, tmax, nullptr, nullptr, nullptr, nullptr, nullptr,
-                   nullptr, BZR_MODE_FP64, 0u, stream, dev);
+                   nullptr, mode, 0u, stream, dev);
   cudaSetDevice(s->device);
   // the host path ran on the scene's streams; make the counter copy wait for all of them
   for (cudaStream_t q : s->streams)
     if (rc == BZR_OK) rc = wait_stream(q, default_timeout_ms());
   if (rc == BZR_OK) rc = wait_stream(st, default_timeout_ms());
   if (rc == BZR_OK) {
-    unsigned long long h[8];
+    unsigned long long h[16];
     e = cudaMemcpy(h, dev, sizeof h, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess)
       rc = cuda_fail(e, "counter read");
     else
-      for (int k = 0; k < 8; ++k) totals[k] = h[k];
+      for (int k = 0; k < 16; ++k) totals[k] = h[k];
   }
   cudaFree(dev);
   cudaSetDevice(cur);

@@ -212,6 +212,14 @@ int bzr_adjoint_hit(const bzr_scene *scene, size_t n, const double *origins,
 int bzr_work_counts(const bzr_scene *scene, size_t n, const double *origins,
                     const double *directions, const double *tmin, const double *tmax,
                     uint64_t totals[8], void *stream);
+/* The same for either mode (BZR_MODE_FP64 or BZR_MODE_MIXED), with per kind in totals[0..3]
+ * the box tests (FP64: as above; mixed: the root test plus every child of every wide node
+ * fetched), in totals[4..7] the primitive tests, in totals[8..11] the node fetches (FP64
+ * internal nodes, or wide nodes) and in totals[12..15] the leaf fetches (FP64: leaves whose
+ * primitives run; mixed: leaf records read, each with its exact FP64 box test). */
+int bzr_work_counts_ex(const bzr_scene *scene, size_t n, const double *origins,
+                       const double *directions, const double *tmin, const double *tmax,
+                       int mode, uint64_t totals[16], void *stream);
 
 /* Waits for the scene's queued work (bounded by timeout_ms; <= 0 waits without bound) and
  * reports the kernels' error word: BZR_OK, BZR_EDEVICE_FLAG (with *flags receiving the bits)

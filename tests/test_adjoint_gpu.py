@@ -54,25 +54,76 @@ def test_adjoint_matches_analytic_small():
     _adjoint_vs_analytic(spec, o, d, rng, with_uv_normal=True)
 
 
-def test_adjoint_scene_analytic_and_finite_differences():
-    """The differentiation workload (91,920-triangle perturbed icosphere + 500 spheres), loss
-    L = sum w_i t_i^2: CUDA adjoint vs the host analytic gradient on all rays, and vs central
-    differences on a seeded subsample of parameters (rays whose hit primitive changes under the
-    perturbation, and grazing hits, are left out of the difference quotient)."""
-    wl = W.adjoint_scene(n_rays=1 << 20)
+@pytest.fixture(scope="module")
+def adjoint_case():
+    """The differentiation workload at full size (91,920-triangle perturbed icosphere + 500
+    spheres, 4,194,304 rays): its scene, rays, forward results and the loss weights."""
+    wl = W.adjoint_scene()
     spec, R = wl.scene, wl.rays
+    assert R.n == 4_194_304
     rng = np.random.Generator(np.random.PCG64(55))
-    s, f, wt = _adjoint_vs_analytic(spec, R.origins, R.directions, rng, with_uv_normal=False)
+    s = product_scene(spec)
     to, td = _dev(R.origins), _dev(R.directions)
     fwd = s.intersectN(to, td)
-    nv, ns = len(spec.mesh["vertices"]), len(spec.spheres["radii"])
+    f = to_numpy(fwd)
     hit = f["hit"].astype(bool)
-    g = s.adjoint(to, td, fwd, grad_t=_dev(2 * wt * f["t"] * hit), n_vertices=nv, n_spheres=ns)
-    gv, gc, gr = (g[k].cpu().numpy() for k in ("vertices", "centers", "radii"))
+    w = {"t": rng.standard_normal(R.n) * hit,
+         "uv": rng.standard_normal((R.n, 2)) * hit[:, None],
+         "normal": rng.standard_normal((R.n, 3)) * hit[:, None]}
+    yield dict(spec=spec, R=R, s=s, to=to, td=td, fwd=fwd, f=f, hit=hit, w=w, rng=rng)
+    s.close()
 
-    # Grazing hits (|cos| between ray and normal below 0.05) are left out of the difference
-    # quotient: dt/dparameter grows like 1/cos there, and the truncation error of the
-    # difference quotient faster still.
+
+def _upstream(case, loss, mask):
+    """dL/dt, dL/duv, dL/dnormal of the chosen loss, restricted to the rays in `mask`."""
+    f, w = case["f"], case["w"]
+    m = mask.astype(np.float64)
+    gt = 2 * w["t"] * f["t"] * m if loss == "t" else np.zeros(len(m))
+    guv = w["uv"] * m[:, None] if loss == "uv" else None
+    gn = w["normal"] * m[:, None] if loss == "normal" else None
+    return gt, guv, gn
+
+
+def _loss_of(out, case, loss, mask):
+    """Per-ray terms of L over the rays in `mask`: w t^2, w . uv or w . normal (misses 0)."""
+    w = case["w"]
+    h = out["hit"][mask].astype(bool)
+    if loss == "t":
+        return w["t"][mask] * np.where(h, out["t"][mask], 0.0) ** 2
+    key = "uv" if loss == "uv" else "normal"
+    return np.einsum("ij,ij->i", w[key][mask], np.where(h[:, None], out[key][mask], 0.0))
+
+
+def test_adjoint_scene_analytic_full_size(adjoint_case):
+    """All 4,194,304 rays: the CUDA adjoint of t, uv and normal (together) against the host
+    analytic FP64 gradient, per element within 1e-7 relative."""
+    c = adjoint_case
+    spec, R, s = c["spec"], c["R"], c["s"]
+    gt, _, _ = _upstream(c, "t", c["hit"])
+    guv = c["w"]["uv"]
+    gn = c["w"]["normal"]
+    nv, ns = len(spec.mesh["vertices"]), len(spec.spheres["radii"])
+    g = s.adjoint(c["to"], c["td"], c["fwd"], grad_t=_dev(gt), grad_uv=_dev(guv),
+                  grad_normal=_dev(gn), n_vertices=nv, n_spheres=ns)
+    assert s.check() == 0
+    ref = adjoint_ref.gradients(spec, R.origins, R.directions, c["f"], gt, guv, gn)
+    for k in ("origins", "directions", "vertices", "centers", "radii"):
+        assert_close(g[k].cpu().numpy(), ref[k], k)
+
+
+@pytest.mark.parametrize("loss", ["t", "uv", "normal"])
+def test_adjoint_scene_finite_differences(adjoint_case, loss):
+    """Losses L = sum w_i t_i^2, sum w_i . uv_i and sum w_i . normal_i over the full workload:
+    the CUDA adjoint against FP64 central differences of the GPU forward pass (h = 1e-6 and
+    h/2, Richardson-extrapolated) on a seeded subsample of vertex coordinates, sphere centres
+    and radii, to 1e-6 relative.  Rays whose hit primitive changes in any perturbed scene, and
+    grazing hits (|cos| between ray and normal below 0.05, where the difference quotient's
+    truncation error grows like 1/cos^2), are left out of both sides."""
+    c = adjoint_case
+    spec, R, s, f, hit = c["spec"], c["R"], c["s"], c["f"], c["hit"]
+    to, td, fwd = c["to"], c["td"], c["fwd"]
+    rng = np.random.Generator(np.random.PCG64({"t": 55, "uv": 56, "normal": 57}[loss]))
+    nv, ns = len(spec.mesh["vertices"]), len(spec.spheres["radii"])
     dn = R.directions / np.linalg.norm(R.directions, axis=1, keepdims=True)
     well = np.abs(np.einsum("ij,ij->i", dn, f["normal"])) >= 0.05
 
@@ -88,14 +139,18 @@ def test_adjoint_scene_analytic_and_finite_differences():
                     arrs[key][index] += step
                 getattr(s2, "add_" + k)(*arrs.values())
             specs.append(s2)
-        outs = [to_numpy(product_scene(x).intersectN(to, td)) for x in specs]
+        outs = []
+        for x in specs:
+            sx = product_scene(x)
+            outs.append(to_numpy(sx.intersectN(to, td)))
+            sx.close()
         stable = well.copy()
         for out in outs:
             stable &= (out["prim"] == f["prim"]) & (out["geom"] == f["geom"])
-        t2 = [np.where(o_["hit"][stable].astype(bool), o_["t"][stable], 0.0) ** 2 for o_ in outs]
+        terms = [_loss_of(o_, c, loss, stable) for o_ in outs]
         # per-ray differences first: rays the perturbation leaves alone contribute exactly 0
-        d1 = float(np.sum(wt[stable] * (t2[0] - t2[1]))) / (2 * H)
-        d2 = float(np.sum(wt[stable] * (t2[2] - t2[3]))) / H
+        d1 = float(np.sum(terms[0] - terms[1])) / (2 * H)
+        d2 = float(np.sum(terms[2] - terms[3])) / H
         return (4 * d2 - d1) / 3, stable
 
     used = 0
@@ -104,20 +159,25 @@ def test_adjoint_scene_analytic_and_finite_differences():
         vi = int(spec.mesh["faces"][face][0])
         for ax in range(3):
             fdv, stable = fd("mesh", "vertices", (vi, ax))
-            # the adjoint restricted to the same stable rays
-            g2 = s.adjoint(to, td, fwd, grad_t=_dev(2 * wt * f["t"] * hit * stable),
+            gt, guv, gn = _upstream(c, loss, hit & stable)
+            g2 = s.adjoint(to, td, fwd, grad_t=_dev(gt),
+                           grad_uv=None if guv is None else _dev(guv),
+                           grad_normal=None if gn is None else _dev(gn),
                            n_vertices=nv, n_spheres=ns)["vertices"].cpu().numpy()
             an = g2[vi, ax]
-            assert abs(fdv - an) <= 1e-6 * max(abs(an), 1e-3), (vi, ax, fdv, an)
+            assert abs(fdv - an) <= 1e-6 * max(abs(an), 1e-3), (loss, vi, ax, fdv, an)
             used += 1
     sph_candidates = np.unique(f["prim"][hit & (f["geom"] == 1)])
     for si in rng.choice(sph_candidates, 3, replace=False):
         for key, index in (("centers", (si, 0)), ("radii", si)):
             fdv, stable = fd("spheres", key, index)
-            g2 = s.adjoint(to, td, fwd, grad_t=_dev(2 * wt * f["t"] * hit * stable),
+            gt, guv, gn = _upstream(c, loss, hit & stable)
+            g2 = s.adjoint(to, td, fwd, grad_t=_dev(gt),
+                           grad_uv=None if guv is None else _dev(guv),
+                           grad_normal=None if gn is None else _dev(gn),
                            n_vertices=nv, n_spheres=ns)[key].cpu().numpy()
             an = g2[index]
-            assert abs(fdv - an) <= 1e-6 * max(abs(an), 1e-3), (key, index, fdv, an)
+            assert abs(fdv - an) <= 1e-6 * max(abs(an), 1e-3), (loss, key, index, fdv, an)
             used += 1
     assert used == 18
 
