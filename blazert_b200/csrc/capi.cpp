@@ -374,7 +374,6 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
     v.n_wide = img[k].n_wide;
     v.n_leaf16 = img[k].n_leaf16;
     v.wide_root_ref = img[k].wide_root_ref;
-    v.wide_coord_max = img[k].wide_coord_max;
     v.payload = reinterpret_cast<const double *>(base + off_payload[k]);
     v.prim_ids = reinterpret_cast<const uint32_t *>(base + off_ids[k]);
     v.pos_of = reinterpret_cast<const uint32_t *>(base + off_pos[k]);

@@ -97,7 +97,6 @@ struct KindView {
   uint32_t n_wide = 0;
   uint32_t n_leaf16 = 0;
   uint32_t wide_root_ref = 0;            // 0 (wide root) or kLeafBit | offset of a leaf root
-  float wide_coord_max = 0.0f;  // largest |quantised bound| of the wide nodes, rounded up
   float coord_max = 0.0f;       // largest |coordinate| of the root box, rounded up
 };
 

@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
                        io.tmax ? io.tmax[i] : kDblMax);
           r.any_hit = io.any_hit != 0;
           if constexpr (kWide) {
-            f = make_ray_w(r, K.wide_coord_max);
+            f = make_ray_w(r);
             use32 = K.mixed_ok && f.ok;
           }
           if (kWide && use32)
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
                        io.tmax ? io.tmax[i] : kDblMax);
           r.any_hit = io.any_hit != 0;
           if constexpr (kWide) {
-            f = make_ray_w(r, K->wide_coord_max);
+            f = make_ray_w(r);
             use32 = K->mixed_ok && f.ok;
           }
           if (kWide && use32)

@@ -552,14 +552,15 @@ BZR_HD bool traverse(const KindView &K, const Ray &r, KState &st, const Stack &s
 // kWideBytes).
 //
 // Internal levels are walked on the wide nodes with FP32 slab tests of the children's
-// quantised boxes, which contain their exact boxes.  Each FP32 slab distance is within delta
-// (below) of the reference's FP64 distance for the exact box, on the side that can only keep
-// more: a child is kept when its FP32 entry distance is at most both its FP32 exit distance +
-// 2 delta and the current hit distance (rounded up) + delta, so every child the FP64 traversal
-// accepts is kept.  The kept children are visited in the reference's order (the node's rank
-// table for the ray's octant), and a stack entry is dropped at pop time only when its FP32
-// entry distance exceeds the hit distance + delta.  A leaf is processed when the reference's
-// exact FP64 test of the leaf's own box against the current hit distance passes
+// quantised boxes, which contain their exact boxes.  Every FP32 near-plane distance is
+// computed as a lower bound, and every far-plane distance as an upper bound, of the
+// reference's FP64 slab distances for the exact box (the error bound E below is subtracted or
+// added in the same fused multiply-add).  A child is kept when its FP32 entry distance is at
+// most both its FP32 exit distance and the current hit distance rounded up, so every child the
+// FP64 traversal accepts is kept.  The kept children are visited in the reference's order (the
+// node's permutation for the ray's octant), and a stack entry is dropped at pop time only when
+// its FP32 entry distance exceeds the hit distance rounded up.  A leaf is processed when the
+// reference's exact FP64 test of the leaf's own box against the current hit distance passes
 // (blazert/bvh/intersect.h:33-51).
 //
 // Why the results are the FP64 path's: the walk reaches every node the FP64 traversal accepts,
@@ -572,18 +573,22 @@ BZR_HD bool traverse(const KindView &K, const Ray &r, KState &st, const Stack &s
 // test passes, no ancestor failed.  The same leaves are therefore processed in the same order
 // with the same hit distance, and every primitive test and result is identical.
 //
-// delta: the FP32 distance t = fma(q, 2^e * inv_f, (origin - o_f) * inv_f) of a stored bound
-// b = origin + q 2^e differs from (b - o) * inv by at most 5 * 2^-24 * |inv| * (|b| + |o|)
-// (o_f, inv_f, the difference, the product and the fma each round once), the reference's own
-// FP64 roundings and its l1 factor add 2^-49 relative, and fl32(tmin) 2^-24 |tmin|;
-// delta = 2^-20 * (max|inv| * (coord_max + max|o|) + |tmin|) + 1e-30 * (1 + max|inv|) covers
-// these and the roundings of the sums compared.  Rays with a zero, non-finite or huge (> 1e18)
-// inverse direction or origin component, or a non-finite or huge tmin or a NaN tmax, take the
-// FP64 traversal.
+// Error bound, per node and axis: with A = 2^e inv_f, D = (origin - o_hi) - o_lo (the origin
+// held as two floats, so it is exact to 2^-48 relative) and B = D inv_f, the distance of a
+// stored bound origin + q 2^e is t = fma(q, A, B +- E).  Against the real distance T of that
+// bound for the FP64 inverse direction, fma(q, A, B) is off by at most 5 * 2^-24 * (255 |A| +
+// |B|) (inv_f, the two differences, the product and the fma each round once; q 2^e is exact);
+// the FP64 reference rounds T by 2^-49 relative (its l1 factor included) and B +- E rounds
+// once more.  E = 2^-20 (255 |A| + |B|) + 1e-37 covers all of these (and denormal results), so
+// the near distance is below and the far distance above the reference's.  The bound follows
+// the ray's own magnitudes on each axis: an axis whose direction component is tiny has large
+// distances and a large E, but those distances rarely decide the entry or the exit.  Rays with
+// a zero, non-finite or huge (> 1e18) inverse direction or origin component, or a non-finite
+// or huge tmin or a NaN tmax, take the FP64 traversal.
 struct RayW {
-  float o[3], inv[3];
-  float tmin, delta, delta2;  // delta2 = 2 delta, rounded up
-  uint32_t oct;               // sx | sy << 1 | sz << 2
+  float o_hi[3], o_lo[3], inv[3];
+  float tmin;    // tmin rounded down
+  uint32_t oct;  // sx | sy << 1 | sz << 2
   bool ok;
 };
 
@@ -612,31 +617,35 @@ BZR_HD float fma32(float a, float b, float c) {
   return fmaf(a, b, c);
 #endif
 }
-BZR_HD RayW make_ray_w(const Ray &r, float coord_max) {
+BZR_HD float f32_down(double x) {  // x rounded toward -inf
+#if defined(__CUDA_ARCH__)
+  return __double2float_rd(x);
+#else
+  float f = static_cast<float>(x);
+  if (static_cast<double>(f) > x) f = nextafterf(f, -__builtin_inff());
+  return f;
+#endif
+}
+
+BZR_HD RayW make_ray_w(const Ray &r) {
   RayW f;
   const double inv[3] = {r.inv.x, r.inv.y, r.inv.z}, o[3] = {r.o.x, r.o.y, r.o.z};
-  double imax = 0.0, omax = 0.0;
   bool ok = fabs(r.tmin) <= 1e18 && !isnan(r.tmax);
   for (int a = 0; a < 3; ++a) {
     const double ai = fabs(inv[a]), oa = fabs(o[a]);
     ok = ok && ai > 0.0 && ai <= 1e18 && oa <= 1e18;  // false for NaN and infinities
-    imax = ai > imax ? ai : imax;
-    omax = oa > omax ? oa : omax;
-    f.o[a] = static_cast<float>(o[a]);
+    f.o_hi[a] = static_cast<float>(o[a]);
+    f.o_lo[a] = static_cast<float>(o[a] - static_cast<double>(f.o_hi[a]));
     f.inv[a] = static_cast<float>(inv[a]);
   }
-  const double d = 9.5367431640625e-07 /* 2^-20 */ *
-                       (imax * (static_cast<double>(coord_max) + omax) + fabs(r.tmin)) +
-                   1e-30 * (1.0 + imax);
-  f.tmin = static_cast<float>(r.tmin);
-  f.delta = f32_up(d);
-  f.delta2 = f32_up(2.0 * d);
+  f.tmin = f32_down(r.tmin);
   f.oct = r.sx | (r.sy << 1) | (r.sz << 2);
   f.ok = ok;
   return f;
 }
 
-// Pop-time test of the wide walk: drops entries whose FP32 entry distance exceeds hl.
+// Pop-time test of the wide walk: drops entries whose FP32 entry distance exceeds hl (the hit
+// distance rounded up).
 BZR_HD void wtrav_pop(Trav &tv, float hl, const Stack &sk, uint32_t tid) {
   const float *skey = reinterpret_cast<const float *>(sk.key);
   while (tv.sp > 0) {
@@ -650,13 +659,13 @@ BZR_HD void wtrav_pop(Trav &tv, float hl, const Stack &sk, uint32_t tid) {
 }
 
 // The exact root test (trav_begin), then the walk starts at the wide root.  hl is the hit
-// distance rounded up, plus delta.
+// distance rounded up.
 template <int KIND, bool COUNT>
 BZR_HD void wtrav_begin(const KindView &K, const Ray &r, const RayW &f, KState &st, float &hl,
                         Trav &tv, Counts *cnt) {
   trav_begin<KIND, COUNT>(K, r, st, tv, cnt);
   tv.cur = K.wide_root_ref;
-  hl = f32_up(st.hit) + f.delta;
+  hl = f32_up(st.hit);
 }
 
 // Byte `slot` (0..7) of the 8-byte value (w0 low, w1 high) as a float (exact).
@@ -699,13 +708,20 @@ BZR_HD void wtrav_to_leaf(const KindView &K, const Ray &r, const RayW &f, float 
       perm = ldg(words + 24 + f.oct);
     }
     const uint32_t nch = hd.w >> 24;
-    // t(q) = fma(q, 2^e inv, (origin - o) inv) per axis
+    // per axis t(q) = fma(q, A, B -+ E): a lower bound of the reference's near-plane
+    // distance, an upper bound of its far-plane distance
     const float ax = fbits((hd.w & 0xFFu) << 23) * f.inv[0];
     const float ay = fbits(((hd.w >> 8) & 0xFFu) << 23) * f.inv[1];
     const float az = fbits(((hd.w >> 16) & 0xFFu) << 23) * f.inv[2];
-    const float bx = (fbits(hd.x) - f.o[0]) * f.inv[0];
-    const float by = (fbits(hd.y) - f.o[1]) * f.inv[1];
-    const float bz = (fbits(hd.z) - f.o[2]) * f.inv[2];
+    const float bx = ((fbits(hd.x) - f.o_hi[0]) - f.o_lo[0]) * f.inv[0];
+    const float by = ((fbits(hd.y) - f.o_hi[1]) - f.o_lo[1]) * f.inv[1];
+    const float bz = ((fbits(hd.z) - f.o_hi[2]) - f.o_lo[2]) * f.inv[2];
+    constexpr float kErr = 9.5367431640625e-07f;  // 2^-20
+    const float ex = fma32(255.0f, fabsf(ax), fabsf(bx)) * kErr + 1e-37f;
+    const float ey = fma32(255.0f, fabsf(ay), fabsf(by)) * kErr + 1e-37f;
+    const float ez = fma32(255.0f, fabsf(az), fabsf(bz)) * kErr + 1e-37f;
+    const float bnx = bx - ex, bfx = bx + ex, bny = by - ey, bfy = by + ey;
+    const float bnz = bz - ez, bfz = bz + ez;
     // near and far bound words per axis: the hi bounds are near for a negative direction
     const uint32_t nx0 = r.sx ? qx.z : qx.x, nx1 = r.sx ? qx.w : qx.y;
     const uint32_t fx0 = r.sx ? qx.x : qx.z, fx1 = r.sx ? qx.y : qx.w;
@@ -717,28 +733,30 @@ BZR_HD void wtrav_to_leaf(const KindView &K, const Ray &r, const RayW &f, float 
       cnt->node[KIND] += 1;
       cnt->box[KIND] += nch;
     }
+    // The builder bounds the stack: the entries below this node plus its children minus one
+    // never exceed the image's stack size, which the capacity covers.  Checked once per node,
+    // so the child loop below has no exit.
+    if (tv.sp + nch > sk.cap + 1) {
+      flag_error(err, kErrStack);
+      tv.live = false;
+      return;
+    }
     bool have = false;
     uint32_t next = 0;
     float next_key = 0.0f;
 #pragma unroll
     for (int j = kWideMax - 1; j >= 0; --j) {
-      if (uint32_t(j) >= nch) continue;
       const uint32_t slot = (perm >> (4 * j)) & 7u;
-      const float tnx = fma32(qslot(nx0, nx1, slot), ax, bx);
-      const float tny = fma32(qslot(ny0, ny1, slot), ay, by);
-      const float tnz = fma32(qslot(nz0, nz1, slot), az, bz);
-      const float tfx = fma32(qslot(fx0, fx1, slot), ax, bx);
-      const float tfy = fma32(qslot(fy0, fy1, slot), ay, by);
-      const float tfz = fma32(qslot(fz0, fz1, slot), az, bz);
+      const float tnx = fma32(qslot(nx0, nx1, slot), ax, bnx);
+      const float tny = fma32(qslot(ny0, ny1, slot), ay, bny);
+      const float tnz = fma32(qslot(nz0, nz1, slot), az, bnz);
+      const float tfx = fma32(qslot(fx0, fx1, slot), ax, bfx);
+      const float tfy = fma32(qslot(fy0, fy1, slot), ay, bfy);
+      const float tfz = fma32(qslot(fz0, fz1, slot), az, bfz);
       const float entry = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, f.tmin));
-      const float exit = fminf(fminf(tfx, tfy), tfz) + f.delta2;
-      if (entry <= fminf(exit, hl)) {
+      const float exit = fminf(fminf(tfx, tfy), tfz);
+      if (uint32_t(j) < nch && entry <= fminf(exit, hl)) {
         if (have) {
-          if (tv.sp >= sk.cap) {
-            flag_error(err, kErrStack);
-            tv.live = false;
-            return;
-          }
           skey[tv.sp * sk.stride + tid] = next_key;
           sk.ref[tv.sp * sk.stride + tid] = next;
           ++tv.sp;
@@ -796,7 +814,7 @@ BZR_HD void wtrav_leaf(const KindView &K, const Ray &r, const RayW &f, KState &s
         return;
       }
     }
-    if (st.hit != before) hl = f32_up(st.hit) + f.delta;
+    if (st.hit != before) hl = f32_up(st.hit);
   }
   wtrav_pop(tv, hl, sk, tid);
 }
@@ -809,7 +827,7 @@ BZR_HD bool traverse_mixed(const KindView &K, const Ray &r, KState &st, const St
   if constexpr (KIND == kCylinders) {
     return traverse<KIND, COUNT>(K, r, st, sk, tid, err, cnt);
   } else {
-    const RayW f = make_ray_w(r, K.wide_coord_max);
+    const RayW f = make_ray_w(r);
     if (!(K.mixed_ok && f.ok)) return traverse<KIND, COUNT>(K, r, st, sk, tid, err, cnt);
     Trav tv;
     float hl;

@@ -41,7 +41,6 @@ static void commit(Emu *e, bool build) {
     v.n_wide = im.n_wide;
     v.n_leaf16 = im.n_leaf16;
     v.wide_root_ref = im.wide_root_ref;
-    v.wide_coord_max = im.wide_coord_max;
     v.payload = im.payload.data();
     v.prim_ids = im.prim_ids.data();
     v.pos_of = im.pos_of.data();

@@ -138,12 +138,17 @@ def test_bounded_waits_time_out_and_recover():
     od, dd = torch.from_numpy(R.origins).to(dev), torch.from_numpy(R.directions).to(dev)
     ref = to_numpy(scene.intersectN(od, dd))
     torch.cuda.synchronize()
-    stream = torch.cuda.current_stream(dev)
-    for _ in range(4):  # tens of milliseconds of queued work
-        scene.intersectN(od, dd, stream=stream)
+    stream = torch.cuda.Stream(dev)
+    out = scene.intersectN(od, dd, stream=stream)
+    stream.synchronize()
+    done = torch.cuda.Event()
+    for _ in range(32):  # a few hundred milliseconds of queued work
+        scene.intersectN(od, dd, out=out, stream=stream)
+    done.record(stream)
     with pytest.raises(B.BlazertError) as e:
         scene.check(stream=stream.cuda_stream, timeout_ms=1)
     assert e.value.code == B.ETIMEOUT
+    assert not done.query()  # the work was still queued when the wait ran out
     assert scene.check(stream=stream.cuda_stream, timeout_ms=60000) == 0
     # host arrays: the call's own wait runs out while its copies and kernels are queued
     os.environ["BZR_TIMEOUT_MS"] = "1"
