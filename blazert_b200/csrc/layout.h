@@ -61,9 +61,9 @@ constexpr int kVertexDoubles = 4;
 //                 16-byte units
 //   bytes 96..127 u32 perm[8]: for a ray of direction-sign octant s = sx | sy << 1 | sz << 2,
 //                 nibble j of perm[s] is the slot of the j-th child in the reference's visit
-//                 order (the reference visits children[direction_sign[axis]] first at every
-//                 binary node, blazert/bvh/accel.h:100-104, so a treelet's order depends on s
-//                 only).
+//                 order, 15 past the last child (the reference visits
+//                 children[direction_sign[axis]] first at every binary node,
+//                 blazert/bvh/accel.h:100-104, so a treelet's order depends on s only).
 // Leaf records (16-byte aligned): the leaf's exact FP64 box (lo.x, hi.x, lo.y, hi.y, lo.z,
 // hi.z; 48 B), u32 first leaf-ordered position, u32 count, 8 B zero; then the leaf's
 // primitives: triangles {i0, i1, i2, 0} (16 B, indices into the vertex array), spheres and

@@ -645,7 +645,9 @@ void build_wide(const Tree &t, int kind, const std::vector<uint32_t> &leaf_pos, 
     ex |= uint32_t(ch.size()) << 24;
     std::memcpy(node, origin, sizeof origin);
     std::memcpy(node + 12, &ex, sizeof ex);
-    uint32_t ref[kWideMax] = {}, perm[8] = {};
+    // perm nibbles past the children hold 15: no slot, so the walk never takes them
+    uint32_t ref[kWideMax] = {}, perm[8] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu,
+                                            0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
     for (size_t j = 0; j < ch.size(); ++j) {
       const TreeNode &c = t.nodes[ch[j]];
       if (c.leaf == 1) {
@@ -665,6 +667,7 @@ void build_wide(const Tree &t, int kind, const std::vector<uint32_t> &leaf_pos, 
         todo.pop_back();
         const auto it = std::find(ch.begin(), ch.end(), x);
         if (it != ch.end() && x != queue[head]) {
+          perm[oct] &= ~(0xFu << (4 * pos));
           perm[oct] |= uint32_t(it - ch.begin()) << (4 * pos++);
           continue;
         }

@@ -111,9 +111,9 @@ __device__ __forceinline__ void prefetch_kind(const KindView &K) {
 // node fetches, leaf fetches; see Counts).  MIXED: rays the FP32 test covers walk the wide
 // image (cylinders always take the FP64 traversal).
 template <int KIND, bool COUNT, bool MIXED, bool LOCAL>
-__global__ void __launch_bounds__(kMaxTraceThreads)
-    trace_kind_kernel(SceneView S, RayIO io, int first, uint32_t *work_counter,
-                      unsigned long long *totals) {
+__device__ __forceinline__ void trace_kind_body(const SceneView &S, const RayIO &io, int first,
+                                                uint32_t *work_counter,
+                                                unsigned long long *totals) {
   constexpr bool kWide = MIXED && KIND != kCylinders;
   extern __shared__ __align__(16) unsigned char smem[];
   double lkey[LOCAL ? kLocalStack : 1];
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
     if (!__any_sync(kFull, active)) break;
     if (active) {
       if (kWide && use32) {
-        if (tv.live) wtrav_to_leaf<KIND, COUNT>(K, r, f, hl, tv, sk, tid, io.error_word, &cnt);
+        if (tv.live) wtrav_to_leaf<KIND, COUNT>(K, f, hl, tv, sk, tid, io.error_word, &cnt);
         if (tv.live) wtrav_leaf<KIND, COUNT>(K, r, f, st, hl, tv, sk, tid, io.error_word, &cnt);
       } else {
         if (tv.live) trav_to_leaf<KIND, COUNT>(K, r, st, tv, sk64, tid, io.error_word, &cnt);
@@ -217,6 +217,34 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
       }
     }
   }
+}
+
+// The FP64 kernels, and the mixed-precision kernels with a register cap: the wide walk keeps
+// the FP64 ray and hit state live beside its FP32 node state, and its latency-bound loop gains
+// more from resident warps than it loses to the cap.
+template <int KIND, bool COUNT, bool LOCAL>
+__global__ void __launch_bounds__(kMaxTraceThreads)
+    trace_kind_kernel(SceneView S, RayIO io, int first, uint32_t *work_counter,
+                      unsigned long long *totals) {
+  trace_kind_body<KIND, COUNT, false, LOCAL>(S, io, first, work_counter, totals);
+}
+
+#ifndef BZR_WIDE_REGS
+#define BZR_WIDE_REGS 80
+#endif
+template <int KIND, bool COUNT, bool LOCAL>
+__global__ void __maxnreg__(BZR_WIDE_REGS)
+    trace_wide_kernel(SceneView S, RayIO io, int first, uint32_t *work_counter,
+                      unsigned long long *totals) {
+  trace_kind_body<KIND, COUNT, true, LOCAL>(S, io, first, work_counter, totals);
+}
+
+template <int KIND, bool COUNT, bool MIXED, bool LOCAL>
+constexpr auto trace_kernel() {
+  if constexpr (MIXED)
+    return trace_wide_kernel<KIND, COUNT, LOCAL>;
+  else
+    return trace_kind_kernel<KIND, COUNT, LOCAL>;
 }
 
 // Batching form: one kind over many scenes.  Warps take chunks of one scene's rays; a lane
@@ -320,7 +348,7 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
     if (!__any_sync(kFull, active)) break;
     if (active) {
       if (kWide && use32) {
-        if (tv.live) wtrav_to_leaf<KIND, false>(*K, r, f, hl, tv, sk, tid, io.error_word, &cnt);
+        if (tv.live) wtrav_to_leaf<KIND, false>(*K, f, hl, tv, sk, tid, io.error_word, &cnt);
         if (tv.live) wtrav_leaf<KIND, false>(*K, r, f, st, hl, tv, sk, tid, io.error_word, &cnt);
       } else {
         if (tv.live) trav_to_leaf<KIND, false>(*K, r, st, tv, sk, tid, io.error_word, &cnt);
@@ -403,18 +431,18 @@ cudaError_t launch_kind(const SceneView &S, const RayIO &io, int mode, int first
   if (!COUNT && use_local(S, plan)) {
     const size_t smem = trace_kind_smem(S.stack_cap, th, true, io.top_nodes);
     if (mixed)
-      trace_kind_kernel<KIND, false, true, true><<<blocks, th, smem, stream>>>(S, io, first,
+      trace_kernel<KIND, false, true, true>()<<<blocks, th, smem, stream>>>(S, io, first,
                                                                               counter, totals);
     else
-      trace_kind_kernel<KIND, false, false, true><<<blocks, th, smem, stream>>>(S, io, first,
+      trace_kernel<KIND, false, false, true>()<<<blocks, th, smem, stream>>>(S, io, first,
                                                                                counter, totals);
   } else {
     const size_t smem = trace_kind_smem(S.stack_cap, th, false, io.top_nodes);
     if (mixed)
-      trace_kind_kernel<KIND, COUNT, true, false><<<blocks, th, smem, stream>>>(S, io, first,
+      trace_kernel<KIND, COUNT, true, false>()<<<blocks, th, smem, stream>>>(S, io, first,
                                                                                counter, totals);
     else
-      trace_kind_kernel<KIND, COUNT, false, false><<<blocks, th, smem, stream>>>(S, io, first,
+      trace_kernel<KIND, COUNT, false, false>()<<<blocks, th, smem, stream>>>(S, io, first,
                                                                                 counter, totals);
   }
   return cudaGetLastError();
@@ -438,10 +466,10 @@ cudaError_t prepare_kind(const SceneView &S, LaunchPlan *plan) {
   const size_t smem = trace_kind_smem(S.stack_cap, th, false, plan->top_nodes);
   const size_t smem_local = trace_kind_smem(S.stack_cap, th, true, plan->top_nodes);
   const void *shared_fns[4] = {
-      reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, false, false>),
-      reinterpret_cast<const void *>(trace_kind_kernel<KIND, true, false, false>),
-      reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, true, false>),
-      reinterpret_cast<const void *>(trace_kind_kernel<KIND, true, true, false>)};
+      reinterpret_cast<const void *>(trace_kernel<KIND, false, false, false>()),
+      reinterpret_cast<const void *>(trace_kernel<KIND, true, false, false>()),
+      reinterpret_cast<const void *>(trace_kernel<KIND, false, true, false>()),
+      reinterpret_cast<const void *>(trace_kernel<KIND, true, true, false>())};
   int ignored = 0;
   for (const void *fn : shared_fns) {
     const cudaError_t e = grid_for(fn, th, smem, plan->sms, &ignored);
@@ -450,10 +478,10 @@ cudaError_t prepare_kind(const SceneView &S, LaunchPlan *plan) {
   int *blocks = &plan->blocks[KIND], *blocks32 = &plan->blocks32[KIND];
   if (use_local(S, *plan)) {
     const cudaError_t e = grid_for(
-        reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, false, true>), th,
+        reinterpret_cast<const void *>(trace_kernel<KIND, false, false, true>()), th,
         smem_local, plan->sms, blocks);
     if (e != cudaSuccess) return e;
-    return grid_for(reinterpret_cast<const void *>(trace_kind_kernel<KIND, false, true, true>), th,
+    return grid_for(reinterpret_cast<const void *>(trace_kernel<KIND, false, true, true>()), th,
                     smem_local, plan->sms, blocks32);
   }
   const cudaError_t e = grid_for(shared_fns[0], th, smem, plan->sms, blocks);

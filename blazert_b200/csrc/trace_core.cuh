@@ -558,9 +558,8 @@ BZR_HD bool traverse(const KindView &K, const Ray &r, KState &st, const Stack &s
 // added in the same fused multiply-add).  A child is kept when its FP32 entry distance is at
 // most both its FP32 exit distance and the current hit distance rounded up, so every child the
 // FP64 traversal accepts is kept.  The kept children are visited in the reference's order (the
-// node's permutation for the ray's octant), and a stack entry is dropped at pop time only when
-// its FP32 entry distance exceeds the hit distance rounded up.  A leaf is processed when the
-// reference's exact FP64 test of the leaf's own box against the current hit distance passes
+// node's permutation for the ray's octant).  A leaf is processed when the reference's exact
+// FP64 test of the leaf's own box against the current hit distance passes
 // (blazert/bvh/intersect.h:33-51).
 //
 // Why the results are the FP64 path's: the walk reaches every node the FP64 traversal accepts,
@@ -644,18 +643,14 @@ BZR_HD RayW make_ray_w(const Ray &r) {
   return f;
 }
 
-// Pop-time test of the wide walk: drops entries whose FP32 entry distance exceeds hl (the hit
-// distance rounded up).
-BZR_HD void wtrav_pop(Trav &tv, float hl, const Stack &sk, uint32_t tid) {
-  const float *skey = reinterpret_cast<const float *>(sk.key);
-  while (tv.sp > 0) {
+// Next stack entry of the wide walk (entries carry no distance).
+BZR_HD void wtrav_pop(Trav &tv, const Stack &sk, uint32_t tid) {
+  if (tv.sp > 0) {
     --tv.sp;
-    if (!(skey[tv.sp * sk.stride + tid] > hl)) {
-      tv.cur = sk.ref[tv.sp * sk.stride + tid];
-      return;
-    }
+    tv.cur = sk.ref[tv.sp * sk.stride + tid];
+  } else {
+    tv.live = false;
   }
-  tv.live = false;
 }
 
 // The exact root test (trav_begin), then the walk starts at the wide root.  hl is the hit
@@ -668,26 +663,26 @@ BZR_HD void wtrav_begin(const KindView &K, const Ray &r, const RayW &f, KState &
   hl = f32_up(st.hit);
 }
 
-// Byte `slot` (0..7) of the 8-byte value (w0 low, w1 high) as a float (exact).
-BZR_HD float qslot(uint32_t w0, uint32_t w1, uint32_t slot) {
+// Byte `b` (0..3, a compile-time constant in the unrolled loops) of `w` as a float (exact).
+BZR_HD float qbyte(uint32_t w, int b) {
 #if defined(__CUDA_ARCH__)
-  return __uint_as_float(__byte_perm(__byte_perm(w0, w1, slot), 0x4B000000u, 0x7440u)) -
-         8388608.0f;
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, unsigned(b) | 0x7440u)) - 8388608.0f;
 #else
-  const uint64_t w = uint64_t(w0) | (uint64_t(w1) << 32);
-  return static_cast<float>((w >> (8 * slot)) & 0xFFu);
+  return static_cast<float>((w >> (8 * b)) & 0xFFu);
 #endif
 }
 
 // Walks wide nodes until the current reference is a leaf record (or the walk ends).  The
-// children are tested in the reverse of the ray's visit order (the node's permutation for the
-// ray's octant), so each kept child pushes the previously kept one, which lies later in the
-// order, and the last kept, first in the order, becomes current: the stack ends with the next
-// in order on top, as the reference's stack would.
+// children are tested in slot order (fixed byte positions); the kept ones are then taken in
+// the reverse of the ray's visit order (the node's permutation for the ray's octant): each
+// kept child pushes the previously taken one, which lies later in the order, and the last one
+// taken, first in the order, becomes current, so the next in order ends on top of the stack,
+// as in the reference's stack.  Stack entries carry no distance: a popped wide node's children
+// are tested against the hit distance of that moment, and a popped leaf gets its exact test.
 template <int KIND, bool COUNT>
-BZR_HD void wtrav_to_leaf(const KindView &K, const Ray &r, const RayW &f, float hl, Trav &tv,
-                          const Stack &sk, uint32_t tid, uint32_t *err, Counts *cnt) {
-  float *skey = reinterpret_cast<float *>(sk.key);
+BZR_HD void wtrav_to_leaf(const KindView &K, const RayW &f, float hl, Trav &tv, const Stack &sk,
+                          uint32_t tid, uint32_t *err, Counts *cnt) {
+  const bool sx = f.oct & 1u, sy = f.oct & 2u, sz = f.oct & 4u;
   while (tv.live && !(tv.cur & kLeafBit)) {
     if (tv.cur >= K.n_wide) {
       flag_error(err, kErrNodeIndex);
@@ -723,19 +718,33 @@ BZR_HD void wtrav_to_leaf(const KindView &K, const Ray &r, const RayW &f, float 
     const float bnx = bx - ex, bfx = bx + ex, bny = by - ey, bfy = by + ey;
     const float bnz = bz - ez, bfz = bz + ez;
     // near and far bound words per axis: the hi bounds are near for a negative direction
-    const uint32_t nx0 = r.sx ? qx.z : qx.x, nx1 = r.sx ? qx.w : qx.y;
-    const uint32_t fx0 = r.sx ? qx.x : qx.z, fx1 = r.sx ? qx.y : qx.w;
-    const uint32_t ny0 = r.sy ? qy.z : qy.x, ny1 = r.sy ? qy.w : qy.y;
-    const uint32_t fy0 = r.sy ? qy.x : qy.z, fy1 = r.sy ? qy.y : qy.w;
-    const uint32_t nz0 = r.sz ? qz.z : qz.x, nz1 = r.sz ? qz.w : qz.y;
-    const uint32_t fz0 = r.sz ? qz.x : qz.z, fz1 = r.sz ? qz.y : qz.w;
+    const uint32_t nx0 = sx ? qx.z : qx.x, nx1 = sx ? qx.w : qx.y;
+    const uint32_t fx0 = sx ? qx.x : qx.z, fx1 = sx ? qx.y : qx.w;
+    const uint32_t ny0 = sy ? qy.z : qy.x, ny1 = sy ? qy.w : qy.y;
+    const uint32_t fy0 = sy ? qy.x : qy.z, fy1 = sy ? qy.y : qy.w;
+    const uint32_t nz0 = sz ? qz.z : qz.x, nz1 = sz ? qz.w : qz.y;
+    const uint32_t fz0 = sz ? qz.x : qz.z, fz1 = sz ? qz.y : qz.w;
+    uint32_t keep = 0;
+#pragma unroll
+    for (int c = 0; c < kWideMax; ++c) {
+      const int b = c & 3;
+      const float tnx = fma32(qbyte(c < 4 ? nx0 : nx1, b), ax, bnx);
+      const float tny = fma32(qbyte(c < 4 ? ny0 : ny1, b), ay, bny);
+      const float tnz = fma32(qbyte(c < 4 ? nz0 : nz1, b), az, bnz);
+      const float tfx = fma32(qbyte(c < 4 ? fx0 : fx1, b), ax, bfx);
+      const float tfy = fma32(qbyte(c < 4 ? fy0 : fy1, b), ay, bfy);
+      const float tfz = fma32(qbyte(c < 4 ? fz0 : fz1, b), az, bfz);
+      const float entry = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, f.tmin));
+      const float exit = fminf(fminf(tfx, tfy), tfz);
+      keep |= (entry <= fminf(exit, hl) ? 1u : 0u) << c;
+    }
+    keep &= (1u << nch) - 1u;
     if (COUNT) {
       cnt->node[KIND] += 1;
       cnt->box[KIND] += nch;
     }
     // The builder bounds the stack: the entries below this node plus its children minus one
-    // never exceed the image's stack size, which the capacity covers.  Checked once per node,
-    // so the child loop below has no exit.
+    // never exceed the image's stack size, which the capacity covers.  Checked once per node.
     if (tv.sp + nch > sk.cap + 1) {
       flag_error(err, kErrStack);
       tv.live = false;
@@ -743,33 +752,22 @@ BZR_HD void wtrav_to_leaf(const KindView &K, const Ray &r, const RayW &f, float 
     }
     bool have = false;
     uint32_t next = 0;
-    float next_key = 0.0f;
 #pragma unroll
     for (int j = kWideMax - 1; j >= 0; --j) {
-      const uint32_t slot = (perm >> (4 * j)) & 7u;
-      const float tnx = fma32(qslot(nx0, nx1, slot), ax, bnx);
-      const float tny = fma32(qslot(ny0, ny1, slot), ay, bny);
-      const float tnz = fma32(qslot(nz0, nz1, slot), az, bnz);
-      const float tfx = fma32(qslot(fx0, fx1, slot), ax, bfx);
-      const float tfy = fma32(qslot(fy0, fy1, slot), ay, bfy);
-      const float tfz = fma32(qslot(fz0, fz1, slot), az, bfz);
-      const float entry = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, f.tmin));
-      const float exit = fminf(fminf(tfx, tfy), tfz);
-      if (uint32_t(j) < nch && entry <= fminf(exit, hl)) {
+      const uint32_t slot = (perm >> (4 * j)) & 0xFu;  // 15 past the last child
+      if ((keep >> slot) & 1u) {
         if (have) {
-          skey[tv.sp * sk.stride + tid] = next_key;
           sk.ref[tv.sp * sk.stride + tid] = next;
           ++tv.sp;
         }
         next = staged ? words[16 + slot] : ldg(words + 16 + slot);
-        next_key = entry;
         have = true;
       }
     }
     if (have)
       tv.cur = next;
     else
-      wtrav_pop(tv, hl, sk, tid);
+      wtrav_pop(tv, sk, tid);
   }
 }
 
@@ -816,7 +814,7 @@ BZR_HD void wtrav_leaf(const KindView &K, const Ray &r, const RayW &f, KState &s
     }
     if (st.hit != before) hl = f32_up(st.hit);
   }
-  wtrav_pop(tv, hl, sk, tid);
+  wtrav_pop(tv, sk, tid);
 }
 
 // Whole traversal of one kind in mixed precision (the FP64 traversal for cylinders, kinds
@@ -833,7 +831,7 @@ BZR_HD bool traverse_mixed(const KindView &K, const Ray &r, KState &st, const St
     float hl;
     wtrav_begin<KIND, COUNT>(K, r, f, st, hl, tv, cnt);
     while (tv.live) {
-      wtrav_to_leaf<KIND, COUNT>(K, r, f, hl, tv, sk, tid, err, cnt);
+      wtrav_to_leaf<KIND, COUNT>(K, f, hl, tv, sk, tid, err, cnt);
       if (tv.live) wtrav_leaf<KIND, COUNT>(K, r, f, st, hl, tv, sk, tid, err, cnt);
     }
     return st.hit < r.tmax;
