@@ -429,7 +429,30 @@ struct Trav {
   uint32_t cur;  // node index, or kLeafBit | first primitive position of a leaf
   uint32_t sp;   // stack depth
   bool live;     // false once the stack is exhausted
+  // wide walk only: the leaf record found first and not yet processed (kNoLeaf: none), and
+  // whether cur still holds a reference to walk
+  uint32_t post;
+  bool walk;
 };
+constexpr uint32_t kNoLeaf = 0xFFFFFFFFu;  // no leaf record has this reference
+
+// Whether `pred` holds for some lane of the warp among `lanes` (device); for the single ray of
+// a host call, pred itself.
+BZR_HD bool warp_any(unsigned lanes, bool pred) {
+#if defined(__CUDA_ARCH__)
+  return __any_sync(lanes, pred);
+#else
+  (void)lanes;
+  return pred;
+#endif
+}
+BZR_HD unsigned active_lanes() {
+#if defined(__CUDA_ARCH__)
+  return __activemask();
+#else
+  return 1u;
+#endif
+}
 
 template <int KIND, bool COUNT>
 BZR_HD void trav_begin(const KindView &K, const Ray &r, KState &st, Trav &tv, Counts *cnt) {
@@ -573,17 +596,19 @@ BZR_HD bool traverse(const KindView &K, const Ray &r, KState &st, const Stack &s
 // with the same hit distance, and every primitive test and result is identical.
 //
 // Error bound, per node and axis: with A = 2^e inv_f, D = (origin - o_hi) - o_lo (the origin
-// held as two floats, so it is exact to 2^-48 relative) and B = D inv_f, the distance of a
-// stored bound origin + q 2^e is t = fma(q, A, B +- E).  Against the real distance T of that
-// bound for the FP64 inverse direction, fma(q, A, B) is off by at most 5 * 2^-24 * (255 |A| +
-// |B|) (inv_f, the two differences, the product and the fma each round once; q 2^e is exact);
-// the FP64 reference rounds T by 2^-49 relative (its l1 factor included) and B +- E rounds
-// once more.  E = 2^-20 (255 |A| + |B|) + 1e-37 covers all of these (and denormal results), so
-// the near distance is below and the far distance above the reference's.  The bound follows
-// the ray's own magnitudes on each axis: an axis whose direction component is tiny has large
-// distances and a large E, but those distances rarely decide the entry or the exit.  Rays with
-// a zero, non-finite or huge (> 1e18) inverse direction or origin component, or a non-finite
-// or huge tmin or a NaN tmax, take the FP64 traversal.
+// held as two floats, so it is exact to 2^-48 relative), B = D inv_f and C = B - 2^23 A, the
+// distance of a stored bound origin + q 2^e is t = fma(2^23 + q, A, C +- E): the byte q is
+// placed in the mantissa of 2^23 with one byte permute, and the fma cancels the 2^23 A parts
+// exactly.  Against the real distance T of that bound for the FP64 inverse direction: inv_f,
+// the two differences, B and the fma round by at most 5 * 2^-24 * (255 |A| + |B|) in all; C
+// and C +- E are of magnitude 2^23 |A| and round by at most |A| / 2 each; the FP64 reference
+// rounds T by 2^-49 relative (its l1 factor included).  E = (1 + 2^-10) |A| + 2^-20 |B| +
+// 1e-37 covers all of these (and denormal results), so the near distance is below and the far
+// distance above the reference's: one grid cell of slack on top of the outward quantisation.
+// The bound follows the ray's own magnitudes on each axis: an axis whose direction component
+// is tiny has large distances and a large E, but those distances rarely decide the entry or
+// the exit.  Rays with a zero, non-finite or huge (> 1e18) inverse direction or origin
+// component, or a non-finite or huge tmin or a NaN tmax, take the FP64 traversal.
 struct RayW {
   float o_hi[3], o_lo[3], inv[3];
   float tmin;    // tmin rounded down
@@ -649,7 +674,7 @@ BZR_HD void wtrav_pop(Trav &tv, const Stack &sk, uint32_t tid) {
     --tv.sp;
     tv.cur = sk.ref[tv.sp * sk.stride + tid];
   } else {
-    tv.live = false;
+    tv.walk = false;
   }
 }
 
@@ -660,34 +685,54 @@ BZR_HD void wtrav_begin(const KindView &K, const Ray &r, const RayW &f, KState &
                         Trav &tv, Counts *cnt) {
   trav_begin<KIND, COUNT>(K, r, st, tv, cnt);
   tv.cur = K.wide_root_ref;
+  tv.post = kNoLeaf;
+  tv.walk = tv.live;
   hl = f32_up(st.hit);
 }
 
-// Byte `b` (0..3, a compile-time constant in the unrolled loops) of `w` as a float (exact).
+// 2^23 + byte `b` (0..3, a compile-time constant in the unrolled loops) of `w`, as a float
+// (exact: the byte lands in the low mantissa bits of 2^23).
 BZR_HD float qbyte(uint32_t w, int b) {
 #if defined(__CUDA_ARCH__)
-  return __uint_as_float(__byte_perm(w, 0x4B000000u, unsigned(b) | 0x7440u)) - 8388608.0f;
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, unsigned(b) | 0x7440u));
 #else
-  return static_cast<float>((w >> (8 * b)) & 0xFFu);
+  return 8388608.0f + static_cast<float>((w >> (8 * b)) & 0xFFu);
 #endif
 }
 
-// Walks wide nodes until the current reference is a leaf record (or the walk ends).  The
-// children are tested in slot order (fixed byte positions); the kept ones are then taken in
-// the reverse of the ray's visit order (the node's permutation for the ray's octant): each
+// Walks wide nodes until the ray has a leaf record to process (tv.post) or nothing left.
+// The children are tested in slot order (fixed byte positions); the kept ones are then taken
+// in the reverse of the ray's visit order (the node's permutation for the ray's octant): each
 // kept child pushes the previously taken one, which lies later in the order, and the last one
 // taken, first in the order, becomes current, so the next in order ends on top of the stack,
 // as in the reference's stack.  Stack entries carry no distance: a popped wide node's children
 // are tested against the hit distance of that moment, and a popped leaf gets its exact test.
+//
+// Postponed leaves (Aila and Laine, "Understanding the efficiency of ray traversal on GPUs",
+// 2009): a lane that reaches a leaf record keeps it in tv.post and walks on while some lane of
+// the warp has not found one yet, so that the warp's lanes reach their leaf steps together;
+// it stops at a second leaf.  The walk past a postponed leaf uses the hit distance from before
+// that leaf, which keeps more children, never fewer; leaves are still processed in the visit
+// order, each with its exact test.  The counting kernels do not walk ahead, so their counts
+// are the walk's own work.
 template <int KIND, bool COUNT>
 BZR_HD void wtrav_to_leaf(const KindView &K, const RayW &f, float hl, Trav &tv, const Stack &sk,
                           uint32_t tid, uint32_t *err, Counts *cnt) {
   const bool sx = f.oct & 1u, sy = f.oct & 2u, sz = f.oct & 4u;
-  while (tv.live && !(tv.cur & kLeafBit)) {
+  const unsigned lanes = active_lanes();
+  for (;;) {
+    if (tv.walk && (tv.cur & kLeafBit) && tv.post == kNoLeaf) {
+      tv.post = tv.cur;  // the first leaf found: postponed, the walk goes on
+      wtrav_pop(tv, sk, tid);
+    }
+    const bool at_node = tv.walk && !(tv.cur & kLeafBit);
+    const bool searching = at_node && tv.post == kNoLeaf;
+    if (!(COUNT ? searching : warp_any(lanes, searching))) break;
+    if (!at_node) continue;
     if (tv.cur >= K.n_wide) {
       flag_error(err, kErrNodeIndex);
-      tv.live = false;
-      return;
+      tv.walk = false;
+      continue;
     }
     const bool staged = tv.cur < sk.n_top;  // a top-level node staged in shared memory
     const uint4 *nd = staged ? sk.top + size_t(tv.cur) * 8
@@ -703,20 +748,22 @@ BZR_HD void wtrav_to_leaf(const KindView &K, const RayW &f, float hl, Trav &tv, 
       perm = ldg(words + 24 + f.oct);
     }
     const uint32_t nch = hd.w >> 24;
-    // per axis t(q) = fma(q, A, B -+ E): a lower bound of the reference's near-plane
-    // distance, an upper bound of its far-plane distance
+    // per axis t(q) = fma(2^23 + q, A, B - 2^23 A -+ E): a lower bound of the reference's
+    // near-plane distance, an upper bound of its far-plane distance
     const float ax = fbits((hd.w & 0xFFu) << 23) * f.inv[0];
     const float ay = fbits(((hd.w >> 8) & 0xFFu) << 23) * f.inv[1];
     const float az = fbits(((hd.w >> 16) & 0xFFu) << 23) * f.inv[2];
     const float bx = ((fbits(hd.x) - f.o_hi[0]) - f.o_lo[0]) * f.inv[0];
     const float by = ((fbits(hd.y) - f.o_hi[1]) - f.o_lo[1]) * f.inv[1];
     const float bz = ((fbits(hd.z) - f.o_hi[2]) - f.o_lo[2]) * f.inv[2];
-    constexpr float kErr = 9.5367431640625e-07f;  // 2^-20
-    const float ex = fma32(255.0f, fabsf(ax), fabsf(bx)) * kErr + 1e-37f;
-    const float ey = fma32(255.0f, fabsf(ay), fabsf(by)) * kErr + 1e-37f;
-    const float ez = fma32(255.0f, fabsf(az), fabsf(bz)) * kErr + 1e-37f;
-    const float bnx = bx - ex, bfx = bx + ex, bny = by - ey, bfy = by + ey;
-    const float bnz = bz - ez, bfz = bz + ez;
+    const float cx = fma32(-8388608.0f, ax, bx), cy = fma32(-8388608.0f, ay, by);
+    const float cz = fma32(-8388608.0f, az, bz);
+    constexpr float kRel = 9.5367431640625e-07f, kCell = 1.0009765625f;  // 2^-20, 1 + 2^-10
+    const float ex = fma32(kCell, fabsf(ax), kRel * fabsf(bx)) + 1e-37f;
+    const float ey = fma32(kCell, fabsf(ay), kRel * fabsf(by)) + 1e-37f;
+    const float ez = fma32(kCell, fabsf(az), kRel * fabsf(bz)) + 1e-37f;
+    const float bnx = cx - ex, bfx = cx + ex, bny = cy - ey, bfy = cy + ey;
+    const float bnz = cz - ez, bfz = cz + ez;
     // near and far bound words per axis: the hi bounds are near for a negative direction
     const uint32_t nx0 = sx ? qx.z : qx.x, nx1 = sx ? qx.w : qx.y;
     const uint32_t fx0 = sx ? qx.x : qx.z, fx1 = sx ? qx.y : qx.w;
@@ -747,8 +794,8 @@ BZR_HD void wtrav_to_leaf(const KindView &K, const RayW &f, float hl, Trav &tv, 
     // never exceed the image's stack size, which the capacity covers.  Checked once per node.
     if (tv.sp + nch > sk.cap + 1) {
       flag_error(err, kErrStack);
-      tv.live = false;
-      return;
+      tv.walk = false;
+      continue;
     }
     bool have = false;
     uint32_t next = 0;
@@ -769,15 +816,20 @@ BZR_HD void wtrav_to_leaf(const KindView &K, const RayW &f, float hl, Trav &tv, 
     else
       wtrav_pop(tv, sk, tid);
   }
+  if (tv.post == kNoLeaf && !tv.walk) tv.live = false;  // nothing left to process
 }
 
-// A leaf record: the exact FP64 test of the leaf's box, then its primitives in the reference's
-// stored order (blazert/bvh/intersect.h:67-78), then the next stack entry.
+// The postponed leaf record: the exact FP64 test of the leaf's box, then its primitives in the
+// reference's stored order (blazert/bvh/intersect.h:67-78).  The walk then resumes at tv.cur.
 template <int KIND, bool COUNT>
 BZR_HD void wtrav_leaf(const KindView &K, const Ray &r, const RayW &f, KState &st, float &hl,
                        Trav &tv, const Stack &sk, uint32_t tid, uint32_t *err, Counts *cnt) {
+  (void)sk;
+  (void)tid;
   constexpr uint32_t kUnits = KIND == kMesh ? 1u : uint32_t(kPayloadDoubles[KIND] / 2);
-  const uint32_t off = tv.cur & kIdMask;
+  if (tv.post == kNoLeaf) return;
+  const uint32_t off = tv.post & kIdMask;
+  tv.post = kNoLeaf;
   if (uint64_t(off) + kLeafHeaderBytes / 16 > K.n_leaf16) {
     flag_error(err, kErrPrimIndex);
     tv.live = false;
@@ -814,7 +866,7 @@ BZR_HD void wtrav_leaf(const KindView &K, const Ray &r, const RayW &f, KState &s
     }
     if (st.hit != before) hl = f32_up(st.hit);
   }
-  wtrav_pop(tv, sk, tid);
+  if (!tv.walk) tv.live = false;
 }
 
 // Whole traversal of one kind in mixed precision (the FP64 traversal for cylinders, kinds

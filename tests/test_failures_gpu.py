@@ -150,15 +150,21 @@ def test_bounded_waits_time_out_and_recover():
     assert e.value.code == B.ETIMEOUT
     assert not done.query()  # the work was still queued when the wait ran out
     assert scene.check(stream=stream.cuda_stream, timeout_ms=60000) == 0
-    # host arrays: the call's own wait runs out while its copies and kernels are queued
+    # pinned host arrays (copies from pageable memory would return only once done): the call's
+    # own wait runs out while its copies and kernels are queued
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    ho, hd = pin(R.origins), pin(R.directions)
+    hout = dict(t=pin(np.empty(R.n)), uv=pin(np.empty((R.n, 2))), normal=pin(np.empty((R.n, 3))),
+                prim=pin(np.empty(R.n, np.uint32)), geom=pin(np.empty(R.n, np.uint32)),
+                hit=pin(np.empty(R.n, np.uint8)))
     os.environ["BZR_TIMEOUT_MS"] = "1"
     try:
         with pytest.raises(B.BlazertError) as e:
-            scene.intersectN(R.origins, R.directions)
+            scene.intersectN(ho, hd, out=hout)
         assert e.value.code == B.ETIMEOUT
     finally:
         del os.environ["BZR_TIMEOUT_MS"]
-    got = scene.intersectN(R.origins, R.directions)
+    got = scene.intersectN(ho, hd, out=hout)
     for k in ("prim", "geom"):
         ref[k] = ref[k].view(np.uint32)
     assert mismatches(got, ref) == []
