@@ -607,8 +607,11 @@ BZR_HD bool traverse(const KindView &K, const Ray &r, KState &st, const Stack &s
 // distance above the reference's: one grid cell of slack on top of the outward quantisation.
 // The bound follows the ray's own magnitudes on each axis: an axis whose direction component
 // is tiny has large distances and a large E, but those distances rarely decide the entry or
-// the exit.  Rays with a zero, non-finite or huge (> 1e18) inverse direction or origin
-// component, or a non-finite or huge tmin or a NaN tmax, take the FP64 traversal.
+// the exit.  Rays with a zero, non-finite or large (> 2^40) inverse direction component, an
+// origin component beyond 1e18, or a non-finite or huge tmin or a NaN tmax, take the FP64
+// traversal.  Then every FP32 value of the test is finite: node coordinates are within 1e18
+// (the builder's limit), so 2^e <= 2^54, |A| <= 2^94, 2^23 |A| <= 2^117, |B| <= 2^101, and
+// every distance and difference stays below 2^121.
 struct RayW {
   float o_hi[3], o_lo[3], inv[3];
   float tmin;    // tmin rounded down
@@ -657,7 +660,7 @@ BZR_HD RayW make_ray_w(const Ray &r) {
   bool ok = fabs(r.tmin) <= 1e18 && !isnan(r.tmax);
   for (int a = 0; a < 3; ++a) {
     const double ai = fabs(inv[a]), oa = fabs(o[a]);
-    ok = ok && ai > 0.0 && ai <= 1e18 && oa <= 1e18;  // false for NaN and infinities
+    ok = ok && ai > 0.0 && ai <= 0x1p40 && oa <= 1e18;  // false for NaN and infinities
     f.o_hi[a] = static_cast<float>(o[a]);
     f.o_lo[a] = static_cast<float>(o[a] - static_cast<double>(f.o_hi[a]));
     f.inv[a] = static_cast<float>(inv[a]);
@@ -678,35 +681,114 @@ BZR_HD void wtrav_pop(Trav &tv, const Stack &sk, uint32_t tid) {
   }
 }
 
+// FP32 bound of the hit distance for the child tests: rounded up, and +0 for a zero distance,
+// so that the sign test of the node walk (exit - entry) never meets -0 as an exit distance.
+BZR_HD float hit_bound(double h) {
+  const float f = f32_up(h);
+  return f == 0.0f ? 0.0f : f;
+}
+
 // The exact root test (trav_begin), then the walk starts at the wide root.  hl is the hit
 // distance rounded up.
 template <int KIND, bool COUNT>
 BZR_HD void wtrav_begin(const KindView &K, const Ray &r, const RayW &f, KState &st, float &hl,
                         Trav &tv, Counts *cnt) {
+  (void)f;
   trav_begin<KIND, COUNT>(K, r, st, tv, cnt);
   tv.cur = K.wide_root_ref;
   tv.post = kNoLeaf;
   tv.walk = tv.live;
-  hl = f32_up(st.hit);
+  hl = hit_bound(st.hit);
+}
+
+// prmt.b32 in its default mode: byte i of the result is byte (s_i & 7) of the eight bytes
+// {b, a} (a's bytes 0-3, b's bytes 4-7), or, when s_i & 8, the sign bit of that byte
+// replicated over the byte, where s_i is nibble i of s.
+BZR_HD uint32_t prmt(uint32_t a, uint32_t b, uint32_t s) {
+#if defined(__CUDA_ARCH__)
+  uint32_t r;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(s));
+  return r;
+#else
+  const uint64_t src = uint64_t(a) | (uint64_t(b) << 32);
+  uint32_t r = 0;
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t n = (s >> (4 * i)) & 0xFu;
+    uint32_t byte = uint32_t(src >> (8 * (n & 7u))) & 0xFFu;
+    if (n & 8u) byte = (byte & 0x80u) ? 0xFFu : 0u;
+    r |= byte << (8 * i);
+  }
+  return r;
+#endif
 }
 
 // 2^23 + byte `b` (0..3, a compile-time constant in the unrolled loops) of `w`, as a float
 // (exact: the byte lands in the low mantissa bits of 2^23).
-BZR_HD float qbyte(uint32_t w, int b) {
+BZR_HD float qbyte(uint32_t w, int b) { return fbits(prmt(w, 0x4B000000u, unsigned(b) | 0x7440u)); }
+
+BZR_HD float max3f(float a, float b, float c) {
 #if defined(__CUDA_ARCH__)
-  return __uint_as_float(__byte_perm(w, 0x4B000000u, unsigned(b) | 0x7440u));
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
 #else
-  return 8388608.0f + static_cast<float>((w >> (8 * b)) & 0xFFu);
+  return fmaxf(fmaxf(a, b), c);
+#endif
+}
+BZR_HD float min3f(float a, float b, float c) {
+#if defined(__CUDA_ARCH__)
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+#else
+  return fminf(fminf(a, b), c);
+#endif
+}
+// Two independent single-precision fused multiply-adds, each rounded to nearest.
+BZR_HD float2 fma2(float2 a, float2 b, float2 c) {
+#if defined(__CUDA_ARCH__)
+  return __ffma2_rn(a, b, c);
+#else
+  return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+#endif
+}
+BZR_HD int ffs64(uint64_t x) {  // 1 + index of the lowest set bit; 0 for x == 0
+#if defined(__CUDA_ARCH__)
+  return __ffsll(static_cast<long long>(x));
+#else
+  return __builtin_ffsll(static_cast<long long>(x));
+#endif
+}
+BZR_HD int msb64(uint64_t x) {  // index of the highest set bit of x != 0
+#if defined(__CUDA_ARCH__)
+  return 63 - __clzll(static_cast<long long>(x));
+#else
+  return 63 - __builtin_clzll(x);
+#endif
+}
+BZR_HD uint32_t fword(float x) {
+#if defined(__CUDA_ARCH__)
+  return __float_as_uint(x);
+#else
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  return u;
 #endif
 }
 
 // Walks wide nodes until the ray has a leaf record to process (tv.post) or nothing left.
-// The children are tested in slot order (fixed byte positions); the kept ones are then taken
-// in the reverse of the ray's visit order (the node's permutation for the ray's octant): each
-// kept child pushes the previously taken one, which lies later in the order, and the last one
-// taken, first in the order, becomes current, so the next in order ends on top of the stack,
-// as in the reference's stack.  Stack entries carry no distance: a popped wide node's children
-// are tested against the hit distance of that moment, and a popped leaf gets its exact test.
+//
+// Per node, each child slot's near and far distances per axis come from one paired FMA
+// (near and far biases side by side); the child is kept when exit - entry has its sign bit
+// clear, i.e. when entry <= exit, with the entry raised to tmin and the exit lowered to the hit
+// distance (exact as a sign test: every value is finite and the exit is never -0).  The eight
+// sign bytes are gathered into two words in slot order and permuted into the ray's visit order
+// (the node's permutation for the ray's octant) with two byte permutes; a slot past the last
+// child reads as rejected.  The first kept child in visit order becomes current and the other
+// kept ones are pushed from the last in order down, so the next in order ends on top of the
+// stack, as in the reference's stack.  Stack entries carry no distance: a popped wide node's
+// children are tested against the hit distance of that moment, and a popped leaf gets its
+// exact test.
 //
 // Postponed leaves (Aila and Laine, "Understanding the efficiency of ray traversal on GPUs",
 // 2009): a lane that reaches a leaf record keeps it in tv.post and walks on while some lane of
@@ -747,12 +829,11 @@ BZR_HD void wtrav_to_leaf(const KindView &K, const RayW &f, float hl, Trav &tv, 
       hd = ldg(nd), qx = ldg(nd + 1), qy = ldg(nd + 2), qz = ldg(nd + 3);
       perm = ldg(words + 24 + f.oct);
     }
-    const uint32_t nch = hd.w >> 24;
     // per axis t(q) = fma(2^23 + q, A, B - 2^23 A -+ E): a lower bound of the reference's
     // near-plane distance, an upper bound of its far-plane distance
     const float ax = fbits((hd.w & 0xFFu) << 23) * f.inv[0];
-    const float ay = fbits(((hd.w >> 8) & 0xFFu) << 23) * f.inv[1];
-    const float az = fbits(((hd.w >> 16) & 0xFFu) << 23) * f.inv[2];
+    const float ay = fbits((hd.w & 0xFF00u) << 15) * f.inv[1];
+    const float az = fbits((hd.w & 0xFF0000u) << 7) * f.inv[2];
     const float bx = ((fbits(hd.x) - f.o_hi[0]) - f.o_lo[0]) * f.inv[0];
     const float by = ((fbits(hd.y) - f.o_hi[1]) - f.o_lo[1]) * f.inv[1];
     const float bz = ((fbits(hd.z) - f.o_hi[2]) - f.o_lo[2]) * f.inv[2];
@@ -762,8 +843,9 @@ BZR_HD void wtrav_to_leaf(const KindView &K, const RayW &f, float hl, Trav &tv, 
     const float ex = fma32(kCell, fabsf(ax), kRel * fabsf(bx)) + 1e-37f;
     const float ey = fma32(kCell, fabsf(ay), kRel * fabsf(by)) + 1e-37f;
     const float ez = fma32(kCell, fabsf(az), kRel * fabsf(bz)) + 1e-37f;
-    const float bnx = cx - ex, bfx = cx + ex, bny = cy - ey, bfy = cy + ey;
-    const float bnz = cz - ez, bfz = cz + ez;
+    const float2 Ax = make_float2(ax, ax), Ay = make_float2(ay, ay), Az = make_float2(az, az);
+    const float2 Bx = make_float2(cx - ex, cx + ex), By = make_float2(cy - ey, cy + ey);
+    const float2 Bz = make_float2(cz - ez, cz + ez);
     // near and far bound words per axis: the hi bounds are near for a negative direction
     const uint32_t nx0 = sx ? qx.z : qx.x, nx1 = sx ? qx.w : qx.y;
     const uint32_t fx0 = sx ? qx.x : qx.z, fx1 = sx ? qx.y : qx.w;
@@ -771,50 +853,53 @@ BZR_HD void wtrav_to_leaf(const KindView &K, const RayW &f, float hl, Trav &tv, 
     const uint32_t fy0 = sy ? qy.x : qy.z, fy1 = sy ? qy.y : qy.w;
     const uint32_t nz0 = sz ? qz.z : qz.x, nz1 = sz ? qz.w : qz.y;
     const uint32_t fz0 = sz ? qz.x : qz.z, fz1 = sz ? qz.y : qz.w;
-    uint32_t keep = 0;
+    uint32_t sgn[8];  // exit - entry per slot (its sign bit: rejected)
 #pragma unroll
     for (int c = 0; c < kWideMax; ++c) {
       const int b = c & 3;
-      const float tnx = fma32(qbyte(c < 4 ? nx0 : nx1, b), ax, bnx);
-      const float tny = fma32(qbyte(c < 4 ? ny0 : ny1, b), ay, bny);
-      const float tnz = fma32(qbyte(c < 4 ? nz0 : nz1, b), az, bnz);
-      const float tfx = fma32(qbyte(c < 4 ? fx0 : fx1, b), ax, bfx);
-      const float tfy = fma32(qbyte(c < 4 ? fy0 : fy1, b), ay, bfy);
-      const float tfz = fma32(qbyte(c < 4 ? fz0 : fz1, b), az, bfz);
-      const float entry = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, f.tmin));
-      const float exit = fminf(fminf(tfx, tfy), tfz);
-      keep |= (entry <= fminf(exit, hl) ? 1u : 0u) << c;
+      const float2 tx = fma2(make_float2(qbyte(c < 4 ? nx0 : nx1, b), qbyte(c < 4 ? fx0 : fx1, b)),
+                             Ax, Bx);
+      const float2 ty = fma2(make_float2(qbyte(c < 4 ? ny0 : ny1, b), qbyte(c < 4 ? fy0 : fy1, b)),
+                             Ay, By);
+      const float2 tz = fma2(make_float2(qbyte(c < 4 ? nz0 : nz1, b), qbyte(c < 4 ? fz0 : fz1, b)),
+                             Az, Bz);
+      const float entry = max3f(tx.x, ty.x, fmaxf(tz.x, f.tmin));
+      const float exit = min3f(tx.y, ty.y, fminf(tz.y, hl));
+      sgn[c] = fword(exit - entry);
     }
-    keep &= (1u << nch) - 1u;
+    // sign bytes in slot order (byte c of s_lo | s_hi << 32: slot c); slot 7 reads as rejected
+    // when the node has fewer than 8 children, as it then stands for the permutation's unused
+    // positions (nibble 15: slot 7's sign replicated)
+    const uint32_t s_lo = prmt(prmt(sgn[0], sgn[1], 0x0073u), prmt(sgn[2], sgn[3], 0x0073u), 0x5410u);
+    const uint32_t s_hi = prmt(prmt(sgn[4], sgn[5], 0x0073u), prmt(sgn[6], sgn[7], 0x0073u), 0x5410u) |
+                          ((hd.w - 0x08000000u) & 0x80000000u);
+    // bit 8j + 7 of m: the child at visit position j is kept
+    const uint64_t m = (uint64_t(~prmt(s_lo, s_hi, perm >> 16) & 0x80808080u) << 32) |
+                       (~prmt(s_lo, s_hi, perm & 0xFFFFu) & 0x80808080u);
     if (COUNT) {
       cnt->node[KIND] += 1;
-      cnt->box[KIND] += nch;
+      cnt->box[KIND] += hd.w >> 24;
     }
     // The builder bounds the stack: the entries below this node plus its children minus one
     // never exceed the image's stack size, which the capacity covers.  Checked once per node.
-    if (tv.sp + nch > sk.cap + 1) {
+    if (tv.sp + (hd.w >> 24) > sk.cap + 1) {
       flag_error(err, kErrStack);
       tv.walk = false;
       continue;
     }
-    bool have = false;
-    uint32_t next = 0;
-#pragma unroll
-    for (int j = kWideMax - 1; j >= 0; --j) {
-      const uint32_t slot = (perm >> (4 * j)) & 0xFu;  // 15 past the last child
-      if ((keep >> slot) & 1u) {
-        if (have) {
-          sk.ref[tv.sp * sk.stride + tid] = next;
-          ++tv.sp;
-        }
-        next = staged ? words[16 + slot] : ldg(words + 16 + slot);
-        have = true;
-      }
-    }
-    if (have)
-      tv.cur = next;
-    else
+    if (m == 0) {
       wtrav_pop(tv, sk, tid);
+      continue;
+    }
+    for (uint64_t rest = m & (m - 1); rest != 0;) {  // all kept but the first, last first
+      const int bit = msb64(rest);
+      const uint32_t slot = (perm >> ((bit >> 3) * 4)) & 7u;
+      sk.ref[tv.sp * sk.stride + tid] = staged ? words[16 + slot] : ldg(words + 16 + slot);
+      ++tv.sp;
+      rest ^= uint64_t(1) << bit;
+    }
+    const uint32_t slot = (perm >> (((ffs64(m) - 1) >> 3) * 4)) & 7u;
+    tv.cur = staged ? words[16 + slot] : ldg(words + 16 + slot);
   }
   if (tv.post == kNoLeaf && !tv.walk) tv.live = false;  // nothing left to process
 }
@@ -864,7 +949,7 @@ BZR_HD void wtrav_leaf(const KindView &K, const Ray &r, const RayW &f, KState &s
         return;
       }
     }
-    if (st.hit != before) hl = f32_up(st.hit);
+    if (st.hit != before) hl = hit_bound(st.hit);
   }
   if (!tv.walk) tv.live = false;
 }

@@ -29,8 +29,13 @@ def _cross_mat(a):
                      np.stack([-a[:, 1], a[:, 0], z], 1)], 1)
 
 
-def gradients(spec, origins, directions, fwd, gt, guv=None, gnormal=None):
-    """fwd: dict with t, prim, geom, hit (numpy).  Returns dict like Scene.adjoint."""
+def gradients(spec, origins, directions, fwd, gt, guv=None, gnormal=None, absolute=False):
+    """fwd: dict with t, prim, geom, hit (numpy).  Returns dict like Scene.adjoint.  With
+    absolute=True every per-ray and per-face contribution is accumulated by its absolute value
+    instead: the scale against which the rounding of the sums is measured."""
+    def acc(X, i, v):
+        np.add.at(X, i, np.abs(v) if absolute else v)
+
     n = origins.shape[0]
     g_o = np.zeros((n, 3))
     g_w = np.zeros((n, 3))
@@ -107,23 +112,24 @@ def gradients(spec, origins, directions, fwd, gt, guv=None, gnormal=None):
         grads = [sum(coef[:, None] * J[k] for coef, J in ((cA, JA), (cB, JB), (cC, JC), (cD, JD)))
                  for k in range(5)]
         ga, gb, gcc, go, gd = grads
-        np.add.at(gv, ia, ga)
-        np.add.at(gv, ib, gb)
-        np.add.at(gv, ic, gcc)
-        np.add.at(gvn, ia, ds * (1 - u - v)[:, None])
-        np.add.at(gvn, ib, ds * u[:, None])
-        np.add.at(gvn, ic, ds * v[:, None])
-        g_o[idx] += go
-        g_w[idx] += np.einsum("nij,ni->nj", Jw[idx], gd)
+        acc(gv, ia, ga)
+        acc(gv, ib, gb)
+        acc(gv, ic, gcc)
+        acc(gvn, ia, ds * (1 - u - v)[:, None])
+        acc(gvn, ib, ds * u[:, None])
+        acc(gvn, ic, ds * v[:, None])
+        g_o[idx] += np.abs(go) if absolute else go
+        gw_ = np.einsum("nij,ni->nj", Jw[idx], gd)
+        g_w[idx] += np.abs(gw_) if absolute else gw_
         # vertex normals back to vertices: N_x = sum_f normalize(m_f)/3
         gfn = (gvn[F[:, 0]] + gvn[F[:, 1]] + gvn[F[:, 2]]) / 3.0
         gm = np.einsum("nij,ni->nj", _normalize_jac(mf), gfn)
         E1, E2 = f1 - f0, f2 - f0
         gE1 = np.cross(E2, gm)
         gE2 = np.cross(gm, E1)
-        np.add.at(gv, F[:, 0], -(gE1 + gE2))
-        np.add.at(gv, F[:, 1], gE1)
-        np.add.at(gv, F[:, 2], gE2)
+        acc(gv, F[:, 0], -(gE1 + gE2))
+        acc(gv, F[:, 1], gE1)
+        acc(gv, F[:, 2], gE2)
 
     if spec.spheres is not None:
         m = hit & (fwd["geom"] == geom_ids["spheres"])
@@ -160,9 +166,10 @@ def gradients(spec, origins, directions, fwd, gt, guv=None, gnormal=None):
         gT = gt[idx] + np.einsum("ij,ij->i", gp, dd)
         gvv_ = gp + gT[:, None] * dT_dv
         gd = T[:, None] * gp + gT[:, None] * dT_dd
-        np.add.at(gc, P, -gvv_)
-        np.add.at(gr, P, gT * dT_dR)
-        g_o[idx] += gvv_
-        g_w[idx] += np.einsum("nij,ni->nj", Jw[idx], gd)
+        acc(gc, P, -gvv_)
+        acc(gr, P, gT * dT_dR)
+        g_o[idx] += np.abs(gvv_) if absolute else gvv_
+        gw_ = np.einsum("nij,ni->nj", Jw[idx], gd)
+        g_w[idx] += np.abs(gw_) if absolute else gw_
 
     return dict(origins=g_o, directions=g_w, vertices=gv, centers=gc, radii=gr)

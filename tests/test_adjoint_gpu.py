@@ -40,11 +40,15 @@ def _adjoint_vs_analytic(spec, o, d, rng, with_uv_normal):
     return s, f, wt
 
 
-def assert_close(got, ref, what):
+def assert_close(got, ref, what, scale=None):
     """Two independent FP64 evaluations of the same gradient: per element within 1e-7
     relative (rays that graze a triangle have 1/(n.d) condition numbers near 1e8), plus an
-    absolute floor of 1e-10 of the largest magnitude."""
+    absolute floor of 1e-10 of the largest magnitude.  With `scale` (the same sums taken over
+    the absolute values of their terms), also 1e-8 of that scale: a sum whose terms cancel
+    keeps the rounding of its terms, not a fraction of its own size."""
     tol = 1e-7 * np.abs(ref) + 1e-10 * (np.abs(ref).max() + 1e-300)
+    if scale is not None:
+        tol = tol + 1e-8 * scale
     bad = np.abs(got - ref) > tol
     assert not bad.any(), (what, int(bad.sum()), float(np.abs(got - ref).max()))
 
@@ -94,21 +98,60 @@ def _loss_of(out, case, loss, mask):
     return np.einsum("ij,ij->i", w[key][mask], np.where(h[:, None], out[key][mask], 0.0))
 
 
+def _geometric_cos(spec, R, f):
+    """|cos| between each ray's direction and the geometric normal of the surface it hits
+    (the face normal for triangles, the returned normal for spheres); 1 for misses."""
+    d = R.directions / np.linalg.norm(R.directions, axis=1, keepdims=True)
+    hit = f["hit"].astype(bool)
+    n = np.array(f["normal"], copy=True)
+    tri = hit & (f["geom"] == 0)
+    if tri.any():
+        V, F = spec.mesh["vertices"], spec.mesh["faces"].astype(np.int64)
+        P = F[f["prim"][tri].astype(np.int64)]
+        n[tri] = np.cross(V[P[:, 1]] - V[P[:, 0]], V[P[:, 2]] - V[P[:, 0]])
+    n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-300)
+    return np.where(hit, np.abs(np.einsum("ij,ij->i", d, n)), 1.0)
+
+
 def test_adjoint_scene_analytic_full_size(adjoint_case):
     """All 4,194,304 rays: the CUDA adjoint of t, uv and normal (together) against the host
-    analytic FP64 gradient, per element within 1e-7 relative."""
+    analytic FP64 gradient.  Both sides are FP64 evaluations of the same closed form in
+    different operation orders, so they agree to about eps times the condition number, which
+    grows like 1/cos^2 of the angle between the ray and the surface.  Rays with |cos| >= 1e-3
+    (all but about one in a thousand) are compared on every output at 1e-7 relative; the
+    grazing rest, in a call of their own, on their per-ray origin and direction gradient
+    vectors at max(1e-7, 64 eps / cos^2) of the vector's length.  Per-vertex and per-sphere
+    sums also get 1e-8 of the sum of their terms' magnitudes, since terms of both signs cancel
+    in them."""
     c = adjoint_case
     spec, R, s = c["spec"], c["R"], c["s"]
-    gt, _, _ = _upstream(c, "t", c["hit"])
-    guv = c["w"]["uv"]
-    gn = c["w"]["normal"]
+    cos = _geometric_cos(spec, R, c["f"])
     nv, ns = len(spec.mesh["vertices"]), len(spec.spheres["radii"])
-    g = s.adjoint(c["to"], c["td"], c["fwd"], grad_t=_dev(gt), grad_uv=_dev(guv),
-                  grad_normal=_dev(gn), n_vertices=nv, n_spheres=ns)
-    assert s.check() == 0
-    ref = adjoint_ref.gradients(spec, R.origins, R.directions, c["f"], gt, guv, gn)
-    for k in ("origins", "directions", "vertices", "centers", "radii"):
-        assert_close(g[k].cpu().numpy(), ref[k], k)
+    for part in ("well", "grazing"):
+        mask = c["hit"] & ((cos >= 1e-3) if part == "well" else (cos < 1e-3))
+        gt, _, _ = _upstream(c, "t", mask)
+        guv = c["w"]["uv"] * mask[:, None]
+        gn = c["w"]["normal"] * mask[:, None]
+        g = s.adjoint(c["to"], c["td"], c["fwd"], grad_t=_dev(gt), grad_uv=_dev(guv),
+                      grad_normal=_dev(gn), n_vertices=nv, n_spheres=ns)
+        assert s.check() == 0
+        ref = adjoint_ref.gradients(spec, R.origins, R.directions, c["f"], gt, guv, gn)
+        if part == "well":
+            assert mask.sum() > 0.99 * c["hit"].sum()
+            scale = adjoint_ref.gradients(spec, R.origins, R.directions, c["f"], gt, guv, gn,
+                                          absolute=True)
+            for k in ("origins", "directions", "vertices", "centers", "radii"):
+                assert_close(g[k].cpu().numpy(), ref[k], k, scale[k])
+        else:
+            rel = np.maximum(1e-7, 64 * np.finfo(np.float64).eps / np.maximum(cos, 1e-300) ** 2)
+            for k in ("origins", "directions"):
+                got = g[k].cpu().numpy()
+                size = np.linalg.norm(ref[k], axis=1)
+                err = np.linalg.norm(got - ref[k], axis=1)
+                bad = err > rel * size + 1e-300
+                worst = int(np.argmax(err / (rel * size + 1e-300)))
+                assert not bad.any(), (k, int(bad.sum()), float(cos[worst]), float(err[worst]),
+                                       float(size[worst]))
 
 
 @pytest.mark.parametrize("loss", ["t", "uv", "normal"])

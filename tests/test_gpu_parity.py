@@ -192,7 +192,7 @@ def test_tuning_changes_speed_not_results():
             assert s.check() == 0
             assert mismatches(out, ref) == [], (cfg, mode)
     res = autotune(s, o, d, sample=100_000)
-    assert set(res["choice"]) == {"sort", "threads", "shared_stack", "chunk"}
+    assert set(res["choice"]) == {"sort", "threads", "shared_stack", "chunk", "top_nodes"}
     out = s.intersectN(o, d)
     torch.cuda.synchronize()
     assert mismatches(out, ref) == []
