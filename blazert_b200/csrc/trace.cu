@@ -196,12 +196,14 @@ __device__ __forceinline__ void trace_kind_body(const SceneView &S, const RayIO 
     if (active) {
       if (kWide && use32) {
         if (tv.live) wtrav_to_leaf<KIND, COUNT>(K, f, hl, tv, sk, tid, io.error_word, &cnt);
-        if (tv.live) wtrav_leaf<KIND, COUNT>(K, r, f, st, hl, tv, sk, tid, io.error_word, &cnt);
+        while (tv.live && tv.post != kNoLeaf)
+          wtrav_leaf<KIND, COUNT>(K, r, f, st, hl, tv, sk, tid, io.error_word, &cnt);
       } else {
         if (tv.live) trav_to_leaf<KIND, COUNT>(K, r, st, tv, sk64, tid, io.error_word, &cnt);
         if (tv.live) trav_leaf<KIND, COUNT>(K, r, st, tv, sk64, tid, io.error_word, &cnt);
       }
       if (!tv.live) {
+        if (kWide && use32) wtrav_end<KIND>(K, r, st);
         finalize_kind<KIND>(S, r, st, i, first != 0, io.t, io.uv, io.normal, io.prim, io.geom,
                             io.hit);
         active = false;
@@ -230,7 +232,7 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
 }
 
 #ifndef BZR_WIDE_REGS
-#define BZR_WIDE_REGS 80
+#define BZR_WIDE_REGS 72
 #endif
 template <int KIND, bool COUNT, bool LOCAL>
 __global__ void __maxnreg__(BZR_WIDE_REGS)
@@ -349,12 +351,14 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
     if (active) {
       if (kWide && use32) {
         if (tv.live) wtrav_to_leaf<KIND, false>(*K, f, hl, tv, sk, tid, io.error_word, &cnt);
-        if (tv.live) wtrav_leaf<KIND, false>(*K, r, f, st, hl, tv, sk, tid, io.error_word, &cnt);
+        while (tv.live && tv.post != kNoLeaf)
+          wtrav_leaf<KIND, false>(*K, r, f, st, hl, tv, sk, tid, io.error_word, &cnt);
       } else {
         if (tv.live) trav_to_leaf<KIND, false>(*K, r, st, tv, sk, tid, io.error_word, &cnt);
         if (tv.live) trav_leaf<KIND, false>(*K, r, st, tv, sk, tid, io.error_word, &cnt);
       }
       if (!tv.live) {
+        if (kWide && use32) wtrav_end<KIND>(*K, r, st);
         finalize_kind<KIND>(B.views[sc], r, st, i, B.first_kind[sc] == KIND, io.t, io.uv,
                             io.normal, io.prim, io.geom, io.hit);
         if (B.last_kind[sc] == KIND && B.scene_left) {

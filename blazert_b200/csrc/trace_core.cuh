@@ -163,33 +163,58 @@ BZR_HD D3 ld_vertex(const double *verts, uint32_t i) {
   return d3(xy.x, xy.y, z0.x);
 }
 
-// blazert/primitives/trimesh.h:153-181.  F holds the triangle's three vertex indices; v0,
-// e1 = v0 - v1, e2 = v2 - v0 (the reference Triangle's members, trimesh.h:19-31) and
-// n = cross(e1, e2) are formed here with the reference's operations, hence the same bits.
-BZR_HD bool isect_triangle(const double *verts, uint4 F, uint32_t pos, const Ray &r,
-                           KState &st) {
+// blazert/primitives/trimesh.h:153-181, the quantities of one test before its decisions.  F
+// holds the triangle's three vertex indices; v0, e1 = v0 - v1, e2 = v2 - v0 (the reference
+// Triangle's members, trimesh.h:19-31) and n = cross(e1, e2) are formed here with the
+// reference's operations, hence the same bits.
+struct TriTest {
+  double u, v, w, det, abs_det;  // unnormalised barycentrics, det and |det|
+  D3 n, c;                       // for the unnormalised distance product_sign(dot(n, c), det)
+};
+BZR_HD TriTest tri_test(const double *verts, uint4 F, const Ray &r) {
   const D3 v0 = ld_vertex(verts, F.x), v1 = ld_vertex(verts, F.y), v2 = ld_vertex(verts, F.z);
   const D3 e1 = sub(v0, v1), e2 = sub(v2, v0);
-  const D3 n = cross(e1, e2);
-  const D3 c = sub(v0, r.o);
-  const D3 rr = cross(r.d, c);
-  const double det = dot(n, r.d);
-  const double abs_det = fabs(det);
-  const double u = product_sign(dot(rr, e2), det);
-  const double v = product_sign(dot(rr, e1), det);
-  const double w = (abs_det - u) - v;
-  if (u >= -kTol && v >= -kTol && w >= -kTol) {
-    const double t = product_sign(dot(n, c), det);
-    if (t >= abs_det * r.tmin && abs_det * st.hit > t) {
-      const double inv_det = 1.0 / abs_det;
+  TriTest q;
+  q.n = cross(e1, e2);
+  q.c = sub(v0, r.o);
+  const D3 rr = cross(r.d, q.c);
+  q.det = dot(q.n, r.d);
+  q.abs_det = fabs(q.det);
+  q.u = product_sign(dot(rr, e2), q.det);
+  q.v = product_sign(dot(rr, e1), q.det);
+  q.w = (q.abs_det - q.u) - q.v;
+  return q;
+}
+
+// The whole test.  UV: store the hit's barycentrics in st (the mixed-precision walk leaves
+// them out while it walks and forms them once at the end, tri_uv).
+template <bool UV = true>
+BZR_HD bool isect_triangle(const double *verts, uint4 F, uint32_t pos, const Ray &r,
+                           KState &st) {
+  const TriTest q = tri_test(verts, F, r);
+  if (q.u >= -kTol && q.v >= -kTol && q.w >= -kTol) {
+    const double t = product_sign(dot(q.n, q.c), q.det);
+    if (t >= q.abs_det * r.tmin && q.abs_det * st.hit > t) {
+      const double inv_det = 1.0 / q.abs_det;
       st.hit = t * inv_det;
-      st.u = u * inv_det;
-      st.v = v * inv_det;
+      if (UV) {
+        st.u = q.u * inv_det;
+        st.v = q.v * inv_det;
+      }
       st.pos = pos;
       return true;
     }
   }
   return false;
+}
+
+// The barycentrics isect_triangle<true> stores for the triangle at leaf position st.pos (the
+// same operations, hence the same bits).
+BZR_HD void tri_uv(const KindView &K, const Ray &r, KState &st) {
+  const TriTest q = tri_test(K.verts, ldg(reinterpret_cast<const uint4 *>(K.tri) + st.pos), r);
+  const double inv_det = 1.0 / q.abs_det;
+  st.u = q.u * inv_det;
+  st.v = q.v * inv_det;
 }
 
 // blazert/primitives/sphere.h:135-177
@@ -429,9 +454,9 @@ struct Trav {
   uint32_t cur;  // node index, or kLeafBit | first primitive position of a leaf
   uint32_t sp;   // stack depth
   bool live;     // false once the stack is exhausted
-  // wide walk only: the leaf record found first and not yet processed (kNoLeaf: none), and
-  // whether cur still holds a reference to walk
-  uint32_t post;
+  // wide walk only: the leaf records found and not yet processed, in visit order (kNoLeaf:
+  // none; post2 is set only after post), and whether cur still holds a reference to walk
+  uint32_t post, post2;
   bool walk;
 };
 constexpr uint32_t kNoLeaf = 0xFFFFFFFFu;  // no leaf record has this reference
@@ -696,7 +721,7 @@ BZR_HD void wtrav_begin(const KindView &K, const Ray &r, const RayW &f, KState &
   (void)f;
   trav_begin<KIND, COUNT>(K, r, st, tv, cnt);
   tv.cur = K.wide_root_ref;
-  tv.post = kNoLeaf;
+  tv.post = tv.post2 = kNoLeaf;
   tv.walk = tv.live;
   hl = hit_bound(st.hit);
 }
@@ -776,7 +801,37 @@ BZR_HD uint32_t fword(float x) {
 #endif
 }
 
-// Walks wide nodes until the ray has a leaf record to process (tv.post) or nothing left.
+// 32 bytes at p (32-byte aligned) as two uint4, kept in L2 with priority on the device.
+BZR_HD void ld32_keep(const void *p, uint4 &a, uint4 &b) {
+#if defined(__CUDA_ARCH__)
+  asm("ld.global.nc.L2::evict_last.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+      : "l"(p));
+#else
+  std::memcpy(&a, p, 16);
+  std::memcpy(&b, static_cast<const char *>(p) + 16, 16);
+#endif
+}
+
+BZR_HD uint32_t pick8(uint4 a, uint4 b, uint32_t slot) {
+  const uint4 q = (slot & 4u) ? b : a;
+  const uint32_t lo = (slot & 1u) ? q.y : q.x, hi = (slot & 1u) ? q.w : q.z;
+  return (slot & 2u) ? hi : lo;
+}
+
+// A lane at a leaf reference with room in its queue of two postponed leaves appends the leaf
+// and pops the next entry.
+BZR_HD void wtrav_postpone(Trav &tv, const Stack &sk, uint32_t tid) {
+  if (tv.walk && (tv.cur & kLeafBit) && tv.post2 == kNoLeaf) {
+    if (tv.post == kNoLeaf)
+      tv.post = tv.cur;
+    else
+      tv.post2 = tv.cur;
+    wtrav_pop(tv, sk, tid);
+  }
+}
+
+// The wide walk.
 //
 // Per node, each child slot's near and far distances per axis come from one paired FMA
 // (near and far biases side by side); the child is kept when exit - entry has its sign bit
@@ -791,121 +846,131 @@ BZR_HD uint32_t fword(float x) {
 // exact test.
 //
 // Postponed leaves (Aila and Laine, "Understanding the efficiency of ray traversal on GPUs",
-// 2009): a lane that reaches a leaf record keeps it in tv.post and walks on while some lane of
-// the warp has not found one yet, so that the warp's lanes reach their leaf steps together;
-// it stops at a second leaf.  The walk past a postponed leaf uses the hit distance from before
-// that leaf, which keeps more children, never fewer; leaves are still processed in the visit
-// order, each with its exact test.  The counting kernels do not walk ahead, so their counts
-// are the walk's own work.
+// 2009): a lane that reaches a leaf record keeps it (tv.post, then tv.post2) and walks on while
+// some lane of the warp has not found one yet, so that the warp's lanes reach their leaf steps
+// together; it stops at a third leaf, and its leaf step processes every leaf it holds.  (A
+// queue of two measured 8-10 % faster than one on the workloads here; three or four, slower.)
+// The walk past a postponed leaf uses the hit distance from before that leaf, which keeps more
+// children, never fewer; leaves are still processed in the visit order, each with its exact
+// test.  The counting kernels do not walk ahead, so their counts are the walk's own work.
+//
+// wtrav_node tests one wide node (the lane is at a node: tv.walk and tv.cur not a leaf).
+template <int KIND, bool COUNT>
+BZR_HD void wtrav_node(const KindView &K, const RayW &f, float hl, Trav &tv, const Stack &sk,
+                       uint32_t tid, uint32_t *err, Counts *cnt) {
+  const bool sx = f.oct & 1u, sy = f.oct & 2u, sz = f.oct & 4u;
+  if (tv.cur >= K.n_wide) {
+    flag_error(err, kErrNodeIndex);
+    tv.walk = false;
+    return;
+  }
+  const bool staged = tv.cur < sk.n_top;  // a top-level node staged in shared memory
+  const uint4 *nd = staged ? sk.top + size_t(tv.cur) * 8
+                           : reinterpret_cast<const uint4 *>(K.wide + size_t(tv.cur) * kWideBytes);
+  const uint32_t *words = reinterpret_cast<const uint32_t *>(nd);
+  uint4 hd, qx, qy, qz, ra, rb;
+  uint32_t perm;
+  if (staged) {
+    hd = nd[0], qx = nd[1], qy = nd[2], qz = nd[3];
+    ra = nd[4], rb = nd[5];
+    perm = words[24 + f.oct];
+  } else {
+    ld32_keep(nd, hd, qx);
+    ld32_keep(nd + 2, qy, qz);
+    ld32_keep(nd + 4, ra, rb);
+    perm = ldg(words + 24 + f.oct);
+  }
+  // per axis t(q) = fma(2^23 + q, A, B - 2^23 A -+ E): a lower bound of the reference's
+  // near-plane distance, an upper bound of its far-plane distance
+  const float ax = fbits((hd.w & 0xFFu) << 23) * f.inv[0];
+  const float ay = fbits((hd.w & 0xFF00u) << 15) * f.inv[1];
+  const float az = fbits((hd.w & 0xFF0000u) << 7) * f.inv[2];
+  const float bx = ((fbits(hd.x) - f.o_hi[0]) - f.o_lo[0]) * f.inv[0];
+  const float by = ((fbits(hd.y) - f.o_hi[1]) - f.o_lo[1]) * f.inv[1];
+  const float bz = ((fbits(hd.z) - f.o_hi[2]) - f.o_lo[2]) * f.inv[2];
+  const float cx = fma32(-8388608.0f, ax, bx), cy = fma32(-8388608.0f, ay, by);
+  const float cz = fma32(-8388608.0f, az, bz);
+  constexpr float kRel = 9.5367431640625e-07f, kCell = 1.0009765625f;  // 2^-20, 1 + 2^-10
+  const float ex = fma32(kCell, fabsf(ax), kRel * fabsf(bx)) + 1e-37f;
+  const float ey = fma32(kCell, fabsf(ay), kRel * fabsf(by)) + 1e-37f;
+  const float ez = fma32(kCell, fabsf(az), kRel * fabsf(bz)) + 1e-37f;
+  const float2 Ax = make_float2(ax, ax), Ay = make_float2(ay, ay), Az = make_float2(az, az);
+  const float2 Bx = make_float2(cx - ex, cx + ex), By = make_float2(cy - ey, cy + ey);
+  const float2 Bz = make_float2(cz - ez, cz + ez);
+  // near and far bound words per axis: the hi bounds are near for a negative direction
+  const uint32_t nx0 = sx ? qx.z : qx.x, nx1 = sx ? qx.w : qx.y;
+  const uint32_t fx0 = sx ? qx.x : qx.z, fx1 = sx ? qx.y : qx.w;
+  const uint32_t ny0 = sy ? qy.z : qy.x, ny1 = sy ? qy.w : qy.y;
+  const uint32_t fy0 = sy ? qy.x : qy.z, fy1 = sy ? qy.y : qy.w;
+  const uint32_t nz0 = sz ? qz.z : qz.x, nz1 = sz ? qz.w : qz.y;
+  const uint32_t fz0 = sz ? qz.x : qz.z, fz1 = sz ? qz.y : qz.w;
+  uint32_t sgn[8];  // exit - entry per slot (its sign bit: rejected)
+#pragma unroll
+  for (int c = 0; c < kWideMax; ++c) {
+    const int b = c & 3;
+    const float2 tx = fma2(make_float2(qbyte(c < 4 ? nx0 : nx1, b), qbyte(c < 4 ? fx0 : fx1, b)),
+                           Ax, Bx);
+    const float2 ty = fma2(make_float2(qbyte(c < 4 ? ny0 : ny1, b), qbyte(c < 4 ? fy0 : fy1, b)),
+                           Ay, By);
+    const float2 tz = fma2(make_float2(qbyte(c < 4 ? nz0 : nz1, b), qbyte(c < 4 ? fz0 : fz1, b)),
+                           Az, Bz);
+    const float entry = max3f(tx.x, ty.x, fmaxf(tz.x, f.tmin));
+    const float exit = min3f(tx.y, ty.y, fminf(tz.y, hl));
+    sgn[c] = fword(exit - entry);
+  }
+  // sign bytes in slot order (byte c of s_lo | s_hi << 32: slot c); slot 7 reads as rejected
+  // when the node has fewer than 8 children, as it then stands for the permutation's unused
+  // positions (nibble 15: slot 7's sign replicated)
+  const uint32_t s_lo = prmt(prmt(sgn[0], sgn[1], 0x0073u), prmt(sgn[2], sgn[3], 0x0073u), 0x5410u);
+  const uint32_t s_hi = prmt(prmt(sgn[4], sgn[5], 0x0073u), prmt(sgn[6], sgn[7], 0x0073u), 0x5410u) |
+                        ((hd.w - 0x08000000u) & 0x80000000u);
+  // bit 8j + 7 of m: the child at visit position j is kept
+  const uint64_t m = (uint64_t(~prmt(s_lo, s_hi, perm >> 16) & 0x80808080u) << 32) |
+                     (~prmt(s_lo, s_hi, perm & 0xFFFFu) & 0x80808080u);
+  if (COUNT) {
+    cnt->node[KIND] += 1;
+    cnt->box[KIND] += hd.w >> 24;
+  }
+  // The builder bounds the stack: the entries below this node plus its children minus one
+  // never exceed the image's stack size, which the capacity covers.  Checked once per node.
+  if (tv.sp + (hd.w >> 24) > sk.cap + 1) {
+    flag_error(err, kErrStack);
+    tv.walk = false;
+    return;
+  }
+  if (m == 0) {
+    wtrav_pop(tv, sk, tid);
+    return;
+  }
+  for (uint64_t rest = m & (m - 1); rest != 0;) {  // all kept but the first, last first
+    const int bit = msb64(rest);
+    const uint32_t slot = (perm >> ((bit >> 3) * 4)) & 7u;
+    sk.ref[tv.sp * sk.stride + tid] = pick8(ra, rb, slot);
+    ++tv.sp;
+    rest ^= uint64_t(1) << bit;
+  }
+  const uint32_t slot = (perm >> (((ffs64(m) - 1) >> 3) * 4)) & 7u;
+  tv.cur = pick8(ra, rb, slot);
+}
+
+// Walks wide nodes until the ray has a leaf record to process (tv.post) or nothing left.
 template <int KIND, bool COUNT>
 BZR_HD void wtrav_to_leaf(const KindView &K, const RayW &f, float hl, Trav &tv, const Stack &sk,
                           uint32_t tid, uint32_t *err, Counts *cnt) {
-  const bool sx = f.oct & 1u, sy = f.oct & 2u, sz = f.oct & 4u;
   const unsigned lanes = active_lanes();
   for (;;) {
-    if (tv.walk && (tv.cur & kLeafBit) && tv.post == kNoLeaf) {
-      tv.post = tv.cur;  // the first leaf found: postponed, the walk goes on
-      wtrav_pop(tv, sk, tid);
-    }
+    wtrav_postpone(tv, sk, tid);
     const bool at_node = tv.walk && !(tv.cur & kLeafBit);
     const bool searching = at_node && tv.post == kNoLeaf;
     if (!(COUNT ? searching : warp_any(lanes, searching))) break;
-    if (!at_node) continue;
-    if (tv.cur >= K.n_wide) {
-      flag_error(err, kErrNodeIndex);
-      tv.walk = false;
-      continue;
-    }
-    const bool staged = tv.cur < sk.n_top;  // a top-level node staged in shared memory
-    const uint4 *nd = staged ? sk.top + size_t(tv.cur) * 8
-                             : reinterpret_cast<const uint4 *>(K.wide + size_t(tv.cur) * kWideBytes);
-    const uint32_t *words = reinterpret_cast<const uint32_t *>(nd);
-    uint4 hd, qx, qy, qz;
-    uint32_t perm;
-    if (staged) {
-      hd = nd[0], qx = nd[1], qy = nd[2], qz = nd[3];
-      perm = words[24 + f.oct];
-    } else {
-      hd = ldg(nd), qx = ldg(nd + 1), qy = ldg(nd + 2), qz = ldg(nd + 3);
-      perm = ldg(words + 24 + f.oct);
-    }
-    // per axis t(q) = fma(2^23 + q, A, B - 2^23 A -+ E): a lower bound of the reference's
-    // near-plane distance, an upper bound of its far-plane distance
-    const float ax = fbits((hd.w & 0xFFu) << 23) * f.inv[0];
-    const float ay = fbits((hd.w & 0xFF00u) << 15) * f.inv[1];
-    const float az = fbits((hd.w & 0xFF0000u) << 7) * f.inv[2];
-    const float bx = ((fbits(hd.x) - f.o_hi[0]) - f.o_lo[0]) * f.inv[0];
-    const float by = ((fbits(hd.y) - f.o_hi[1]) - f.o_lo[1]) * f.inv[1];
-    const float bz = ((fbits(hd.z) - f.o_hi[2]) - f.o_lo[2]) * f.inv[2];
-    const float cx = fma32(-8388608.0f, ax, bx), cy = fma32(-8388608.0f, ay, by);
-    const float cz = fma32(-8388608.0f, az, bz);
-    constexpr float kRel = 9.5367431640625e-07f, kCell = 1.0009765625f;  // 2^-20, 1 + 2^-10
-    const float ex = fma32(kCell, fabsf(ax), kRel * fabsf(bx)) + 1e-37f;
-    const float ey = fma32(kCell, fabsf(ay), kRel * fabsf(by)) + 1e-37f;
-    const float ez = fma32(kCell, fabsf(az), kRel * fabsf(bz)) + 1e-37f;
-    const float2 Ax = make_float2(ax, ax), Ay = make_float2(ay, ay), Az = make_float2(az, az);
-    const float2 Bx = make_float2(cx - ex, cx + ex), By = make_float2(cy - ey, cy + ey);
-    const float2 Bz = make_float2(cz - ez, cz + ez);
-    // near and far bound words per axis: the hi bounds are near for a negative direction
-    const uint32_t nx0 = sx ? qx.z : qx.x, nx1 = sx ? qx.w : qx.y;
-    const uint32_t fx0 = sx ? qx.x : qx.z, fx1 = sx ? qx.y : qx.w;
-    const uint32_t ny0 = sy ? qy.z : qy.x, ny1 = sy ? qy.w : qy.y;
-    const uint32_t fy0 = sy ? qy.x : qy.z, fy1 = sy ? qy.y : qy.w;
-    const uint32_t nz0 = sz ? qz.z : qz.x, nz1 = sz ? qz.w : qz.y;
-    const uint32_t fz0 = sz ? qz.x : qz.z, fz1 = sz ? qz.y : qz.w;
-    uint32_t sgn[8];  // exit - entry per slot (its sign bit: rejected)
-#pragma unroll
-    for (int c = 0; c < kWideMax; ++c) {
-      const int b = c & 3;
-      const float2 tx = fma2(make_float2(qbyte(c < 4 ? nx0 : nx1, b), qbyte(c < 4 ? fx0 : fx1, b)),
-                             Ax, Bx);
-      const float2 ty = fma2(make_float2(qbyte(c < 4 ? ny0 : ny1, b), qbyte(c < 4 ? fy0 : fy1, b)),
-                             Ay, By);
-      const float2 tz = fma2(make_float2(qbyte(c < 4 ? nz0 : nz1, b), qbyte(c < 4 ? fz0 : fz1, b)),
-                             Az, Bz);
-      const float entry = max3f(tx.x, ty.x, fmaxf(tz.x, f.tmin));
-      const float exit = min3f(tx.y, ty.y, fminf(tz.y, hl));
-      sgn[c] = fword(exit - entry);
-    }
-    // sign bytes in slot order (byte c of s_lo | s_hi << 32: slot c); slot 7 reads as rejected
-    // when the node has fewer than 8 children, as it then stands for the permutation's unused
-    // positions (nibble 15: slot 7's sign replicated)
-    const uint32_t s_lo = prmt(prmt(sgn[0], sgn[1], 0x0073u), prmt(sgn[2], sgn[3], 0x0073u), 0x5410u);
-    const uint32_t s_hi = prmt(prmt(sgn[4], sgn[5], 0x0073u), prmt(sgn[6], sgn[7], 0x0073u), 0x5410u) |
-                          ((hd.w - 0x08000000u) & 0x80000000u);
-    // bit 8j + 7 of m: the child at visit position j is kept
-    const uint64_t m = (uint64_t(~prmt(s_lo, s_hi, perm >> 16) & 0x80808080u) << 32) |
-                       (~prmt(s_lo, s_hi, perm & 0xFFFFu) & 0x80808080u);
-    if (COUNT) {
-      cnt->node[KIND] += 1;
-      cnt->box[KIND] += hd.w >> 24;
-    }
-    // The builder bounds the stack: the entries below this node plus its children minus one
-    // never exceed the image's stack size, which the capacity covers.  Checked once per node.
-    if (tv.sp + (hd.w >> 24) > sk.cap + 1) {
-      flag_error(err, kErrStack);
-      tv.walk = false;
-      continue;
-    }
-    if (m == 0) {
-      wtrav_pop(tv, sk, tid);
-      continue;
-    }
-    for (uint64_t rest = m & (m - 1); rest != 0;) {  // all kept but the first, last first
-      const int bit = msb64(rest);
-      const uint32_t slot = (perm >> ((bit >> 3) * 4)) & 7u;
-      sk.ref[tv.sp * sk.stride + tid] = staged ? words[16 + slot] : ldg(words + 16 + slot);
-      ++tv.sp;
-      rest ^= uint64_t(1) << bit;
-    }
-    const uint32_t slot = (perm >> (((ffs64(m) - 1) >> 3) * 4)) & 7u;
-    tv.cur = staged ? words[16 + slot] : ldg(words + 16 + slot);
+    if (at_node) wtrav_node<KIND, COUNT>(K, f, hl, tv, sk, tid, err, cnt);
   }
   if (tv.post == kNoLeaf && !tv.walk) tv.live = false;  // nothing left to process
 }
 
-// The postponed leaf record: the exact FP64 test of the leaf's box, then its primitives in the
-// reference's stored order (blazert/bvh/intersect.h:67-78).  The walk then resumes at tv.cur.
+// The first postponed leaf record: the exact FP64 test of the leaf's box, then its primitives in
+// the reference's stored order (blazert/bvh/intersect.h:67-78); the queue moves up by one.  The
+// walk then resumes at tv.cur.
 template <int KIND, bool COUNT>
 BZR_HD void wtrav_leaf(const KindView &K, const Ray &r, const RayW &f, KState &st, float &hl,
                        Trav &tv, const Stack &sk, uint32_t tid, uint32_t *err, Counts *cnt) {
@@ -914,7 +979,8 @@ BZR_HD void wtrav_leaf(const KindView &K, const Ray &r, const RayW &f, KState &s
   constexpr uint32_t kUnits = KIND == kMesh ? 1u : uint32_t(kPayloadDoubles[KIND] / 2);
   if (tv.post == kNoLeaf) return;
   const uint32_t off = tv.post & kIdMask;
-  tv.post = kNoLeaf;
+  tv.post = tv.post2;
+  tv.post2 = kNoLeaf;
   if (uint64_t(off) + kLeafHeaderBytes / 16 > K.n_leaf16) {
     flag_error(err, kErrPrimIndex);
     tv.live = false;
@@ -939,7 +1005,7 @@ BZR_HD void wtrav_leaf(const KindView &K, const Ray &r, const RayW &f, KState &s
       if (COUNT) cnt->prim[KIND] += 1;
       bool h;
       if (KIND == kMesh)
-        h = isect_triangle(K.verts, ldg(reinterpret_cast<const uint4 *>(P)), pos, r, st);
+        h = isect_triangle<false>(K.verts, ldg(reinterpret_cast<const uint4 *>(P)), pos, r, st);
       else if (KIND == kSpheres)
         h = isect_sphere(P, pos, r, st);
       else
@@ -951,7 +1017,13 @@ BZR_HD void wtrav_leaf(const KindView &K, const Ray &r, const RayW &f, KState &s
     }
     if (st.hit != before) hl = hit_bound(st.hit);
   }
-  if (!tv.walk) tv.live = false;
+  if (!tv.walk && tv.post == kNoLeaf) tv.live = false;
+}
+
+// The end of a wide walk: the barycentrics of a triangle hit, which the walk does not keep.
+template <int KIND>
+BZR_HD void wtrav_end(const KindView &K, const Ray &r, KState &st) {
+  if (KIND == kMesh && st.pos != 0xFFFFFFFFu) tri_uv(K, r, st);
 }
 
 // Whole traversal of one kind in mixed precision (the FP64 traversal for cylinders, kinds
@@ -969,8 +1041,10 @@ BZR_HD bool traverse_mixed(const KindView &K, const Ray &r, KState &st, const St
     wtrav_begin<KIND, COUNT>(K, r, f, st, hl, tv, cnt);
     while (tv.live) {
       wtrav_to_leaf<KIND, COUNT>(K, f, hl, tv, sk, tid, err, cnt);
-      if (tv.live) wtrav_leaf<KIND, COUNT>(K, r, f, st, hl, tv, sk, tid, err, cnt);
+      while (tv.live && tv.post != kNoLeaf)
+        wtrav_leaf<KIND, COUNT>(K, r, f, st, hl, tv, sk, tid, err, cnt);
     }
+    wtrav_end<KIND>(K, r, st);
     return st.hit < r.tmax;
   }
 }

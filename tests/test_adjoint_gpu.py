@@ -117,10 +117,11 @@ def test_adjoint_scene_analytic_full_size(adjoint_case):
     """All 4,194,304 rays: the CUDA adjoint of t, uv and normal (together) against the host
     analytic FP64 gradient.  Both sides are FP64 evaluations of the same closed form in
     different operation orders, so they agree to about eps times the condition number, which
-    grows like 1/cos^2 of the angle between the ray and the surface.  Rays with |cos| >= 1e-3
+    grows like a power of 1/cos of the angle between the ray and the surface (up to 1/cos^3
+    for the barycentric and normal terms, measured).  Rays with |cos| >= 1e-3
     (all but about one in a thousand) are compared on every output at 1e-7 relative; the
     grazing rest, in a call of their own, on their per-ray origin and direction gradient
-    vectors at max(1e-7, 64 eps / cos^2) of the vector's length.  Per-vertex and per-sphere
+    vectors at max(1e-7, 64 eps / cos^3) of the vector's length.  Per-vertex and per-sphere
     sums also get 1e-8 of the sum of their terms' magnitudes, since terms of both signs cancel
     in them."""
     c = adjoint_case
@@ -143,7 +144,7 @@ def test_adjoint_scene_analytic_full_size(adjoint_case):
             for k in ("origins", "directions", "vertices", "centers", "radii"):
                 assert_close(g[k].cpu().numpy(), ref[k], k, scale[k])
         else:
-            rel = np.maximum(1e-7, 64 * np.finfo(np.float64).eps / np.maximum(cos, 1e-300) ** 2)
+            rel = np.maximum(1e-7, 64 * np.finfo(np.float64).eps / np.maximum(cos, 1e-300) ** 3)
             for k in ("origins", "directions"):
                 got = g[k].cpu().numpy()
                 size = np.linalg.norm(ref[k], axis=1)
