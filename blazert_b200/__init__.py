@@ -612,12 +612,18 @@ class Batch:
         except Exception:
             pass
 
-    def tune(self, threads=None, shared_stack=None):
-        """Launch shape of the batch kernels (bzr_batch_tune); results do not depend on it."""
+    def tune(self, threads=None, shared_stack=None, stack_depth=None, sort=None):
+        """Launch shape and ray order of the batch kernels (bzr_batch_tune): threads per block,
+        stack storage, entries of the thread-local stack (32 or 64) and the per-scene
+        coherence sort; results do not depend on them."""
         if threads is not None:
             _check(self._lib.bzr_batch_tune(self._h, 3, int(threads)))
         if shared_stack is not None:
             _check(self._lib.bzr_batch_tune(self._h, 4, int(bool(shared_stack))))
+        if stack_depth is not None:
+            _check(self._lib.bzr_batch_tune(self._h, 11, int(stack_depth)))
+        if sort is not None:
+            _check(self._lib.bzr_batch_tune(self._h, 1, int(bool(sort))))
 
     def intersect(self, ray_offsets, origins, directions, tmin=None, tmax=None, out=None,
                   timestamps=None, mode="fp64", stream=None):

@@ -26,6 +26,11 @@ struct bzr_batch {
   uint32_t *d_rays = nullptr, *d_left = nullptr, *d_words = nullptr;  // words: 4 counters, error
   bzr::BatchChunk *d_chunks = nullptr;
   size_t chunk_cap = 0;
+  // coherence sort (bzr_batch_tune BZR_TUNE_SORT): per-scene quantisation boxes, and the
+  // keys, permutation and bucket counts (grown with the batch)
+  bzr::RaySort *d_sort = nullptr;
+  uint32_t *d_sort_words = nullptr;
+  size_t sort_cap = 0;  // rays the sort scratch holds
   cudaStream_t capture = nullptr;
   // graph of the last argument set
   cudaGraphExec_t exec = nullptr;
@@ -46,6 +51,8 @@ struct bzr_batch {
     cudaFree(d_left);
     cudaFree(d_words);
     cudaFree(d_chunks);
+    cudaFree(d_sort);
+    cudaFree(d_sort_words);
     cudaSetDevice(cur);
   }
 };
@@ -108,6 +115,31 @@ int bzr_batch_create(bzr_batch **out, const bzr_scene *const *scenes, size_t n_s
   if (e == cudaSuccess) e = cudaMemcpy(b->d_first, b->first_kind.data(), n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->d_last, b->last_kind.data(), n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(b->d_words, 0, 8 * sizeof(uint32_t));
+  if (e == cudaSuccess) {
+    // per scene the box of its root boxes, as the single-scene coherence sort quantises origins
+    std::vector<bzr::RaySort> sorts(n);
+    for (size_t s = 0; s < n; ++s) {
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      for (int k = 0; k < bzr::kNumKinds; ++k) {
+        const bzr::KindView &kv = b->views[s].k[k];
+        if (!kv.present || !kv.n_prims) continue;
+        for (int a = 0; a < 3; ++a) {
+          lo[a] = std::min(lo[a], kv.root_box[2 * a]);
+          hi[a] = std::max(hi[a], kv.root_box[2 * a + 1]);
+        }
+      }
+      for (int a = 0; a < 3; ++a) {
+        const double ext = hi[a] - lo[a];
+        const bool finite = ext > 0.0 && ext < 1e300;
+        sorts[s].lo[a] = finite ? float(lo[a]) : 0.0f;
+        sorts[s].scale[a] = finite ? float(512.0 / ext) : 0.0f;
+      }
+      sorts[s].enabled = true;
+    }
+    e = bzr::dev_malloc(&b->d_sort, n * sizeof(bzr::RaySort));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(b->d_sort, sorts.data(), n * sizeof(bzr::RaySort), cudaMemcpyHostToDevice);
+  }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking);
   cudaSetDevice(cur);
   if (e != cudaSuccess) {
@@ -157,7 +189,9 @@ int bzr_batch_intersect(bzr_batch *b, const uint64_t *ray_offsets, const double 
     std::vector<uint32_t> rays(ns);
     for (size_t s = 0; s < ns; ++s) {
       rays[s] = uint32_t(ray_offsets[s + 1] - ray_offsets[s]);
-      if (b->first_kind[s] < 0) continue;  // nothing to trace: filled with defaults below
+      // nothing to trace: filled with defaults below (a sorted batch still needs its chunks
+      // to give its rays sort keys; the kernels skip scenes without the kind they trace)
+      if (b->first_kind[s] < 0 && !b->plan.sort) continue;
       for (uint64_t a = ray_offsets[s]; a < ray_offsets[s + 1]; a += bzr::kBatchChunk)
         chunks.push_back({uint32_t(s), uint32_t(a),
                           uint32_t(std::min<uint64_t>(a + bzr::kBatchChunk, ray_offsets[s + 1]))});
@@ -179,8 +213,29 @@ int bzr_batch_intersect(bzr_batch *b, const uint64_t *ray_offsets, const double 
                      cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
       e = cudaMemcpy(b->d_rays, rays.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice);
+    bzr::BatchSortScratch scratch;
+    if (e == cudaSuccess && b->plan.sort) {
+      if (total > b->sort_cap) {
+        cudaFree(b->d_sort_words);
+        b->d_sort_words = nullptr;
+        b->sort_cap = 0;
+        e = bzr::dev_malloc(&b->d_sort_words,
+                            (2 * size_t(total) + bzr::kSortBuckets) * sizeof(uint32_t));
+        if (e != cudaSuccess) {
+          cudaSetDevice(cur);
+          return fail(BZR_ENOMEM, "sort scratch allocation failed");
+        }
+        b->sort_cap = total;
+      }
+      scratch.keys = b->d_sort_words;
+      scratch.perm = b->d_sort_words + total;
+      scratch.counts = b->d_sort_words + 2 * total;
+    }
     bzr::BatchView B;
     B.views = b->d_views;
+    B.scene_sort = b->d_sort;
+    for (B.scene_bits = 1; (size_t(1) << B.scene_bits) < ns; ++B.scene_bits) {
+    }
     B.chunks = b->d_chunks;
     B.n_chunks = uint32_t(chunks.size());
     B.n_scenes = uint32_t(ns);
@@ -206,7 +261,7 @@ int bzr_batch_intersect(bzr_batch *b, const uint64_t *ray_offsets, const double 
     cudaGraph_t graph = nullptr;
     if (e == cudaSuccess) e = cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      cudaError_t le = bzr::launch_batch(B, io, mode, b->plan, b->capture, b->d_words);
+      cudaError_t le = bzr::launch_batch(B, io, mode, b->plan, b->capture, b->d_words, scratch);
       for (size_t s = 0; le == cudaSuccess && s < ns; ++s) {
         if (b->first_kind[s] >= 0 || ray_offsets[s + 1] == ray_offsets[s]) continue;
         bzr::RayIO sub = io;  // a scene with nothing to trace gets the RayHit defaults
@@ -247,6 +302,17 @@ int bzr_batch_tune(bzr_batch *b, int option, int64_t value) {
   } else if (option == BZR_TUNE_STACK) {
     if (value != 0 && value != 1) return fail(BZR_EINVAL, "stack storage must be 0 or 1");
     p.shared_stack = value == 1;
+  } else if (option == BZR_TUNE_STACK_DEPTH) {
+    if (value != 32 && value != 64)
+      return fail(BZR_EINVAL, "the thread-local stack holds 32 or 64 entries");
+    if (value == 32 && p.stack_cap > 32)
+      return fail(BZR_EINVAL, "a scene of the batch needs more than 32 stack entries");
+    p.local_stack = static_cast<uint32_t>(value);
+  } else if (option == BZR_TUNE_SORT) {
+    if (value != 0 && value != 1) return fail(BZR_EINVAL, "sort must be 0 or 1");
+    if (value == 1 && b->scenes.size() > bzr::kBatchSortMaxScenes)
+      return fail(BZR_EINVAL, "the coherence sort takes batches of at most 4,096 scenes");
+    p.sort = value == 1;
   } else {
     return fail(BZR_EINVAL, "unknown tuning option for a batch");
   }

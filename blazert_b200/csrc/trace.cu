@@ -37,6 +37,7 @@
 #include "trace_core.cuh"
 
 namespace bzr {
+static_assert(kSortBuckets == (size_t(1) << kSortBits), "batch sort scratch size");
 namespace {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
@@ -53,12 +54,12 @@ __device__ __forceinline__ size_t stack_smem_bytes(uint32_t stack_cap) {
 // memory to L1 and the occupancy to the register count).  Otherwise shared memory sized from
 // the tree, entry j of thread t at [j * blockDim.x + t].  The capacity is clamped to the
 // storage, so a mismatch is reported as kErrStack, never written past.
-template <bool LOCAL>
+template <bool LOCAL, uint32_t LCAP = kLocalStack>
 __device__ __forceinline__ void init_stack(Stack &sk, uint32_t &tid, uint32_t cap,
                                            unsigned char *smem, double *lkey, uint32_t *lref) {
   if (LOCAL) {
     sk.stride = 1;
-    sk.cap = cap < kLocalStack ? cap : kLocalStack;
+    sk.cap = cap < LCAP ? cap : LCAP;
     sk.key = lkey;
     sk.ref = lref;
     tid = 0;
@@ -253,16 +254,17 @@ constexpr auto trace_kernel() {
 // keeps its own ray's scene, so a warp may finish rays of one scene while starting another's.
 // The pass of a scene's first kind writes its whole record; the pass of its last kind
 // completes it and stamps the scene's completion time.
-template <int KIND, bool MIXED, bool LOCAL>
+// LCAP: entries of the thread-local stack (the batch's stack-depth knob: 32 or 64).
+template <int KIND, bool MIXED, bool LOCAL, uint32_t LCAP>
 __global__ void __launch_bounds__(kMaxTraceThreads)
     trace_batch_kernel(BatchView B, RayIO io, uint32_t *chunk_counter, uint32_t stack_cap) {
   constexpr bool kWide = MIXED && KIND != kCylinders;
   extern __shared__ __align__(16) unsigned char smem[];
-  double lkey[LOCAL ? kLocalStack : 1];
-  uint32_t lref[LOCAL ? kLocalStack : 1];
+  double lkey[LOCAL ? LCAP : 1];
+  uint32_t lref[LOCAL ? LCAP : 1];
   Stack sk;
   uint32_t tid;
-  init_stack<LOCAL>(sk, tid, stack_cap, smem, lkey, lref);
+  init_stack<LOCAL, LCAP>(sk, tid, stack_cap, smem, lkey, lref);
   const unsigned lane = threadIdx.x & 31u;
   const unsigned below = (1u << lane) - 1u;
   uint32_t pool_next = 0, pool_end = 0, pool_scene = 0;  // warp-uniform
@@ -317,7 +319,7 @@ __global__ void __launch_bounds__(kMaxTraceThreads)
           ok = true;
         }
         if (ok) {
-          i = idx;
+          i = io.perm ? io.perm[idx] : idx;  // a sorted batch keeps each scene's range
           sc = s2;
           active = true;
           K = &B.views[sc].k[KIND];
@@ -399,6 +401,37 @@ __global__ void fill_defaults_kernel(RayIO io) {
 }
 
 // -------------------------------------------------------------------------- coherence sort
+// Sort keys of a batch of many scenes: the scene index in the top scene_bits bits, then the
+// single-scene key (direction octant over the origin's Morton code in the scene's box), so
+// that the counting sort keeps every scene's rays in the scene's own range.  One warp per
+// chunk of the chunk table, which covers every ray of the batch when the batch is sorted
+// (scenes with nothing to trace included).
+__global__ void batch_sort_key_kernel(BatchView B, RayIO io, uint32_t *keys, uint32_t *counts) {
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < B.n_chunks;
+       c += warps) {
+    const BatchChunk ch = B.chunks[c];
+    const RaySort rs = B.scene_sort[ch.scene];
+    for (uint32_t p = ch.begin + lane; p < ch.end; p += 32) {
+      const double *o = io.org + 3 * size_t(p), *d = io.dir + 3 * size_t(p);
+      uint32_t q[3];
+      for (int a = 0; a < 3; ++a) {
+        float x = (float(o[a]) - rs.lo[a]) * rs.scale[a];
+        x = fminf(fmaxf(x, 0.0f), 511.0f);  // NaN maps to 0
+        q[a] = uint32_t(x);
+      }
+      const uint32_t oct = (d[0] < 0.0 ? 4u : 0u) | (d[1] < 0.0 ? 2u : 0u) | (d[2] < 0.0 ? 1u : 0u);
+      const uint32_t low = (oct << 27) | (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+      const uint32_t k = B.scene_bits >= 2 ? (uint32_t(ch.scene) << (32 - B.scene_bits)) |
+                                                 (low >> (B.scene_bits - 2))
+                                           : (uint32_t(ch.scene) << 31) | (low << 1);
+      keys[p] = k;
+      atomicAdd(counts + (k >> (32 - kSortBits)), 1u);
+    }
+  }
+}
+
 __device__ __forceinline__ uint32_t ray_key(const RayIO &io, const RaySort &rs, uint32_t i) {
   const double *o = io.org + 3 * size_t(i), *d = io.dir + 3 * size_t(i);
   uint32_t q[3];
@@ -600,19 +633,29 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
 }
 
 namespace {
+// The kernel a batch launch uses for one kind: stack storage (thread-local with 32 or 64
+// entries, or shared) and mode.
+template <int KIND, bool MIXED>
+const void *batch_kernel(bool local, uint32_t lcap) {
+  if (local && lcap == 32) return reinterpret_cast<const void *>(trace_batch_kernel<KIND, MIXED, true, 32>);
+  if (local) return reinterpret_cast<const void *>(trace_batch_kernel<KIND, MIXED, true, kLocalStack>);
+  return reinterpret_cast<const void *>(trace_batch_kernel<KIND, MIXED, false, kLocalStack>);
+}
+
+inline bool batch_local(uint32_t stack_cap, const BatchPlan &plan) {
+  return !plan.shared_stack && stack_cap <= plan.local_stack;
+}
+
 template <int KIND>
 cudaError_t prepare_batch_kind(uint32_t stack_cap, const BatchPlan &plan, int *blocks,
                                int *blocks32) {
   const int sms = plan.sms, th = plan.threads;
-  const bool local = !plan.shared_stack && stack_cap <= kLocalStack;
+  const bool local = batch_local(stack_cap, plan);
   const size_t smem = local ? 0 : trace_smem_bytes(stack_cap, th);
-  const void *fp64 = local ? reinterpret_cast<const void *>(trace_batch_kernel<KIND, false, true>)
-                           : reinterpret_cast<const void *>(trace_batch_kernel<KIND, false, false>);
-  const void *mixed = local ? reinterpret_cast<const void *>(trace_batch_kernel<KIND, true, true>)
-                            : reinterpret_cast<const void *>(trace_batch_kernel<KIND, true, false>);
-  const cudaError_t e = grid_for(fp64, th, smem, sms, blocks);
+  const cudaError_t e = grid_for(batch_kernel<KIND, false>(local, plan.local_stack), th, smem, sms,
+                                 blocks);
   if (e != cudaSuccess) return e;
-  return grid_for(mixed, th, smem, sms, blocks32);
+  return grid_for(batch_kernel<KIND, true>(local, plan.local_stack), th, smem, sms, blocks32);
 }
 }  // namespace
 
@@ -638,12 +681,29 @@ cudaError_t batch_prepare(uint32_t stack_cap, BatchPlan *plan) {
 }
 
 cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const BatchPlan &plan,
-                         cudaStream_t stream, uint32_t *counters) {
+                         cudaStream_t stream, uint32_t *counters,
+                         const BatchSortScratch &sort_scratch) {
   cudaError_t e = cudaMemsetAsync(counters, 0, kNumKinds * sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
   batch_start_kernel<<<1, 256, 0, stream>>>(B, B.n_scenes);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const bool local = !plan.shared_stack && plan.stack_cap <= kLocalStack;
+  RayIO run = io;
+  if (plan.sort && sort_scratch.perm && B.n_chunks) {
+    // every ray of the batch gets a scene-major key; rays of scenes without chunks are never
+    // taken from the permutation, so their keys only need to land in their scene's range
+    e = cudaMemsetAsync(sort_scratch.counts, 0, (size_t(1) << kSortBits) * sizeof(uint32_t),
+                        stream);
+    if (e != cudaSuccess) return e;
+    const int blocks = plan.sms * 8;
+    batch_sort_key_kernel<<<blocks, 256, 0, stream>>>(B, io, sort_scratch.keys,
+                                                      sort_scratch.counts);
+    bucket_scan_kernel<<<1, 1024, 0, stream>>>(sort_scratch.counts);
+    bucket_scatter_kernel<<<blocks, 256, 0, stream>>>(io.n, sort_scratch.keys,
+                                                      sort_scratch.counts, sort_scratch.perm);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    run.perm = sort_scratch.perm;
+  }
+  const bool local = batch_local(plan.stack_cap, plan);
   const int th = plan.threads;
   const size_t smem = local ? 0 : trace_smem_bytes(plan.stack_cap, th);
   for (int k = 0; k < kNumKinds; ++k) {
@@ -651,19 +711,26 @@ cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const Ba
     const bool m = mode == kModeMixed && k != kCylinders;  // cylinders: FP64 traversal
     const int b = m ? plan.blocks32[k] : plan.blocks[k];
     uint32_t *c = counters + k;
-#define BZR_BATCH_LAUNCH(KK)                                                                 \
-  if (local && m)                                                                            \
-    trace_batch_kernel<KK, true, true><<<b, th, 0, stream>>>(B, io, c,                       \
-                                                                        plan.stack_cap);     \
-  else if (local)                                                                            \
-    trace_batch_kernel<KK, false, true><<<b, th, 0, stream>>>(B, io, c,                      \
-                                                                         plan.stack_cap);    \
-  else if (m)                                                                                \
-    trace_batch_kernel<KK, true, false><<<b, th, smem, stream>>>(B, io, c,                   \
-                                                                            plan.stack_cap); \
-  else                                                                                       \
-    trace_batch_kernel<KK, false, false><<<b, th, smem, stream>>>(B, io, c,                  \
-                                                                             plan.stack_cap);
+#define BZR_BATCH_LAUNCH(KK)                                                                   \
+  if (local && plan.local_stack == 32) {                                                       \
+    if (m)                                                                                     \
+      trace_batch_kernel<KK, true, true, 32><<<b, th, 0, stream>>>(B, run, c, plan.stack_cap);  \
+    else                                                                                       \
+      trace_batch_kernel<KK, false, true, 32><<<b, th, 0, stream>>>(B, run, c, plan.stack_cap); \
+  } else if (local) {                                                                          \
+    if (m)                                                                                     \
+      trace_batch_kernel<KK, true, true, kLocalStack><<<b, th, 0, stream>>>(B, run, c,          \
+                                                                          plan.stack_cap);     \
+    else                                                                                       \
+      trace_batch_kernel<KK, false, true, kLocalStack><<<b, th, 0, stream>>>(B, run, c,         \
+                                                                           plan.stack_cap);    \
+  } else if (m) {                                                                              \
+    trace_batch_kernel<KK, true, false, kLocalStack><<<b, th, smem, stream>>>(B, run, c,        \
+                                                                            plan.stack_cap);   \
+  } else {                                                                                     \
+    trace_batch_kernel<KK, false, false, kLocalStack><<<b, th, smem, stream>>>(B, run, c,       \
+                                                                             plan.stack_cap);  \
+  }
     switch (k) {
       case kMesh: BZR_BATCH_LAUNCH(kMesh); break;
       case kSpheres: BZR_BATCH_LAUNCH(kSpheres); break;

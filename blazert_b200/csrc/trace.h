@@ -81,11 +81,24 @@ struct BatchView {
   uint32_t *scene_left = nullptr;      // per scene: rays not yet completed (set to scene_rays)
   unsigned long long *scene_done_ns = nullptr;  // per scene completion time (%globaltimer), or null
   unsigned long long *start_ns = nullptr;       // batch start time, or null
+  // coherence sort of each scene's rays (BatchPlan::sort): per scene the origin quantisation
+  // box, and the bits of the sort key that hold the scene index
+  const RaySort *scene_sort = nullptr;
+  uint32_t scene_bits = 0;
 };
+// Scratch of the batch coherence sort: keys and permutation (one word per ray each) and the
+// 2^kSortBits bucket counts.
+struct BatchSortScratch {
+  uint32_t *keys = nullptr, *perm = nullptr, *counts = nullptr;
+};
+constexpr uint32_t kBatchSortMaxScenes = 1u << 12;  // the key keeps at least 4 bits per scene
+constexpr size_t kSortBuckets = size_t(1) << 16;     // buckets of the counting sort (kSortBits)
 struct BatchPlan {
   int sms = 0;
   int threads = kTraceThreads;  // threads per block: 64, 128 or 256
   bool shared_stack = false;    // traversal stack in shared memory even when it fits locally
+  uint32_t local_stack = 64;    // entries of the thread-local stack: 32 or 64 (kLocalStack)
+  bool sort = false;            // coherence sort of each scene's rays before tracing
   int blocks[kNumKinds] = {0, 0, 0, 0};
   int blocks32[kNumKinds] = {0, 0, 0, 0};
   uint32_t stack_cap = 32;
@@ -95,7 +108,8 @@ struct BatchPlan {
 cudaError_t batch_prepare(uint32_t stack_cap, BatchPlan *plan);
 // counters: kNumKinds device words (chunk counters), zeroed here.
 cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const BatchPlan &plan,
-                         cudaStream_t stream, uint32_t *counters);
+                         cudaStream_t stream, uint32_t *counters,
+                         const BatchSortScratch &sort_scratch = BatchSortScratch());
 
 // RayHit defaults for every ray of io (a scene without primitives).
 cudaError_t launch_defaults(const RayIO &io, int sms, cudaStream_t stream);

@@ -184,9 +184,12 @@ int bzr_batch_intersect(bzr_batch *batch, const uint64_t *ray_offsets, const dou
                         void *stream);
 /* Waits for `stream` and reports the batch kernels' error word (as bzr_scene_check). */
 int bzr_batch_check(bzr_batch *batch, void *stream, uint32_t *flags);
-/* Launch shape of the batch's kernels: BZR_TUNE_BLOCK (64, 128, 256 threads per block) or
- * BZR_TUNE_STACK (0 thread-local, 1 shared memory); see bzr_scene_tune.  Drops the cached
- * graph; the next bzr_batch_intersect captures a new one.  Results do not change. */
+/* Launch shape of the batch's kernels: BZR_TUNE_BLOCK (64, 128, 256 threads per block),
+ * BZR_TUNE_STACK (0 thread-local, 1 shared memory), BZR_TUNE_STACK_DEPTH (32 or 64 entries of
+ * the thread-local stack) or BZR_TUNE_SORT (1: each scene's rays are traced in the order of
+ * their direction octant and origin Morton code in the scene's box, sorted inside the graph;
+ * batches of at most 4,096 scenes); see bzr_scene_tune.  Drops the cached graph; the next
+ * bzr_batch_intersect captures a new one.  Results do not change. */
 int bzr_batch_tune(bzr_batch *batch, int option, int64_t value);
 
 /* Adjoint of the closest-hit outputs (no counterpart in the reference): given a batch's
@@ -255,6 +258,9 @@ int bzr_scene_check(const bzr_scene *scene, void *stream, int timeout_ms, uint32
  * memory at launch and reads from there: the first nodes of the breadth-first node array the
  * kernel walks (the FP64 nodes, or the wide nodes of the mixed path), which every ray visits. */
 #define BZR_TUNE_TOP_NODES 10
+/* Entries of the traversal kernels' thread-local stack (batches only, bzr_batch_tune): 32 or
+ * 64 (the default); 32 only when every scene's tree needs at most 32. */
+#define BZR_TUNE_STACK_DEPTH 11
 int bzr_scene_tune(bzr_scene *scene, int option, int64_t value);
 
 /* Statistics of the last commit: per kind (0 mesh, 1 spheres, 2 planes, 3 cylinders) the

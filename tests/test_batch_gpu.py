@@ -70,9 +70,37 @@ def test_batch_tuning_changes_speed_not_results():
             assert mismatches({k: v[a:b] for k, v in got.items()}, ref) == [], s
 
     for cfg in (dict(threads=64), dict(threads=256), dict(shared_stack=True),
-                dict(threads=128, shared_stack=False)):
+                dict(threads=128, shared_stack=False), dict(stack_depth=32), dict(sort=True),
+                dict(sort=True, threads=64, stack_depth=64), dict(sort=False)):
         batch.tune(**cfg)
         check()
     res = autotune_batch(batch, offs, o, d)
-    assert set(res["choice"]) == {"threads", "shared_stack"}
+    assert set(res["choice"]) == {"threads", "shared_stack", "stack_depth", "sort"}
     check()
+
+
+def test_batch_full_size_matches_oracle():
+    """The batching workload at its full size: 256 perturbed icospheres (levels 3-7), each with
+    its own log-uniform ray batch (about 36M rays in all), in one graph replay per mode; every
+    scene's results equal the oracle's (OpenMP over the host cores) bit for bit, in both modes
+    and with the per-scene coherence sort on."""
+    import torch
+
+    wls = W.batched_icospheres()
+    assert len(wls) == 256
+    scenes = [product_scene(w.scene) for w in wls]
+    batch = B.Batch(scenes)
+    offs = np.concatenate([[0], np.cumsum([w.rays.n for w in wls])])
+    assert offs[-1] > 30_000_000
+    o = torch.from_numpy(np.concatenate([w.rays.origins for w in wls])).cuda()
+    d = torch.from_numpy(np.concatenate([w.rays.directions for w in wls])).cuda()
+    outs = {}
+    for mode, sort in (("fp64", False), ("mixed", False), ("mixed", True)):
+        batch.tune(sort=sort)
+        outs[(mode, sort)] = to_numpy(batch.intersect(offs, o, d, mode=mode))
+        assert batch.check() == 0
+    for s, w in enumerate(wls):
+        ref = Oracle(w.scene).intersect(w.rays.origins, w.rays.directions)
+        a, b = offs[s], offs[s + 1]
+        for key, got in outs.items():
+            assert mismatches({k: v[a:b] for k, v in got.items()}, ref) == [], (s, key)
