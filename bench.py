@@ -153,9 +153,10 @@ class ClockSampler:
 
 # Rays of the bounded CPU samples (all host cores; one core), per workload: about 10 s and 5 s
 # of the reference's ray loop.
-CPU_SAMPLE_RAYS = {"heightfield": 1 << 20}
+CPU_SAMPLE_RAYS = {"heightfield": 1 << 20, "adjoint_scene": 1 << 20}
 CPU_ONE_CORE_RAYS = {"heightfield": 1 << 16, "mixed_primitives": 1 << 16,
-                     "icosphere_pinhole": 1 << 18, "adjoint_scene": 1 << 16}
+                     "icosphere_pinhole": 1 << 18, "adjoint_scene": 1 << 16,
+                     "batched_icospheres": 1 << 12}
 
 
 def cpu_baseline(workload, seconds, max_rays=0):
@@ -315,6 +316,24 @@ def run_batched(args):
     total_ms = sum(step_ms)
     lat = np.concatenate(lat)
     value = world * n * args.steps / (total_ms / 1e3) / 1e6
+    # compulsory HBM bytes of a step: every ray's I/O and every scene's FP64 device image once
+    # (internal nodes, triangle index words and vertices)
+    s_bytes = 0
+    for sc, w in zip(scenes, wls):
+        st = sc.build_statistics("mesh")
+        s_bytes += 128 * st["branch_nodes"] + 16 * len(w.scene.mesh["faces"]) + \
+            32 * len(w.scene.mesh["vertices"])
+    hbm_peak, peak_src = load_peaks()
+    mean_ms = statistics.mean(step_ms)
+    hbm_achieved = (n * RAY_IO_BYTES + s_bytes) / (mean_ms / 1e3) / 1e9
+    roofline = {"bound": "latency", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": hbm_achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
+                "what": "compulsory bytes (ray I/O 121 B per ray + each scene's device image "
+                        "once) per step against the measured HBM copy bandwidth; the walk is "
+                        "bound by dependent-load latency, far below it"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline("batched_icospheres", args.cpu_seconds)
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world,
@@ -329,6 +348,7 @@ def run_batched(args):
             "gpu_launches": args.steps * 2,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "max": float(lat.max())},
+            "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clocks, "commit_seconds": commit_s, "tuning": tuning}), flush=True)
     return 0
 
@@ -735,6 +755,13 @@ def run_adjoint(args):
                "h2d_bytes_per_step": n * (24 + 24 + 8),
                "d2h_bytes_per_step": 8 * (3 * nv + 3 * ns + ns + 6 * n)}
 
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the reference has no adjoint: its intersect1 loop over the same rays (the forward
+        # pass only) is the CPU figure
+        cpu = cpu_baseline("adjoint_scene", args.cpu_seconds,
+                           max_rays=CPU_SAMPLE_RAYS.get("adjoint_scene", 0))
+        cpu["what"] = "forward pass only (the reference has no adjoint)"
     if rank == 0:
         print(json.dumps({
             "metric": METRIC + " (forward + adjoint)", "value": value, "unit": "Mrays/s",
@@ -749,7 +776,7 @@ def run_adjoint(args):
             "gpu_launches": args.steps * 4,  # two kind passes, the ray and face adjoint kernels
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_source": peak_src},
-            "clocks": clocks}), flush=True)
+            "cpu_baseline": cpu, "clocks": clocks}), flush=True)
     if pg:
         pg.destroy_process_group()
     return 0

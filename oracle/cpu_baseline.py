@@ -126,6 +126,46 @@ def measure_distance(workload="distance_queries", seconds=10.0, threads=0, max_q
                 seconds_per_batch=med, queries=n, repetitions=len(times))
 
 
+def measure_batched(seconds=10.0, threads=0, max_rays=0, min_reps=3, flavour="bench", stride=8):
+    """The batching workload's sample: every `stride`-th of its 256 scenes (the level mix of the
+    whole batch) with its own rays (at most max_rays per scene when given), each scene's
+    intersect1 loop in turn; Mrays/s over the sample's rays.  The scenes' BVH builds are not
+    timed."""
+    wls = W.batched_icospheres()[::stride]
+    threads = threads or os.cpu_count() or 1
+    kind = "reference" if RefScene.available(flavour) else "port"
+    runs = []
+    for w in wls:
+        rays = w.rays if not max_rays else w.rays.slice(0, min(max_rays, w.rays.n))
+        if kind == "reference":
+            sc = RefScene(w.scene, flavour=flavour)
+            runs.append((rays, lambda sc=sc, r=rays: sc.intersect(
+                r.origins, r.directions, r.tmin, r.tmax, nthreads=threads)["seconds"]))
+        else:
+            sc = Oracle(w.scene)
+
+            def run(sc=sc, r=rays):
+                t0 = time.perf_counter()
+                sc.intersect(r.origins, r.directions, r.tmin, r.tmax, nthreads=threads)
+                return time.perf_counter() - t0
+            runs.append((rays, run))
+    n = sum(r.n for r, _ in runs)
+    for _, run in runs:  # warm-up
+        run()
+    times = []
+    t_end = time.perf_counter() + seconds
+    while len(times) < min_reps or time.perf_counter() < t_end:
+        times.append(sum(run() for _, run in runs))
+        if len(times) >= 1000:
+            break
+    med = statistics.median(times)
+    return dict(value=n / med / 1e6, unit="Mrays/s", cores=threads, kind=kind,
+                sample=f"batched_icospheres: every {stride}th scene ({len(runs)} scenes, "
+                       f"{n} rays) x {len(times)} repetitions ({sum(times):.1f} s of CPU ray "
+                       f"loop), median",
+                seconds_per_batch=med, rays=n, repetitions=len(times), **host_cpu())
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="mixed_primitives")
@@ -134,7 +174,9 @@ def main(argv=None):
     ap.add_argument("--max-rays", type=int, default=0)
     ap.add_argument("--min-reps", type=int, default=3)
     a = ap.parse_args(argv)
-    if a.workload in W.DISTANCE_WORKLOADS:
+    if a.workload == "batched_icospheres":
+        print(json.dumps(measure_batched(a.seconds, a.threads, a.max_rays, a.min_reps)))
+    elif a.workload in W.DISTANCE_WORKLOADS:
         print(json.dumps(measure_distance(a.workload, a.seconds, a.threads, a.max_rays,
                                           a.min_reps)))
     else:

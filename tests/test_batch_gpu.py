@@ -72,7 +72,12 @@ def test_batch_tuning_changes_speed_not_results():
     for cfg in (dict(threads=64), dict(threads=256), dict(shared_stack=True),
                 dict(threads=128, shared_stack=False), dict(stack_depth=32), dict(sort=True),
                 dict(sort=True, threads=64, stack_depth=64), dict(sort=False)):
-        batch.tune(**cfg)
+        try:
+            batch.tune(**cfg)
+        except B.BlazertError as e:  # 32 entries only when every scene's tree fits them
+            assert cfg == dict(stack_depth=32) and e.code == B.EINVAL
+            assert "more than 32" in str(e)
+            continue
         check()
     res = autotune_batch(batch, offs, o, d)
     assert set(res["choice"]) == {"threads", "shared_stack", "stack_depth", "sort"}
