@@ -40,10 +40,12 @@ int cuda_fail(cudaError_t e, const char *what) {
 // Allocations left before the injected failure (bzr_debug_fail_allocation); 0: none armed.
 std::atomic<int64_t> g_alloc_countdown{0};
 
-// Per-call device words: kSlots slots of kSlotWords = {work counter per kind pass (4), error
-// word, 3 spare}; one sticky error word for device-array calls follows the slots.
+// Per-call device words: kSlots slots of kSlotWords = {launch_trace's counters
+// (kTraceCounterWords), error word, 3 spare}; one sticky error word for device-array calls
+// follows the slots.
 constexpr int kSlots = 256;
-constexpr int kSlotWords = 8;
+constexpr int kSlotWords = 16;
+static_assert(bzr::kTraceCounterWords + 4 <= kSlotWords, "slot layout");
 constexpr int kStickyWord = kSlots * kSlotWords;
 // Host-array batches: split into at most host_chunks (default kHostChunks, at most kMaxChunks)
 // chunks of at least host_min_chunk (default kMinChunk) rays.
@@ -705,6 +707,9 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
   // chunks on the round-robin streams may run side by side on smaller grids, so that one
   // chunk's tail idles only its share of the SMs
   bzr::LaunchPlan chunk_plan = s->plan;
+  // chunks run on several streams at once: a pass's blocks that wait in place for the previous
+  // pass would hold SMs that another chunk's kernels could use
+  chunk_plan.early_launch = false;
   for (int k = 0; k < bzr::kNumKinds; ++k) {
     chunk_plan.blocks[k] = std::max(1, chunk_plan.blocks[k] / s->host_grid_div);
     chunk_plan.blocks32[k] = std::max(1, chunk_plan.blocks32[k] / s->host_grid_div);
@@ -736,7 +741,7 @@ static int run_batch(const bzr_scene *cs, size_t n, const double *org, const dou
     ci.prim = d_prim ? d_prim + a : nullptr;
     ci.geom = d_geom ? d_geom + a : nullptr;
     ci.hit = d_hit ? d_hit + a : nullptr;
-    ci.error_word = cnt + bzr::kNumKinds;
+    ci.error_word = cnt + bzr::kTraceCounterWords;
     if (e == cudaSuccess) e = cudaEventRecord(s->ev_in[c], s->copy_in);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(st, s->ev_in[c], 0);
     if (e == cudaSuccess) e = cudaMemsetAsync(ci.error_word, 0, sizeof(uint32_t), st);

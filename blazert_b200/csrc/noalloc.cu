@@ -7,14 +7,15 @@
 // not acceptable: it synchronises the whole device (stalling the host's frame) or fails because
 // the memory budget is already spent.  bzr_intersectN allocates in two places per call -- a
 // stream-ordered scratch for the closest distance carried between the per-kind passes when the
-// caller asks for no distances, and the coherence sort's buffers.  This entry point needs
-// neither allocation: its scratch (the per-pass work counters and that distance carry) lives in
-// one file-scope device array, kScratchBytes long, which every GPU that loads this library holds
+// caller asks for no distances, and one for the coherence sort's buffers and the list of rays a
+// mixed-precision pass hands to its FP64 pass.  This entry point needs no allocation: its
+// scratch (the per-pass work counters, that distance carry and that list) lives in one
+// file-scope device array, kScratchBytes long, which every GPU that loads this library holds
 // until the process exits; it does not sort.
 //
 // Limits and rules:
-//  * at most kMaxRays rays per call (the distance carry is 8 bytes per ray); larger batches are
-//    rejected with BZR_EINVAL -- split them;
+//  * at most kMaxRays rays per call (the distance carry and the list take 12 bytes per ray);
+//    larger batches are rejected with BZR_EINVAL -- split them;
 //  * every array must be device memory of the scene's device; the work is queued on `stream`;
 //  * every call on a device shares the one array and it keeps the last call's contents: the call
 //    clears the work counters it needs on `stream` before its kernels run, but two calls whose
@@ -37,8 +38,10 @@
 namespace {
 
 constexpr size_t kMaxRays = size_t(1) << 20;                  // 1,048,576 rays per call
-constexpr size_t kCounterBytes = 256;                         // per-kind work counters
-constexpr size_t kScratchBytes = kCounterBytes + 8 * kMaxRays;  // 8 MiB + 256 B per device
+constexpr size_t kCounterBytes = 256;  // launch_trace's counters
+constexpr size_t kDeferOffset = kCounterBytes + 8 * kMaxRays;  // after the distance carry
+constexpr size_t kScratchBytes = kDeferOffset + 4 * kMaxRays;  // 12 MiB + 256 B per device
+static_assert(bzr::kTraceCounterWords * sizeof(uint32_t) <= kCounterBytes, "counter words");
 constexpr int kMaxDevices = 64;
 
 // The scratch of every call on this device.  In host code the name is only a stand-in for
@@ -106,6 +109,7 @@ extern "C" int bzr_intersectN_noalloc(const bzr_scene *scene, size_t n, const do
     io.geom = geom_id;
     io.hit = hit;
     io.error_word = h.error_word;
+    io.defer = reinterpret_cast<uint32_t *>(scratch + kDeferOffset);
     bzr::LaunchPlan plan = *h.plan;
     plan.sort.enabled = false;  // the sort would need per-call buffers
     // launch_trace clears the counters on `st` before the kernels run

@@ -107,15 +107,32 @@ __device__ __forceinline__ void prefetch_kind(const KindView &K) {
   }
 }
 
+// Programmatic dependent launch (sm_90 and later): a kernel launched with programmatic stream
+// serialisation may start while the kernel before it on the stream still runs, once every
+// block of that kernel has called griddep_launch_dependents (or exited); griddep_wait blocks
+// until that kernel has completed and its writes are visible.  Both are no-ops for a kernel
+// launched without the attribute.
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void griddep_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // One kind over the whole batch.  first: this pass writes the whole output record.
 // COUNT: also sums the work counters into totals[16] (per kind: box tests, primitive tests,
-// node fetches, leaf fetches; see Counts).  MIXED: rays the FP32 test covers walk the wide
-// image (cylinders always take the FP64 traversal).
+// node fetches, leaf fetches; see Counts).  MIXED: the rays the FP32 test covers walk the wide
+// image; the others are appended to io.defer for the FP64 pass that follows (cylinders always
+// take the FP64 traversal).  Keeping the FP64 walk out of the wide kernel keeps its registers
+// for the wide walk.  io.n_dev: the FP64 pass over a deferred list reads its ray count there.
 template <int KIND, bool COUNT, bool MIXED, bool LOCAL>
 __device__ __forceinline__ void trace_kind_body(const SceneView &S, const RayIO &io, int first,
                                                 uint32_t *work_counter,
                                                 unsigned long long *totals) {
   constexpr bool kWide = MIXED && KIND != kCylinders;
+  // The next kernel on the stream may be scheduled now: it waits (griddep_wait) for this grid
+  // to complete before it reads anything this grid writes.
+  griddep_launch_dependents();
   extern __shared__ __align__(16) unsigned char smem[];
   double lkey[LOCAL ? kLocalStack : 1];
   uint32_t lref[LOCAL ? kLocalStack : 1];
@@ -123,24 +140,26 @@ __device__ __forceinline__ void trace_kind_body(const SceneView &S, const RayIO 
   uint32_t tid;
   init_stack<LOCAL>(sk, tid, S.stack_cap, smem, lkey, lref);
   const KindView &K = S.k[KIND];
-  if (!COUNT) prefetch_kind<KIND, kWide>(K);
+  // (a deferred list is short: its pass leaves L2 to the rays)
+  if (!COUNT && !io.n_dev) prefetch_kind<KIND, kWide>(K);
   // The first io.top_nodes nodes of the array this kernel walks (the top levels every ray
-  // visits) are staged in shared memory after the stack.  Rays of a mixed kernel that take
-  // the FP64 walk use the global FP64 nodes (sk64 has no staged nodes then).
-  const bool walk_wide = kWide && K.mixed_ok;
-  Stack sk64 = sk;
+  // visits) are staged in shared memory after the stack.
   {
-    const uint32_t avail = walk_wide ? K.n_wide : K.n_internal;
+    const uint32_t avail = kWide ? K.n_wide : K.n_internal;
     const uint32_t n_top = io.top_nodes < avail ? io.top_nodes : avail;
     uint4 *top = reinterpret_cast<uint4 *>(smem + stack_smem_bytes<LOCAL>(S.stack_cap));
-    const uint4 *src = walk_wide ? reinterpret_cast<const uint4 *>(K.wide)
-                                 : reinterpret_cast<const uint4 *>(K.nodes64);
+    const uint4 *src = kWide ? reinterpret_cast<const uint4 *>(K.wide)
+                             : reinterpret_cast<const uint4 *>(K.nodes64);
     for (uint32_t j = threadIdx.x; j < n_top * 8; j += blockDim.x) top[j] = ldg(src + j);
     if (n_top) __syncthreads();
     sk.top = top;
     sk.n_top = n_top;
-    if (!walk_wide) sk64 = sk;
   }
+  // Up to here only the scene was read; the counters, the rays' closest distances and the
+  // deferred list come from earlier kernels of the stream.
+  griddep_wait();
+  const uint32_t n = io.n_dev ? *io.n_dev : io.n;
+  if (n == 0) return;  // the same for every thread of the grid
   const unsigned lane = threadIdx.x & 31u;
   const unsigned below = (1u << lane) - 1u;
   uint32_t pool_next = 0, pool_end = 0;  // warp-uniform
@@ -150,61 +169,69 @@ __device__ __forceinline__ void trace_kind_body(const SceneView &S, const RayIO 
   Ray r;
   RayW f;
   float hl = 0.0f;
-  bool use32 = false;
   KState st;
   Trav tv;
   Counts cnt = {};
   for (;;) {
-    const unsigned idle = __ballot_sync(kFull, !active);
-    if (idle && !exhausted) {
-      const uint32_t want = __popc(idle), avail = pool_end - pool_next;
-      // rays taken per fetch: io.chunk (>= 32, so one fetch serves every idle lane), or with
-      // io.chunk == 0 exactly the number of idle lanes the pool cannot serve
-      const uint32_t take = io.chunk ? io.chunk : want - avail;
-      uint32_t base = 0;
-      if (want > avail) {
-        if (lane == 0) base = atomicAdd(work_counter, take);
-        base = __shfl_sync(kFull, base, 0);
-      }
-      if (!active) {
-        const uint32_t rank = __popc(idle & below);
-        const uint32_t idx = rank < avail ? pool_next + rank : base + (rank - avail);
-        if (idx < io.n) {
-          i = io.perm ? io.perm[idx] : idx;
-          active = true;
-          r = make_ray(io.org + 3 * size_t(i), io.dir + 3 * size_t(i), io.tmin ? io.tmin[i] : 0.0,
-                       io.tmax ? io.tmax[i] : kDblMax);
-          r.any_hit = io.any_hit != 0;
-          if constexpr (kWide) {
-            f = make_ray_w(r);
-            use32 = K.mixed_ok && f.ok;
+    for (;;) {  // refill the idle lanes; repeats only after a lane handed its ray on
+      const unsigned idle = __ballot_sync(kFull, !active);
+      bool deferred = false;
+      if (idle && !exhausted) {
+        const uint32_t want = __popc(idle), avail = pool_end - pool_next;
+        // rays taken per fetch: io.chunk (>= 32, so one fetch serves every idle lane), or
+        // with io.chunk == 0 exactly the number of idle lanes the pool cannot serve
+        const uint32_t take = io.chunk ? io.chunk : want - avail;
+        uint32_t base = 0;
+        if (want > avail) {
+          if (lane == 0) base = atomicAdd(work_counter, take);
+          base = __shfl_sync(kFull, base, 0);
+        }
+        if (!active) {
+          const uint32_t rank = __popc(idle & below);
+          const uint32_t idx = rank < avail ? pool_next + rank : base + (rank - avail);
+          if (idx < n) {
+            i = io.perm ? io.perm[idx] : idx;
+            active = true;
+            r = make_ray(io.org + 3 * size_t(i), io.dir + 3 * size_t(i),
+                         io.tmin ? io.tmin[i] : 0.0, io.tmax ? io.tmax[i] : kDblMax);
+            r.any_hit = io.any_hit != 0;
+            if constexpr (kWide) {
+              f = make_ray_w(r);
+              if (K.mixed_ok && f.ok) {
+                wtrav_begin<KIND, COUNT>(K, r, f, st, hl, tv, &cnt);
+              } else {
+                io.defer[atomicAdd(io.defer_count, 1u)] = i;
+                active = false;
+                deferred = true;
+              }
+            } else {
+              trav_begin<KIND, COUNT>(K, r, st, tv, &cnt);
+            }
           }
-          if (kWide && use32)
-            wtrav_begin<KIND, COUNT>(K, r, f, st, hl, tv, &cnt);
-          else
-            trav_begin<KIND, COUNT>(K, r, st, tv, &cnt);
+        }
+        if (want > avail) {
+          pool_next = base + (want - avail);
+          pool_end = base + take;
+          if (base >= n) exhausted = true;
+        } else {
+          pool_next += want;
         }
       }
-      if (want > avail) {
-        pool_next = base + (want - avail);
-        pool_end = base + take;
-        if (base >= io.n) exhausted = true;
-      } else {
-        pool_next += want;
-      }
+      if (!kWide || !__any_sync(kFull, deferred)) break;
     }
+    // every lane idle: the global counter has passed the end of the batch
     if (!__any_sync(kFull, active)) break;
     if (active) {
-      if (kWide && use32) {
+      if constexpr (kWide) {
         if (tv.live) wtrav_to_leaf<KIND, COUNT>(K, f, hl, tv, sk, tid, io.error_word, &cnt);
         while (tv.live && tv.post != kNoLeaf)
           wtrav_leaf<KIND, COUNT>(K, r, f, st, hl, tv, sk, tid, io.error_word, &cnt);
       } else {
-        if (tv.live) trav_to_leaf<KIND, COUNT>(K, r, st, tv, sk64, tid, io.error_word, &cnt);
-        if (tv.live) trav_leaf<KIND, COUNT>(K, r, st, tv, sk64, tid, io.error_word, &cnt);
+        if (tv.live) trav_to_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, io.error_word, &cnt);
+        if (tv.live) trav_leaf<KIND, COUNT>(K, r, st, tv, sk, tid, io.error_word, &cnt);
       }
       if (!tv.live) {
-        if (kWide && use32) wtrav_end<KIND>(K, r, st);
+        if constexpr (kWide) wtrav_end<KIND>(K, r, st);
         finalize_kind<KIND>(S, r, st, i, first != 0, io.t, io.uv, io.normal, io.prim, io.geom,
                             io.hit);
         active = false;
@@ -459,30 +486,61 @@ inline bool use_local(const SceneView &S, const LaunchPlan &plan) {
   return !plan.shared_stack && S.stack_cap <= kLocalStack;
 }
 
+// Whether a pass of KIND in `mode` walks the wide image (and defers the rays it cannot).
+template <int KIND>
+bool walks_wide(const SceneView &S, int mode) {
+  return mode == kModeMixed && KIND != kCylinders && S.k[KIND].present && S.k[KIND].n_prims &&
+         S.k[KIND].mixed_ok;
+}
+
+using TraceFn = void (*)(SceneView, RayIO, int, uint32_t *, unsigned long long *);
+
+// One trace kernel on `stream`; early: launched with programmatic stream serialisation (the
+// kernel before it on the stream is a trace kernel of the same call; see griddep_wait).
+cudaError_t launch_one(TraceFn fn, int blocks, int threads, size_t smem, cudaStream_t stream,
+                       bool early, const SceneView &S, const RayIO &io, int first,
+                       uint32_t *counter, unsigned long long *totals) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(blocks));
+  cfg.blockDim = dim3(unsigned(threads));
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = early ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, fn, S, io, first, counter, totals);
+}
+
+// The pass of one kind: one kernel, or for a wide walk the wide kernel and then the FP64
+// kernel over the rays it deferred.  counters: the kTraceCounterWords words of the call;
+// after_trace: a trace kernel of this call precedes the pass on the stream.
 template <int KIND, bool COUNT>
-cudaError_t launch_kind(const SceneView &S, const RayIO &io, int mode, int first, int blocks,
-                        const LaunchPlan &plan, cudaStream_t stream, uint32_t *counter,
-                        unsigned long long *totals) {
-  const bool mixed = mode == kModeMixed && KIND != kCylinders;
+cudaError_t launch_kind(const SceneView &S, const RayIO &io, int mode, int first,
+                        bool after_trace, const LaunchPlan &plan, cudaStream_t stream,
+                        uint32_t *counters, unsigned long long *totals) {
   const int th = plan.threads;
-  if (!COUNT && use_local(S, plan)) {
-    const size_t smem = trace_kind_smem(S.stack_cap, th, true, io.top_nodes);
-    if (mixed)
-      trace_kernel<KIND, false, true, true>()<<<blocks, th, smem, stream>>>(S, io, first,
-                                                                              counter, totals);
-    else
-      trace_kernel<KIND, false, false, true>()<<<blocks, th, smem, stream>>>(S, io, first,
-                                                                               counter, totals);
-  } else {
-    const size_t smem = trace_kind_smem(S.stack_cap, th, false, io.top_nodes);
-    if (mixed)
-      trace_kernel<KIND, COUNT, true, false>()<<<blocks, th, smem, stream>>>(S, io, first,
-                                                                               counter, totals);
-    else
-      trace_kernel<KIND, COUNT, false, false>()<<<blocks, th, smem, stream>>>(S, io, first,
-                                                                                counter, totals);
-  }
-  return cudaGetLastError();
+  const bool local = !COUNT && use_local(S, plan);
+  const size_t smem = trace_kind_smem(S.stack_cap, th, local, io.top_nodes);
+  const bool early = after_trace && plan.early_launch;
+  const TraceFn fp64 = local ? trace_kernel<KIND, false, false, true>()
+                             : trace_kernel<KIND, COUNT, false, false>();
+  if (!walks_wide<KIND>(S, mode))
+    return launch_one(fp64, plan.blocks[KIND], th, smem, stream, early, S, io, first,
+                      counters + KIND, totals);
+  const TraceFn wide_fn = local ? trace_kernel<KIND, false, true, true>()
+                                : trace_kernel<KIND, COUNT, true, false>();
+  RayIO wide = io;
+  wide.defer_count = counters + kNumKinds + KIND;
+  RayIO rest = io;
+  rest.perm = io.defer;  // ray indices
+  rest.n_dev = wide.defer_count;
+  const cudaError_t e = launch_one(wide_fn, plan.blocks32[KIND], th, smem, stream, early, S,
+                                   wide, first, counters + KIND, totals);
+  if (e != cudaSuccess) return e;
+  return launch_one(fp64, plan.blocks[KIND], th, smem, stream, plan.early_launch, S, rest, first,
+                    counters + 2 * kNumKinds + KIND, totals);
 }
 
 // Resident blocks per SM of `fn` with `threads` per block and `smem` bytes of dynamic shared
@@ -566,17 +624,27 @@ int trace_passes(const SceneView &S) {
 
 cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const LaunchPlan &plan,
                          cudaStream_t stream, uint32_t *counters, unsigned long long *totals) {
-  cudaError_t e = cudaMemsetAsync(counters, 0, kNumKinds * sizeof(uint32_t), stream);
+  cudaError_t e = cudaMemsetAsync(counters, 0, kTraceCounterWords * sizeof(uint32_t), stream);
   if (e != cudaSuccess) return e;
   RayIO sorted = io;
   sorted.chunk = plan.chunk;
   sorted.top_nodes = plan.top_nodes;
+  sorted.n_dev = nullptr;
+  // scratch from the pool: the sort's keys, permutation and bucket counts, then the deferred
+  // list of the wide passes unless the caller gave one
+  const bool sort = plan.sort.enabled && io.n >= plan.sort_min_rays && trace_passes(S) > 0;
+  const bool defer = !io.defer && (walks_wide<kMesh>(S, mode) || walks_wide<kSpheres>(S, mode) ||
+                                   walks_wide<kPlanes>(S, mode));
+  const size_t nb = size_t(1) << kSortBits;
+  const size_t sort_words = sort ? 2 * size_t(io.n) + nb : 0;
   uint32_t *scratch = nullptr;
-  if (plan.sort.enabled && io.n >= plan.sort_min_rays && trace_passes(S) > 0) {
-    const size_t nb = size_t(1) << kSortBits;
-    e = bzr::pool_malloc(&scratch,
-                                (2 * size_t(io.n) + nb) * sizeof(uint32_t), plan.pool, stream);
+  if (sort || defer) {
+    e = bzr::pool_malloc(&scratch, (sort_words + (defer ? io.n : 0)) * sizeof(uint32_t),
+                         plan.pool, stream);
     if (e != cudaSuccess) return e;
+    if (defer) sorted.defer = scratch + sort_words;
+  }
+  if (sort) {
     uint32_t *keys = scratch, *perm = scratch + io.n, *counts = scratch + 2 * size_t(io.n);
     e = cudaMemsetAsync(counts, 0, nb * sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
@@ -591,34 +659,37 @@ cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const La
   int first = 1;
   for (int k = 0; k < kNumKinds; ++k) {
     if (!S.k[k].present || S.k[k].n_prims == 0) continue;
-    const int b = mode == kModeMixed && k != kCylinders ? plan.blocks32[k] : plan.blocks[k];
-    uint32_t *c = counters + k;
+    uint32_t *c = counters;
+    const bool after = !first;
     switch (k) {
       case kMesh:
-        e = totals ? launch_kind<kMesh, true>(S, run, mode, first, b, plan, stream, c, totals)
-                   : launch_kind<kMesh, false>(S, run, mode, first, b, plan, stream, c, nullptr);
+        e = totals ? launch_kind<kMesh, true>(S, run, mode, first, after, plan, stream, c, totals)
+                   : launch_kind<kMesh, false>(S, run, mode, first, after, plan, stream, c,
+                                               nullptr);
         break;
       case kSpheres:
-        e = totals
-                ? launch_kind<kSpheres, true>(S, run, mode, first, b, plan, stream, c, totals)
-                : launch_kind<kSpheres, false>(S, run, mode, first, b, plan, stream, c, nullptr);
+        e = totals ? launch_kind<kSpheres, true>(S, run, mode, first, after, plan, stream, c,
+                                                 totals)
+                   : launch_kind<kSpheres, false>(S, run, mode, first, after, plan, stream, c,
+                                                  nullptr);
         break;
       case kPlanes:
-        e = totals
-                ? launch_kind<kPlanes, true>(S, run, mode, first, b, plan, stream, c, totals)
-                : launch_kind<kPlanes, false>(S, run, mode, first, b, plan, stream, c, nullptr);
-        break;
-      default:
-        e = totals
-                ? launch_kind<kCylinders, true>(S, run, mode, first, b, plan, stream, c, totals)
-                : launch_kind<kCylinders, false>(S, run, mode, first, b, plan, stream, c,
+        e = totals ? launch_kind<kPlanes, true>(S, run, mode, first, after, plan, stream, c,
+                                                totals)
+                   : launch_kind<kPlanes, false>(S, run, mode, first, after, plan, stream, c,
                                                  nullptr);
         break;
+      default:
+        e = totals ? launch_kind<kCylinders, true>(S, run, mode, first, after, plan, stream, c,
+                                                   totals)
+                   : launch_kind<kCylinders, false>(S, run, mode, first, after, plan, stream, c,
+                                                    nullptr);
+        break;
     }
-    if (e != cudaSuccess) return e;
+    if (e != cudaSuccess) break;  // the scratch is still released below
     first = 0;
   }
-  if (first) {  // nothing to trace
+  if (first && e == cudaSuccess) {  // nothing to trace
     const int threads = 256;
     const uint64_t want = (uint64_t(io.n) + threads - 1) / threads;
     const int blocks = int(want < uint64_t(plan.sms) * 8 ? want : uint64_t(plan.sms) * 8);

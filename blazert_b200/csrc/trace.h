@@ -14,6 +14,10 @@ constexpr int kMaxTraceThreads = 256;  // largest block the trace kernels are co
 constexpr uint32_t kRayChunk = 32;     // default rays a warp takes from the global counter
 constexpr int kModeFp64 = 0;   // BZR_MODE_FP64
 constexpr int kModeMixed = 1;  // BZR_MODE_MIXED
+// Device words launch_trace takes per call: the work counter of each kind's pass, then for
+// each kind the count of rays its mixed pass deferred and the work counter of the FP64 pass
+// over them.
+constexpr int kTraceCounterWords = 3 * kNumKinds;
 
 // Device pointers of one batch.  tmin / tmax may be null (0 and DBL_MAX); each output except t
 // may be null.  error_word collects kErr* bits.
@@ -35,6 +39,12 @@ struct RayIO {
   uint32_t chunk = kRayChunk;      // rays a warp takes per fetch: 32, 64, 128, or 0 for
                                    // exactly the lanes that are idle
   uint32_t top_nodes = 0;          // top-level nodes each block stages in shared memory
+  // Mixed-precision passes: rays the FP32 walk does not cover are appended to defer (one
+  // word per ray of the batch, or null for launch_trace to take it from plan.pool) and traced
+  // by an FP64 pass over that list right after.  Set by launch_trace.
+  uint32_t *defer = nullptr;
+  uint32_t *defer_count = nullptr;
+  const uint32_t *n_dev = nullptr;  // when set, the pass's ray count is *n_dev (not n)
 };
 
 // Coherence sort of a batch: rays are processed in the order of a 32-bit key -- the direction
@@ -55,6 +65,9 @@ struct LaunchPlan {
   bool shared_stack = false;       // traversal stack in shared memory even when it fits locally
   uint32_t chunk = kRayChunk;      // rays per warp fetch: 32, 64, 128 or 0 (exactly the idle lanes)
   uint32_t top_nodes = 0;          // top-level nodes each block stages in shared memory (0..256)
+  // the trace kernels after a call's first one are launched with programmatic stream
+  // serialisation: each is resident when its predecessor ends (it waits for it on the device)
+  bool early_launch = true;
   int blocks[kNumKinds] = {0, 0, 0, 0};    // FP64 kernels
   int blocks32[kNumKinds] = {0, 0, 0, 0};  // mixed-precision kernels
   RaySort sort;
@@ -126,9 +139,14 @@ int trace_passes(const SceneView &S);
 // be non-null when trace_passes(S) > 1 (it carries the closest distance between passes).
 // When plan.sort.enabled and the batch has at least plan.sort_min_rays rays, a coherence sort
 // runs first (scratch from plan.pool, stream-ordered).
-// counters: kNumKinds device words, zeroed here.  totals (device, 8 x uint64, or null): when
-// given, the counting kernels add per kind the box tests (totals[0..3]) and primitive tests
-// (totals[4..7]) of every ray.
+// counters: kTraceCounterWords device words, zeroed here.  totals (device, 8 x uint64, or
+// null): when given, the counting kernels add per kind the box tests (totals[0..3]) and
+// primitive tests (totals[4..7]) of every ray.
+// A mixed-precision pass of a kind whose wide image exists is two kernels: the wide walk over
+// the batch, which appends the rays its FP32 test does not cover (a direction component of 0
+// or below 2^-40 in magnitude, an origin coordinate or tmin beyond 1e18, NaN) to io.defer,
+// then the FP64 walk over that list.  io.defer may carry io.n words of scratch; null takes
+// them from plan.pool.
 cudaError_t launch_trace(const SceneView &S, const RayIO &io, int mode, const LaunchPlan &plan,
                          cudaStream_t stream, uint32_t *counters,
                          unsigned long long *totals = nullptr);

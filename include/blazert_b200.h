@@ -155,7 +155,7 @@ int bzr_intersectN_ex(const bzr_scene *scene, size_t n, const double *origins,
  * application's frame loop, where a cudaMalloc/cudaFree would synchronise the whole device, or
  * a service whose device memory budget is handed out up front.  Same arguments and results as
  * bzr_intersectN, but device arrays only, at most 1,048,576 rays per call (larger batches get
- * BZR_EINVAL), and no coherence sort.  The call allocates nothing: its scratch is one 8 MiB
+ * BZR_EINVAL), and no coherence sort.  The call allocates nothing: its scratch is one 12 MiB
  * static device array per GPU, held until the process exits.  All calls on a device share that
  * array; calls whose GPU work overlaps race -- order them on one stream.  The first call on each
  * device looks up the array's address and keeps it; make it before any stream capture, and do

@@ -134,3 +134,34 @@ def golden_image_classes():
     red = np.unpackbits(g["red"])[:n].reshape(hh, ww).astype(bool)
     green = np.unpackbits(g["green"])[:n].reshape(hh, ww).astype(bool)
     return np.where(red, 1, np.where(green, 2, 0))
+
+
+def uncovered_workload(n_rays=200_000, seed=41):
+    """All four kinds overlapping in space, with rays that the FP32 walk of the mixed mode does
+    not cover mixed among ordinary ones (a mixed pass hands them to its FP64 pass): axis
+    directions (two zero components), one zero component, a component of 1e-13 (its inverse is
+    above 2^40), an origin 2e18 back along the ray, and ordinary rays.  Returns the workload and
+    the class of each ray (0 ordinary, 1 axis, 2 one zero, 3 tiny, 4 far origin)."""
+    from blazert_b200 import workloads as W
+
+    wl = W.mixed_primitives(n_rays=n_rays, n_spheres=2000, n_cylinders=400, n_planes=60, seed=seed)
+    v, f = W.icosphere(3)
+    spec = W.SceneSpec().add_mesh(v * 60.0, f)
+    for k in wl.scene.order:
+        getattr(spec, "add_" + k)(*getattr(wl.scene, k).values())
+    rng = np.random.default_rng(seed)
+    o, d = wl.rays.origins.copy(), wl.rays.directions.copy()
+    cls = rng.integers(0, 5, n_rays)
+    rows = np.arange(n_rays)
+    big, small = np.argmax(np.abs(d), 1), np.argmin(np.abs(d), 1)
+    axis = np.zeros_like(d)
+    axis[rows, big] = np.sign(d[rows, big])
+    d = np.where((cls == 1)[:, None], axis, d)
+    one = cls == 2
+    d[rows[one], small[one]] = 0.0
+    tiny = cls == 3
+    d[rows[tiny], small[tiny]] = np.copysign(1e-13, d[rows[tiny], small[tiny]])
+    far = cls == 4
+    o[far] = o[far] - 2e18 * d[far]
+    rays = W.RayBatch(o, d, np.zeros(n_rays), np.full(n_rays, np.inf))
+    return W.Workload("uncovered_rays", spec, rays, {}), cls

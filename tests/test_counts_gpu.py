@@ -7,14 +7,16 @@ import pytest
 
 from blazert_b200 import workloads as W
 from tests.emu.emu import EmuScene
-from tests.helpers import product_scene
+from tests.helpers import product_scene, uncovered_workload
 
 pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("mode", ["fp64", "mixed"])
-@pytest.mark.parametrize("name", ["icosphere_pinhole", "mixed_primitives", "heightfield"])
+@pytest.mark.parametrize("name", ["icosphere_pinhole", "mixed_primitives", "heightfield",
+                                  "uncovered_rays"])
 def test_device_counts_equal_emulator(name, mode):
+    """(uncovered_rays: rays the mixed passes hand to their FP64 passes, which count them.)"""
     import torch
 
     kw = {"n_rays": 200_000}
@@ -22,7 +24,10 @@ def test_device_counts_equal_emulator(name, mode):
         kw["grid"] = 512
     if name == "icosphere_pinhole":
         kw = {}
-    wl = W.WORKLOADS[name](**kw)
+    if name == "uncovered_rays":
+        wl = uncovered_workload()[0]
+    else:
+        wl = W.WORKLOADS[name](**kw)
     R = wl.rays
     s = product_scene(wl.scene)
     dev = torch.device("cuda", 0)

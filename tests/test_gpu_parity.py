@@ -277,3 +277,66 @@ def test_small_host_batches():
     hit = ref["hit"].astype(bool)
     assert np.array_equal(prim[hit], ref["prim"][hit])
     assert np.array_equal(t.view(np.uint64), np.asarray(ref["t"]).view(np.uint64))
+
+
+def test_mixed_defers_uncovered_rays():
+    """Rays the FP32 walk does not cover (zero and tiny direction components, far origins),
+    mixed among ordinary rays on a scene of all four kinds: the mixed passes hand them to their
+    FP64 passes, and every form of the call equals the oracle -- device arrays, host arrays (the
+    latency path and the chunked pipeline), a sorted batch, shared-memory stacks, any-hit rays,
+    and the entry point without allocations, whose scratch carries the list."""
+    import ctypes as C
+
+    import torch
+
+    import blazert_b200 as B
+    from tests.helpers import uncovered_workload
+
+    wl, cls = uncovered_workload()
+    R = wl.rays
+    orc = Oracle(wl.scene)
+    ref = orc.intersect(R.origins, R.directions, R.tmin, R.tmax)
+    ref_any = orc.intersect(R.origins, R.directions, R.tmin, R.tmax, any_hit=True)
+    for c in range(1, 5):
+        assert ref["hit"][cls == c].sum() > 100
+    s = product_scene(wl.scene)
+    dev = torch.device("cuda", 0)
+    o, d = torch.from_numpy(R.origins).to(dev), torch.from_numpy(R.directions).to(dev)
+    tmn, tmx = torch.from_numpy(R.tmin).to(dev), torch.from_numpy(R.tmax).to(dev)
+    for cfg in (dict(sort=False), dict(sort=True, sort_min_rays=0), dict(shared_stack=True)):
+        s.tune(**cfg)
+        out = s.intersectN(o, d, tmn, tmx, mode="mixed")
+        torch.cuda.synchronize()
+        assert s.check() == 0
+        assert mismatches(out, ref) == [], cfg
+        out = s.intersectN(o, d, tmn, tmx, mode="mixed", any_hit=True)
+        torch.cuda.synchronize()
+        assert mismatches(out, ref_any) == [], cfg
+    s.tune(sort=False)
+    assert mismatches(s.intersectN(R.origins, R.directions, R.tmin, R.tmax, mode="mixed"), ref) == []
+    few = {k: v[:500] for k, v in ref.items()}
+    assert mismatches(s.intersectN(R.origins[:500], R.directions[:500], R.tmin[:500],
+                                   R.tmax[:500], mode="mixed"), few) == []
+    lib = B.library()
+    lib.bzr_intersectN_noalloc.argtypes = [C.c_void_p, C.c_size_t] + [C.c_void_p] * 10 + \
+        [C.c_int, C.c_void_p]
+    n = R.n
+    f64 = torch.float64
+    got = dict(t=torch.empty(n, dtype=f64, device=dev), uv=torch.empty((n, 2), dtype=f64, device=dev),
+               normal=torch.empty((n, 3), dtype=f64, device=dev),
+               prim=torch.empty(n, dtype=torch.int32, device=dev),
+               geom=torch.empty(n, dtype=torch.int32, device=dev),
+               hit=torch.empty(n, dtype=torch.uint8, device=dev))
+    ptr = lambda a: C.c_void_p(a.data_ptr())
+    for _ in range(2):
+        for v in got.values():
+            v.fill_(7)
+        rc = lib.bzr_intersectN_noalloc(s._h, n, ptr(o), ptr(d), ptr(tmn), ptr(tmx), ptr(got["t"]),
+                                        ptr(got["uv"]), ptr(got["normal"]), ptr(got["prim"]),
+                                        ptr(got["geom"]), ptr(got["hit"]), 1,
+                                        C.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+        assert rc == 0
+        torch.cuda.synchronize()
+        assert mismatches(got, ref) == []
+    assert s.check() == 0
+    s.close()
