@@ -524,6 +524,11 @@ def run_ours(args):
             "step_ms_min_max": [min(res["mixed"]["step_ms"]), max(res["mixed"]["step_ms"])]}
     # one traversal kernel per primitive kind present, per step
     n_passes = sum(1 for k in wl.scene.order if len(next(iter(getattr(wl.scene, k).values()))))
+    # kernels per call: one per kind present; in the mixed mode the triangle, sphere and plane
+    # passes add the FP64 pass over the rays their FP32 test does not cover
+    n_wide = sum(1 for k in wl.scene.order
+                 if k != "cylinders" and len(next(iter(getattr(wl.scene, k).values()))))
+    launches_per_call = {"fp64": n_passes, "mixed": n_passes + n_wide}
 
     # roofline of the primary path's traversal kernel.  Algorithmic bytes from the kernel's own
     # work counts (untimed counting run): ray I/O + 64 B per box test (half a 128-byte two-child
@@ -623,7 +628,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)", "config": config_of(args, wl, world, primary),
-            "e2e": e2e, "gpu_launches": args.steps * n_passes * len(modes),
+            "e2e": e2e, "gpu_launches": args.steps * sum(launches_per_call[m] for m in modes),
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "hit_fraction": hits,
             "precision": precision, "commit_seconds": commit_s, "wall_seconds_timed": wall,
             "tuning": res[primary]["tuning"], "step_ms_min_max": [min(step_ms), max(step_ms)],
