@@ -323,7 +323,7 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
     return off;
   };
   size_t off_nodes64[4], off_wide[4], off_leaves[4], off_payload[4], off_ids[4], off_tri[4],
-      off_tv[4], off_pos[4];
+      off_tv[4], off_pos[4], off_vnorm[4];
   uint32_t wide_stack = 0;
   for (int k = 0; k < bzr::kNumKinds; ++k) {
     off_nodes64[k] = place(img[k].nodes64.data(), img[k].nodes64.size() * sizeof(double));
@@ -335,6 +335,7 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
     off_pos[k] = place(img[k].pos_of.data(), img[k].pos_of.size() * sizeof(uint32_t));
     off_tri[k] = place(img[k].tri.data(), img[k].tri.size() * sizeof(uint32_t));
     off_tv[k] = place(img[k].verts.data(), img[k].verts.size() * sizeof(double));
+    off_vnorm[k] = place(img[k].vnorm.data(), img[k].vnorm.size() * sizeof(double));
   }
   const size_t off_faces = place(s->host.faces.data(), s->host.faces.size() * sizeof(uint32_t));
   const size_t off_vn = place(s->host.vert_n.data(), s->host.vert_n.size() * sizeof(double));
@@ -381,6 +382,7 @@ static int commit_scene(bzr_scene *s, uint32_t flags, bool trees_given) {
     v.pos_of = reinterpret_cast<const uint32_t *>(base + off_pos[k]);
     v.tri = reinterpret_cast<const uint32_t *>(base + off_tri[k]);
     v.verts = reinterpret_cast<const double *>(base + off_tv[k]);
+    v.vnorm = reinterpret_cast<const double *>(base + off_vnorm[k]);
     v.n_internal = img[k].n_internal;
     v.n_prims = static_cast<uint32_t>(img[k].prim_ids.size());
     v.n_verts = static_cast<uint32_t>(img[k].verts.size() / bzr::kVertexDoubles);

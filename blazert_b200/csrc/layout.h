@@ -81,6 +81,8 @@ struct KindView {
   const double *payload = nullptr;  // n_prims * kPayloadDoubles[kind] (spheres, planes, cylinders)
   const uint32_t *tri = nullptr;    // triangles: n_prims * 4 {i0, i1, i2, id word}
   const double *verts = nullptr;    // triangles: kVertexDoubles per vertex {x, y, z, 0}
+  const double *vnorm = nullptr;    // triangles: kVertexDoubles per vertex of verts: its vertex
+                                    // normal {nx, ny, nz, 0}
   const uint32_t *prim_ids = nullptr;  // n_prims: id | kLastBit on a leaf's last primitive
   const uint32_t *pos_of = nullptr;    // n_prims: leaf-ordered position of each primitive id
   uint32_t n_internal = 0;

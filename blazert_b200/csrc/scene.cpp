@@ -282,8 +282,8 @@ constexpr size_t kFacesPerRange = size_t(1) << 14;
 constexpr size_t kMaxRangeWorkers = 16;
 
 // Mesh part of the image: the vertices numbered in order of first use by the leaf-ordered
-// triangles (use u = 3 at + j for corner j of the triangle at position at), stored once each,
-// and per triangle {i0, i1, i2, id word}.  With several workers this takes four passes over
+// triangles (use u = 3 at + j for corner j of the triangle at position at), stored once each
+// with their vertex normals in the same numbering, and per triangle {i0, i1, i2, id word}.  With several workers this takes four passes over
 // ranges of triangles: the first use of every vertex (an atomic minimum), the number of first
 // uses in each range, the vertex numbers from the prefix sums of those counts, and the
 // triangles' indices.  Both ways give the same numbering.
@@ -294,6 +294,7 @@ void number_vertices(const HostScene &s, KindImage *img, size_t workers) {
   if (workers <= 1 || 3 * uint64_t(np) >= kNone) {
     std::vector<uint32_t> remap(nv, kNone);
     img->verts.reserve(kVertexDoubles * std::min(nv, 3 * np));
+    img->vnorm.reserve(kVertexDoubles * std::min(nv, 3 * np));
     for (size_t at = 0; at < np; ++at) {
       const uint32_t *F = &s.faces[3 * size_t(img->prim_ids[at] & kIdMask)];
       for (int j = 0; j < 3; ++j) {
@@ -302,6 +303,8 @@ void number_vertices(const HostScene &s, KindImage *img, size_t workers) {
           r = static_cast<uint32_t>(img->verts.size() / kVertexDoubles);
           const double *v = &s.vertices[3 * size_t(F[j])];
           img->verts.insert(img->verts.end(), {v[0], v[1], v[2], 0.0});
+          const double *vn = &s.vert_n[3 * size_t(F[j])];
+          img->vnorm.insert(img->vnorm.end(), {vn[0], vn[1], vn[2], 0.0});
         }
         img->tri[4 * at + j] = r;
       }
@@ -338,6 +341,7 @@ void number_vertices(const HostScene &s, KindImage *img, size_t workers) {
   });
   for (size_t w = 0; w < workers; ++w) base[w + 1] += base[w];
   img->verts.resize(kVertexDoubles * base[workers]);
+  img->vnorm.resize(kVertexDoubles * base[workers]);
   RawVector<uint32_t> number(nv);  // read only for the vertices numbered below
   run_ranges(np, workers, [&](size_t a0, size_t a1, size_t w) {
     auto r = static_cast<uint32_t>(base[w]);
@@ -352,6 +356,12 @@ void number_vertices(const HostScene &s, KindImage *img, size_t workers) {
         o[1] = v[1];
         o[2] = v[2];
         o[3] = 0.0;
+        const double *vn = &s.vert_n[3 * size_t(F[j])];
+        double *on = &img->vnorm[kVertexDoubles * size_t(r)];
+        on[0] = vn[0];
+        on[1] = vn[1];
+        on[2] = vn[2];
+        on[3] = 0.0;
         ++r;
       }
     }

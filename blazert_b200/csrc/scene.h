@@ -154,6 +154,8 @@ struct KindImage {
   std::vector<uint32_t> pos_of;  // leaf-ordered position of each primitive id
   RawVector<uint32_t> tri;       // triangles: {i0, i1, i2, id word} per leaf-ordered triangle
   RawVector<double> verts;       // triangles: {x, y, z, 0} per vertex, in order of first use
+  RawVector<double> vnorm;       // triangles: {nx, ny, nz, 0}, the vertex normal of each vertex
+                                 // of verts (same numbering)
   uint32_t n_internal = 0;
   uint32_t root_ref = 0;
   double root_box[6] = {0, 0, 0, 0, 0, 0};

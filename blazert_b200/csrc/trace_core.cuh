@@ -1064,25 +1064,27 @@ BZR_HD void take(const SceneView &S, const Ray &r, const KState &st,
   best.t = st.hit;
   best.u = st.u;
   best.v = st.v;
-  best.prim = ldg(K.prim_ids + st.pos) & kIdMask;
   best.geom = K.geom_id;
   best.hit = true;
   if (KIND == kMesh) {
-    const uint32_t *F = S.faces + 3 * size_t(best.prim);
-    const uint32_t f0 = ldg(F), f1 = ldg(F + 1), f2 = ldg(F + 2);
-    const D3 n0 = d3(ldg(S.vert_n + 3 * f0), ldg(S.vert_n + 3 * f0 + 1),
-                     ldg(S.vert_n + 3 * f0 + 2));
-    const D3 n1 = d3(ldg(S.vert_n + 3 * f1), ldg(S.vert_n + 3 * f1 + 1),
-                     ldg(S.vert_n + 3 * f1 + 2));
-    const D3 n2 = d3(ldg(S.vert_n + 3 * f2), ldg(S.vert_n + 3 * f2 + 1),
-                     ldg(S.vert_n + 3 * f2 + 2));
+    // the triangle's words give its id and its vertices, whose normals are stored in the
+    // vertices' numbering: one dependent load before the normals
+    const uint4 w4 = ldg(reinterpret_cast<const uint4 *>(K.tri) + st.pos);
+    best.prim = w4.w & kIdMask;
+    auto vn = [&](uint32_t j) {
+      const double2 a = ld2(K.vnorm + kVertexDoubles * size_t(j));
+      return d3(a.x, a.y, ldg(K.vnorm + kVertexDoubles * size_t(j) + 2));
+    };
+    const D3 n0 = vn(w4.x), n1 = vn(w4.y), n2 = vn(w4.z);
     const double w = (1.0 - st.u) - st.v;
     best.n = normalize(add(add(mul(n0, w), mul(n1, st.u)), mul(n2, st.v)));
   } else if (KIND == kSpheres) {
+    best.prim = ldg(K.prim_ids + st.pos) & kIdMask;
     const double *P = K.payload + size_t(st.pos) * kPayloadDoubles[kSpheres];
     const D3 c = d3(ldg(P), ldg(P + 1), ldg(P + 2));
     best.n = normalize(sub(add(r.o, mul(r.d, st.hit)), c));
   } else {
+    best.prim = ldg(K.prim_ids + st.pos) & kIdMask;
     best.n = normalize(st.n);
   }
 }

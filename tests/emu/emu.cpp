@@ -46,6 +46,7 @@ static void commit(Emu *e, bool build) {
     v.pos_of = im.pos_of.data();
     v.tri = im.tri.data();
     v.verts = im.verts.data();
+    v.vnorm = im.vnorm.data();
     v.n_internal = im.n_internal;
     v.n_prims = static_cast<uint32_t>(im.prim_ids.size());
     v.n_verts = static_cast<uint32_t>(im.verts.size() / bzr::kVertexDoubles);
@@ -473,6 +474,7 @@ int emu_image_digest(void *h, int kind, long workers, uint64_t *digest) {
   mix_array(im.pos_of);
   mix_array(im.tri);
   mix_array(im.verts);
+  mix_array(im.vnorm);
   const uint8_t ok = im.mixed_ok;
   mix(&im.n_internal, sizeof im.n_internal);
   mix(&im.root_ref, sizeof im.root_ref);
