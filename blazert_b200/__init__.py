@@ -612,10 +612,12 @@ class Batch:
         except Exception:
             pass
 
-    def tune(self, threads=None, shared_stack=None, stack_depth=None, sort=None):
+    def tune(self, threads=None, shared_stack=None, stack_depth=None, sort=None,
+             node_width=None):
         """Launch shape and ray order of the batch kernels (bzr_batch_tune): threads per block,
-        stack storage, entries of the thread-local stack (32 or 64) and the per-scene
-        coherence sort; results do not depend on them."""
+        stack storage, entries of the thread-local stack (32 or 64), the per-scene coherence
+        sort and the node width of the mixed mode's walk (8 wide nodes or 2 binary nodes);
+        results do not depend on them."""
         if threads is not None:
             _check(self._lib.bzr_batch_tune(self._h, 3, int(threads)))
         if shared_stack is not None:
@@ -624,6 +626,8 @@ class Batch:
             _check(self._lib.bzr_batch_tune(self._h, 11, int(stack_depth)))
         if sort is not None:
             _check(self._lib.bzr_batch_tune(self._h, 1, int(bool(sort))))
+        if node_width is not None:
+            _check(self._lib.bzr_batch_tune(self._h, 12, int(node_width)))
 
     def intersect(self, ray_offsets, origins, directions, tmin=None, tmax=None, out=None,
                   timestamps=None, mode="fp64", stream=None):

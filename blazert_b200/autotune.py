@@ -75,19 +75,21 @@ def autotune(scene, origins, directions, tmin=None, tmax=None, mode="fp64", reps
 
 
 BATCH_KNOBS = {"threads": (128, 64, 256), "shared_stack": (False, True), "stack_depth": (64, 32),
-               "sort": (False, True)}
+               "sort": (False, True), "node_width": (8, 2)}
 
 
 def autotune_batch(batch, ray_offsets, origins, directions, tmin=None, tmax=None, mode="fp64",
                    reps=3, stream=None, knobs=None):
     """The batching form's knobs (threads per block, stack storage, entries of the thread-local
-    stack, per-scene coherence sort), timed on the caller's whole batch (each candidate
-    captures its own graph, then replays it `reps` times).  A candidate the batch refuses
-    (a stack that does not fit) scores infinity.  Applies and returns the choice with the
-    per-candidate timings (ms)."""
+    stack, per-scene coherence sort and, in the mixed mode, the node width of the walk), timed
+    on the caller's whole batch (each candidate captures its own graph, then replays it `reps`
+    times).  A candidate the batch refuses (a stack that does not fit) scores infinity.
+    Applies and returns the choice with the per-candidate timings (ms)."""
     import torch
 
     knobs = dict(BATCH_KNOBS if knobs is None else knobs)
+    if mode != "mixed":
+        knobs.pop("node_width", None)  # the FP64 mode always walks the binary nodes
     st = stream or torch.cuda.current_stream(origins.device)
     out = None
     timings = {}

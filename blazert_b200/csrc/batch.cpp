@@ -313,6 +313,9 @@ int bzr_batch_tune(bzr_batch *b, int option, int64_t value) {
     if (value == 1 && b->scenes.size() > bzr::kBatchSortMaxScenes)
       return fail(BZR_EINVAL, "the coherence sort takes batches of at most 4,096 scenes");
     p.sort = value == 1;
+  } else if (option == BZR_TUNE_NODE_WIDTH) {
+    if (value != 2 && value != 8) return fail(BZR_EINVAL, "node width must be 2 or 8");
+    p.node_width = static_cast<uint32_t>(value);
   } else {
     return fail(BZR_EINVAL, "unknown tuning option for a batch");
   }

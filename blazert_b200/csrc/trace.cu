@@ -779,7 +779,8 @@ cudaError_t launch_batch(const BatchView &B, const RayIO &io, int mode, const Ba
   const size_t smem = local ? 0 : trace_smem_bytes(plan.stack_cap, th);
   for (int k = 0; k < kNumKinds; ++k) {
     if (!(plan.kinds_present & (1 << k))) continue;
-    const bool m = mode == kModeMixed && k != kCylinders;  // cylinders: FP64 traversal
+    // cylinders, and every kind at node width 2: the FP64 traversal
+    const bool m = mode == kModeMixed && k != kCylinders && plan.node_width == 8;
     const int b = m ? plan.blocks32[k] : plan.blocks[k];
     uint32_t *c = counters + k;
 #define BZR_BATCH_LAUNCH(KK)                                                                   \

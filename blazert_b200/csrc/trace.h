@@ -112,6 +112,7 @@ struct BatchPlan {
   bool shared_stack = false;    // traversal stack in shared memory even when it fits locally
   uint32_t local_stack = 64;    // entries of the thread-local stack: 32 or 64 (kLocalStack)
   bool sort = false;            // coherence sort of each scene's rays before tracing
+  uint32_t node_width = 8;      // mixed mode: 8 walks the wide nodes, 2 the binary FP64 nodes
   int blocks[kNumKinds] = {0, 0, 0, 0};
   int blocks32[kNumKinds] = {0, 0, 0, 0};
   uint32_t stack_cap = 32;

@@ -186,9 +186,10 @@ int bzr_batch_intersect(bzr_batch *batch, const uint64_t *ray_offsets, const dou
 int bzr_batch_check(bzr_batch *batch, void *stream, uint32_t *flags);
 /* Launch shape of the batch's kernels: BZR_TUNE_BLOCK (64, 128, 256 threads per block),
  * BZR_TUNE_STACK (0 thread-local, 1 shared memory), BZR_TUNE_STACK_DEPTH (32 or 64 entries of
- * the thread-local stack) or BZR_TUNE_SORT (1: each scene's rays are traced in the order of
+ * the thread-local stack), BZR_TUNE_SORT (1: each scene's rays are traced in the order of
  * their direction octant and origin Morton code in the scene's box, sorted inside the graph;
- * batches of at most 4,096 scenes); see bzr_scene_tune.  Drops the cached graph; the next
+ * batches of at most 4,096 scenes) or BZR_TUNE_NODE_WIDTH (2 or 8, the mixed mode's walk);
+ * see bzr_scene_tune.  Drops the cached graph; the next
  * bzr_batch_intersect captures a new one.  Results do not change. */
 int bzr_batch_tune(bzr_batch *batch, int option, int64_t value);
 
@@ -261,6 +262,11 @@ int bzr_scene_check(const bzr_scene *scene, void *stream, int timeout_ms, uint32
 /* Entries of the traversal kernels' thread-local stack (batches only, bzr_batch_tune): 32 or
  * 64 (the default); 32 only when every scene's tree needs at most 32. */
 #define BZR_TUNE_STACK_DEPTH 11
+/* Node width of a batch's walk in BZR_MODE_MIXED (batches only, bzr_batch_tune): 8 (the
+ * default) walks the 8-wide nodes with the FP32 child tests, 2 the binary FP64 nodes of the FP64
+ * mode.  Both process the same leaves in the same order, so the results are the same bits;
+ * BZR_MODE_FP64 always walks the binary nodes. */
+#define BZR_TUNE_NODE_WIDTH 12
 int bzr_scene_tune(bzr_scene *scene, int option, int64_t value);
 
 /* Statistics of the last commit: per kind (0 mesh, 1 spheres, 2 planes, 3 cylinders) the

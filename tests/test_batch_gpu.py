@@ -48,8 +48,9 @@ def test_batch_matches_per_scene_oracle(mode):
 
 
 def test_batch_tuning_changes_speed_not_results():
-    """The batch kernels' launch shape (threads per block, stack storage; bzr_batch_tune) and
-    the batch autotuner's choice re-capture the graph and give the same results."""
+    """The batch kernels' launch shape (threads per block, stack storage, stack depth, sort and
+    the mixed mode's node width; bzr_batch_tune) and the batch autotuner's choice, in both
+    modes, re-capture the graph and give the oracle's results."""
     import torch
 
     from blazert_b200.autotune import autotune_batch
@@ -62,16 +63,17 @@ def test_batch_tuning_changes_speed_not_results():
     d = torch.from_numpy(np.concatenate([w.rays.directions for w in wls])).cuda()
     refs = [Oracle(w.scene).intersect(w.rays.origins, w.rays.directions) for w in wls]
 
-    def check():
-        got = to_numpy(batch.intersect(offs, o, d))
+    def check(mode="fp64"):
+        got = to_numpy(batch.intersect(offs, o, d, mode=mode))
         assert batch.check() == 0
         for s, ref in enumerate(refs):
             a, b = offs[s], offs[s + 1]
-            assert mismatches({k: v[a:b] for k, v in got.items()}, ref) == [], s
+            assert mismatches({k: v[a:b] for k, v in got.items()}, ref) == [], (s, mode)
 
     for cfg in (dict(threads=64), dict(threads=256), dict(shared_stack=True),
                 dict(threads=128, shared_stack=False), dict(stack_depth=32), dict(sort=True),
-                dict(sort=True, threads=64, stack_depth=64), dict(sort=False)):
+                dict(sort=True, threads=64, stack_depth=64), dict(sort=False),
+                dict(node_width=2), dict(node_width=2, sort=True), dict(node_width=8)):
         try:
             batch.tune(**cfg)
         except B.BlazertError as e:  # 32 entries only when every scene's tree fits them
@@ -79,9 +81,16 @@ def test_batch_tuning_changes_speed_not_results():
             assert "more than 32" in str(e)
             continue
         check()
+        check("mixed")
+    with pytest.raises(B.BlazertError) as e:
+        batch.tune(node_width=4)
+    assert e.value.code == B.EINVAL
     res = autotune_batch(batch, offs, o, d)
     assert set(res["choice"]) == {"threads", "shared_stack", "stack_depth", "sort"}
     check()
+    res = autotune_batch(batch, offs, o, d, mode="mixed")
+    assert set(res["choice"]) == {"threads", "shared_stack", "stack_depth", "sort", "node_width"}
+    check("mixed")
 
 
 def test_batch_full_size_matches_oracle():
