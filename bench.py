@@ -582,18 +582,22 @@ def run_ours(args):
                     prim=torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
                     geom=torch.empty(n, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
                     hit=torch.empty(n, dtype=torch.uint8).pin_memory().numpy())
-        host_tuning = None
-        if args.sort == "auto" and not args.any_hit:
-            from blazert_b200.autotune import autotune_host
-            host_tuning = autotune_host(scene, ho, hd, htmn, htmx, out=hout, mode=primary)
-            host_tuning = {"choice": host_tuning["choice"], "best_ms": host_tuning["best_ms"]}
-
-        def e2e_of(m):
+        def device_knobs(m):
             if res[m]["tuning"]:  # the device knobs this mode was timed with
                 c = res[m]["tuning"]["choice"]
                 scene.tune(sort=c["sort"], sort_min_rays=0 if c["sort"] else 1 << 16,
                            threads=c["threads"], shared_stack=c["shared_stack"], chunk=c["chunk"],
                            top_nodes=c.get("top_nodes", 0))
+
+        host_tuning = None
+        if args.sort == "auto" and not args.any_hit:
+            from blazert_b200.autotune import autotune_host
+            device_knobs(primary)
+            host_tuning = autotune_host(scene, ho, hd, htmn, htmx, out=hout, mode=primary)
+            host_tuning = {"choice": host_tuning["choice"], "best_ms": host_tuning["best_ms"]}
+
+        def e2e_of(m):
+            device_knobs(m)
             for _ in range(max(1, args.warmup)):
                 scene.intersectN(ho, hd, htmn, htmx, mode=m, out=hout, any_hit=args.any_hit)
             if pg:
@@ -614,7 +618,15 @@ def run_ours(args):
         e2e = e2e_of(primary)
         e2e["host_tuning"] = host_tuning
         if precision is not None and primary != "mixed":
+            mixed_tuning = None
+            if host_tuning is not None:  # the pipeline's knobs, chosen again for this mode
+                from blazert_b200.autotune import autotune_host
+                device_knobs("mixed")
+                mixed_tuning = autotune_host(scene, ho, hd, htmn, htmx, out=hout, mode="mixed")
+                mixed_tuning = {"choice": mixed_tuning["choice"],
+                                "best_ms": mixed_tuning["best_ms"]}
             e2e_mixed = e2e_of("mixed")
+            e2e_mixed["host_tuning"] = mixed_tuning
             precision["e2e"] = e2e_mixed
 
     cpu = None
