@@ -125,15 +125,17 @@ def autotune_batch(batch, ray_offsets, origins, directions, tmin=None, tmax=None
     return dict(choice=best, best_ms=timings[str(sorted(best.items()))], timings_ms=timings)
 
 
-HOST_KNOBS = {"host_chunks": (8, 4, 6, 12, 16), "host_grid_div": (1, 2, 3),
+HOST_KNOBS = {"host_min_chunk": (1 << 17, 1 << 16, 1 << 15, 1 << 14),
+              "host_chunks": (8, 4, 6, 12, 16), "host_grid_div": (1, 2, 3),
               "host_edge": (0, 1 << 16, 1 << 17)}
 
 
 def autotune_host(scene, origins, directions, tmin=None, tmax=None, out=None, mode="fp64",
                   reps=3, knobs=None, sweeps=2):
-    """The pipeline of host-array calls (bzr_scene_tune HOST_CHUNKS / HOST_GRID_DIV /
-    HOST_EDGE): how many chunks the batch is split into, what share of the grid each chunk's
-    kernels take and the size of small first and last chunks, timed
+    """The pipeline of host-array calls (bzr_scene_tune HOST_MIN_CHUNK / HOST_CHUNKS /
+    HOST_GRID_DIV / HOST_EDGE): the smallest chunk and how many chunks the batch is split into,
+    what share of the grid each chunk's kernels take and the size of small first and last
+    chunks, timed
     end to end (wall clock, host arrays, copies included) on the caller's whole batch.  The
     device-path knobs stay as they are.  Applies and returns the choice with the timings (ms)."""
     import time

@@ -220,7 +220,7 @@ def test_host_pipeline_knobs_change_speed_not_results():
     with pytest.raises(Exception):
         s.tune(host_grid_div=0)
     res = autotune_host(s, R.origins, R.directions, R.tmin, R.tmax, reps=1, sweeps=1)
-    assert set(res["choice"]) == {"host_chunks", "host_grid_div", "host_edge"}
+    assert set(res["choice"]) == {"host_min_chunk", "host_chunks", "host_grid_div", "host_edge"}
     assert mismatches(s.intersectN(R.origins, R.directions, R.tmin, R.tmax), ref) == []
 
 
