@@ -353,6 +353,32 @@ def run_batched(args):
     return 0
 
 
+def pcie_ceiling(in_bytes, out_bytes, dev, reps=3):
+    """The copy ceiling of an end-to-end step: `in_bytes` from pinned host memory to the device
+    and `out_bytes` back, on two streams at once (the two directions of PCIe run side by side),
+    best of `reps`, timed by the wall clock around a synchronize like the e2e steps.  Returns
+    milliseconds."""
+    import torch
+
+    hin = torch.empty(in_bytes, dtype=torch.uint8).pin_memory()
+    hout = torch.empty(out_bytes, dtype=torch.uint8).pin_memory()
+    din = torch.empty(in_bytes, dtype=torch.uint8, device=dev)
+    dout = torch.empty(out_bytes, dtype=torch.uint8, device=dev)
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    best = float("inf")
+    for _ in range(reps + 1):  # the first round is a warm-up
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        with torch.cuda.stream(s_in):
+            din.copy_(hin, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            hout.copy_(dout, non_blocking=True)
+        torch.cuda.synchronize(dev)
+        best = min(best, (time.perf_counter() - t0) * 1e3)
+    del hin, hout, din, dout
+    return best
+
+
 def l2_read_peak():
     """Measured L2 -> SM read bandwidth of the current GPU (GB/s): the probe library's
     ld.global.cg read of buffers that fit in L2, best over a few sizes (per-size figures too)."""
@@ -617,6 +643,13 @@ def run_ours(args):
 
         e2e = e2e_of(primary)
         e2e["host_tuning"] = host_tuning
+        # the step's own copies, alone: what the copy engines allow for these bytes
+        copy_ms = pcie_ceiling(e2e["h2d_bytes_per_step"], e2e["d2h_bytes_per_step"], dev)
+        copy_value = world * n / (copy_ms / 1e3) / 1e6
+        e2e["ceiling"] = {"value": copy_value, "unit": "Mrays/s", "copy_ms": copy_ms,
+                          "frac": e2e["value"] / copy_value,
+                          "what": "the step's host<->device bytes copied alone, both directions "
+                                  "at once from pinned memory (no kernels)"}
         if precision is not None and primary != "mixed":
             mixed_tuning = None
             if host_tuning is not None:  # the pipeline's knobs, chosen again for this mode
