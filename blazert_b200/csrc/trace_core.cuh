@@ -157,10 +157,32 @@ BZR_HD double2 ld2(const double *p) {
   return ldg(reinterpret_cast<const double2 *>(p));
 }
 
+// 32 bytes at p (32-byte aligned) as two uint4, kept in L2 with priority on the device.
+BZR_HD void ld32_keep(const void *p, uint4 &a, uint4 &b) {
+#if defined(__CUDA_ARCH__)
+  asm("ld.global.nc.L2::evict_last.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+      : "l"(p));
+#else
+  std::memcpy(&a, p, 16);
+  std::memcpy(&b, static_cast<const char *>(p) + 16, 16);
+#endif
+}
+
+// One 32-byte load of a 32-byte aligned {x, y, z, w} entry (vertices, vertex normals).
+BZR_HD D3 ld_d4xyz(const double *p) {
+#if defined(__CUDA_ARCH__)
+  double x, y, z, w;
+  asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(x), "=d"(y), "=d"(z), "=d"(w) : "l"(p));
+  (void)w;
+  return d3(x, y, z);
+#else
+  return d3(p[0], p[1], p[2]);
+#endif
+}
+
 BZR_HD D3 ld_vertex(const double *verts, uint32_t i) {
-  const double *p = verts + size_t(i) * kVertexDoubles;
-  const double2 xy = ld2(p), z0 = ld2(p + 2);
-  return d3(xy.x, xy.y, z0.x);
+  return ld_d4xyz(verts + size_t(i) * kVertexDoubles);
 }
 
 // blazert/primitives/trimesh.h:153-181, the quantities of one test before its decisions.  F
@@ -525,8 +547,12 @@ BZR_HD void trav_to_leaf(const KindView &K, const Ray &r, const KState &st, Trav
       meta = q[6];
     } else {
       const double *nd = K.nodes64 + size_t(tv.cur) * kNode64Doubles;
-      a0 = ld2(nd), a1 = ld2(nd + 2), a2 = ld2(nd + 4);
-      b0 = ld2(nd + 6), b1 = ld2(nd + 8), b2 = ld2(nd + 10);
+      uint4 w0, w1, w2, w3, w4, w5;  // the two child boxes in three 32-byte loads
+      ld32_keep(nd, w0, w1);
+      ld32_keep(nd + 4, w2, w3);
+      ld32_keep(nd + 8, w4, w5);
+      a0 = as_d2(w0), a1 = as_d2(w1), a2 = as_d2(w2);
+      b0 = as_d2(w3), b1 = as_d2(w4), b2 = as_d2(w5);
       meta = ldg(reinterpret_cast<const uint4 *>(nd + 12));
     }
     double k0, k1;
@@ -801,18 +827,6 @@ BZR_HD uint32_t fword(float x) {
 #endif
 }
 
-// 32 bytes at p (32-byte aligned) as two uint4, kept in L2 with priority on the device.
-BZR_HD void ld32_keep(const void *p, uint4 &a, uint4 &b) {
-#if defined(__CUDA_ARCH__)
-  asm("ld.global.nc.L2::evict_last.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-      : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
-      : "l"(p));
-#else
-  std::memcpy(&a, p, 16);
-  std::memcpy(&b, static_cast<const char *>(p) + 16, 16);
-#endif
-}
-
 BZR_HD uint32_t pick8(uint4 a, uint4 b, uint32_t slot) {
   const uint4 q = (slot & 4u) ? b : a;
   const uint32_t lo = (slot & 1u) ? q.y : q.x, hi = (slot & 1u) ? q.w : q.z;
@@ -1071,10 +1085,7 @@ BZR_HD void take(const SceneView &S, const Ray &r, const KState &st,
     // vertices' numbering: one dependent load before the normals
     const uint4 w4 = ldg(reinterpret_cast<const uint4 *>(K.tri) + st.pos);
     best.prim = w4.w & kIdMask;
-    auto vn = [&](uint32_t j) {
-      const double2 a = ld2(K.vnorm + kVertexDoubles * size_t(j));
-      return d3(a.x, a.y, ldg(K.vnorm + kVertexDoubles * size_t(j) + 2));
-    };
+    auto vn = [&](uint32_t j) { return ld_d4xyz(K.vnorm + kVertexDoubles * size_t(j)); };
     const D3 n0 = vn(w4.x), n1 = vn(w4.y), n2 = vn(w4.z);
     const double w = (1.0 - st.u) - st.v;
     best.n = normalize(add(add(mul(n0, w), mul(n1, st.u)), mul(n2, st.v)));
